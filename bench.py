@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Throughput of the crabSAXS scattering hot path on B200.
+
+Workload (one step): the per-atom-type-pair Debye pair sums of a 20,000-atom
+seeded protein-like structure (radius 45 Å, C/N/O/S) plus its adaptive
+hydration shell on a 3 Å grid, at 500 uniform q values on [0.001, 0.5] Å⁻¹
+(the scale configuration of the Debye engine).  Unit: pair·q evaluations per
+second, pairs = M(M-1)/2 over the M atoms + sites.
+
+* ``value``: the pair kernel on device-resident inputs (a pair plan), timed with
+  CUDA events on the launch stream, L2 flushed (256 MiB memset) before every
+  step outside the events.
+* ``e2e``: the public C-ABI call ``crab_debye_solvent_basis`` from pinned host
+  buffers (structure upload, hydration grid, pair sums, partials read back),
+  wall-clocked per step.
+* ``roofline``: 4 FLOP per pair·q (recurrence step + weighted accumulate)
+  against the FP32 FMA peak measured in this run.
+* ``cpu_baseline``: the oracle (C++ f64 restatement of the reference CPU
+  algorithm) on all host threads, on a q subset of the same workload.
+
+``--impl reference`` times that CPU restatement alone (the reference crate is
+Rust and cannot be built here) with the same metric.  Under torchrun each rank
+runs its own structure on its own GPU (independent objects, weak scaling, no
+data-path collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "pair·q/s (Debye); batched χ²+∇ curves/s vs plain GPU; both at ≤1e-5 rel err"
+UNIT = "pair·q/s"
+N_ATOMS, RADIUS, SEED = 20000, 45.0, 2
+Q = np.linspace(0.001, 0.5, 500)
+FLUSH_BYTES = 256 << 20
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+class Dist:
+    def __init__(self, world: int, backend: str):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self._dev())
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self._dev())
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def _dev(self):
+        import torch
+
+        return f"cuda:{torch.cuda.current_device()}" if self.dist.get_backend() == "nccl" else "cpu"
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 7 and parts[0].replace(".", "").isdigit():
+                    rows.append(parts)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def workload(rank: int):
+    """Structure of this rank plus its adaptive 3 Å hydration sites, as typed pair-sum arrays."""
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import synth
+
+    s = synth.protein(SEED + 1000 * rank, N_ATOMS, RADIUS)
+    return s
+
+
+def typed_arrays(s, sites):
+    # scattering types: C, N, O, S (element Cromer–Mann classes) and the water site W
+    el = s.element.astype(np.int64)
+    classes = sorted(set(el.tolist()))
+    t_atoms = np.searchsorted(classes, el)
+    xyz = np.concatenate([s.xyz, sites])
+    w = np.concatenate([s.occupancy, np.ones(len(sites))])
+    t = np.concatenate([t_atoms, np.full(len(sites), len(classes))]).astype(np.int32)
+    return xyz, w, t, len(classes) + 1
+
+
+def traffic_per_launch():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "debye_pair_fp32_config2.txt"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline_run(s, sites, threads: int):
+    """Oracle f64 Debye solvent basis (adaptive grid built inside) on `threads` q values."""
+    import oracle as O
+
+    sub = Q[np.linspace(0, len(Q) - 1, threads).astype(int)]
+    a = O.Atoms(s.xyz, s.element, s.group, s.occupancy)
+    m = s.atom_count + len(sites)
+    t0 = time.perf_counter()
+    O.debye_solvent_basis(a, sub, 1.0, 0.0, model=2, spacing=3.0)
+    dt = time.perf_counter() - t0
+    return (m * (m - 1) / 2.0) * len(sub) / dt, len(sub), dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import synth
+
+    s = synth.protein(SEED, N_ATOMS, RADIUS)
+    import oracle as O
+
+    sites, _ = O.adaptive_grid(s.xyz, 3.0)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline_run(s, sites, threads)
+    vals, times = [], []
+    for _ in range(args.steps):
+        v, nq, dt = cpu_baseline_run(s, sites, threads)
+        vals.append(v)
+        times.append(dt)
+    value = float(np.median(vals))
+    sample = (f"20,000-atom structure + {len(sites)} adaptive 3 Å sites, {threads} of the 500 q values "
+              f"(one per thread), f64 C++ restatement of solvent.rs debye_solvent_basis")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "debye pair sums, 20k-atom structure + adaptive 3 Å hydration sites, 500 q",
+                   "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_q": len(Q)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import _native as N
+
+    dist = Dist(world, "nccl")
+    if world > 1:
+        import torch
+
+        torch.cuda.set_device(local)
+    eng = cs.Engine(local)
+    lib = N.lib
+    peak = C.c_double()
+    eng.check(lib.crab_measure_fp32_peak(eng.handle, 150.0, C.byref(peak)))
+
+    s = workload(rank)
+    sites, vol = cs.hydration_grid_adaptive(s, 3.0, engine=eng)
+    xyz, w, t, T = typed_arrays(s, sites)
+    m = len(w)
+    plan = C.c_void_p()
+    eng.check(lib.crab_pair_plan_create(eng.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
+                                        t.ctypes.data_as(N.I32P), m, T, Q.ctypes.data_as(N.D), len(Q),
+                                        C.byref(plan)))
+    pairq = lib.crab_pair_plan_pairq(plan)
+
+    # warm-up, then K timed steps (each a flushed, event-bracketed kernel)
+    eng.check(lib.crab_pair_plan_run(eng.handle, plan, args.warmup, FLUSH_BYTES, None))
+    step_ms = np.zeros(args.steps)
+    eng.reset_stats()
+    with ClockSampler(local) as clocks:
+        dist.barrier()
+        t0 = time.perf_counter()
+        eng.check(lib.crab_pair_plan_run(eng.handle, plan, args.steps, FLUSH_BYTES, step_ms.ctypes.data_as(N.D)))
+        wall = time.perf_counter() - t0
+        dist.barrier()
+    launches, _, _ = eng.stats()
+    device_s = float(step_ms.sum()) / 1e3
+    max_s = dist.max(device_s)
+    total_units = dist.sum(pairq * args.steps)
+    value = total_units / max_s
+    ms_per_step = 1e3 * max_s / args.steps
+    achieved = 4.0 * pairq / (float(step_ms.mean()) * 1e-3) / 1e12
+
+    # accuracy of this curve against the FP64 device reference (outside the timed region)
+    import crabsaxs_b200.synth as synth
+
+    c1, c2 = synth.solvent_draw(SEED)
+    sp = cs.SolventParams(c1=c1, c2=c2, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                          hydration_grid_spacing_angstrom=3.0)
+    b32 = cs.debye_solvent_basis(s, Q, sp, engine=eng)
+    b64 = cs.debye_solvent_basis(s, Q, sp, engine=eng, fp64=True)
+    i32 = cs.combine_solvent_basis(b32, Q, c1, c2)
+    i64 = cs.combine_solvent_basis(b64, Q, c1, c2)
+    max_rel = float(np.max(np.abs(i32 - i64) / np.abs(i64)))
+
+    # end to end through the public C-ABI call with pinned host buffers
+    import torch
+
+    def pinned(a):
+        tt = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return tt, tt.numpy()
+
+    _, hx = pinned(s.xyz)
+    _, ho = pinned(s.occupancy)
+    _, he = pinned(s.element)
+    _, hg = pinned(s.group)
+    _, hq = pinned(Q)
+    _, hout = pinned(np.zeros((6, len(Q))))
+    solv = sp.to_c()
+
+    def e2e_step():
+        st = C.c_void_p()
+        eng.check(lib.crab_structure_create(eng.handle, hx.ctypes.data_as(N.D), ho.ctypes.data_as(N.D),
+                                            he.ctypes.data_as(N.I8P), hg.ctypes.data_as(N.I8P), len(ho),
+                                            C.byref(st)))
+        eng.check(lib.crab_debye_solvent_basis(eng.handle, st, hq.ctypes.data_as(N.D), len(hq), C.byref(solv), 1,
+                                               hout.ctypes.data_as(N.D)))
+        lib.crab_structure_destroy(st)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    eng.reset_stats()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    dist.barrier()
+    e2e_launches, _, _ = eng.stats()
+    h2d, d2h = C.c_int64(), C.c_int64()
+    lib.crab_ctx_transfer_stats(eng.handle, C.byref(h2d), C.byref(d2h))
+    e2e_value = total_units / dist.max(e2e_s)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, nq, dt = cpu_baseline_run(s, sites, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"same structure + sites, {nq} of 500 q values (one per thread), {dt:.1f} s; "
+                         "f64 C++ restatement of solvent.rs debye_solvent_basis"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "debye pair sums per type pair, 20k-atom structure + adaptive 3 Å hydration "
+                                   "sites, 500 q on [0.001, 0.5]",
+                       "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_types": T, "n_q": len(Q),
+                       "parallelism": f"independent structure per GPU x{world}",
+                       "l2": "flushed before every step (256 MiB memset, outside the step events)"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value, "traffic": traffic_per_launch(),
+                         "peak_source": "FFMA microbenchmark measured in this run (MEASURED_PEAKS.json has no FP32)",
+                         "flop_per_unit": 4},
+            "parity": {"max_rel_err_vs_fp64": max_rel, "c1": c1, "c2": c2},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
+                    "d2h_bytes_per_step": d2h.value // args.steps,
+                    "ms_per_step": 1e3 * e2e_s / args.steps},
+            "gpu_launches": int(launches),
+            "e2e_gpu_launches": int(e2e_launches),
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    lib.crab_pair_plan_destroy(plan)
+    dist.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,636 @@
+// Debye pair sums per atom-type pair on B200 (sm_100a).
+//
+// Replaces the O(N²·Nq) pair loops of crabSAXS src/scattering.rs:99-106 and
+// src/solvent.rs:533-577.  Instead of summing amplitude products per q, the
+// kernel produces, for every unordered type pair (a<=b),
+//     P_ab(q) = Σ_{i<j, {t_i,t_j}={a,b}} w_i w_j sinc(q r_ij),
+// from which every Debye term (vacuum, excluded volume, hydration, their
+// cross terms, any c1/c2) is a small f64 recombination on the host.
+//
+// FP32 kernel (uniform q grid):
+//  * atoms are grouped by type and padded per type to 128-atom tiles, so each
+//    (i-tile, j-tile) block has one type pair and the per-thread accumulators
+//    stay in registers with static indices;
+//  * a CTA of 128 threads keeps one i atom per thread in registers and stages
+//    j tiles (float4 x,y,z,w; 2 KB) in shared memory with a bulk async copy;
+//  * for each pair the thread seeds sin(q0 r) and cos(q0 r) once per block of
+//    Q consecutive q values and advances sin(q r) along the grid with the
+//    three-term (Chebyshev) recurrence in Reinsch's difference form
+//        d_{k+1} = d_k - λ s_k,  s_{k+1} = s_k + d_{k+1},  λ = 4 sin²(Δr/2),
+//    which keeps the frequency exact in FP32 for small Δr (the plain form
+//    s_{k+1} = 2cos(Δr) s_k - s_{k-1} loses it: 2cos(Δr) rounds to ~1e-7
+//    absolute while 2-2cos(Δr) may be 1e-6);
+//  * the accumulated quantity is Σ w_i w_j sin(q r)/r; the host divides by q
+//    in f64 (q = 0 is the exact Σ w_i w_j);
+//  * per thread FP32 sums cover at most one run of same-type j tiles, then a
+//    warp-shuffle reduction and an FP64 atomic add per (type pair, q).
+// FP64 kernel: the same tiling with direct f64 sinc per pair and q; it is the
+// on-device reference for the error reports and large-size checks.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace crab {
+namespace {
+
+constexpr int kThreads = 128;  // one i atom per thread; equals kTile
+static_assert(kThreads == kTile, "tile size and CTA size must match");
+
+// ---- bulk async copy of one j tile into shared memory (1D TMA) ------------
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+               "l"(src), "r"(bytes), "r"(b)
+               : "memory");
+}
+// Bounded wait on an mbarrier phase. Returns false when the iteration budget
+// runs out (the caller records an error and stops using the buffer).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// sin(h), cos(h) for |h| <= 0.8 by their Taylor series (error < 1e-11 before
+// rounding); used for the half-step angle h = Δr/2.
+__device__ __forceinline__ void sincos_small(float h, float* sh, float* ch) {
+  const float h2 = h * h;
+  float ps = fmaf(h2, -1.0f / 39916800.0f, 1.0f / 362880.0f);
+  ps = fmaf(h2, ps, -1.0f / 5040.0f);
+  ps = fmaf(h2, ps, 1.0f / 120.0f);
+  ps = fmaf(h2, ps, -1.0f / 6.0f);
+  *sh = fmaf(h * h2, ps, h);
+  float pc = fmaf(h2, 1.0f / 479001600.0f, -1.0f / 3628800.0f);
+  pc = fmaf(h2, pc, 1.0f / 40320.0f);
+  pc = fmaf(h2, pc, -1.0f / 720.0f);
+  pc = fmaf(h2, pc, 1.0f / 24.0f);
+  pc = fmaf(h2, pc, -0.5f);
+  *ch = fmaf(h2, pc, 1.0f);
+}
+
+// sin(x), cos(x) for 0 <= x < 4096·π/2: Cody–Waite reduction by π/2 split
+// into C1 + C2 + C3 (C1 and C2 carry 12 significant bits, so k·C1 and k·C2
+// are exact for k < 4096), then Taylor polynomials on |y| <= π/4 (truncation
+// below 2e-9) and quadrant selection.  Used for the per-pair seed sin(q0 r).
+__device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
+  const float k = rintf(x * 0x1.45f306p-1f);  // x·2/π
+  float y = fmaf(-k, 0x1.92p+0f, x);
+  y = fmaf(-k, 0x1.fb4p-12f, y);
+  y = fmaf(-k, 0x1.4442d2p-24f, y);
+  const float y2 = y * y;
+  float ps = fmaf(y2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  ps = fmaf(y2, ps, 1.0f / 120.0f);
+  ps = fmaf(y2, ps, -1.0f / 6.0f);
+  const float sy = fmaf(y * y2, ps, y);
+  float pc = fmaf(y2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+  pc = fmaf(y2, pc, -1.0f / 720.0f);
+  pc = fmaf(y2, pc, 1.0f / 24.0f);
+  pc = fmaf(y2, pc, -0.5f);
+  const float cy = fmaf(y2, pc, 1.0f);
+  const int qd = __float2int_rn(k) & 3;
+  const float ss = (qd & 1) ? cy : sy;
+  const float cc = (qd & 1) ? sy : cy;
+  *s = (qd & 2) ? -ss : ss;
+  *c = ((qd + 1) & 2) ? -cc : cc;
+}
+
+template <int Q>
+__device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int ab, int qstart, int qcount, int nq,
+                                           double* __restrict__ partials) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < Q; ++k) {
+    float v = acc[k];
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    if (lane == 0) red[warp][k] = v;
+    acc[k] = 0.0f;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < qcount; k += kThreads) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += (double)red[w][k];
+    atomicAdd(&partials[(size_t)ab * nq + qstart + k], s);
+  }
+  __syncthreads();
+}
+
+// Work item: (i tile, first j tile, end j tile, q block).
+// qpar[b] = (q0_hi, q0_lo, halfstep_hi, halfstep_lo), qrange[b] = (start, count).
+template <int Q>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_pair_fp32(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
+                int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T, int wide,
+                double* __restrict__ partials, int* __restrict__ status) {
+  __shared__ __align__(16) float4 sj[2][kTile];
+  __shared__ float red[kThreads / 32][Q];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned phase_bits = 0u;  // bit b: parity of the next completion of bar[b]
+  bool ok = true;
+
+  for (int w = blockIdx.x; w < n_work && ok; w += gridDim.x) {
+    const int4 wk = work[w];
+    const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
+    const float4 ai = atoms[(size_t)it * kTile + tid];
+    const float4 qp = qpar[qb];
+    const int2 qr = qrange[qb];
+    const int ti = tile_type[it];
+    float acc[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) acc[k] = 0.0f;
+    int cur = tile_type[jt0];
+
+    // prefetch the first j tile
+    if (tid == 0) {
+      mbar_expect_tx(&bar[0], kTile * sizeof(float4));
+      bulk_g2s(&sj[0][0], atoms + (size_t)jt0 * kTile, kTile * sizeof(float4), &bar[0]);
+    }
+    int buf = 0;
+    for (int jt = jt0; jt < jt1; ++jt) {
+      const int tj = tile_type[jt];
+      if (tj != cur) {
+        const int a = min(ti, cur), b = max(ti, cur);
+        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, partials);
+        cur = tj;
+      }
+      // issue the next tile into the other buffer (its previous readers
+      // finished at the __syncthreads that closed the previous iteration)
+      if (tid == 0 && jt + 1 < jt1) {
+        mbar_expect_tx(&bar[buf ^ 1], kTile * sizeof(float4));
+        bulk_g2s(&sj[buf ^ 1][0], atoms + (size_t)(jt + 1) * kTile, kTile * sizeof(float4), &bar[buf ^ 1]);
+      }
+      if (!mbar_wait(&bar[buf], (phase_bits >> buf) & 1u)) {
+        if (tid == 0) atomicExch(status, CRAB_ETIMEOUT);
+        ok = false;
+      }
+      phase_bits ^= 1u << buf;
+      if (!__syncthreads_and(ok)) { ok = false; break; }
+      const bool diag = (jt == it);
+#pragma unroll 2
+      for (int j = 0; j < kTile; ++j) {
+        const float4 aj = sj[buf][j];
+        const float wj = (diag && j <= tid) ? 0.0f : aj.w;
+        const float dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float r = fmaxf(sqrtf(r2), 1e-4f);
+        const float u = ai.w * wj * rsqrtf(fmaxf(r2, 1e-8f));
+        const float phi = fmaf(qp.x, r, qp.y * r);
+        const float h = fmaf(qp.z, r, qp.w * r);
+        float s0, c0, sh, ch;
+        sincos_seed(phi, &s0, &c0);
+        if (wide) sincos_seed(h, &sh, &ch);
+        else sincos_small(h, &sh, &ch);
+        const float nl = -4.0f * sh * sh;
+        float d = 2.0f * sh * fmaf(s0, sh, c0 * ch);
+        float s = s0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+          acc[k] = fmaf(u, s, acc[k]);
+          d = fmaf(nl, s, d);
+          s += d;
+        }
+      }
+      __syncthreads();
+      buf ^= 1;
+    }
+    if (ok) {
+      const int a = min(ti, cur), b = max(ti, cur);
+      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, partials);
+    }
+  }
+}
+
+// FP64 reference: direct sinc per pair and q, QD q values per work item.
+constexpr int kQD = 8;
+__global__ void __launch_bounds__(kThreads)
+    k_pair_fp64(const double4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
+                int n_work, const double* __restrict__ q, int nq, int T, double* __restrict__ partials) {
+  __shared__ double4 sj[kTile];
+  __shared__ double red[kThreads / 32][kQD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    const int4 wk = work[w];
+    const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
+    const double4 ai = atoms[(size_t)it * kTile + tid];
+    const int qstart = qb * kQD, qcount = min(kQD, nq - qstart);
+    double qv[kQD], acc[kQD];
+#pragma unroll
+    for (int k = 0; k < kQD; ++k) {
+      qv[k] = (k < qcount) ? q[qstart + k] : 0.0;
+      acc[k] = 0.0;
+    }
+    const int ti = tile_type[it];
+    int cur = tile_type[jt0];
+    auto flush = [&](int tj) {
+      const int a = min(ti, tj), b = max(ti, tj);
+      const int ab = a * T - a * (a - 1) / 2 + (b - a);
+#pragma unroll
+      for (int k = 0; k < kQD; ++k) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+        acc[k] = 0.0;
+      }
+      __syncthreads();
+      if (tid < qcount) {
+        double s = 0.0;
+        for (int w2 = 0; w2 < kThreads / 32; ++w2) s += red[w2][tid];
+        atomicAdd(&partials[(size_t)ab * nq + qstart + tid], s);
+      }
+      __syncthreads();
+    };
+    for (int jt = jt0; jt < jt1; ++jt) {
+      const int tj = tile_type[jt];
+      if (tj != cur) {
+        flush(cur);
+        cur = tj;
+      }
+      sj[tid] = atoms[(size_t)jt * kTile + tid];
+      __syncthreads();
+      const bool diag = (jt == it);
+      for (int j = 0; j < kTile; ++j) {
+        const double4 aj = sj[j];
+        const double wij = (diag && j <= tid) ? 0.0 : ai.w * aj.w;
+        const double dx = ai.x - aj.x, dy = ai.y - aj.y, dz = ai.z - aj.z;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+#pragma unroll
+        for (int k = 0; k < kQD; ++k) {
+          const double x = qv[k] * r;
+          const double s = fabs(x) < 1e-8 ? 1.0 : sin(x) / x;
+          acc[k] = fma(wij, s, acc[k]);
+        }
+      }
+      __syncthreads();
+    }
+    flush(cur);
+  }
+}
+
+uint32_t morton10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// Work list: i tile x runs of up to `run` j tiles (j >= i) x q blocks, q block
+// fastest so concurrently running CTAs add into different q ranges.
+std::vector<int4> make_work(const Layout& L, int n_qblocks, int run) {
+  std::vector<int4> work;
+  for (int it = 0; it < L.n_tiles; ++it)
+    for (int j0 = it; j0 < L.n_tiles; j0 += run)
+      for (int b = 0; b < n_qblocks; ++b) work.push_back(make_int4(it, j0, std::min(j0 + run, L.n_tiles), b));
+  return work;
+}
+
+template <int Q>
+void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
+                 const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status) {
+  int per_sm = 0;
+  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q>, kThreads, 0));
+  int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
+  k_pair_fp32<Q><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials, status);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <class T>
+T* upload(crab_ctx* ctx, std::vector<void*>& owned, const T* src, size_t count, cudaStream_t s) {
+  void* p = nullptr;
+  CRAB_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+  owned.push_back(p);
+  if (count && src) copy_h2d(ctx, p, src, count * sizeof(T), s);
+  return (T*)p;
+}
+
+}  // namespace
+
+Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64) {
+  Layout L;
+  L.T = T;
+  L.n = n;
+  L.self_w2.assign(T, 0.0);
+  L.sum_w.assign(T, 0.0);
+  double c[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) c[d] += xyz[3 * i + d];
+  for (int d = 0; d < 3; ++d) c[d] = n ? c[d] / (double)n : 0.0;
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, rmax = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    double r2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      double v = xyz[3 * i + d] - c[d];
+      lo[d] = std::min(lo[d], v);
+      hi[d] = std::max(hi[d], v);
+      r2 += v * v;
+    }
+    rmax = std::max(rmax, std::sqrt(r2));
+  }
+  L.extent = 2.0 * rmax;
+  // order: type, then Morton code of the centred position
+  std::vector<uint64_t> key(n);
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t m = 0;
+    for (int d = 0; d < 3; ++d) {
+      double span = std::max(hi[d] - lo[d], 1e-9);
+      double cell = std::floor((xyz[3 * i + d] - c[d] - lo[d]) / span * 1024.0);
+      m |= morton10((uint32_t)std::min(1023.0, std::max(0.0, cell))) << d;
+    }
+    key[i] = ((uint64_t)(uint32_t)type[i] << 32) | m;
+  }
+  std::vector<int64_t> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+  std::vector<int64_t> count(T, 0);
+  for (int64_t i = 0; i < n; ++i) count[type[i]]++;
+  int64_t n_pad = 0;
+  for (int t = 0; t < T; ++t) n_pad += (count[t] + kTile - 1) / kTile * kTile;
+  L.n_pad = n_pad;
+  L.n_tiles = (int)(n_pad / kTile);
+  L.atoms.assign((size_t)n_pad * 4, 0.0f);
+  if (with_f64) L.atoms64.assign((size_t)n_pad * 4, 0.0);
+  L.tile_type.resize(L.n_tiles);
+  int64_t slot = 0, k = 0;
+  for (int t = 0; t < T; ++t) {
+    const int64_t start = slot;
+    for (int64_t m = 0; m < count[t]; ++m, ++k, ++slot) {
+      const int64_t i = order[k];
+      for (int d = 0; d < 3; ++d) {
+        const double v = xyz[3 * i + d] - c[d];
+        L.atoms[4 * slot + d] = (float)v;
+        if (with_f64) L.atoms64[4 * slot + d] = v;
+      }
+      L.atoms[4 * slot + 3] = (float)w[i];
+      if (with_f64) L.atoms64[4 * slot + 3] = w[i];
+      L.self_w2[t] += w[i] * w[i];
+      L.sum_w[t] += w[i];
+    }
+    slot = start + (count[t] + kTile - 1) / kTile * kTile;
+    for (int64_t tt = start / kTile; tt < slot / kTile; ++tt) L.tile_type[tt] = t;
+  }
+  return L;
+}
+
+bool q_grid_uniform(const double* q, int64_t nq) {
+  if (nq < 3) return true;
+  const double dq = (q[nq - 1] - q[0]) / (double)(nq - 1);
+  const double tol = 1e-9 * std::max(std::fabs(q[nq - 1]), 1e-12);
+  for (int64_t k = 1; k < nq; ++k)
+    if (std::fabs(q[k] - (q[0] + (double)k * dq)) > tol) return false;
+  return true;
+}
+
+PairPlan::~PairPlan() {
+  for (void* p : owned) cudaFree(p);
+}
+
+std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64) {
+  std::unique_ptr<PairPlan> P(new PairPlan());
+  P->L = std::move(L);
+  P->fp64 = fp64;
+  P->nq = nq;
+  P->q.assign(q, q + nq);
+  const int T = P->L.T;
+  P->n_pairs = T * (T + 1) / 2;
+  cudaStream_t s = ctx->stream;
+  if (nq == 0 || P->L.n_tiles == 0) return P;
+  if (!fp64) {
+    // q blocks: greedy runs of uniformly spaced q values, seeded exactly at
+    // their first point; the block length Q (a template) is chosen to
+    // minimise launched steps plus a per-block seed cost.
+    auto blocks_for = [&](int Qmax, std::vector<int2>& out) {
+      out.clear();
+      const double tol = 1e-9 * std::max(std::fabs(q[nq - 1]), 1e-12);
+      int64_t s0 = 0;
+      while (s0 < nq) {
+        int64_t e = s0 + 1;
+        if (e < nq) {
+          const double dq = q[s0 + 1] - q[s0];
+          e = s0 + 2;
+          while (e < nq && e - s0 < Qmax && std::fabs(q[e] - (q[s0] + (double)(e - s0) * dq)) <= tol) ++e;
+        }
+        out.push_back(make_int2((int)s0, (int)(e - s0)));
+        s0 = e;
+      }
+    };
+    std::vector<int2> best, cand;
+    long best_cost = -1;
+    for (int Qc = 8; Qc <= 64; Qc += 8) {
+      blocks_for(Qc, cand);
+      const long cost = (long)cand.size() * (Qc + 20);
+      if (best_cost < 0 || cost < best_cost) {
+        best_cost = cost;
+        best = cand;
+        P->Q = Qc;
+      }
+    }
+    P->n_qblocks = (int)best.size();
+    std::vector<float4> qpar(P->n_qblocks);
+    std::vector<int2>& qrange = best;
+    double max_half = 0.0;
+    for (int b = 0; b < P->n_qblocks; ++b) {
+      const int64_t st = qrange[b].x, cnt = qrange[b].y;
+      const double q0 = q[st];
+      const double half = cnt > 1 ? 0.5 * (q[st + cnt - 1] - q[st]) / (double)(cnt - 1) : 0.0;
+      const float q0h = (float)q0, hh = (float)half;
+      qpar[b] = make_float4(q0h, (float)(q0 - (double)q0h), hh, (float)(half - (double)hh));
+      max_half = std::max(max_half, std::fabs(half));
+    }
+    P->wide = (max_half * (P->L.extent + 1.0) > 0.8) ? 1 : 0;
+    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8);
+    P->n_work = (int)work.size();
+    P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
+    P->d_work = upload(ctx, P->owned, work.data(), work.size(), s);
+    P->d_qpar = upload(ctx, P->owned, qpar.data(), qpar.size(), s);
+    P->d_qrange = upload(ctx, P->owned, qrange.data(), qrange.size(), s);
+  } else {
+    P->n_qblocks = (int)((nq + kQD - 1) / kQD);
+    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8);
+    P->n_work = (int)work.size();
+    P->d_atoms64 = upload(ctx, P->owned, (const double4*)P->L.atoms64.data(), (size_t)P->L.n_pad, s);
+    P->d_work = upload(ctx, P->owned, work.data(), work.size(), s);
+    P->d_q = upload(ctx, P->owned, q, (size_t)nq, s);
+  }
+  P->d_tile_type = upload(ctx, P->owned, P->L.tile_type.data(), P->L.tile_type.size(), s);
+  P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)P->n_pairs * nq, s);
+  P->d_status = upload<int>(ctx, P->owned, nullptr, 1, s);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  return P;
+}
+
+void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
+  if (P.nq == 0 || P.L.n_tiles == 0) return;
+  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_out, 0, (size_t)P.n_pairs * P.nq * sizeof(double), s));
+  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_status, 0, sizeof(int), s));
+  if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_start, s));
+  const int T = P.L.T, nq = (int)P.nq;
+  if (P.fp64) {
+    int per_sm = 0;
+    CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp64, kThreads, 0));
+    const int grid = std::max(1, std::min(P.n_work, ctx->sm_count * std::max(per_sm, 1)));
+    k_pair_fp64<<<grid, kThreads, 0, s>>>(P.d_atoms64, P.d_tile_type, P.d_work, P.n_work, P.d_q, nq, T, P.d_out);
+    CRAB_CUDA_CHECK(cudaGetLastError());
+  } else {
+#define CRAB_LAUNCH(QQ)                                                                                          \
+  case QQ:                                                                                                       \
+    launch_fp32<QQ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, T, \
+                    P.wide, P.d_out, P.d_status);                                                                \
+    break;
+    switch (P.Q) {
+      CRAB_LAUNCH(8)
+      CRAB_LAUNCH(16)
+      CRAB_LAUNCH(24)
+      CRAB_LAUNCH(32)
+      CRAB_LAUNCH(40)
+      CRAB_LAUNCH(48)
+      CRAB_LAUNCH(56)
+      CRAB_LAUNCH(64)
+      default: throw Error(CRAB_EINVAL, "unsupported q block");
+    }
+#undef CRAB_LAUNCH
+  }
+  if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_stop, s));
+  ctx->launches += 1;
+}
+
+void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
+  const int T = P.L.T;
+  const int64_t nq = P.nq;
+  std::fill(out, out + (size_t)P.n_pairs * nq, 0.0);
+  if (nq > 0 && P.L.n_tiles > 0) {
+    int status = 0;
+    copy_d2h(ctx, out, P.d_out, (size_t)P.n_pairs * nq * sizeof(double), ctx->stream);
+    copy_d2h(ctx, &status, P.d_status, sizeof(int), ctx->stream);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    if (timed) {
+      float ms = 0.0f;
+      CRAB_CUDA_CHECK(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+      ctx->last_pair_ms = ms;
+      ctx->last_pair_q = ((double)P.L.n * (double)(P.L.n - 1) / 2.0) * (double)nq;
+    }
+    if (status) throw Error(status, "pair kernel: a bounded wait on a j-tile copy ran out");
+  }
+  if (P.fp64) {
+    for (int64_t k = 0; k < nq; ++k)
+      if (P.q[k] == 0.0) {
+        for (int a = 0; a < T; ++a)
+          for (int b = a; b < T; ++b)
+            out[(size_t)pair_index(a, b, T) * nq + k] =
+                (a == b) ? 0.5 * (P.L.sum_w[a] * P.L.sum_w[a] - P.L.self_w2[a]) : P.L.sum_w[a] * P.L.sum_w[b];
+      }
+    return;
+  }
+  // raw sums are Σ w_i w_j sin(q r)/r: divide by q; q = 0 takes the exact Σ w_i w_j
+  for (int a = 0; a < T; ++a)
+    for (int b = a; b < T; ++b) {
+      const int ab = pair_index(a, b, T);
+      const double w0 = (a == b) ? 0.5 * (P.L.sum_w[a] * P.L.sum_w[a] - P.L.self_w2[a]) : P.L.sum_w[a] * P.L.sum_w[b];
+      for (int64_t k = 0; k < nq; ++k) {
+        double& v = out[(size_t)ab * nq + k];
+        v = (P.q[k] == 0.0) ? w0 : v / P.q[k];
+      }
+    }
+}
+
+void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, Partials& out) {
+  const bool fp64 = force_fp64;
+  if (fp64 && L.atoms64.empty()) throw Error(CRAB_EINVAL, "layout lacks an f64 copy");
+  out.T = L.T;
+  out.nq = nq;
+  out.self = L.self_w2;
+  std::unique_ptr<PairPlan> P = make_pair_plan(ctx, std::move(L), q, nq, fp64);
+  out.pair.assign((size_t)P->n_pairs * nq, 0.0);
+  pair_plan_launch(ctx, *P, ctx->stream, !fp64);
+  pair_plan_fetch(ctx, *P, out.pair.data(), !fp64);
+}
+
+void quadratic_terms(const Partials& P, const double* X, const double* Y, double* out) {
+  const int T = P.T;
+  const int64_t nq = P.nq;
+  for (int64_t k = 0; k < nq; ++k) {
+    double s = 0.0;
+    for (int a = 0; a < T; ++a) s += X[(size_t)a * nq + k] * Y[(size_t)a * nq + k] * P.self[a];
+    for (int a = 0; a < T; ++a)
+      for (int b = a; b < T; ++b) {
+        const double coef = (a == b) ? 2.0 * X[(size_t)a * nq + k] * Y[(size_t)a * nq + k]
+                                     : X[(size_t)a * nq + k] * Y[(size_t)b * nq + k] +
+                                           X[(size_t)b * nq + k] * Y[(size_t)a * nq + k];
+        s += coef * P.pair[(size_t)pair_index(a, b, T) * nq + k];
+      }
+    out[k] = s;
+  }
+}
+
+}  // namespace crab
+
+namespace crab {
+
+void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_bytes, double* step_ms) {
+  cudaStream_t s = ctx->stream;
+  void* flush = flush_bytes > 0 ? ctx->dev("bench.flush", (size_t)flush_bytes) : nullptr;
+  std::vector<cudaEvent_t> ev(2 * (size_t)std::max(repeats, 0), nullptr);
+  struct Guard {
+    std::vector<cudaEvent_t>& e;
+    ~Guard() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } guard{ev};
+  for (auto& e : ev) CRAB_CUDA_CHECK(cudaEventCreate(&e));
+  for (int r = 0; r < repeats; ++r) {
+    if (flush) CRAB_CUDA_CHECK(cudaMemsetAsync(flush, r & 0xff, (size_t)flush_bytes, s));
+    CRAB_CUDA_CHECK(cudaEventRecord(ev[2 * r], s));
+    pair_plan_launch(ctx, P, s, false);
+    CRAB_CUDA_CHECK(cudaEventRecord(ev[2 * r + 1], s));
+  }
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int r = 0; r < repeats; ++r) {
+    float ms = 0.0f;
+    CRAB_CUDA_CHECK(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]));
+    if (step_ms) step_ms[r] = ms;
+    ctx->last_pair_ms = ms;
+  }
+  ctx->last_pair_q = ((double)P.L.n * (double)(P.L.n - 1) / 2.0) * (double)P.nq;
+  int status = 0;
+  copy_d2h(ctx, &status, P.d_status, sizeof(int), s);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (status) throw Error(status, "pair kernel: a bounded wait on a j-tile copy ran out");
+}
+
+}  // namespace crab

@@ -1,0 +1,202 @@
+// Internal declarations of the crabsaxs_b200 engine (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/crab_cuda.h"
+
+namespace crab {
+
+// Error carrying a crab status code; every extern "C" entry point catches it
+// and stores the message in the context.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CRAB_CUDA_CHECK(expr)                                                                              \
+  do {                                                                                                     \
+    cudaError_t _e = (expr);                                                                               \
+    if (_e != cudaSuccess)                                                                                 \
+      throw ::crab::Error(_e == cudaErrorMemoryAllocation ? CRAB_ENOMEM : CRAB_ECUDA,                      \
+                          std::string(#expr) + ": " + cudaGetErrorString(_e));                             \
+  } while (0)
+
+inline void require(bool ok, const std::string& msg) {
+  if (!ok) throw Error(CRAB_EINVAL, msg);
+}
+
+// Grow-only device buffer: one per named slot in the context, so repeated
+// calls reuse memory instead of allocating.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// Pinned host staging buffer, grow-only.
+struct HostBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace crab
+
+struct crab_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::mutex mu;
+  std::string last_error;
+  std::map<std::string, crab::DevBuf> bufs;
+  std::map<std::string, crab::HostBuf> hbufs;
+  int64_t launches = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;
+  double last_pair_ms = 0.0;
+  double last_pair_q = 0.0;
+
+  void* dev(const std::string& name, size_t bytes);
+  void* host(const std::string& name, size_t bytes);
+};
+
+namespace crab {
+
+// Counted host<->device copies on the context stream.
+inline void copy_h2d(crab_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (!bytes) return;
+  CRAB_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  ctx->h2d_bytes += (int64_t)bytes;
+}
+inline void copy_d2h(crab_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (!bytes) return;
+  CRAB_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  ctx->d2h_bytes += (int64_t)bytes;
+}
+
+// ---------------------------------------------------------------- tables
+// Scattering class of an atom: element plus the united-atom group that is in
+// effect for the requested hydrogen mode (-1 in explicit mode).
+struct AtomClass {
+  int element;
+  int group;
+  bool operator<(const AtomClass& o) const { return element != o.element ? element < o.element : group < o.group; }
+  bool operator==(const AtomClass& o) const { return element == o.element && group == o.group; }
+};
+
+double form_factor_value(int element, int group, double q);  // without occupancy
+double form_factor(int element, int group, double occ, bool implicit_h, double q);
+double excluded_volume_for_atom(int element, int group, bool implicit_h);
+double vdw_radius(int element);
+double water_form_factor(double q);
+double excluded_volume_scale(double q, double c1);
+double fraser_gaussian(double q, double volume);
+double adaptive_shell_width(double rg);
+double adaptive_site_volume(double spacing);
+int united_atom_group(const char* residue, const char* name);
+double sinc(double x);
+
+// Per-class amplitudes without occupancy for the Debye solvent model
+// (solvent.rs:454-488): vacuum, excluded (times density), analytic shell.
+void debye_class_amplitudes(const AtomClass& c, bool implicit_h, double q, double density, double thickness,
+                            double* v, double* e, double* h);
+// Same for the multipole solvent model (spherical.rs:205-231).
+void multipole_class_amplitudes(const AtomClass& c, bool implicit_h, double q, double density, double thickness,
+                                double* v, double* e, double* h);
+
+// ---------------------------------------------------------------- layout
+// Atoms of one pair-sum problem, grouped by type, spatially ordered inside
+// each type, and padded per type to whole tiles of kTile atoms.
+constexpr int kTile = 128;
+
+struct Layout {
+  int T = 0;
+  int64_t n = 0;         // real atoms
+  int64_t n_pad = 0;     // padded length
+  int n_tiles = 0;
+  std::vector<float> atoms;      // 4 floats per slot: x, y, z, w (centred)
+  std::vector<double> atoms64;   // 4 doubles per slot (for the FP64 reference)
+  std::vector<int32_t> tile_type;
+  std::vector<float> tile_sphere;  // per tile: centre xyz + radius (for near/far tests)
+  std::vector<double> self_w2;     // per type Σ w²
+  std::vector<double> sum_w;       // per type Σ w
+  double extent = 0.0;             // max pair distance bound
+};
+
+Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64);
+
+// Self + pair partials of a layout at every q (P = T(T+1)/2 rows).
+struct Partials {
+  int T = 0;
+  int64_t nq = 0;
+  std::vector<double> pair;  // [P][nq]
+  std::vector<double> self;  // [T]
+};
+
+// Device-resident pair-sum problem: layout, work list and q-block
+// parameters uploaded once; launched any number of times.
+struct PairPlan {
+  Layout L;
+  bool fp64 = false;
+  int64_t nq = 0;
+  std::vector<double> q;
+  int n_pairs = 0, Q = 0, n_qblocks = 0, n_work = 0, wide = 0;
+  std::vector<void*> owned;
+  float4* d_atoms = nullptr;
+  double4* d_atoms64 = nullptr;
+  int* d_tile_type = nullptr;
+  int4* d_work = nullptr;
+  float4* d_qpar = nullptr;
+  int2* d_qrange = nullptr;
+  double* d_q = nullptr;
+  double* d_out = nullptr;  // [n_pairs][nq] raw sums
+  int* d_status = nullptr;
+  ~PairPlan();
+};
+bool q_grid_uniform(const double* q, int64_t nq);
+std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64);
+// Enqueue the pair kernel on stream s (device time recorded when timed).
+void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed);
+// Copy back and convert raw sums to P_ab(q) (divide by q; exact q = 0).
+void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed);
+// One-shot: FP32 recurrence on a uniform grid, FP64 direct otherwise.
+void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, struct Partials& out);
+
+void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_bytes, double* step_ms);
+double measure_fp32_peak(crab_ctx* ctx, double target_ms);
+
+// Quadratic form Σ_ij X_i Y_j sinc(q r_ij) for per-type amplitude tables
+// X[t*nq+k], Y[t*nq+k] from partials.
+void quadratic_terms(const Partials& P, const double* X, const double* Y, double* out);
+inline int pair_index(int a, int b, int T) {
+  if (a > b) { int t = a; a = b; b = t; }
+  return a * T - a * (a - 1) / 2 + (b - a);
+}
+
+// ---------------------------------------------------------------- hydration grids
+struct GridResult {
+  std::vector<double> sites;  // 3 per site, z→y→x order
+  double voxel_volume = 0.0;
+};
+GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, double spacing, double clearance,
+                                double padding);
+GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* elem, int64_t n, double spacing,
+                                double probe, double thickness);
+
+}  // namespace crab
+
+struct crab_struct {
+  crab_ctx* ctx = nullptr;
+  int64_t n = 0;
+  std::vector<double> xyz;
+  std::vector<double> occ;
+  std::vector<int8_t> elem;
+  std::vector<int8_t> group;
+};

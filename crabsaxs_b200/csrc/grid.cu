@@ -1,0 +1,383 @@
+// Hydration-shell site placement on a voxel grid, bit-exact against the
+// reference.
+//
+// Adaptive coarse shell (crabSAXS src/solvent.rs:121-223): a voxel centre is a
+// site when it lies within the outer radius (clearance + shell width) of some
+// atom and not within the clearance of any atom; sites are listed in z→y→x
+// voxel order.  Exterior shell (src/solvent.rs:259-401): voxels inside a vdW +
+// probe sphere are molecular, the unknown voxels 6-connected to the box
+// boundary are exterior, and exterior voxels within vdW + probe + thickness of
+// an atom are sites.
+//
+// Exactness: every per-voxel decision in the reference is an OR over atoms of
+// (voxel inside the atom's clipped bounding box) AND (squared distance <=
+// r² + 1e-10), and the flood fill's result is the connected component of the
+// boundary, independent of visiting order.  The device evaluates the same f64
+// expressions in the same order with explicitly rounded intrinsics (no fused
+// multiply-add), so the site set and its order equal the reference's.  The
+// O(N) prologue (centroid, Rg, bounding box) runs on the host in the
+// reference's sequential order.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "engine.hpp"
+
+namespace crab {
+namespace {
+
+struct Box {
+  double mn[3];
+  double spacing;
+  uint64_t n[3];
+};
+
+__device__ __forceinline__ double norm2_rn(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Clipped voxel range of one atom (solvent.rs:187-194 / 322-329).
+__device__ __forceinline__ void atom_range(const Box& b, const double* p, double radius, uint64_t* lo, uint64_t* hi) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lower = __ddiv_rn(__dsub_rn(__dsub_rn(p[d], radius), b.mn[d]), b.spacing);
+    const double upper = __ddiv_rn(__dsub_rn(__dadd_rn(p[d], radius), b.mn[d]), b.spacing);
+    const double f = fmax(floor(__dsub_rn(lower, 1e-10)), 0.0);
+    const double c = ceil(__dadd_rn(upper, 1e-10));
+    lo[d] = (uint64_t)f;
+    const uint64_t cu = c > 0.0 ? (uint64_t)c : 0ull;
+    hi[d] = cu < b.n[d] - 1 ? cu : b.n[d] - 1;
+  }
+}
+
+// One warp per atom: mark voxels of the atom's box within the radius.
+// mode 0: mask[c] = value.  mode 1: only where mask[c] == 2 (exterior).
+__global__ void k_rasterize(const double* __restrict__ xyz, const double* __restrict__ radius_per_atom,
+                            double radius_all, double extra, int64_t n, Box b, uint8_t* __restrict__ mask,
+                            uint8_t value, int exterior_only) {
+  const int lane = threadIdx.x & 31;
+  const int64_t atom = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (atom >= n) return;
+  const double p[3] = {xyz[3 * atom], xyz[3 * atom + 1], xyz[3 * atom + 2]};
+  const double radius = radius_per_atom ? __dadd_rn(radius_per_atom[atom], extra) : radius_all;
+  const double thr = __dadd_rn(__dmul_rn(radius, radius), 1e-10);
+  uint64_t lo[3], hi[3];
+  atom_range(b, p, radius, lo, hi);
+  if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2]) return;
+  const uint64_t ex = hi[0] - lo[0] + 1, ey = hi[1] - lo[1] + 1, ez = hi[2] - lo[2] + 1;
+  const uint64_t total = ex * ey * ez;
+  for (uint64_t v = lane; v < total; v += 32) {
+    const uint64_t x = lo[0] + v % ex, y = lo[1] + (v / ex) % ey, z = lo[2] + v / (ex * ey);
+    const double px = __dadd_rn(b.mn[0], __dmul_rn((double)x, b.spacing));
+    const double py = __dadd_rn(b.mn[1], __dmul_rn((double)y, b.spacing));
+    const double pz = __dadd_rn(b.mn[2], __dmul_rn((double)z, b.spacing));
+    if (norm2_rn(__dsub_rn(px, p[0]), __dsub_rn(py, p[1]), __dsub_rn(pz, p[2])) <= thr) {
+      const uint64_t c = (z * b.n[1] + y) * b.n[0] + x;
+      if (!exterior_only) mask[c] = value;
+      else if (mask[c] == 2) mask[c] = value;
+    }
+  }
+}
+
+// Site flag of a voxel for the two shells.
+__device__ __forceinline__ bool site_flag(const uint8_t* a, const uint8_t* b, uint64_t c, int kind) {
+  return kind == 0 ? (a[c] != 0 && b[c] == 0) : (a[c] == 3);
+}
+
+constexpr int kScanThreads = 256;
+constexpr int kPerThread = 16;
+constexpr int kChunk = kScanThreads * kPerThread;
+
+__global__ void k_count(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint64_t count, int kind,
+                        uint32_t* __restrict__ chunk_count) {
+  __shared__ uint32_t s[kScanThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kPerThread;
+  uint32_t c = 0;
+  for (int i = 0; i < kPerThread; ++i)
+    if (base + i < count && site_flag(a, b, base + i, kind)) ++c;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) t += s[w];
+    chunk_count[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of chunk counts in one block; total at offsets[n].
+__global__ void k_scan_chunks(const uint32_t* __restrict__ cnt, uint64_t n, uint64_t* __restrict__ offsets) {
+  __shared__ uint64_t part[1024];
+  const uint64_t per = (n + blockDim.x - 1) / blockDim.x;
+  const uint64_t b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+  uint64_t s = 0;
+  for (uint64_t i = b0; i < b1; ++i) s += cnt[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t run = 0;
+    for (unsigned t = 0; t < blockDim.x; ++t) {
+      uint64_t v = part[t];
+      part[t] = run;
+      run += v;
+    }
+    offsets[n] = run;
+  }
+  __syncthreads();
+  uint64_t run = part[threadIdx.x];
+  for (uint64_t i = b0; i < b1; ++i) {
+    offsets[i] = run;
+    run += cnt[i];
+  }
+}
+
+__global__ void k_emit(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint64_t count, int kind, Box bx,
+                       const uint64_t* __restrict__ offsets, double* __restrict__ sites) {
+  __shared__ uint32_t warp_tot[kScanThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kPerThread;
+  uint32_t c = 0;
+  for (int i = 0; i < kPerThread; ++i)
+    if (base + i < count && site_flag(a, b, base + i, kind)) ++c;
+  // block exclusive scan of c in thread order (= voxel order)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_tot[w];
+  uint64_t pos = offsets[blockIdx.x] + before + incl - c;
+  for (int i = 0; i < kPerThread; ++i) {
+    const uint64_t v = base + i;
+    if (v < count && site_flag(a, b, v, kind)) {
+      const uint64_t x = v % bx.n[0], y = (v / bx.n[0]) % bx.n[1], z = v / (bx.n[0] * bx.n[1]);
+      sites[3 * pos] = __dadd_rn(bx.mn[0], __dmul_rn((double)x, bx.spacing));
+      sites[3 * pos + 1] = __dadd_rn(bx.mn[1], __dmul_rn((double)y, bx.spacing));
+      sites[3 * pos + 2] = __dadd_rn(bx.mn[2], __dmul_rn((double)z, bx.spacing));
+      ++pos;
+    }
+  }
+}
+
+// Exterior flood fill: boundary seeds, then line sweeps along x, y and z that
+// carry the exterior label (2) through unknown voxels (0), repeated until no
+// voxel changes.  The fixed point is the 6-connected component of the
+// boundary's unknown voxels, i.e. the reference's BFS result.
+__global__ void k_seed_boundary(uint8_t* __restrict__ s, Box b) {
+  const uint64_t count = b.n[0] * b.n[1] * b.n[2];
+  for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < count; c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t x = c % b.n[0], y = (c / b.n[0]) % b.n[1], z = c / (b.n[0] * b.n[1]);
+    const bool edge = x == 0 || x + 1 == b.n[0] || y == 0 || y + 1 == b.n[1] || z == 0 || z + 1 == b.n[2];
+    if (edge && s[c] == 0) s[c] = 2;
+  }
+}
+
+// axis 0: lines along x (one per (y,z)); 1: along y; 2: along z.
+__global__ void k_sweep(uint8_t* __restrict__ s, Box b, int axis, int* __restrict__ changed) {
+  const uint64_t nx = b.n[0], ny = b.n[1], nz = b.n[2];
+  uint64_t lines, len, stride;
+  if (axis == 0) { lines = ny * nz; len = nx; stride = 1; }
+  else if (axis == 1) { lines = nx * nz; len = ny; stride = nx; }
+  else { lines = nx * ny; len = nz; stride = nx * ny; }
+  const uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= lines) return;
+  uint64_t start;
+  if (axis == 0) start = l * nx;                       // l = z*ny + y
+  else if (axis == 1) start = (l / nx) * nx * ny + (l % nx);  // l = z*nx + x
+  else start = l;                                       // l = y*nx + x
+  int any = 0;
+  bool carry = false;
+  for (uint64_t i = 0; i < len; ++i) {
+    uint8_t& v = s[start + i * stride];
+    if (v == 2) carry = true;
+    else if (v == 0) { if (carry) { v = 2; any = 1; } }
+    else carry = false;
+  }
+  carry = false;
+  for (uint64_t i = len; i-- > 0;) {
+    uint8_t& v = s[start + i * stride];
+    if (v == 2) carry = true;
+    else if (v == 0) { if (carry) { v = 2; any = 1; } }
+    else carry = false;
+  }
+  if (any) atomicOr(changed, 1);
+}
+
+struct Scratch {
+  std::vector<void*> owned;
+  ~Scratch() {
+    for (void* p : owned) cudaFree(p);
+  }
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    CRAB_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    owned.push_back(p);
+    return (T*)p;
+  }
+};
+
+GridResult compact_sites(crab_ctx* ctx, Scratch& sc, const uint8_t* a, const uint8_t* b, uint64_t count, int kind,
+                         const Box& bx) {
+  cudaStream_t s = ctx->stream;
+  const uint64_t chunks = (count + kChunk - 1) / kChunk;
+  uint32_t* d_cnt = sc.alloc<uint32_t>(chunks);
+  uint64_t* d_off = sc.alloc<uint64_t>(chunks + 1);
+  k_count<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, d_cnt);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  k_scan_chunks<<<1, 1024, 0, s>>>(d_cnt, chunks, d_off);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  uint64_t m = 0;
+  copy_d2h(ctx, &m, d_off + chunks, sizeof(uint64_t), s);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  GridResult r;
+  r.sites.resize(3 * m);
+  if (m) {
+    double* d_sites = sc.alloc<double>(3 * m);
+    k_emit<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, bx, d_off, d_sites);
+    CRAB_CUDA_CHECK(cudaGetLastError());
+    copy_d2h(ctx, r.sites.data(), d_sites, 3 * m * sizeof(double), s);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  }
+  ctx->launches += m ? 4 : 3;
+  return r;
+}
+
+// Box set-up shared by both grids (solvent.rs:160-176 / 290-306).
+bool make_box(const double* xyz, int64_t n, double pad, double spacing, Box* b, uint64_t* count) {
+  double mn[3] = {xyz[0], xyz[1], xyz[2]}, mx[3] = {xyz[0], xyz[1], xyz[2]};
+  for (int64_t i = 1; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = std::fmin(mn[d], xyz[3 * i + d]);
+      mx[d] = std::fmax(mx[d], xyz[3 * i + d]);
+    }
+  for (int d = 0; d < 3; ++d) {
+    b->mn[d] = mn[d] - pad;
+    mx[d] = mx[d] + pad;
+  }
+  b->spacing = spacing;
+  unsigned __int128 total = 1;
+  for (int d = 0; d < 3; ++d) {
+    const double span = std::ceil(((mx[d] - b->mn[d]) / spacing) - 1e-10);
+    if (!(span < 9.0e18)) return false;
+    b->n[d] = (uint64_t)std::max(span, 0.0) + 1;
+    total *= b->n[d];
+    if (total > (unsigned __int128)UINT64_MAX) return false;
+  }
+  *count = (uint64_t)total;
+  return true;
+}
+
+}  // namespace
+
+GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, double spacing, double clearance,
+                                double padding) {
+  GridResult r;
+  if (n == 0) {
+    r.voxel_volume = adaptive_site_volume(spacing);
+    return r;
+  }
+  require(std::isfinite(spacing) && spacing > 0.0 && std::isfinite(clearance) && clearance > 0.0 &&
+              std::isfinite(padding) && padding >= 0.0,
+          "adaptive hydration-grid dimensions must be finite and positive");
+  // centroid and radius of gyration in the reference's order (solvent.rs:144-155)
+  double c[3] = {0, 0, 0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) c[d] = c[d] + xyz[3 * i + d];
+  for (int d = 0; d < 3; ++d) c[d] = c[d] / (double)n;
+  double acc = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double dx = xyz[3 * i] - c[0], dy = xyz[3 * i + 1] - c[1], dz = xyz[3 * i + 2] - c[2];
+    acc += ((0.0 + dx * dx) + dy * dy) + dz * dz;
+  }
+  const double rg = std::sqrt(acc / (double)n);
+  const double inner = clearance, outer = clearance + adaptive_shell_width(rg);
+  Box b;
+  uint64_t count = 0;
+  require(make_box(xyz, n, padding, spacing, &b, &count), "adaptive hydration grid is too large");
+  require(count <= (uint64_t)4000000000ull, "adaptive hydration grid exceeds 4e9 voxels");
+  Scratch sc;
+  cudaStream_t s = ctx->stream;
+  uint8_t* shell = sc.alloc<uint8_t>(count);
+  uint8_t* mol = sc.alloc<uint8_t>(count);
+  double* d_xyz = sc.alloc<double>(3 * n);
+  CRAB_CUDA_CHECK(cudaMemsetAsync(shell, 0, count, s));
+  CRAB_CUDA_CHECK(cudaMemsetAsync(mol, 0, count, s));
+  copy_h2d(ctx, d_xyz, xyz, 3 * n * sizeof(double), s);
+  const unsigned blocks = (unsigned)((n * 32 + 255) / 256);
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, nullptr, outer, 0.0, n, b, shell, 1, 0);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, nullptr, inner, 0.0, n, b, mol, 1, 0);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  ctx->launches += 2;
+  r = compact_sites(ctx, sc, shell, mol, count, 0, b);
+  r.voxel_volume = adaptive_site_volume(spacing);
+  return r;
+}
+
+GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* elem, int64_t n, double spacing,
+                                double probe, double thickness) {
+  GridResult r;
+  if (n == 0) {
+    r.voxel_volume = (spacing * spacing) * spacing;
+    return r;
+  }
+  require(std::isfinite(spacing) && spacing > 0.0 && std::isfinite(probe) && probe >= 0.0 &&
+              std::isfinite(thickness) && thickness > 0.0,
+          "solvent-grid dimensions must be finite and positive");
+  double vmax = 0.0;
+  std::vector<double> radius(n);
+  for (int64_t i = 0; i < n; ++i) {
+    radius[i] = vdw_radius(elem[i]);
+    vmax = std::fmax(vmax, radius[i]);
+  }
+  const double margin = vmax + probe + thickness + spacing;
+  Box b;
+  uint64_t count = 0;
+  require(make_box(xyz, n, margin, spacing, &b, &count), "solvent grid is too large");
+  if (count > 250000000ull)
+    throw Error(CRAB_EINVAL, "solvent grid requires " + std::to_string(count) + " voxels; limit is 250000000");
+  Scratch sc;
+  cudaStream_t s = ctx->stream;
+  uint8_t* state = sc.alloc<uint8_t>(count);
+  double* d_xyz = sc.alloc<double>(3 * n);
+  double* d_rad = sc.alloc<double>(n);
+  int* d_changed = sc.alloc<int>(1);
+  CRAB_CUDA_CHECK(cudaMemsetAsync(state, 0, count, s));
+  copy_h2d(ctx, d_xyz, xyz, 3 * n * sizeof(double), s);
+  copy_h2d(ctx, d_rad, radius.data(), n * sizeof(double), s);
+  const unsigned blocks = (unsigned)((n * 32 + 255) / 256);
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, d_rad, 0.0, probe, n, b, state, 1, 0);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  k_seed_boundary<<<std::max<unsigned>(1, (unsigned)std::min<uint64_t>((count + 255) / 256, 65535)), 256, 0, s>>>(state, b);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  ctx->launches += 2;
+  // sweep until the fixed point; every round is bounded and the total number
+  // of rounds cannot exceed the number of voxels
+  for (uint64_t round = 0; round <= count; ++round) {
+    CRAB_CUDA_CHECK(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
+    for (int axis = 0; axis < 3; ++axis) {
+      const uint64_t lines = axis == 0 ? b.n[1] * b.n[2] : axis == 1 ? b.n[0] * b.n[2] : b.n[0] * b.n[1];
+      k_sweep<<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(state, b, axis, d_changed);
+      CRAB_CUDA_CHECK(cudaGetLastError());
+      ctx->launches += 1;
+    }
+    int changed = 0;
+    copy_d2h(ctx, &changed, d_changed, sizeof(int), s);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (!changed) break;
+  }
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, d_rad, 0.0, probe + thickness, n, b, state, 3, 1);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  ctx->launches += 1;
+  r = compact_sites(ctx, sc, state, state, count, 1, b);
+  r.voxel_volume = (spacing * spacing) * spacing;
+  return r;
+}
+
+}  // namespace crab

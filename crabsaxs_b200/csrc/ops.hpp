@@ -1,0 +1,51 @@
+// Host orchestration shared by the entry points: typing, amplitude tables,
+// basis assembly and the multipole/fit/ensemble drivers.
+#pragma once
+
+#include <functional>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace crab {
+
+int guarded_impl(crab_ctx* ctx, const std::function<void()>& fn);
+void validate_q(const double* q, int64_t nq);
+void validate_solvent(const crab_solvent& s);
+
+// Which amplitude terms a pair sum feeds; decides which atoms may be dropped
+// because all their amplitudes vanish.
+enum class TermSet { Vacuum, SolventAnalytic, SolventGrid };
+
+// Atoms (plus optional hydration sites as the last type, element -1) mapped
+// to dense scattering types.
+struct TypedAtoms {
+  std::vector<AtomClass> cls;
+  std::vector<double> xyz, w;
+  std::vector<int32_t> type;
+  int T = 0;
+};
+TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites);
+
+// Per-type Debye amplitude tables [T][nq] (no occupancy).  solvent == NULL
+// means vacuum form factors only.
+void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const crab_solvent* solvent, bool implicit,
+                      double site_volume, std::vector<double>& V, std::vector<double>& E, std::vector<double>& H);
+Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64);
+std::vector<double> hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s, double* volume);
+void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
+                 bool implicit, double* out6, bool fp64);
+void debye_vacuum(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, bool implicit, double* out,
+                  bool fp64);
+void combine_basis(const double* q, int64_t nq, const double* b, double c1, double c2, double* out);
+void centre_and_rmax(const crab_struct* st, double* c, double* rmax);
+
+// Multipole engine (multipole.cu).
+void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                              bool implicit, int precision, double* out);
+void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                                  const crab_solvent& s, bool implicit, int precision, double* out6);
+void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                                      const crab_solvent& s, bool implicit, int precision, double* out);
+
+}  // namespace crab

@@ -1,0 +1,293 @@
+/*
+ * crab_cuda.h — C ABI of the B200 (sm_100a) scattering engine.
+ *
+ * This is the boundary a host program (the crabSAXS Rust crate through
+ * `extern "C"` declarations, Python through ctypes, C/C++ directly) binds to
+ * replace crabSAXS's CPU engines.  Every entry point takes plain pointers and
+ * sizes, returns an int status, and never retains a caller pointer after it
+ * returns.  Host arrays are f64 (the reference's `Vec<f64>`); device memory
+ * belongs to the context.
+ *
+ * Reference interfaces replaced (file:line in the crabSAXS repository):
+ *   crab_debye_intensity          src/scattering.rs:86-110  debye_intensity_with_hydrogens
+ *   crab_compute_curve            src/scattering.rs:112-212 compute_curve (Auto/Debye/Multipole dispatch)
+ *   crab_debye_solvent_basis      src/solvent.rs:504-584    debye_solvent_basis
+ *   crab_combine_solvent_basis    src/spherical.rs:567-584  combine_solvent_basis
+ *   crab_hydration_grid_adaptive  src/solvent.rs:121-223    build_adaptive_hydration_grid
+ *   crab_hydration_grid_exterior  src/solvent.rs:259-401    build_hydration_grid
+ *   crab_multipole_intensity      src/spherical.rs:266-403  multipole_intensity(_streaming)
+ *   crab_multipole_solvent_basis  src/spherical.rs:474-565  multipole_solvent_basis
+ *   crab_fit                      src/fit.rs:288-454        fit_to_experimental_with_options
+ *                                 (behind SaxsFitter::fit analysis.rs:76-87 and SaxsScorer::score analysis.rs:156-177)
+ *   crab_ensemble_fit             src/ensemble.rs:127-299   EnsembleFitter::fit / fit_core
+ *   crab_reweight_curves          src/reweight.rs:84-154    reweight_curves
+ *
+ * Status codes map onto crabSAXS's SaxsError (src/error.rs:4-25):
+ *   CRAB_EINVAL -> SaxsError::InvalidInput, CRAB_ENOTCONV -> FitDidNotConverge,
+ *   every other non-zero code -> SaxsError::Other (message from crab_ctx_last_error).
+ *
+ * Threading: a context serialises its own calls with an internal mutex; use
+ * one context per host thread for concurrency (rayon workers in the reference
+ * call compute_curve concurrently, ensemble.rs:244).
+ */
+#ifndef CRAB_CUDA_H
+#define CRAB_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRAB_OK 0
+#define CRAB_EINVAL 1       /* invalid input (SaxsError::InvalidInput) */
+#define CRAB_ENOMEM 2       /* device or host allocation failed */
+#define CRAB_ECUDA 3        /* CUDA runtime error */
+#define CRAB_ETIMEOUT 4     /* a bounded device-side wait ran out */
+#define CRAB_ENOTCONV 5     /* fit did not converge (SaxsError::FitDidNotConverge) */
+#define CRAB_ECAPACITY 6    /* caller buffer too small (two-call size query) */
+#define CRAB_ENODEVICE 7    /* no CUDA device / extension not usable */
+
+/* Element codes, in crabSAXS's `Element` order (src/structure.rs:90-106). */
+enum {
+  CRAB_EL_H = 0, CRAB_EL_C, CRAB_EL_N, CRAB_EL_O, CRAB_EL_S, CRAB_EL_P, CRAB_EL_NA, CRAB_EL_MG,
+  CRAB_EL_CL, CRAB_EL_CA, CRAB_EL_FE, CRAB_EL_ZN, CRAB_EL_K, CRAB_EL_I, CRAB_EL_OTHER
+};
+
+/* Hydration models (src/solvent.rs:18-25). */
+enum { CRAB_HYD_ANALYTIC = 0, CRAB_HYD_GRID = 1, CRAB_HYD_ADAPTIVE = 2 };
+/* Scattering methods (src/scattering.rs:16-21). */
+enum { CRAB_METHOD_AUTO = 0, CRAB_METHOD_DEBYE = 1, CRAB_METHOD_MULTIPOLE = 2 };
+/* Multipole GEMM precision. */
+enum { CRAB_PREC_FP64 = 0, CRAB_PREC_TF32 = 1, CRAB_PREC_BF16 = 2, CRAB_PREC_BF16_SPLIT = 3, CRAB_PREC_TF32_SPLIT = 4,
+       CRAB_PREC_FP32 = 5 };
+/* fit.rs:30-47 modes. */
+enum { CRAB_SCALE_FIT = 0, CRAB_SCALE_FIXED = 1 };
+enum { CRAB_BG_FIT = 0, CRAB_BG_FIXED_ZERO = 1, CRAB_BG_FIXED = 2 };
+
+/* SolventParams (src/solvent.rs:27-50). Defaults: c1=1, c2=0, t=3 Å, ρ=0.334, Analytic, 4 Å. */
+typedef struct crab_solvent {
+  double c1;
+  double c2;
+  double shell_thickness;   /* Å */
+  double bulk_density;      /* e/Å^3 */
+  int32_t hydration_model;  /* CRAB_HYD_* */
+  int32_t _pad;
+  double grid_spacing;      /* Å, adaptive grid */
+} crab_solvent;
+
+/* ComputeOptions (src/scattering.rs:28-47); has_solvent=0 means `solvent: None`. */
+typedef struct crab_compute_options {
+  int32_t method;           /* CRAB_METHOD_* */
+  int32_t implicit_hydrogen;/* HydrogenMode::Implicit = 1, Explicit = 0 */
+  int32_t l_max;            /* 0 = adaptive (None), else 8..64 */
+  int32_t has_solvent;
+  crab_solvent solvent;
+} crab_compute_options;
+
+/* FitOptions (src/fit.rs:49-82). */
+typedef struct crab_fit_options {
+  int32_t method;
+  int32_t implicit_hydrogen;
+  double c1_lo, c1_hi, c2_lo, c2_hi;
+  int32_t max_iterations;
+  int32_t q_sampling_stride;
+  crab_solvent solvent;
+  int32_t scale_mode;       /* CRAB_SCALE_* */
+  int32_t bg_mode;          /* CRAB_BG_* */
+  double scale_value;
+  double bg_value;
+  int32_t optimizer;        /* 0 Nelder-Mead (reference), 1 L-BFGS-B on the analytic gradient */
+  int32_t _pad;
+} crab_fit_options;
+
+/* FitResult (src/fit.rs:19-27), fitted curve written to a caller buffer. */
+typedef struct crab_fit_result {
+  double scale, background, c1, c2;
+  double chi2;              /* reduced chi^2, N-1 convention (fit.rs:185-196) */
+  int32_t iterations;
+  int32_t converged;
+} crab_fit_result;
+
+typedef struct crab_ctx crab_ctx;
+typedef struct crab_struct crab_struct;
+
+/* ---- context ------------------------------------------------------------ */
+int crab_ctx_create(int device, crab_ctx** out);
+int crab_ctx_destroy(crab_ctx* ctx);
+const char* crab_ctx_last_error(const crab_ctx* ctx);
+/* Launch counter and the device time (ms, CUDA events on the context stream)
+ * of the most recent pair-sum kernel; for measurement harnesses. */
+int crab_ctx_stats(crab_ctx* ctx, int64_t* kernel_launches, double* last_pair_kernel_ms, double* last_pair_kernel_pairq);
+int crab_ctx_reset_stats(crab_ctx* ctx);
+/* Device-resident workspace size in bytes (for sizing studies). */
+int crab_ctx_workspace_bytes(crab_ctx* ctx, int64_t* bytes);
+
+/* ---- atom typing (host) ------------------------------------------------- */
+/* formfactor.rs:357-417 united_atom_group: residue + atom name -> group code,
+ * -1 when the atom is not a standard united atom. */
+int crab_united_atom_group(const char* residue_name, const char* atom_name);
+/* formfactor.rs:425-439 form_factor_for_atom, f64, host. */
+double crab_form_factor(int element, int group, double occupancy, int implicit_hydrogen, double q);
+/* solvent.rs:428-438 excluded_volume_for_atom. */
+double crab_excluded_volume_for_atom(int element, int group, int implicit_hydrogen);
+
+/* ---- structures --------------------------------------------------------- */
+/* Upload a structure (src/structure.rs:151-165 Atom/Structure): xyz is n*3 f64,
+ * occupancy n f64, element n codes (CRAB_EL_*), group n codes (-1 = none).
+ * Coordinates are centred and cast to FP32 on upload; an f64 copy is kept for
+ * the bit-exact hydration grids. */
+int crab_structure_create(crab_ctx* ctx, const double* xyz, const double* occupancy, const int8_t* element,
+                          const int8_t* group, int64_t n, crab_struct** out);
+int crab_structure_destroy(crab_struct* st);
+int64_t crab_structure_atom_count(const crab_struct* st);
+
+/* ---- Debye engine ------------------------------------------------------- */
+/* Vacuum Debye intensity, clamp >= 0 (scattering.rs:86-110). */
+int crab_debye_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int implicit_hydrogen,
+                         double* out);
+/* Six Debye terms vv, ee, hh, ve, vh, eh, out6 is [6][nq] (solvent.rs:504-584).
+ * The hydration grid (if any) is built on the device. */
+int crab_debye_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq,
+                             const crab_solvent* solvent, int implicit_hydrogen, double* out6);
+/* Same six terms with the pair sums in the chosen precision: CRAB_PREC_FP32
+ * (the recurrence kernel, as crab_debye_solvent_basis) or CRAB_PREC_FP64
+ * (direct f64 sinc on the device: the FP64 reference for error reports). */
+int crab_debye_solvent_basis_ex(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq,
+                                const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6);
+/* Recombination I = vv + G²ee + c2²hh − 2G·ve + 2c2·vh − 2G·c2·eh, clamp ≥0
+ * (spherical.rs:567-584; G from solvent.rs:448-452). Host-only, f64. */
+int crab_combine_solvent_basis(const double* q, int64_t nq, const double* basis6, double c1, double c2, double* out);
+/* Low level: per atom-type-pair partial sums for caller-supplied types.
+ *   out[ab*nq+k] = Σ_{i<j,{t_i,t_j}={a,b}} w_i w_j sinc(q_k r_ij), a<=b,
+ *   ab = a*T - a*(a-1)/2 + (b-a);  self_out[a] = Σ_{t_i=a} w_i².
+ * xyz n*3 f64, w n f64, type n in [0,T). The pair sum runs in FP32 on the
+ * device with FP64 cross-block reduction. */
+int crab_debye_partials(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                        int32_t n_types, const double* q, int64_t nq, double* out, double* self_out);
+/* Same partials computed in FP64 on the device with direct sin (no
+ * recurrence): the on-device FP64 reference used to report errors. */
+int crab_debye_partials_fp64(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                             int32_t n_types, const double* q, int64_t nq, double* out, double* self_out);
+
+/* Device-resident pair-sum plan: the layout (typed, tiled atoms), work list
+ * and q-block parameters are uploaded once; each run launches only the pair
+ * kernel on the context stream.  For throughput measurement and repeated
+ * evaluation of one structure. */
+typedef struct crab_pair_plan crab_pair_plan;
+int crab_pair_plan_create(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                          int32_t n_types, const double* q, int64_t nq, crab_pair_plan** out);
+/* Launch the pair kernel `repeats` times.  Before each launch, when
+ * flush_bytes > 0, a buffer of that size is overwritten on the same stream
+ * (evicting L2); each launch is bracketed by CUDA events and its device time
+ * in ms written to step_ms[i] (may be NULL). */
+int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int64_t flush_bytes, double* step_ms);
+/* Copy the partials of the last run to the host (layout of crab_debye_partials). */
+int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double* self_out);
+/* Pair·q evaluations of one run: (n(n-1)/2) * nq. */
+double crab_pair_plan_pairq(const crab_pair_plan* plan);
+int crab_pair_plan_destroy(crab_pair_plan* plan);
+
+/* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 FLOP): a
+ * register-resident FFMA loop on every SM for about `ms` milliseconds. */
+int crab_measure_fp32_peak(crab_ctx* ctx, double ms, double* tflops);
+/* Bytes copied host->device and device->host by this context since the last
+ * crab_ctx_reset_stats. */
+int crab_ctx_transfer_stats(crab_ctx* ctx, int64_t* h2d_bytes, int64_t* d2h_bytes);
+
+/* ---- public calculation boundary -------------------------------------- */
+/* compute_curve (scattering.rs:112-212): validation, Auto rule, adaptive
+ * l_max, dispatch to Debye or multipole, solvent recombination.
+ * method_used (may be NULL) receives CRAB_METHOD_DEBYE or CRAB_METHOD_MULTIPOLE. */
+int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, const crab_compute_options* opt,
+                       double* out, int32_t* method_used);
+
+/* ---- hydration grids ---------------------------------------------------- */
+/* Adaptive coarse shell (solvent.rs:121-223), bit-exact site list in z→y→x
+ * order. Two-call size query: pass sites=NULL to read *m. */
+int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing, double clearance, double padding,
+                                 double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
+/* Exterior flood-fill shell (solvent.rs:259-401), bit-exact. */
+int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing, double probe, double thickness,
+                                 double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
+
+/* ---- multipole engine ------------------------------------------------- */
+/* multipole_intensity (spherical.rs:266-403) with per-q adaptive order.
+ * precision: CRAB_PREC_*; tensor-core GEMM per l for TF32/BF16 modes. */
+int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                             int implicit_hydrogen, int precision, double* out);
+/* multipole_solvent_basis (spherical.rs:474-565), out6 [6][nq]. */
+int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                 const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6);
+
+/* ---- fitting and gradients --------------------------------------------- */
+/* fit_to_experimental_with_options (fit.rs:288-454). fitted (nq) may be NULL. */
+int crab_fit(crab_ctx* ctx, crab_struct* st, const double* q, const double* intensity, const double* sigma,
+             int64_t nq, const crab_fit_options* opt, double init_c1, double init_c2, crab_fit_result* result,
+             double* fitted);
+/* Reduced chi^2 of model = scale*I(q;x,c1,c2)+background against (y, sigma)
+ * for the analytic-hydration Debye model, and its gradient with respect to
+ * every coordinate (grad_xyz, n*3, may be NULL) and (c1, c2, scale,
+ * background) (grad_params, 4, may be NULL). New in this engine: the
+ * reference has no gradient (its fit is derivative-free, fit.rs:401-418). */
+int crab_chi2_grad(crab_ctx* ctx, crab_struct* st, const double* q, const double* y, const double* sigma, int64_t nq,
+                   const crab_solvent* solvent, int implicit_hydrogen, double scale, double background, double* chi2,
+                   double* grad_xyz, double* grad_params);
+
+/* ---- ensembles ------------------------------------------------------------ */
+/* EnsembleFitter::fit (ensemble.rs:127-232) over k structures sharing one q
+ * grid. All conformers' per-type partials are produced by one persistent
+ * launch; the 25 (c1,c2) candidates recombine them. weights (k), fitted (nq).
+ * Options follow EnsembleOptions (ensemble.rs:14-38); fit_opt follows FitOptions. */
+typedef struct crab_ensemble_options {
+  int32_t fit_weights;
+  int32_t uniform;
+  double regularization;
+  int32_t max_conformers;   /* 0 = None */
+  int32_t bootstrap;
+  double min_weight;
+  uint64_t seed;
+} crab_ensemble_options;
+typedef struct crab_ensemble_result {
+  double scale, background, c1, c2;
+  double chi2, reduced_chi2;
+  int32_t iterations;
+  int32_t n_selected;
+} crab_ensemble_result;
+int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, const double* y,
+                      const double* sigma, int64_t nq, const crab_ensemble_options* eopt,
+                      const crab_fit_options* fopt, crab_ensemble_result* result, int32_t* selected,
+                      double* weights, double* fitted);
+/* Batched curves for k conformers at every (c1,c2) candidate: curves is
+ * [n_cand][k][nq]; cand is n_cand (c1,c2) pairs. One persistent launch for
+ * all conformers' partials, one recombination launch. */
+int crab_ensemble_curves(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, int64_t nq,
+                         const crab_solvent* solvent, int implicit_hydrogen, const double* cand, int32_t n_cand,
+                         double* curves);
+
+/* reweight_curves (reweight.rs:84-154), curves [k][nq]; prior may be NULL. */
+typedef struct crab_reweight_options {
+  double kl_strength, step_size, tolerance, min_weight;
+  int32_t max_iterations;
+  int32_t scale_mode, bg_mode;
+  int32_t _pad;
+  double scale_value, bg_value;
+} crab_reweight_options;
+typedef struct crab_reweight_result {
+  double scale, background, chi2, reduced_chi2, kl_divergence, effective_sample_size;
+  int32_t iterations, converged;
+} crab_reweight_result;
+int crab_reweight_curves(const double* curves, int32_t k, const double* q, const double* y, const double* sigma,
+                         int64_t nq, const double* prior, const crab_reweight_options* opt, double* weights,
+                         crab_reweight_result* result);
+
+/* ---- synthetic inputs (no counterpart in the reference) ----------------- */
+/* Seeded protein-like structure: Cα-style self-avoiding walk (3.8 Å steps,
+ * 3.0 Å exclusion) inside a sphere of `radius`, 4-8 side atoms per residue at
+ * N(0, 1.5 Å), elements C/N/O/S at 63/17/19/1 %. xyz n*3, element n. */
+int crab_synth_protein(uint64_t seed, int64_t n_atoms, double radius, double* xyz, int8_t* element);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRAB_CUDA_H */
