@@ -117,7 +117,10 @@ _SIGS = {
                                        C.POINTER(ReweightResult)]),
     "crab_synth_protein": (C.c_int, [C.c_uint64, I64, C.c_double, D, I8P]),
     "crab_pair_plan_create": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, C.POINTER(P)]),
+    "crab_pair_plan_create_lattice": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, I32P, I64, C.c_double,
+                                                C.POINTER(P)]),
     "crab_pair_plan_run": (C.c_int, [P, P, C.c_int32, I64, D]),
+    "crab_pair_plan_autotune": (C.c_int, [P, P, I32P]),
     "crab_pair_plan_read": (C.c_int, [P, P, D, D]),
     "crab_pair_plan_pairq": (C.c_double, [P]),
     "crab_pair_plan_destroy": (C.c_int, [P]),

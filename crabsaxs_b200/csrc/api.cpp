@@ -162,34 +162,36 @@ void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const cr
     }
 }
 
-Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64) {
+Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,
+                      const GridResult* lattice_sites) {
   Partials P;
   Layout L = build_layout(t.xyz.data(), t.w.data(), t.type.data(), (int64_t)t.w.size(), t.T, fp64);
-  compute_partials(ctx, std::move(L), q, nq, fp64, P);
+  LatticeSpec spec;
+  if (lattice_sites) {
+    spec.cells = lattice_sites->cells.data();
+    spec.m = (int64_t)lattice_sites->cells.size() / 3;
+    spec.spacing = lattice_sites->spacing;
+  }
+  compute_partials(ctx, std::move(L), q, nq, fp64, P, lattice_sites ? &spec : nullptr);
   return P;
 }
 
-std::vector<double> hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s, double* volume) {
-  GridResult g;
+GridResult hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s) {
   if (s.hydration_model == CRAB_HYD_ADAPTIVE)
-    g = adaptive_grid_device(ctx, st->xyz.data(), st->n, s.grid_spacing, 3.0, 12.0);
-  else
-    g = exterior_grid_device(ctx, st->xyz.data(), st->elem.data(), st->n, 1.0, 1.4, s.shell_thickness);
-  *volume = g.voxel_volume;
-  return g.sites;
+    return adaptive_grid_device(ctx, st->xyz.data(), st->n, s.grid_spacing, 3.0, 12.0);
+  return exterior_grid_device(ctx, st->xyz.data(), st->elem.data(), st->n, 1.0, 1.4, s.shell_thickness);
 }
 
 void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
                  bool implicit, double* out6, bool fp64) {
-  std::vector<double> sites;
-  double volume = 0.0;
+  GridResult g;
   const bool grid = s.hydration_model != CRAB_HYD_ANALYTIC;
-  if (grid) sites = hydration_sites(ctx, st, s, &volume);
+  if (grid) g = hydration_sites(ctx, st, s);
   TypedAtoms t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic,
-                            grid ? &sites : nullptr);
+                            grid ? &g.sites : nullptr);
   std::vector<double> V, E, H;
-  amplitude_tables(t, q, nq, &s, implicit, volume, V, E, H);
-  Partials P = partials_for(ctx, t, q, nq, fp64);
+  amplitude_tables(t, q, nq, &s, implicit, g.voxel_volume, V, E, H);
+  Partials P = partials_for(ctx, t, q, nq, fp64, grid ? &g : nullptr);
   quadratic_terms(P, V.data(), V.data(), out6);
   quadratic_terms(P, E.data(), E.data(), out6 + nq);
   quadratic_terms(P, H.data(), H.data(), out6 + 2 * nq);
@@ -203,7 +205,7 @@ void debye_vacuum(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t
   TypedAtoms t = type_atoms(st, implicit, TermSet::Vacuum, nullptr);
   std::vector<double> V, E, H;
   amplitude_tables(t, q, nq, nullptr, implicit, 0.0, V, E, H);
-  Partials P = partials_for(ctx, t, q, nq, fp64);
+  Partials P = partials_for(ctx, t, q, nq, fp64, nullptr);
   quadratic_terms(P, V.data(), V.data(), out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
@@ -433,6 +435,31 @@ int crab_pair_plan_create(crab_ctx* ctx, const double* xyz, const double* w, con
   });
 }
 
+int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                                  int32_t T, const double* q, int64_t nq, const int32_t* cells, int64_t m,
+                                  double spacing, crab_pair_plan** out) {
+  if (!ctx || !out || T <= 0 || n < 0 || nq < 0 || (n > 0 && (!xyz || !w || !type)) || (nq > 0 && !q) ||
+      m < 0 || (m > 0 && !cells) || !(spacing > 0.0))
+    return CRAB_EINVAL;
+  *out = nullptr;
+  GUARD(ctx, {
+    validate_q(q, nq);
+    int64_t last = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      require(type[i] >= 0 && type[i] < T, "atom type out of range");
+      if (type[i] == T - 1) {
+        require(w[i] == 1.0, "lattice sites must have unit weight");
+        ++last;
+      }
+    }
+    require(last == m, "cells must list every atom of the last type");
+    Layout L = build_layout(xyz, w, type, n, T, false);
+    LatticeSpec spec{cells, m, spacing};
+    crab_pair_plan* p = new crab_pair_plan{ctx, make_pair_plan(ctx, std::move(L), q, nq, false, &spec)};
+    *out = p;
+  });
+}
+
 int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int64_t flush_bytes, double* step_ms) {
   if (!ctx || !plan || repeats < 0 || flush_bytes < 0) return CRAB_EINVAL;
   GUARD(ctx, { pair_plan_run_timed(ctx, *plan->plan, repeats, flush_bytes, step_ms); });
@@ -443,6 +470,14 @@ int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double
   GUARD(ctx, {
     pair_plan_fetch(ctx, *plan->plan, out, false);
     if (self_out) std::copy(plan->plan->L.self_w2.begin(), plan->plan->L.self_w2.end(), self_out);
+  });
+}
+
+int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* q_block) {
+  if (!ctx || !plan) return CRAB_EINVAL;
+  GUARD(ctx, {
+    const int Q = pair_plan_autotune(ctx, *plan->plan);
+    if (q_block) *q_block = Q;
   });
 }
 

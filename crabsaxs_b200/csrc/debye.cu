@@ -40,6 +40,7 @@ namespace crab {
 namespace {
 
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
+constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 128};  // compiled q-block lengths
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
 // ---- bulk async copy of one j tile into shared memory (1D TMA) ------------
@@ -143,16 +144,56 @@ __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int
   __syncthreads();
 }
 
-// Work item: (i tile, first j tile, end j tile, q block).
+// Packed pair of FP32 values in one 64-bit register pair (Blackwell f32x2 ops).
+__device__ __forceinline__ unsigned long long pack2(float x, float y) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& x, float& y) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+}
+
+// Per-pair set-up of the recurrence: weight u = w_i w_j / r, λ = 4 sin²(h),
+// seed s0 = sin(q0 r) and first difference d0 = sin(q0 r) - sin((q0-Δ) r)
+// = 2 sin(h) cos(q0 r - h), with h = Δr/2.  r and 1/r come from one MUFU
+// reciprocal square root y0 refined with FMA residuals (Markstein): with
+// s = x·y0, e = x - s² and t = 1 - s·y0 formed exactly by FMA,
+// r = s + e·y0/2 and 1/r = y0 + t·y0/2, both within about half an ulp and
+// unbiased.  (A refinement y0·(1.5 - 0.5·x·y0²) does not work in FP32: the
+// correction factor rounds to 1.0 when y0 is already close.)
+__device__ __forceinline__ void pair_setup(const float4& ai, const float4& aj, float wj, const float4& qp, int wide,
+                                           float& u, float& nl, float& s, float& d) {
+  const float dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
+  const float x = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-8f);
+  const float y0 = rsqrtf(x);
+  const float sq = x * y0;
+  const float hy = 0.5f * y0;
+  const float r = fmaf(fmaf(-sq, sq, x), hy, sq);
+  const float rinv = fmaf(fmaf(-sq, y0, 1.0f), hy, y0);
+  u = ai.w * wj * rinv;
+  const float phi = fmaf(qp.x, r, qp.y * r);
+  const float h = fmaf(qp.z, r, qp.w * r);
+  float c0, sh, ch;
+  sincos_seed(phi, &s, &c0);
+  if (wide) sincos_seed(h, &sh, &ch);
+  else sincos_small(h, &sh, &ch);
+  nl = -4.0f * sh * sh;
+  d = 2.0f * sh * fmaf(s, sh, c0 * ch);
+}
+
+// Work item: (i tile, first j tile, end j tile, q block); items are taken
+// from a global counter (longest first) so CTAs finish together.
 // qpar[b] = (q0_hi, q0_lo, halfstep_hi, halfstep_lo), qrange[b] = (start, count).
 template <int Q>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
     k_pair_fp32(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                 int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T, int wide,
-                double* __restrict__ partials, int* __restrict__ status) {
+                double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work) {
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_item;
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -163,7 +204,12 @@ __global__ void __launch_bounds__(kThreads, 4)
   unsigned phase_bits = 0u;  // bit b: parity of the next completion of bar[b]
   bool ok = true;
 
-  for (int w = blockIdx.x; w < n_work && ok; w += gridDim.x) {
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(next_work, 1);
+    __syncthreads();
+    const int w = s_item;
+    __syncthreads();
+    if (w >= n_work || !ok) break;
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
     const float4 ai = atoms[(size_t)it * kTile + tid];
@@ -201,28 +247,26 @@ __global__ void __launch_bounds__(kThreads, 4)
       phase_bits ^= 1u << buf;
       if (!__syncthreads_and(ok)) { ok = false; break; }
       const bool diag = (jt == it);
-#pragma unroll 2
-      for (int j = 0; j < kTile; ++j) {
-        const float4 aj = sj[buf][j];
-        const float wj = (diag && j <= tid) ? 0.0f : aj.w;
-        const float dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float r = fmaxf(sqrtf(r2), 1e-4f);
-        const float u = ai.w * wj * rsqrtf(fmaxf(r2, 1e-8f));
-        const float phi = fmaf(qp.x, r, qp.y * r);
-        const float h = fmaf(qp.z, r, qp.w * r);
-        float s0, c0, sh, ch;
-        sincos_seed(phi, &s0, &c0);
-        if (wide) sincos_seed(h, &sh, &ch);
-        else sincos_small(h, &sh, &ch);
-        const float nl = -4.0f * sh * sh;
-        float d = 2.0f * sh * fmaf(s0, sh, c0 * ch);
-        float s = s0;
+      // two j atoms per iteration: their recurrences advance together in
+      // packed f32x2 registers (two independent chains per instruction)
+#pragma unroll 1
+      for (int j = 0; j < kTile; j += 2) {
+        const float4 aA = sj[buf][j], aB = sj[buf][j + 1];
+        const float wA = (diag && j <= tid) ? 0.0f : aA.w;
+        const float wB = (diag && j + 1 <= tid) ? 0.0f : aB.w;
+        float uA, nlA, sA, dA, uB, nlB, sB, dB;
+        pair_setup(ai, aA, wA, qp, wide, uA, nlA, sA, dA);
+        pair_setup(ai, aB, wB, qp, wide, uB, nlB, sB, dB);
+        unsigned long long s2 = pack2(sA, sB), d2 = pack2(dA, dB);
+        const unsigned long long nl2 = pack2(nlA, nlB);
 #pragma unroll
         for (int k = 0; k < Q; ++k) {
-          acc[k] = fmaf(u, s, acc[k]);
-          d = fmaf(nl, s, d);
-          s += d;
+          float xa, xb;
+          unpack2(s2, xa, xb);
+          acc[k] = fmaf(uA, xa, acc[k]);
+          acc[k] = fmaf(uB, xb, acc[k]);
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2) : "l"(nl2), "l"(s2));
+          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(d2));
         }
       }
       __syncthreads();
@@ -310,23 +354,36 @@ uint32_t morton10(uint32_t v) {
   return v;
 }
 
-// Work list: i tile x runs of up to `run` j tiles (j >= i) x q blocks, q block
-// fastest so concurrently running CTAs add into different q ranges.
-std::vector<int4> make_work(const Layout& L, int n_qblocks, int run) {
-  std::vector<int4> work;
-  for (int it = 0; it < L.n_tiles; ++it)
-    for (int j0 = it; j0 < L.n_tiles; j0 += run)
-      for (int b = 0; b < n_qblocks; ++b) work.push_back(make_int4(it, j0, std::min(j0 + run, L.n_tiles), b));
+// Work list: i tile x runs of up to `run` j tiles (j >= i) x q blocks.
+// Tile pairs with both tiles at or beyond `skip_from` are left out (that
+// block is summed elsewhere).  Items are ordered longest first; equal-cost
+// items keep the q block fastest so concurrently running CTAs add into
+// different q ranges.
+std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_from) {
+  std::vector<std::pair<int, int4>> items;
+  for (int it = 0; it < L.n_tiles; ++it) {
+    if (it >= skip_from) break;
+    for (int j0 = it; j0 < L.n_tiles; j0 += run) {
+      const int j1 = std::min(j0 + run, L.n_tiles);
+      const int cost = 2 * (j1 - j0) - (j0 == it ? 1 : 0);
+      for (int b = 0; b < n_qblocks; ++b) items.push_back({cost, make_int4(it, j0, j1, b)});
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<int4> work(items.size());
+  for (size_t i = 0; i < items.size(); ++i) work[i] = items[i].second;
   return work;
 }
 
 template <int Q>
 void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
-                 const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status) {
+                 const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
+                 int* next_work) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
-  k_pair_fp32<Q><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials, status);
+  k_pair_fp32<Q><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials, status,
+                                                 next_work);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -418,9 +475,57 @@ bool q_grid_uniform(const double* q, int64_t nq) {
 
 PairPlan::~PairPlan() {
   for (void* p : owned) cudaFree(p);
+  for (void* p : qcfg) cudaFree(p);
 }
 
-std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64) {
+// q blocks: greedy runs of at most Qmax uniformly spaced q values, each
+// seeded exactly at its first point (any non-decreasing grid works).
+std::vector<int2> q_blocks(const std::vector<double>& q, int Qmax) {
+  std::vector<int2> out;
+  const int64_t nq = (int64_t)q.size();
+  if (nq == 0) return out;
+  const double tol = 1e-9 * std::max(std::fabs(q[nq - 1]), 1e-12);
+  int64_t s0 = 0;
+  while (s0 < nq) {
+    int64_t e = s0 + 1;
+    if (e < nq) {
+      const double dq = q[s0 + 1] - q[s0];
+      e = s0 + 2;
+      while (e < nq && e - s0 < Qmax && std::fabs(q[e] - (q[s0] + (double)(e - s0) * dq)) <= tol) ++e;
+    }
+    out.push_back(make_int2((int)s0, (int)(e - s0)));
+    s0 = e;
+  }
+  return out;
+}
+
+// (Re)build the q blocks and the work list of an FP32 plan for block length Q.
+void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q) {
+  for (void* p : P.qcfg) cudaFree(p);
+  P.qcfg.clear();
+  const std::vector<int2> qrange = q_blocks(P.q, Q);
+  P.Q = Q;
+  P.n_qblocks = (int)qrange.size();
+  std::vector<float4> qpar(P.n_qblocks);
+  double max_half = 0.0;
+  for (int b = 0; b < P.n_qblocks; ++b) {
+    const int64_t st = qrange[b].x, cnt = qrange[b].y;
+    const double q0 = P.q[st];
+    const double half = cnt > 1 ? 0.5 * (P.q[st + cnt - 1] - P.q[st]) / (double)(cnt - 1) : 0.0;
+    const float q0h = (float)q0, hh = (float)half;
+    qpar[b] = make_float4(q0h, (float)(q0 - (double)q0h), hh, (float)(half - (double)hh));
+    max_half = std::max(max_half, std::fabs(half));
+  }
+  P.wide = (max_half * (P.L.extent + 1.0) > 0.8) ? 1 : 0;
+  const std::vector<int4> work = make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile);
+  P.n_work = (int)work.size();
+  P.d_work = upload(ctx, P.qcfg, work.data(), work.size(), ctx->stream);
+  P.d_qpar = upload(ctx, P.qcfg, qpar.data(), qpar.size(), ctx->stream);
+  P.d_qrange = upload(ctx, P.qcfg, qrange.data(), qrange.size(), ctx->stream);
+}
+
+std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
+                                         const LatticeSpec* lattice) {
   std::unique_ptr<PairPlan> P(new PairPlan());
   P->L = std::move(L);
   P->fp64 = fp64;
@@ -430,58 +535,32 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   P->n_pairs = T * (T + 1) / 2;
   cudaStream_t s = ctx->stream;
   if (nq == 0 || P->L.n_tiles == 0) return P;
+  if (lattice && fp64) lattice = nullptr;  // the FP64 reference sums every pair directly
+  P->lattice_first_tile = P->L.n_tiles;
+  if (lattice) {
+    require(T >= 1, "lattice type needs a layout");
+    int first = P->L.n_tiles;
+    for (int t = 0; t < P->L.n_tiles; ++t)
+      if (P->L.tile_type[t] == T - 1) { first = t; break; }
+    P->lattice_first_tile = first;
+  }
   if (!fp64) {
-    // q blocks: greedy runs of uniformly spaced q values, seeded exactly at
-    // their first point; the block length Q (a template) is chosen to
-    // minimise launched steps plus a per-block seed cost.
-    auto blocks_for = [&](int Qmax, std::vector<int2>& out) {
-      out.clear();
-      const double tol = 1e-9 * std::max(std::fabs(q[nq - 1]), 1e-12);
-      int64_t s0 = 0;
-      while (s0 < nq) {
-        int64_t e = s0 + 1;
-        if (e < nq) {
-          const double dq = q[s0 + 1] - q[s0];
-          e = s0 + 2;
-          while (e < nq && e - s0 < Qmax && std::fabs(q[e] - (q[s0] + (double)(e - s0) * dq)) <= tol) ++e;
-        }
-        out.push_back(make_int2((int)s0, (int)(e - s0)));
-        s0 = e;
-      }
-    };
-    std::vector<int2> best, cand;
+    P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
+    // block length Q by a cost model: launched steps (3 FP32 ops each) plus
+    // a per-pair seed of about 60 ops per block
+    int bestQ = 64;
     long best_cost = -1;
-    for (int Qc = 8; Qc <= 64; Qc += 8) {
-      blocks_for(Qc, cand);
-      const long cost = (long)cand.size() * (Qc + 20);
+    for (int Qc : kQBlocks) {
+      const long cost = (long)q_blocks(P->q, Qc).size() * (3 * Qc + 60);
       if (best_cost < 0 || cost < best_cost) {
         best_cost = cost;
-        best = cand;
-        P->Q = Qc;
+        bestQ = Qc;
       }
     }
-    P->n_qblocks = (int)best.size();
-    std::vector<float4> qpar(P->n_qblocks);
-    std::vector<int2>& qrange = best;
-    double max_half = 0.0;
-    for (int b = 0; b < P->n_qblocks; ++b) {
-      const int64_t st = qrange[b].x, cnt = qrange[b].y;
-      const double q0 = q[st];
-      const double half = cnt > 1 ? 0.5 * (q[st + cnt - 1] - q[st]) / (double)(cnt - 1) : 0.0;
-      const float q0h = (float)q0, hh = (float)half;
-      qpar[b] = make_float4(q0h, (float)(q0 - (double)q0h), hh, (float)(half - (double)hh));
-      max_half = std::max(max_half, std::fabs(half));
-    }
-    P->wide = (max_half * (P->L.extent + 1.0) > 0.8) ? 1 : 0;
-    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8);
-    P->n_work = (int)work.size();
-    P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
-    P->d_work = upload(ctx, P->owned, work.data(), work.size(), s);
-    P->d_qpar = upload(ctx, P->owned, qpar.data(), qpar.size(), s);
-    P->d_qrange = upload(ctx, P->owned, qrange.data(), qrange.size(), s);
+    configure_fp32(ctx, *P, bestQ);
   } else {
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
-    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8);
+    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8, P->L.n_tiles);
     P->n_work = (int)work.size();
     P->d_atoms64 = upload(ctx, P->owned, (const double4*)P->L.atoms64.data(), (size_t)P->L.n_pad, s);
     P->d_work = upload(ctx, P->owned, work.data(), work.size(), s);
@@ -489,7 +568,9 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   }
   P->d_tile_type = upload(ctx, P->owned, P->L.tile_type.data(), P->L.tile_type.size(), s);
   P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)P->n_pairs * nq, s);
-  P->d_status = upload<int>(ctx, P->owned, nullptr, 1, s);
+  P->d_status = upload<int>(ctx, P->owned, nullptr, 2, s);
+  P->d_next = P->d_status + 1;
+  if (lattice) lattice_plan_init(ctx, *P, lattice->cells, lattice->m, lattice->spacing);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   return P;
 }
@@ -497,7 +578,7 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
 void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
   if (P.nq == 0 || P.L.n_tiles == 0) return;
   CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_out, 0, (size_t)P.n_pairs * P.nq * sizeof(double), s));
-  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_status, 0, sizeof(int), s));
+  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_status, 0, 2 * sizeof(int), s));  // status and work counter
   if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_start, s));
   const int T = P.L.T, nq = (int)P.nq;
   if (P.fp64) {
@@ -510,23 +591,23 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH(QQ)                                                                                          \
   case QQ:                                                                                                       \
     launch_fp32<QQ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, T, \
-                    P.wide, P.d_out, P.d_status);                                                                \
+                    P.wide, P.d_out, P.d_status, P.d_next);                                                                \
     break;
     switch (P.Q) {
       CRAB_LAUNCH(8)
       CRAB_LAUNCH(16)
-      CRAB_LAUNCH(24)
       CRAB_LAUNCH(32)
-      CRAB_LAUNCH(40)
       CRAB_LAUNCH(48)
-      CRAB_LAUNCH(56)
       CRAB_LAUNCH(64)
+      CRAB_LAUNCH(96)
+      CRAB_LAUNCH(128)
       default: throw Error(CRAB_EINVAL, "unsupported q block");
     }
 #undef CRAB_LAUNCH
   }
-  if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_stop, s));
   ctx->launches += 1;
+  if (P.lattice.active) lattice_plan_launch(ctx, P, s);
+  if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_stop, s));
 }
 
 void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
@@ -566,15 +647,22 @@ void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
         v = (P.q[k] == 0.0) ? w0 : v / P.q[k];
       }
     }
+  if (P.lattice.active && nq > 0) {
+    // site weights are one: the lattice sums are the site–site partial itself
+    copy_d2h(ctx, out + (size_t)pair_index(T - 1, T - 1, T) * nq, P.lattice.d_out, (size_t)nq * sizeof(double),
+             ctx->stream);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  }
 }
 
-void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, Partials& out) {
+void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, Partials& out,
+                      const LatticeSpec* lattice) {
   const bool fp64 = force_fp64;
   if (fp64 && L.atoms64.empty()) throw Error(CRAB_EINVAL, "layout lacks an f64 copy");
   out.T = L.T;
   out.nq = nq;
   out.self = L.self_w2;
-  std::unique_ptr<PairPlan> P = make_pair_plan(ctx, std::move(L), q, nq, fp64);
+  std::unique_ptr<PairPlan> P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice);
   out.pair.assign((size_t)P->n_pairs * nq, 0.0);
   pair_plan_launch(ctx, *P, ctx->stream, !fp64);
   pair_plan_fetch(ctx, *P, out.pair.data(), !fp64);
@@ -631,6 +719,39 @@ void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_
   copy_d2h(ctx, &status, P.d_status, sizeof(int), s);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   if (status) throw Error(status, "pair kernel: a bounded wait on a j-tile copy ran out");
+}
+
+}  // namespace crab
+
+namespace crab {
+
+int pair_plan_autotune(crab_ctx* ctx, PairPlan& P) {
+  if (P.fp64 || P.nq == 0 || P.L.n_tiles == 0) return P.Q;
+  int bestQ = P.Q;
+  float best_ms = -1.0f;
+  cudaEvent_t a, b;
+  CRAB_CUDA_CHECK(cudaEventCreate(&a));
+  CRAB_CUDA_CHECK(cudaEventCreate(&b));
+  for (int Qc : kQBlocks) {
+    if (Qc < 32) continue;
+    configure_fp32(ctx, P, Qc);
+    pair_plan_launch(ctx, P, ctx->stream, false);  // warm-up
+    CRAB_CUDA_CHECK(cudaEventRecord(a, ctx->stream));
+    pair_plan_launch(ctx, P, ctx->stream, false);
+    CRAB_CUDA_CHECK(cudaEventRecord(b, ctx->stream));
+    CRAB_CUDA_CHECK(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    CRAB_CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+    if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      bestQ = Qc;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  configure_fp32(ctx, P, bestQ);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+  return bestQ;
 }
 
 }  // namespace crab

@@ -140,6 +140,17 @@ struct Partials {
   std::vector<double> self;  // [T]
 };
 
+// Site–site block of a lattice type summed exactly by distance histogram.
+struct LatticePart {
+  bool active = false;
+  int64_t m = 0;       // sites
+  double spacing = 0.0;
+  int bins = 0;        // squared lattice distances 0..bins-1
+  int4* d_cells = nullptr;
+  unsigned long long* d_hist = nullptr;
+  double* d_out = nullptr;  // [nq] Σ_{i<j} sinc(q r_ij) over sites
+};
+
 // Device-resident pair-sum problem: layout, work list and q-block
 // parameters uploaded once; launched any number of times.
 struct PairPlan {
@@ -149,6 +160,7 @@ struct PairPlan {
   std::vector<double> q;
   int n_pairs = 0, Q = 0, n_qblocks = 0, n_work = 0, wide = 0;
   std::vector<void*> owned;
+  std::vector<void*> qcfg;  // q-block and work-list buffers (rebuilt when Q changes)
   float4* d_atoms = nullptr;
   double4* d_atoms64 = nullptr;
   int* d_tile_type = nullptr;
@@ -158,18 +170,34 @@ struct PairPlan {
   double* d_q = nullptr;
   double* d_out = nullptr;  // [n_pairs][nq] raw sums
   int* d_status = nullptr;
+  int* d_next = nullptr;  // work-queue counter (the int after d_status)
+  int lattice_first_tile = 0;
+  LatticePart lattice;
   ~PairPlan();
 };
+// Lattice description of the last type (hydration sites on a voxel grid):
+// cells are the sites' integer voxel indices (3 per site, in any order).
+struct LatticeSpec {
+  const int32_t* cells = nullptr;
+  int64_t m = 0;
+  double spacing = 0.0;
+};
+void lattice_plan_init(crab_ctx* ctx, PairPlan& P, const int32_t* cells, int64_t m, double spacing);
+void lattice_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s);
 bool q_grid_uniform(const double* q, int64_t nq);
-std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64);
+std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
+                                         const LatticeSpec* lattice = nullptr);
 // Enqueue the pair kernel on stream s (device time recorded when timed).
 void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed);
 // Copy back and convert raw sums to P_ab(q) (divide by q; exact q = 0).
 void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed);
 // One-shot: FP32 recurrence on a uniform grid, FP64 direct otherwise.
-void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, struct Partials& out);
+void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, struct Partials& out,
+                      const LatticeSpec* lattice = nullptr);
 
 void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_bytes, double* step_ms);
+// Time each compiled q-block length once on this plan and keep the fastest.
+int pair_plan_autotune(crab_ctx* ctx, PairPlan& P);
 double measure_fp32_peak(crab_ctx* ctx, double target_ms);
 
 // Quadratic form Σ_ij X_i Y_j sinc(q r_ij) for per-type amplitude tables
@@ -182,7 +210,9 @@ inline int pair_index(int a, int b, int T) {
 
 // ---------------------------------------------------------------- hydration grids
 struct GridResult {
-  std::vector<double> sites;  // 3 per site, z→y→x order
+  std::vector<double> sites;   // 3 per site, z→y→x order
+  std::vector<int32_t> cells;  // 3 voxel indices per site
+  double spacing = 0.0;
   double voxel_volume = 0.0;
 };
 GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, double spacing, double clearance,

@@ -134,7 +134,7 @@ __global__ void k_scan_chunks(const uint32_t* __restrict__ cnt, uint64_t n, uint
 }
 
 __global__ void k_emit(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, uint64_t count, int kind, Box bx,
-                       const uint64_t* __restrict__ offsets, double* __restrict__ sites) {
+                       const uint64_t* __restrict__ offsets, double* __restrict__ sites, int32_t* __restrict__ cells) {
   __shared__ uint32_t warp_tot[kScanThreads / 32];
   const uint64_t base = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kPerThread;
   uint32_t c = 0;
@@ -159,6 +159,9 @@ __global__ void k_emit(const uint8_t* __restrict__ a, const uint8_t* __restrict_
       sites[3 * pos] = __dadd_rn(bx.mn[0], __dmul_rn((double)x, bx.spacing));
       sites[3 * pos + 1] = __dadd_rn(bx.mn[1], __dmul_rn((double)y, bx.spacing));
       sites[3 * pos + 2] = __dadd_rn(bx.mn[2], __dmul_rn((double)z, bx.spacing));
+      cells[3 * pos] = (int32_t)x;
+      cells[3 * pos + 1] = (int32_t)y;
+      cells[3 * pos + 2] = (int32_t)z;
       ++pos;
     }
   }
@@ -237,11 +240,16 @@ GridResult compact_sites(crab_ctx* ctx, Scratch& sc, const uint8_t* a, const uin
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   GridResult r;
   r.sites.resize(3 * m);
+  r.cells.resize(3 * m);
+  r.spacing = bx.spacing;
   if (m) {
+    require(bx.n[0] < (1ull << 31) && bx.n[1] < (1ull << 31) && bx.n[2] < (1ull << 31), "grid axis too long");
     double* d_sites = sc.alloc<double>(3 * m);
-    k_emit<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, bx, d_off, d_sites);
+    int32_t* d_cells = sc.alloc<int32_t>(3 * m);
+    k_emit<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, bx, d_off, d_sites, d_cells);
     CRAB_CUDA_CHECK(cudaGetLastError());
     copy_d2h(ctx, r.sites.data(), d_sites, 3 * m * sizeof(double), s);
+    copy_d2h(ctx, r.cells.data(), d_cells, 3 * m * sizeof(int32_t), s);
     CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   }
   ctx->launches += m ? 4 : 3;

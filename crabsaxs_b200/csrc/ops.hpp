@@ -31,8 +31,9 @@ TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const 
 // means vacuum form factors only.
 void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const crab_solvent* solvent, bool implicit,
                       double site_volume, std::vector<double>& V, std::vector<double>& E, std::vector<double>& H);
-Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64);
-std::vector<double> hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s, double* volume);
+Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,
+                      const GridResult* lattice_sites);
+GridResult hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s);
 void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
                  bool implicit, double* out6, bool fp64);
 void debye_vacuum(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, bool implicit, double* out,

@@ -177,11 +177,21 @@ int crab_debye_partials_fp64(crab_ctx* ctx, const double* xyz, const double* w, 
 typedef struct crab_pair_plan crab_pair_plan;
 int crab_pair_plan_create(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                           int32_t n_types, const double* q, int64_t nq, crab_pair_plan** out);
+/* Same, with the last type a lattice of hydration sites (unit weights) whose
+ * integer voxel indices are `cells` (m*3): their site–site block is summed
+ * exactly by a squared-distance histogram instead of the pair kernel. */
+int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                                  int32_t n_types, const double* q, int64_t nq, const int32_t* cells, int64_t m,
+                                  double spacing, crab_pair_plan** out);
 /* Launch the pair kernel `repeats` times.  Before each launch, when
  * flush_bytes > 0, a buffer of that size is overwritten on the same stream
  * (evicting L2); each launch is bracketed by CUDA events and its device time
  * in ms written to step_ms[i] (may be NULL). */
 int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int64_t flush_bytes, double* step_ms);
+/* Autotune: time every compiled q-block length (the number of q values one
+ * thread advances per pair between exact re-seeds) on this plan and keep the
+ * fastest; *q_block (may be NULL) receives it. */
+int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* q_block);
 /* Copy the partials of the last run to the host (layout of crab_debye_partials). */
 int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double* self_out);
 /* Pair·q evaluations of one run: (n(n-1)/2) * nq. */

@@ -265,3 +265,40 @@ def test_pair_kernel_launches_are_counted(engine):
     cs.debye_partials(xyz, w, t, 2, np.linspace(0.01, 0.3, 40), engine=engine)
     launches, ms, pq = engine.stats()
     assert launches >= 1 and ms > 0 and pq == pytest.approx(300 * 299 / 2 * 40)
+
+
+def test_lattice_plan_matches_fp64_config2(engine):
+    """The site–site block from the lattice histogram equals the FP64 pair sum
+    over the same sites; every other block stays within the FP32 bound."""
+    import ctypes as C
+
+    from crabsaxs_b200 import _native as N
+    from crabsaxs_b200 import synth
+
+    w = synth.CONFIG2
+    s = synth.protein(w.seed, w.n_atoms, w.radius)
+    sites, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
+    el = s.element.astype(np.int64)
+    classes = sorted(set(el.tolist()))
+    t = np.concatenate([np.searchsorted(classes, el), np.full(len(sites), len(classes))]).astype(np.int32)
+    xyz = np.ascontiguousarray(np.concatenate([s.xyz, sites]))
+    wts = np.ones(len(xyz))
+    T = len(classes) + 1
+    q = np.ascontiguousarray(w.q)
+    cells = np.ascontiguousarray(np.rint((sites - sites.min(axis=0)) / 3.0).astype(np.int32))
+    plan = C.c_void_p()
+    engine.check(N.lib.crab_pair_plan_create_lattice(engine.handle, xyz.ctypes.data_as(N.D), wts.ctypes.data_as(N.D),
+                                                     t.ctypes.data_as(N.I32P), len(wts), T, q.ctypes.data_as(N.D),
+                                                     len(q), cells.ctypes.data_as(N.I32P), len(sites), 3.0,
+                                                     C.byref(plan)))
+    try:
+        engine.check(N.lib.crab_pair_plan_run(engine.handle, plan, 2, 0, None))
+        P = np.empty((T * (T + 1) // 2, len(q)))
+        engine.check(N.lib.crab_pair_plan_read(engine.handle, plan, P.ctypes.data_as(N.D), None))
+    finally:
+        N.lib.crab_pair_plan_destroy(plan)
+    P64, _ = cs.debye_partials(xyz, wts, t, T, q, fp64=True, engine=engine)
+    scale = _partials_scale(wts, t, T)[:, None]
+    err = np.abs(P - P64) / scale
+    assert err[-1].max() <= 1e-12  # site–site row: exact lattice sums
+    assert err.max() <= PARTIAL_ATOL

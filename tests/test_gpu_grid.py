@@ -77,6 +77,6 @@ def test_exterior_grid_single_atom_bounds(engine):  # solvent.rs:688-705
 
 
 def test_exterior_grid_limit(engine):
-    xyz = np.array([[0.0, 0.0, 0.0], [700.0, 0.0, 0.0]])
+    xyz = np.array([[0.0, 0.0, 0.0], [700.0, 700.0, 700.0]])
     with pytest.raises(cs.InvalidInput):
         cs.hydration_grid_exterior(cs.Structure(xyz, [1, 1]), 0.1, engine=engine)
