@@ -232,6 +232,63 @@ def run_reference(args, rank, world):
     return 0
 
 
+def ensemble_section(eng, rank):
+    """Config 5: 256 conformers (log-uniform 2k-40k atoms), 300 q, the 25 (c1, c2)
+    candidates of ensemble.rs:302-315.  Batched: one CUDA graph per scoring pass
+    (pair sums of all conformers, 25x256 curves, per-candidate simplex weights,
+    gradients, KL reweighting).  Plain: one compute_curve per conformer per
+    candidate, the call structure of ensemble.rs:244-261, timed for one candidate
+    (each further candidate repeats the same work)."""
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import synth
+
+    confs = synth.ensemble(256, 5 + 7919 * rank)
+    q = synth.CONFIG5_Q
+    fo = cs.FitOptions(method=cs.ScatteringMethod.Debye)
+    cand = cs.solvent_candidates(fo)
+    rng = np.random.default_rng(55)
+    hidden = rng.choice(len(confs), 8, replace=False)
+    opt0 = cs.ComputeOptions(method=cs.ScatteringMethod.Debye, solvent=cs.SolventParams())
+    ih = np.array([cs.compute_curve(confs[h], q, opt0, engine=eng).intensity for h in hidden])
+    clean = rng.dirichlet(np.ones(8)) @ ih
+    sigma = 0.01 * clean
+    y = clean + sigma * rng.normal(size=len(q))
+    plan = cs.EnsemblePlan(confs, q, cs.SolventParams(), cand, engine=eng)
+    try:
+        plan.score(y, sigma, fo, cs.MaximumEntropyOptions())
+        eng.reset_stats()
+        runs = [plan.score(y, sigma, fo, cs.MaximumEntropyOptions()) for _ in range(3)]
+        launches, _, _ = eng.stats()
+    finally:
+        plan.close()
+    graph_ms = float(np.median([r["elapsed_ms"] for r in runs]))
+    n_curves = len(cand) * len(confs)
+    # plain per-structure GPU path for one candidate, wall-clocked end to end
+    c1, c2 = cand[12]
+    optc = cs.ComputeOptions(method=cs.ScatteringMethod.Debye, solvent=cs.SolventParams(c1=c1, c2=c2))
+    t0 = time.perf_counter()
+    plain = [cs.compute_curve(c, q, optc, engine=eng).intensity for c in confs]
+    plain_s = time.perf_counter() - t0
+    # accuracy of batched curves against the FP64 device reference on four conformers
+    order = np.argsort([c.atom_count for c in confs])
+    pick = [order[0], order[len(order) // 3], order[2 * len(order) // 3], order[-1]]
+    bc = cs.ensemble_curves([confs[i] for i in pick], q, cs.SolventParams(), [[c1, c2]], engine=eng)[0]
+    err = 0.0
+    for j, i in enumerate(pick):
+        b64 = cs.debye_solvent_basis(confs[i], q, cs.SolventParams(c1=c1, c2=c2), engine=eng, fp64=True)
+        i64 = cs.combine_solvent_basis(b64, q, c1, c2)
+        err = max(err, float(np.max(np.abs(bc[j] - i64) / i64)), float(np.max(np.abs(plain[i] - i64) / i64)))
+    pairq = sum(c.atom_count * (c.atom_count - 1) / 2.0 for c in confs) * len(q)
+    best = runs[-1]
+    return {"curves_per_s": n_curves / (graph_ms * 1e-3), "plain_gpu_curves_per_s": len(confs) / plain_s,
+            "speedup_vs_plain": (n_curves / (graph_ms * 1e-3)) / (len(confs) / plain_s),
+            "graph_ms": graph_ms, "conformers": len(confs), "candidates": len(cand), "n_q": len(q),
+            "atoms": int(sum(c.atom_count for c in confs)), "pair_q_per_pass": pairq,
+            "pair_q_per_s": pairq / (graph_ms * 1e-3), "kernels_per_pass": int(launches // 3),
+            "max_rel_err_vs_fp64": err, "best_candidate": [float(best["c1"]), float(best["c2"])],
+            "reduced_chi2": float(best["reduced_chi2"]), "kl_reduced_chi2": float(best["kl_reduced_chi2"])}
+
+
 def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
@@ -256,8 +313,13 @@ def run_ours(args, rank, world, local):
     eng.check(lib.crab_pair_plan_create_lattice(eng.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
                                                 t.ctypes.data_as(N.I32P), m, T, Q.ctypes.data_as(N.D), len(Q),
                                                 cells.ctypes.data_as(N.I32P), len(sites), 3.0, C.byref(plan)))
-    q_block = C.c_int32()
-    eng.check(lib.crab_pair_plan_autotune(eng.handle, plan, C.byref(q_block)))
+    chosen = C.c_int32()
+    tv = np.zeros(16, dtype=np.int32)
+    tms = np.zeros(16)
+    ntv = C.c_int32()
+    eng.check(lib.crab_pair_plan_autotune(eng.handle, plan, C.byref(chosen), tv.ctypes.data_as(N.I32P),
+                                          tms.ctypes.data_as(N.D), 16, C.byref(ntv)))
+    tuning = {f"Q{v // 16}xJ{v % 16}": round(float(t), 3) for v, t in zip(tv[:ntv.value], tms[:ntv.value])}
     pairq = lib.crab_pair_plan_pairq(plan)
     ns = len(sites)
     kernel_pairq = pairq - ns * (ns - 1) / 2.0 * len(Q)  # the lattice path sums the site–site pairs
@@ -338,6 +400,8 @@ def run_ours(args, rank, world, local):
                "sample": f"same structure + its {mm - N_ATOMS} sites, {nq} of 500 q values (one per thread), "
                          f"{dt:.1f} s; f64 C++ restatement of solvent.rs debye_solvent_basis"}
 
+    ens = None if args.no_ensemble else ensemble_section(eng, rank)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -346,7 +410,7 @@ def run_ours(args, rank, world, local):
             "config": {"workload": "debye pair sums per type pair, 20k-atom structure + adaptive 3 Å hydration "
                                    "sites, 500 q on [0.001, 0.5]",
                        "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_types": T, "n_q": len(Q),
-                       "q_block": q_block.value,
+                       "kernel_variant": f"Q{chosen.value // 16}xJ{chosen.value % 16}", "autotune_ms": tuning,
                        "parallelism": f"independent structure per GPU x{world}",
                        "l2": "flushed before every step (256 MiB memset, outside the step events)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
@@ -355,6 +419,7 @@ def run_ours(args, rank, world, local):
                          "peak_source": "FFMA microbenchmark measured in this run (MEASURED_PEAKS.json has no FP32)",
                          "flop_per_unit": 4},
             "parity": {"max_rel_err_vs_fp64": max_rel, "c1": c1, "c2": c2},
+            "ensemble": ens,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,
@@ -377,6 +442,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -110,7 +110,13 @@ _SIGS = {
                            C.POINTER(FitResult), D]),
     "crab_chi2_grad": (C.c_int, [P, P, D, D, D, I64, C.POINTER(Solvent), C.c_int, C.c_double, C.c_double, D, D, D]),
     "crab_ensemble_fit": (C.c_int, [P, C.POINTER(P), C.c_int32, D, D, D, I64, C.POINTER(EnsembleOpts),
-                                    C.POINTER(FitOpts), C.POINTER(EnsembleResult), I32P, D, D]),
+                                    C.POINTER(FitOpts), C.POINTER(EnsembleResult), I32P, D, D, D, D]),
+    "crab_ensemble_plan_create": (C.c_int, [P, C.POINTER(P), C.c_int32, D, I64, C.POINTER(Solvent), C.c_int, D,
+                                            C.c_int32, C.POINTER(P)]),
+    "crab_ensemble_plan_autotune": (C.c_int, [P, P, I32P]),
+    "crab_ensemble_plan_score": (C.c_int, [P, P, D, D, C.POINTER(FitOpts), C.POINTER(ReweightOpts), D, D, D, D,
+                                           D, D]),
+    "crab_ensemble_plan_destroy": (C.c_int, [P]),
     "crab_ensemble_curves": (C.c_int, [P, C.POINTER(P), C.c_int32, D, I64, C.POINTER(Solvent), C.c_int, D,
                                        C.c_int32, D]),
     "crab_reweight_curves": (C.c_int, [D, C.c_int32, D, D, D, I64, D, C.POINTER(ReweightOpts), D,
@@ -120,7 +126,7 @@ _SIGS = {
     "crab_pair_plan_create_lattice": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, I32P, I64, C.c_double,
                                                 C.POINTER(P)]),
     "crab_pair_plan_run": (C.c_int, [P, P, C.c_int32, I64, D]),
-    "crab_pair_plan_autotune": (C.c_int, [P, P, I32P]),
+    "crab_pair_plan_autotune": (C.c_int, [P, P, I32P, I32P, D, C.c_int32, I32P]),
     "crab_pair_plan_read": (C.c_int, [P, P, D, D]),
     "crab_pair_plan_pairq": (C.c_double, [P]),
     "crab_pair_plan_destroy": (C.c_int, [P]),

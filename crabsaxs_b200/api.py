@@ -638,6 +638,13 @@ class EnsembleOptions:
 
 
 @dataclass
+class WeightInterval:
+    median: float
+    lower: float
+    upper: float
+
+
+@dataclass
 class EnsembleResult:
     conformers: list
     weights: np.ndarray
@@ -647,6 +654,8 @@ class EnsembleResult:
     fitted_curve: np.ndarray
     iterations: int
     converged: bool
+    weight_intervals: list = field(default_factory=list)
+    bootstrap_reduced_chi2: list = field(default_factory=list)
 
 
 class EnsembleFitter:
@@ -683,13 +692,16 @@ class EnsembleFitter:
         w = np.empty(k)
         fitted = np.empty(len(self.experimental))
         ex = self.experimental
+        intervals = np.empty((k, 3))
+        boot = np.empty(max(o.bootstrap, 1))
         e.check(N.lib.crab_ensemble_fit(e.handle, handles, k, _dp(ex.q), _dp(ex.intensity), _dp(ex.sigma), len(ex),
                                         C.byref(eo), C.byref(fo), C.byref(res), sel.ctypes.data_as(N.I32P), _dp(w),
-                                        _dp(fitted)))
+                                        _dp(fitted), _dp(intervals), _dp(boot)))
         n = res.n_selected
         return EnsembleResult([self.names[i] for i in sel[:n]], w[:n].copy(),
                               FitParams(res.scale, res.background, res.c1, res.c2), res.chi2, res.reduced_chi2,
-                              fitted, res.iterations, True)
+                              fitted, res.iterations, True,
+                              [WeightInterval(*row) for row in intervals[:n]], list(boot[:o.bootstrap]))
 
 
 def ensemble_curves(conformers: Sequence[Structure], q, solvent: SolventParams, candidates,
@@ -705,6 +717,72 @@ def ensemble_curves(conformers: Sequence[Structure], q, solvent: SolventParams, 
     e.check(N.lib.crab_ensemble_curves(e.handle, handles, k, _dp(qa), len(qa), C.byref(s),
                                        1 if implicit_hydrogen else 0, _dp(cand), cand.shape[0], _dp(out)))
     return out
+
+
+def solvent_candidates(fit: FitOptions) -> np.ndarray:
+    """ensemble.rs:302-315: the 5x5 (c1, c2) grid over the fit bounds."""
+    c1 = fit.c1_bounds[0] + (fit.c1_bounds[1] - fit.c1_bounds[0]) * np.arange(5) / 4.0
+    c2 = fit.c2_bounds[0] + (fit.c2_bounds[1] - fit.c2_bounds[0]) * np.arange(5) / 4.0
+    return np.array([(a, b) for a in c1 for b in c2])
+
+
+class EnsemblePlan:
+    """Device-resident ensemble scoring (crab_ensemble_plan_*): one CUDA graph
+    per score() call covering pair sums of every conformer, curves at every
+    (c1, c2) candidate, simplex weight fits, gradients and KL reweighting."""
+
+    def __init__(self, conformers: Sequence[Structure], q, solvent: Optional[SolventParams] = None,
+                 candidates=None, implicit_hydrogen: bool = True, engine: Optional[Engine] = None):
+        self.engine = engine or Engine.default()
+        e = self.engine
+        self.k = len(conformers)
+        self.q = _f64(q)
+        self.cand = _f64(solvent_candidates(FitOptions()) if candidates is None else candidates).reshape(-1, 2)
+        self._keep = list(conformers)
+        handles = (C.c_void_p * self.k)(*[c.handle(e) for c in conformers])
+        s = (solvent or SolventParams()).to_c()
+        self.handle = C.c_void_p()
+        e.check(N.lib.crab_ensemble_plan_create(e.handle, handles, self.k, _dp(self.q), len(self.q), C.byref(s),
+                                                1 if implicit_hydrogen else 0, _dp(self.cand), self.cand.shape[0],
+                                                C.byref(self.handle)))
+
+    def autotune(self) -> int:
+        c = C.c_int32()
+        self.engine.check(N.lib.crab_ensemble_plan_autotune(self.engine.handle, self.handle, C.byref(c)))
+        return c.value
+
+    def score(self, y, sigma, fit: Optional[FitOptions] = None, reweight: Optional["MaximumEntropyOptions"] = None):
+        e = self.engine
+        yy, ss = _f64(y), _f64(sigma)
+        fo = (fit or FitOptions()).to_c()
+        ro = None
+        if reweight is not None:
+            f = reweight.fit
+            ro = N.ReweightOpts(reweight.kl_strength, reweight.step_size, reweight.tolerance, reweight.min_weight,
+                                reweight.max_iterations, N.SCALE_FIT if f.scale_mode.fixed is None else N.SCALE_FIXED,
+                                f.background_mode.kind, 0, f.scale_mode.fixed or 0.0, f.background_mode.value)
+        ms = C.c_double()
+        best = np.empty(8)
+        w, gw, kw = np.empty(self.k), np.empty(self.k), np.empty(self.k)
+        rw = np.empty(6)
+        e.check(N.lib.crab_ensemble_plan_score(e.handle, self.handle, _dp(yy), _dp(ss), C.byref(fo),
+                                               None if ro is None else C.byref(ro), C.byref(ms), _dp(best), _dp(w),
+                                               _dp(gw), _dp(kw), _dp(rw)))
+        return dict(elapsed_ms=ms.value, candidate=int(best[0]), c1=best[1], c2=best[2], scale=best[3],
+                    background=best[4], reduced_chi2=best[5], dchi2_dc1=best[6], dchi2_dc2=best[7], weights=w,
+                    dchi2_dw=gw, kl_weights=kw, kl_scale=rw[0], kl_background=rw[1], kl_reduced_chi2=rw[2],
+                    kl_divergence=rw[3], kl_iterations=int(rw[4]), kl_converged=bool(rw[5]))
+
+    def close(self):
+        if self.handle:
+            N.lib.crab_ensemble_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

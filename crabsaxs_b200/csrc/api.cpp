@@ -120,11 +120,13 @@ TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const 
   t.xyz.resize(3 * (keep.size() + ns));
   t.w.resize(keep.size() + ns);
   t.type.resize(keep.size() + ns);
+  t.src.assign(keep.size() + ns, -1);
   for (size_t k = 0; k < keep.size(); ++k) {
     const int64_t i = keep[k];
     for (int d = 0; d < 3; ++d) t.xyz[3 * k + d] = st->xyz[3 * i + d];
     t.w[k] = st->occ[i];
     t.type[k] = index[cls_of[k]];
+    t.src[k] = i;
   }
   for (int64_t s = 0; s < ns; ++s) {
     const size_t k = keep.size() + s;
@@ -473,11 +475,17 @@ int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double
   });
 }
 
-int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* q_block) {
-  if (!ctx || !plan) return CRAB_EINVAL;
+int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen, int32_t* variants, double* ms,
+                            int32_t capacity, int32_t* n_variants) {
+  if (!ctx || !plan || capacity < 0) return CRAB_EINVAL;
   GUARD(ctx, {
-    const int Q = pair_plan_autotune(ctx, *plan->plan);
-    if (q_block) *q_block = Q;
+    std::vector<int> v(capacity);
+    int n = 0;
+    const int c = pair_plan_autotune(ctx, *plan->plan, v.data(), ms, capacity, &n);
+    if (chosen) *chosen = c;
+    if (variants)
+      for (int i = 0; i < n; ++i) variants[i] = v[i];
+    if (n_variants) *n_variants = n;
   });
 }
 

@@ -34,90 +34,17 @@
 #include <cstring>
 #include <numeric>
 
+#include "device_math.cuh"
 #include "engine.hpp"
 
 namespace crab {
 namespace {
 
+using namespace dev;
+
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
 constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 128};  // compiled q-block lengths
 static_assert(kThreads == kTile, "tile size and CTA size must match");
-
-// ---- bulk async copy of one j tile into shared memory (1D TMA) ------------
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  unsigned b = (unsigned)__cvta_generic_to_shared(bar);
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
-               "l"(src), "r"(bytes), "r"(b)
-               : "memory");
-}
-// Bounded wait on an mbarrier phase. Returns false when the iteration budget
-// runs out (the caller records an error and stops using the buffer).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
-  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(phase)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-// sin(h), cos(h) for |h| <= 0.8 by their Taylor series (error < 1e-11 before
-// rounding); used for the half-step angle h = Δr/2.
-__device__ __forceinline__ void sincos_small(float h, float* sh, float* ch) {
-  const float h2 = h * h;
-  float ps = fmaf(h2, -1.0f / 39916800.0f, 1.0f / 362880.0f);
-  ps = fmaf(h2, ps, -1.0f / 5040.0f);
-  ps = fmaf(h2, ps, 1.0f / 120.0f);
-  ps = fmaf(h2, ps, -1.0f / 6.0f);
-  *sh = fmaf(h * h2, ps, h);
-  float pc = fmaf(h2, 1.0f / 479001600.0f, -1.0f / 3628800.0f);
-  pc = fmaf(h2, pc, 1.0f / 40320.0f);
-  pc = fmaf(h2, pc, -1.0f / 720.0f);
-  pc = fmaf(h2, pc, 1.0f / 24.0f);
-  pc = fmaf(h2, pc, -0.5f);
-  *ch = fmaf(h2, pc, 1.0f);
-}
-
-// sin(x), cos(x) for 0 <= x < 4096·π/2: Cody–Waite reduction by π/2 split
-// into C1 + C2 + C3 (C1 and C2 carry 12 significant bits, so k·C1 and k·C2
-// are exact for k < 4096), then Taylor polynomials on |y| <= π/4 (truncation
-// below 2e-9) and quadrant selection.  Used for the per-pair seed sin(q0 r).
-__device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
-  const float k = rintf(x * 0x1.45f306p-1f);  // x·2/π
-  float y = fmaf(-k, 0x1.92p+0f, x);
-  y = fmaf(-k, 0x1.fb4p-12f, y);
-  y = fmaf(-k, 0x1.4442d2p-24f, y);
-  const float y2 = y * y;
-  float ps = fmaf(y2, 1.0f / 362880.0f, -1.0f / 5040.0f);
-  ps = fmaf(y2, ps, 1.0f / 120.0f);
-  ps = fmaf(y2, ps, -1.0f / 6.0f);
-  const float sy = fmaf(y * y2, ps, y);
-  float pc = fmaf(y2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
-  pc = fmaf(y2, pc, -1.0f / 720.0f);
-  pc = fmaf(y2, pc, 1.0f / 24.0f);
-  pc = fmaf(y2, pc, -0.5f);
-  const float cy = fmaf(y2, pc, 1.0f);
-  const int qd = __float2int_rn(k) & 3;
-  const float ss = (qd & 1) ? cy : sy;
-  const float cc = (qd & 1) ? sy : cy;
-  *s = (qd & 2) ? -ss : ss;
-  *c = ((qd + 1) & 2) ? -cc : cc;
-}
 
 template <int Q>
 __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int ab, int qstart, int qcount, int nq,
@@ -142,16 +69,6 @@ __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int
     atomicAdd(&partials[(size_t)ab * nq + qstart + k], s);
   }
   __syncthreads();
-}
-
-// Packed pair of FP32 values in one 64-bit register pair (Blackwell f32x2 ops).
-__device__ __forceinline__ unsigned long long pack2(float x, float y) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
-  return r;
-}
-__device__ __forceinline__ void unpack2(unsigned long long v, float& x, float& y) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
 }
 
 // Per-pair set-up of the recurrence: weight u = w_i w_j / r, λ = 4 sin²(h),
@@ -185,11 +102,12 @@ __device__ __forceinline__ void pair_setup(const float4& ai, const float4& aj, f
 // Work item: (i tile, first j tile, end j tile, q block); items are taken
 // from a global counter (longest first) so CTAs finish together.
 // qpar[b] = (q0_hi, q0_lo, halfstep_hi, halfstep_lo), qrange[b] = (start, count).
-template <int Q>
-__global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
+template <int Q, int JB>
+__global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)) : (Q <= 64 ? 3 : 2))
     k_pair_fp32(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                 int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T, int wide,
-                double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work) {
+                double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
+                const int64_t* __restrict__ work_out) {
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
@@ -212,6 +130,7 @@ __global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
     if (w >= n_work || !ok) break;
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
+    double* __restrict__ out = partials + (work_out ? work_out[w] : 0);  // per-structure output in a batch
     const float4 ai = atoms[(size_t)it * kTile + tid];
     const float4 qp = qpar[qb];
     const int2 qr = qrange[qb];
@@ -231,7 +150,7 @@ __global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, partials);
+        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
         cur = tj;
       }
       // issue the next tile into the other buffer (its previous readers
@@ -247,26 +166,35 @@ __global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
       phase_bits ^= 1u << buf;
       if (!__syncthreads_and(ok)) { ok = false; break; }
       const bool diag = (jt == it);
-      // two j atoms per iteration: their recurrences advance together in
-      // packed f32x2 registers (two independent chains per instruction)
+      // JB j atoms per iteration, their recurrences advanced in pairs in
+      // packed f32x2 registers (JB/2 independent chains per instruction stream)
 #pragma unroll 1
-      for (int j = 0; j < kTile; j += 2) {
-        const float4 aA = sj[buf][j], aB = sj[buf][j + 1];
-        const float wA = (diag && j <= tid) ? 0.0f : aA.w;
-        const float wB = (diag && j + 1 <= tid) ? 0.0f : aB.w;
-        float uA, nlA, sA, dA, uB, nlB, sB, dB;
-        pair_setup(ai, aA, wA, qp, wide, uA, nlA, sA, dA);
-        pair_setup(ai, aB, wB, qp, wide, uB, nlB, sB, dB);
-        unsigned long long s2 = pack2(sA, sB), d2 = pack2(dA, dB);
-        const unsigned long long nl2 = pack2(nlA, nlB);
+      for (int j = 0; j < kTile; j += JB) {
+        float u[JB];
+        unsigned long long s2[JB / 2], d2[JB / 2], nl2[JB / 2];
+#pragma unroll
+        for (int p = 0; p < JB / 2; ++p) {
+          const float4 aA = sj[buf][j + 2 * p], aB = sj[buf][j + 2 * p + 1];
+          const float wA = (diag && j + 2 * p <= tid) ? 0.0f : aA.w;
+          const float wB = (diag && j + 2 * p + 1 <= tid) ? 0.0f : aB.w;
+          float nlA, sA, dA, nlB, sB, dB;
+          pair_setup(ai, aA, wA, qp, wide, u[2 * p], nlA, sA, dA);
+          pair_setup(ai, aB, wB, qp, wide, u[2 * p + 1], nlB, sB, dB);
+          s2[p] = pack2(sA, sB);
+          d2[p] = pack2(dA, dB);
+          nl2[p] = pack2(nlA, nlB);
+        }
 #pragma unroll
         for (int k = 0; k < Q; ++k) {
-          float xa, xb;
-          unpack2(s2, xa, xb);
-          acc[k] = fmaf(uA, xa, acc[k]);
-          acc[k] = fmaf(uB, xb, acc[k]);
-          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2) : "l"(nl2), "l"(s2));
-          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(d2));
+#pragma unroll
+          for (int p = 0; p < JB / 2; ++p) {
+            float xa, xb;
+            unpack2(s2[p], xa, xb);
+            acc[k] = fmaf(u[2 * p], xa, acc[k]);
+            acc[k] = fmaf(u[2 * p + 1], xb, acc[k]);
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2[p]) : "l"(nl2[p]), "l"(s2[p]));
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2[p]) : "l"(d2[p]));
+          }
         }
       }
       __syncthreads();
@@ -274,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, partials);
+      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
     }
   }
 }
@@ -375,15 +303,15 @@ std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_fr
   return work;
 }
 
-template <int Q>
+template <int Q, int JB>
 void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
                  const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
-                 int* next_work) {
+                 int* next_work, const int64_t* work_out) {
   int per_sm = 0;
-  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q>, kThreads, 0));
+  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q, JB>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
-  k_pair_fp32<Q><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials, status,
-                                                 next_work);
+  k_pair_fp32<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
+                                                     status, next_work, work_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -443,6 +371,7 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
   L.atoms.assign((size_t)n_pad * 4, 0.0f);
   if (with_f64) L.atoms64.assign((size_t)n_pad * 4, 0.0);
   L.tile_type.resize(L.n_tiles);
+  L.source.assign((size_t)n_pad, -1);
   int64_t slot = 0, k = 0;
   for (int t = 0; t < T; ++t) {
     const int64_t start = slot;
@@ -454,6 +383,7 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
         if (with_f64) L.atoms64[4 * slot + d] = v;
       }
       L.atoms[4 * slot + 3] = (float)w[i];
+      L.source[slot] = i;
       if (with_f64) L.atoms64[4 * slot + 3] = w[i];
       L.self_w2[t] += w[i] * w[i];
       L.sum_w[t] += w[i];
@@ -499,10 +429,38 @@ std::vector<int2> q_blocks(const std::vector<double>& q, int Qmax) {
   return out;
 }
 
+// Work list of a batch: every segment (one structure's tiles) is tiled on its
+// own; items of all segments are ordered longest first and carry the output
+// offset of their segment.
+void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<int4>& work,
+                        std::vector<int64_t>& out) {
+  std::vector<std::pair<int, std::pair<int4, int64_t>>> items;
+  const int K = (int)P.segments.size() - 1;
+  for (int c = 0; c < K; ++c) {
+    const int t0 = P.segments[c], t1 = P.segments[c + 1];
+    const int64_t base = (int64_t)c * P.n_pairs * P.nq;
+    for (int it = t0; it < t1; ++it)
+      for (int j0 = it; j0 < t1; j0 += run) {
+        const int j1 = std::min(j0 + run, t1);
+        const int cost = 2 * (j1 - j0) - (j0 == it ? 1 : 0);
+        for (int b = 0; b < n_qblocks; ++b) items.push_back({cost, {make_int4(it, j0, j1, b), base}});
+      }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  work.resize(items.size());
+  out.resize(items.size());
+  for (size_t i = 0; i < items.size(); ++i) {
+    work[i] = items[i].second.first;
+    out[i] = items[i].second.second;
+  }
+}
+
 // (Re)build the q blocks and the work list of an FP32 plan for block length Q.
-void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q) {
+void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
+  P.jb = jb;
   for (void* p : P.qcfg) cudaFree(p);
   P.qcfg.clear();
+  P.d_work_out = nullptr;
   const std::vector<int2> qrange = q_blocks(P.q, Q);
   P.Q = Q;
   P.n_qblocks = (int)qrange.size();
@@ -517,7 +475,14 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q) {
     max_half = std::max(max_half, std::fabs(half));
   }
   P.wide = (max_half * (P.L.extent + 1.0) > 0.8) ? 1 : 0;
-  const std::vector<int4> work = make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile);
+  std::vector<int4> work;
+  if (P.segments.empty()) {
+    work = make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile);
+  } else {
+    std::vector<int64_t> out;
+    make_work_segments(P, P.n_qblocks, 8, work, out);
+    P.d_work_out = upload(ctx, P.qcfg, out.data(), out.size(), ctx->stream);
+  }
   P.n_work = (int)work.size();
   P.d_work = upload(ctx, P.qcfg, work.data(), work.size(), ctx->stream);
   P.d_qpar = upload(ctx, P.qcfg, qpar.data(), qpar.size(), ctx->stream);
@@ -557,7 +522,7 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
         bestQ = Qc;
       }
     }
-    configure_fp32(ctx, *P, bestQ);
+    configure_fp32(ctx, *P, bestQ, 2);
   } else {
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
     const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8, P->L.n_tiles);
@@ -575,9 +540,60 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   return P;
 }
 
+// One plan over a batch of structures that share types and q grid: their
+// layouts are concatenated (each padded to whole tiles on its own), and the
+// single launch covers every structure's tile pairs; the raw partials of
+// structure c land at d_out + c*n_pairs*nq.
+std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout>&& parts, const double* q,
+                                               int64_t nq) {
+  std::unique_ptr<PairPlan> P(new PairPlan());
+  require(!parts.empty(), "empty batch");
+  const int T = parts[0].T;
+  Layout& L = P->L;
+  L.T = T;
+  L.self_w2.assign(T, 0.0);
+  L.sum_w.assign(T, 0.0);
+  P->segments.push_back(0);
+  for (auto& part : parts) {
+    require(part.T == T, "batch layouts must share the type count");
+    L.n += part.n;
+    L.n_pad += part.n_pad;
+    L.n_tiles += part.n_tiles;
+    L.atoms.insert(L.atoms.end(), part.atoms.begin(), part.atoms.end());
+    L.tile_type.insert(L.tile_type.end(), part.tile_type.begin(), part.tile_type.end());
+    L.extent = std::max(L.extent, part.extent);
+    P->segments.push_back(L.n_tiles);
+  }
+  P->fp64 = false;
+  P->nq = nq;
+  P->q.assign(q, q + nq);
+  P->n_pairs = T * (T + 1) / 2;
+  P->lattice_first_tile = L.n_tiles;
+  cudaStream_t s = ctx->stream;
+  if (nq == 0 || L.n_tiles == 0) return P;
+  P->d_atoms = upload(ctx, P->owned, (const float4*)L.atoms.data(), (size_t)L.n_pad, s);
+  int bestQ = 64;
+  long best_cost = -1;
+  for (int Qc : kQBlocks) {
+    const long cost = (long)q_blocks(P->q, Qc).size() * (3 * Qc + 60);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      bestQ = Qc;
+    }
+  }
+  configure_fp32(ctx, *P, bestQ, 2);
+  P->d_tile_type = upload(ctx, P->owned, L.tile_type.data(), L.tile_type.size(), s);
+  P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)(P->segments.size() - 1) * P->n_pairs * nq, s);
+  P->d_status = upload<int>(ctx, P->owned, nullptr, 2, s);
+  P->d_next = P->d_status + 1;
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  return P;
+}
+
 void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
   if (P.nq == 0 || P.L.n_tiles == 0) return;
-  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_out, 0, (size_t)P.n_pairs * P.nq * sizeof(double), s));
+  const size_t n_out = (size_t)P.n_pairs * P.nq * (P.segments.empty() ? 1 : P.segments.size() - 1);
+  CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_out, 0, n_out * sizeof(double), s));
   CRAB_CUDA_CHECK(cudaMemsetAsync(P.d_status, 0, 2 * sizeof(int), s));  // status and work counter
   if (timed) CRAB_CUDA_CHECK(cudaEventRecord(ctx->ev_start, s));
   const int T = P.L.T, nq = (int)P.nq;
@@ -588,21 +604,23 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     k_pair_fp64<<<grid, kThreads, 0, s>>>(P.d_atoms64, P.d_tile_type, P.d_work, P.n_work, P.d_q, nq, T, P.d_out);
     CRAB_CUDA_CHECK(cudaGetLastError());
   } else {
-#define CRAB_LAUNCH(QQ)                                                                                          \
-  case QQ:                                                                                                       \
-    launch_fp32<QQ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, T, \
-                    P.wide, P.d_out, P.d_status, P.d_next);                                                                \
-    break;
-    switch (P.Q) {
-      CRAB_LAUNCH(8)
-      CRAB_LAUNCH(16)
-      CRAB_LAUNCH(32)
-      CRAB_LAUNCH(48)
-      CRAB_LAUNCH(64)
-      CRAB_LAUNCH(96)
-      CRAB_LAUNCH(128)
-      default: throw Error(CRAB_EINVAL, "unsupported q block");
-    }
+#define CRAB_LAUNCH(QQ, JJ)                                                                                    \
+  if (P.Q == QQ && P.jb == JJ) {                                                                                 \
+    launch_fp32<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
+                        T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);                                  \
+    launched = true;                                                                                             \
+  }
+    bool launched = false;
+    CRAB_LAUNCH(8, 2)
+    CRAB_LAUNCH(16, 2)
+    CRAB_LAUNCH(32, 2)
+    CRAB_LAUNCH(48, 2)
+    CRAB_LAUNCH(64, 2)
+    CRAB_LAUNCH(96, 2)
+    CRAB_LAUNCH(128, 2)
+    CRAB_LAUNCH(64, 4)
+    CRAB_LAUNCH(96, 4)
+    if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
 #undef CRAB_LAUNCH
   }
   ctx->launches += 1;
@@ -725,16 +743,17 @@ void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_
 
 namespace crab {
 
-int pair_plan_autotune(crab_ctx* ctx, PairPlan& P) {
+int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out, int capacity, int* n_out) {
+  if (n_out) *n_out = 0;
   if (P.fp64 || P.nq == 0 || P.L.n_tiles == 0) return P.Q;
-  int bestQ = P.Q;
+  static const int kVariants[][2] = {{64, 2}, {96, 2}, {128, 2}, {64, 4}, {96, 4}};
+  int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;
   CRAB_CUDA_CHECK(cudaEventCreate(&a));
   CRAB_CUDA_CHECK(cudaEventCreate(&b));
-  for (int Qc : kQBlocks) {
-    if (Qc < 32) continue;
-    configure_fp32(ctx, P, Qc);
+  for (const auto& v : kVariants) {
+    configure_fp32(ctx, P, v[0], v[1]);
     pair_plan_launch(ctx, P, ctx->stream, false);  // warm-up
     CRAB_CUDA_CHECK(cudaEventRecord(a, ctx->stream));
     pair_plan_launch(ctx, P, ctx->stream, false);
@@ -742,16 +761,23 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P) {
     CRAB_CUDA_CHECK(cudaEventSynchronize(b));
     float ms = 0.0f;
     CRAB_CUDA_CHECK(cudaEventElapsedTime(&ms, a, b));
+    if (n < capacity) {
+      if (variants) variants[n] = v[0] * 16 + v[1];
+      if (ms_out) ms_out[n] = ms;
+    }
+    ++n;
     if (best_ms < 0.0f || ms < best_ms) {
       best_ms = ms;
-      bestQ = Qc;
+      bestQ = v[0];
+      bestJ = v[1];
     }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  configure_fp32(ctx, P, bestQ);
+  configure_fp32(ctx, P, bestQ, bestJ);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-  return bestQ;
+  if (n_out) *n_out = std::min(n, capacity);
+  return bestQ * 16 + bestJ;
 }
 
 }  // namespace crab

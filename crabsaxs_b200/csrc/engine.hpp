@@ -127,6 +127,7 @@ struct Layout {
   std::vector<float> tile_sphere;  // per tile: centre xyz + radius (for near/far tests)
   std::vector<double> self_w2;     // per type Σ w²
   std::vector<double> sum_w;       // per type Σ w
+  std::vector<int64_t> source;     // per slot: index of the input atom, -1 for padding
   double extent = 0.0;             // max pair distance bound
 };
 
@@ -158,7 +159,7 @@ struct PairPlan {
   bool fp64 = false;
   int64_t nq = 0;
   std::vector<double> q;
-  int n_pairs = 0, Q = 0, n_qblocks = 0, n_work = 0, wide = 0;
+  int n_pairs = 0, Q = 0, jb = 2, n_qblocks = 0, n_work = 0, wide = 0;
   std::vector<void*> owned;
   std::vector<void*> qcfg;  // q-block and work-list buffers (rebuilt when Q changes)
   float4* d_atoms = nullptr;
@@ -171,7 +172,9 @@ struct PairPlan {
   double* d_out = nullptr;  // [n_pairs][nq] raw sums
   int* d_status = nullptr;
   int* d_next = nullptr;  // work-queue counter (the int after d_status)
+  int64_t* d_work_out = nullptr;  // per work item output offset (batches of structures), or null
   int lattice_first_tile = 0;
+  std::vector<int> segments;  // batch: tile start of every structure plus the end, else empty
   LatticePart lattice;
   ~PairPlan();
 };
@@ -195,9 +198,12 @@ void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed);
 void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, struct Partials& out,
                       const LatticeSpec* lattice = nullptr);
 
+std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout>&& parts, const double* q,
+                                               int64_t nq);
 void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_bytes, double* step_ms);
-// Time each compiled q-block length once on this plan and keep the fastest.
-int pair_plan_autotune(crab_ctx* ctx, PairPlan& P);
+// Time each compiled kernel variant (q-block length Q, j atoms per iteration)
+// once on this plan and keep the fastest; returns Q*16 + JB.
+int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out, int capacity, int* n_out);
 double measure_fp32_peak(crab_ctx* ctx, double target_ms);
 
 // Quadratic form Σ_ij X_i Y_j sinc(q r_ij) for per-type amplitude tables

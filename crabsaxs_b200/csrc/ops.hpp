@@ -23,6 +23,7 @@ struct TypedAtoms {
   std::vector<AtomClass> cls;
   std::vector<double> xyz, w;
   std::vector<int32_t> type;
+  std::vector<int64_t> src;  // input atom index of each entry, -1 for hydration sites
   int T = 0;
 };
 TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites);

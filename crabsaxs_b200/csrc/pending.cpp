@@ -27,16 +27,4 @@ int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q
                                  const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6) {
   return guarded_impl(ctx, [&]() { multipole_solvent_basis_impl(ctx, st, q, nq, l_max, *solvent, implicit_hydrogen, precision, out6); });
 }
-int crab_chi2_grad(crab_ctx* ctx, crab_struct*, const double*, const double*, const double*, int64_t, const crab_solvent*, int,
-                   double, double, double*, double*, double*) {
-  return guarded_impl(ctx, [&]() { throw Error(CRAB_EINVAL, "gradient engine not built in this version"); });
-}
-int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const*, int32_t, const double*, const double*, const double*, int64_t,
-                      const crab_ensemble_options*, const crab_fit_options*, crab_ensemble_result*, int32_t*, double*, double*) {
-  return guarded_impl(ctx, [&]() { throw Error(CRAB_EINVAL, "ensemble engine not built in this version"); });
-}
-int crab_ensemble_curves(crab_ctx* ctx, crab_struct* const*, int32_t, const double*, int64_t, const crab_solvent*, int,
-                         const double*, int32_t, double*) {
-  return guarded_impl(ctx, [&]() { throw Error(CRAB_EINVAL, "ensemble engine not built in this version"); });
-}
 }

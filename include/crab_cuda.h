@@ -188,10 +188,13 @@ int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double
  * (evicting L2); each launch is bracketed by CUDA events and its device time
  * in ms written to step_ms[i] (may be NULL). */
 int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int64_t flush_bytes, double* step_ms);
-/* Autotune: time every compiled q-block length (the number of q values one
- * thread advances per pair between exact re-seeds) on this plan and keep the
- * fastest; *q_block (may be NULL) receives it. */
-int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* q_block);
+/* Autotune: time every compiled kernel variant on this plan (q-block length Q
+ * = q values one thread advances per pair between exact re-seeds, and JB = j
+ * atoms per thread iteration) and keep the fastest.  *chosen = Q*16 + JB;
+ * the first `capacity` variants and their times (ms) are written to
+ * variants/ms (may be NULL), their count to *n_variants. */
+int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen, int32_t* variants, double* ms,
+                            int32_t capacity, int32_t* n_variants);
 /* Copy the partials of the last run to the host (layout of crab_debye_partials). */
 int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double* self_out);
 /* Pair·q evaluations of one run: (n(n-1)/2) * nq. */
@@ -267,7 +270,10 @@ typedef struct crab_ensemble_result {
 int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, const double* y,
                       const double* sigma, int64_t nq, const crab_ensemble_options* eopt,
                       const crab_fit_options* fopt, crab_ensemble_result* result, int32_t* selected,
-                      double* weights, double* fitted);
+                      double* weights, double* fitted, double* intervals, double* bootstrap_chi2);
+/* (intervals: 3 per selected conformer, median/lower/upper of the bootstrap
+ * weights (ensemble.rs:174-216); bootstrap_chi2: one per replicate; both may
+ * be NULL.) */
 /* Batched curves for k conformers at every (c1,c2) candidate: curves is
  * [n_cand][k][nq]; cand is n_cand (c1,c2) pairs. One persistent launch for
  * all conformers' partials, one recombination launch. */
@@ -290,6 +296,28 @@ typedef struct crab_reweight_result {
 int crab_reweight_curves(const double* curves, int32_t k, const double* q, const double* y, const double* sigma,
                          int64_t nq, const double* prior, const crab_reweight_options* opt, double* weights,
                          crab_reweight_result* result);
+
+/* Ensemble scoring plan: the structures' layouts, the (c1,c2) candidate
+ * amplitude tables and all device buffers, built once.  crab_ensemble_plan_score
+ * replays one CUDA graph that computes every conformer's pair sums (one
+ * persistent launch), every (candidate, conformer) curve, the simplex weight
+ * fit per candidate (ensemble.rs:317-381), ∂χ²/∂w and ∂χ²/∂(c1,c2) at the best
+ * candidate, and the KL-penalised reweighting (reweight.rs:84-154, uniform
+ * prior) of the best candidate's curves.
+ * best_fit (8): candidate index, c1, c2, scale, background, reduced χ²,
+ * ∂χ²/∂c1, ∂χ²/∂c2.  weights, grad_w, kl_weights: k values each.
+ * reweight_out (6): scale, background, reduced χ², KL, iterations, converged.
+ * Any output may be NULL; elapsed_ms is the device time of the graph. */
+typedef struct crab_ensemble_plan crab_ensemble_plan;
+int crab_ensemble_plan_create(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, int64_t nq,
+                              const crab_solvent* solvent, int implicit_hydrogen, const double* cand, int32_t n_cand,
+                              crab_ensemble_plan** out);
+int crab_ensemble_plan_autotune(crab_ctx* ctx, crab_ensemble_plan* plan, int32_t* chosen);
+int crab_ensemble_plan_score(crab_ctx* ctx, crab_ensemble_plan* plan, const double* y, const double* sigma,
+                             const crab_fit_options* fit_options, const crab_reweight_options* reweight_options,
+                             double* elapsed_ms, double* best_fit, double* weights, double* grad_w,
+                             double* kl_weights, double* reweight_out);
+int crab_ensemble_plan_destroy(crab_ensemble_plan* plan);
 
 /* ---- synthetic inputs (no counterpart in the reference) ----------------- */
 /* Seeded protein-like structure: Cα-style self-avoiding walk (3.8 Å steps,
