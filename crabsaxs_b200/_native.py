@@ -104,6 +104,8 @@ _SIGS = {
                                                C.POINTER(I64), D]),
     "crab_hydration_grid_exterior": (C.c_int, [P, P, C.c_double, C.c_double, C.c_double, D, I64,
                                                C.POINTER(I64), D]),
+    "crab_hydration_grid_adaptive_noalloc": (C.c_int, [D, I64, C.c_double, C.c_double, C.c_double, D, I64,
+                                                       C.POINTER(I64), D, P]),
     "crab_multipole_intensity": (C.c_int, [P, P, D, I64, C.c_int, C.c_int, C.c_int, D]),
     "crab_multipole_solvent_basis": (C.c_int, [P, P, D, I64, C.c_int, C.POINTER(Solvent), C.c_int, C.c_int, D]),
     "crab_fit": (C.c_int, [P, P, D, D, D, I64, C.POINTER(FitOpts), C.c_double, C.c_double,

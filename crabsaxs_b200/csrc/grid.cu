@@ -389,3 +389,186 @@ GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* 
 }
 
 }  // namespace crab
+
+// ------------------------------------------------------- no-allocation variant
+//
+// crab_hydration_grid_adaptive_noalloc is for callers that cannot allocate
+// device memory through the CUDA runtime (a host runtime whose own allocator
+// owns the device, a process that must keep its memory budget fixed, code
+// running inside a callback where cudaMalloc is not allowed).  It takes
+// device pointers for the atoms and the site output and keeps every
+// temporary (voxel masks, chunk counts, offsets, the box header) in one
+// file-scope __device__ array of fixed size, so it calls no cudaMalloc,
+// cudaFree or allocating library routine.
+
+#include <mutex>
+
+namespace crab {
+namespace {
+
+constexpr uint64_t kNoAllocMaxVoxels = CRAB_NOALLOC_MAX_VOXELS;
+static_assert(kNoAllocMaxVoxels % kChunk == 0, "voxel limit must be a whole number of scan chunks");
+constexpr uint64_t kNoAllocChunks = kNoAllocMaxVoxels / kChunk;
+
+struct NoAllocHeader {
+  Box box;
+  uint64_t count;
+  double inner, outer;
+  int status;  // 0 ok, 1 grid larger than the static scratch
+};
+static_assert(sizeof(NoAllocHeader) <= 256, "header must fit its 256-byte slot");
+
+constexpr size_t kHdrBytes = 256;
+constexpr size_t kShellOff = kHdrBytes;
+constexpr size_t kMolOff = kShellOff + kNoAllocMaxVoxels;
+constexpr size_t kCntOff = kMolOff + kNoAllocMaxVoxels;
+constexpr size_t kOffOff = kCntOff + kNoAllocChunks * sizeof(uint32_t);
+constexpr size_t kNoAllocBytes = kOffOff + (kNoAllocChunks + 1) * sizeof(uint64_t);
+
+// The scratch shared by every call on a device; it keeps the last call's
+// contents, and calls whose kernels overlap on the GPU race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Single-thread prologue in the reference's sequential order
+// (solvent.rs:144-176): centroid, radius of gyration, shell radii, padded box.
+__global__ void k_noalloc_prologue(const double* __restrict__ xyz, int64_t n, double spacing, double clearance,
+                                   double padding, NoAllocHeader* hdr) {
+  double c[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) c[d] = __dadd_rn(c[d], xyz[3 * i + d]);
+  for (int d = 0; d < 3; ++d) c[d] = __ddiv_rn(c[d], (double)n);
+  double acc = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double dx = __dsub_rn(xyz[3 * i], c[0]), dy = __dsub_rn(xyz[3 * i + 1], c[1]),
+                 dz = __dsub_rn(xyz[3 * i + 2], c[2]);
+    acc = __dadd_rn(acc, norm2_rn(dx, dy, dz));
+  }
+  const double rg = sqrt(__ddiv_rn(acc, (double)n));
+  const double width = rg <= 15.0 ? 3.0 : (rg >= 20.0 ? 5.0 : __dadd_rn(3.0, __dmul_rn(0.4, __dsub_rn(rg, 15.0))));
+  hdr->inner = clearance;
+  hdr->outer = __dadd_rn(clearance, width);
+  double mn[3] = {xyz[0], xyz[1], xyz[2]}, mx[3] = {xyz[0], xyz[1], xyz[2]};
+  for (int64_t i = 1; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = fmin(mn[d], xyz[3 * i + d]);
+      mx[d] = fmax(mx[d], xyz[3 * i + d]);
+    }
+  double total = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    hdr->box.mn[d] = __dsub_rn(mn[d], padding);
+    const double hi = __dadd_rn(mx[d], padding);
+    const double span = ceil(__dsub_rn(__ddiv_rn(__dsub_rn(hi, hdr->box.mn[d]), spacing), 1e-10));
+    const double nd = fmax(span, 0.0) + 1.0;
+    total *= nd;
+    hdr->box.n[d] = nd < 9.0e15 ? (uint64_t)nd : 0ull;
+  }
+  hdr->box.spacing = spacing;
+  hdr->status = total > (double)kNoAllocMaxVoxels ? 1 : 0;
+  hdr->count = hdr->status ? 0ull : hdr->box.n[0] * hdr->box.n[1] * hdr->box.n[2];
+}
+
+// k_emit restricted to the caller's capacity; no voxel indices.
+__global__ void k_noalloc_emit(const uint8_t* __restrict__ shell, const uint8_t* __restrict__ mol, uint64_t count,
+                               Box bx, const uint64_t* __restrict__ offsets, double* __restrict__ sites,
+                               uint64_t capacity) {
+  __shared__ uint32_t warp_tot[kScanThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kPerThread;
+  uint32_t c = 0;
+  for (int i = 0; i < kPerThread; ++i)
+    if (base + i < count && site_flag(shell, mol, base + i, 0)) ++c;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_tot[w];
+  uint64_t pos = offsets[blockIdx.x] + before + incl - c;
+  for (int i = 0; i < kPerThread; ++i) {
+    const uint64_t v = base + i;
+    if (v < count && site_flag(shell, mol, v, 0)) {
+      if (pos < capacity) {
+        const uint64_t x = v % bx.n[0], y = (v / bx.n[0]) % bx.n[1], z = v / (bx.n[0] * bx.n[1]);
+        sites[3 * pos] = __dadd_rn(bx.mn[0], __dmul_rn((double)x, bx.spacing));
+        sites[3 * pos + 1] = __dadd_rn(bx.mn[1], __dmul_rn((double)y, bx.spacing));
+        sites[3 * pos + 2] = __dadd_rn(bx.mn[2], __dmul_rn((double)z, bx.spacing));
+      }
+      ++pos;
+    }
+  }
+}
+
+// Device address of the scratch array, looked up once per device (the name
+// g_noalloc_scratch is only a host-side handle; kernels need this address).
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_dev[256] = {};
+
+cudaError_t noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_dev[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_dev[dev] = (unsigned char*)p;
+  }
+  *out = g_noalloc_dev[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace crab
+
+extern "C" int crab_hydration_grid_adaptive_noalloc(const double* d_xyz, int64_t n, double spacing, double clearance,
+                                                    double padding, double* d_sites, int64_t capacity, int64_t* m,
+                                                    double* voxel_volume, void* stream) {
+  using namespace crab;
+  if (n < 0 || capacity < 0 || !m || (n > 0 && !d_xyz) || (capacity > 0 && !d_sites)) return CRAB_EINVAL;
+  if (!std::isfinite(spacing) || spacing <= 0.0 || !std::isfinite(clearance) || clearance <= 0.0 ||
+      !std::isfinite(padding) || padding < 0.0)
+    return CRAB_EINVAL;
+  if (voxel_volume) *voxel_volume = adaptive_site_volume(spacing);
+  *m = 0;
+  if (n == 0) return CRAB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* base = nullptr;
+  if (noalloc_scratch(&base) != cudaSuccess) return CRAB_ECUDA;
+  NoAllocHeader* hdr = (NoAllocHeader*)base;
+  k_noalloc_prologue<<<1, 1, 0, s>>>(d_xyz, n, spacing, clearance, padding, hdr);
+  if (cudaGetLastError() != cudaSuccess) return CRAB_ECUDA;
+  NoAllocHeader h;
+  if (cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CRAB_ECUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CRAB_ECUDA;
+  if (h.status) return CRAB_EINVAL;  // grid larger than CRAB_NOALLOC_MAX_VOXELS
+  uint8_t* shell = base + kShellOff;
+  uint8_t* mol = base + kMolOff;
+  uint32_t* cnt = (uint32_t*)(base + kCntOff);
+  uint64_t* off = (uint64_t*)(base + kOffOff);
+  // the masks keep the previous call's voxels: clear the part this grid uses
+  if (cudaMemsetAsync(shell, 0, h.count, s) != cudaSuccess || cudaMemsetAsync(mol, 0, h.count, s) != cudaSuccess)
+    return CRAB_ECUDA;
+  const unsigned blocks = (unsigned)((n * 32 + 255) / 256);
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, nullptr, h.outer, 0.0, n, h.box, shell, 1, 0);
+  k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, nullptr, h.inner, 0.0, n, h.box, mol, 1, 0);
+  const uint64_t chunks = (h.count + kChunk - 1) / kChunk;
+  k_count<<<(unsigned)chunks, kScanThreads, 0, s>>>(shell, mol, h.count, 0, cnt);
+  k_scan_chunks<<<1, 1024, 0, s>>>(cnt, chunks, off);
+  if (cudaGetLastError() != cudaSuccess) return CRAB_ECUDA;
+  uint64_t total = 0;
+  if (cudaMemcpyAsync(&total, off + chunks, sizeof(total), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CRAB_ECUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CRAB_ECUDA;
+  *m = (int64_t)total;
+  if (total > 0 && capacity > 0) {
+    k_noalloc_emit<<<(unsigned)chunks, kScanThreads, 0, s>>>(shell, mol, h.count, h.box, off, d_sites,
+                                                            (uint64_t)capacity);
+    if (cudaGetLastError() != cudaSuccess) return CRAB_ECUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CRAB_ECUDA;
+  }
+  return (capacity > 0 && (int64_t)total > capacity) ? CRAB_ECAPACITY : CRAB_OK;
+}

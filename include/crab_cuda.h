@@ -220,6 +220,28 @@ int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t 
  * order. Two-call size query: pass sites=NULL to read *m. */
 int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing, double clearance, double padding,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
+/* Largest box (voxels) crab_hydration_grid_adaptive_noalloc accepts. */
+#define CRAB_NOALLOC_MAX_VOXELS 4194304ull
+/* No counterpart in the reference.  The adaptive shell of
+ * crab_hydration_grid_adaptive for callers that cannot allocate device
+ * memory (their host runtime owns the device allocator, their memory budget
+ * is fixed, or they run where cudaMalloc is not allowed).  Inputs and outputs
+ * are caller-owned DEVICE pointers: d_xyz (n*3 f64) and d_sites (capacity*3
+ * f64); `stream` is a cudaStream_t (NULL = default stream) on the current
+ * device.  Every temporary lives in one file-scope __device__ array sized for
+ * CRAB_NOALLOC_MAX_VOXELS voxels (about 8 MiB, held by every GPU that loads
+ * the library until the process exits); a larger box returns CRAB_EINVAL.
+ * The function calls no cudaMalloc, cudaFree or allocating library routine.
+ * Its first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the array, so calls whose work overlaps on the GPU race: serialise them.
+ * *m receives the site count; capacity 0 is a size query (returns CRAB_OK);
+ * with a smaller non-zero capacity the sites beyond it are not written and
+ * the call returns CRAB_ECAPACITY.  The call
+ * synchronises `stream` before returning. */
+int crab_hydration_grid_adaptive_noalloc(const double* d_xyz, int64_t n, double spacing, double clearance,
+                                         double padding, double* d_sites, int64_t capacity, int64_t* m,
+                                         double* voxel_volume, void* stream);
 /* Exterior flood-fill shell (solvent.rs:259-401), bit-exact. */
 int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing, double probe, double thickness,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
