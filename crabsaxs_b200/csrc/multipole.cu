@@ -1,0 +1,627 @@
+// Multipole engine: the spherical-harmonic expansion of spherical.rs:266-565,
+//   A_lm(q) = sum_i a_i(q) j_l(q r_i) Y_lm(i),   I(q) = 4 pi sum_{l <= l_q} sum_m A_lm(q)^2,
+// evaluated as one dense GEMM instead of a contraction per (l, q).
+//
+// The only coupling between the angular and the radial factor is j_l(q r_i).
+// As a function of r on [0, R] it is band-limited by q (it is an average of
+// exp(i q r t) over |t| <= 1 weighted by P_l(t)), so interpolating it at nb
+// Chebyshev nodes rho_b is exact to round-off once nb is a little above
+// q_max R / 2 (the Chebyshev coefficients of exp(i w s) are the Bessel J_k(w),
+// which fall off like (e w / 2k)^k beyond k = w):
+//   j_l(q r_i) = sum_b j_l(q rho_b) L_b(r_i)          (L_b: Lagrange basis)
+//   A_lm(q)    = sum_t a_t(q) sum_b j_l(q rho_b) M^t_{lm,b},
+//   M^t_{lm,b} = sum_{i in type t} Y_lm(i) w_i L_b(r_i).
+// M is a GEMM [(L+1)^2 x N] x [N x nb] per scattering type, independent of q;
+// the q dependence is a small f64 pass over (q, lm).  For wide radial ranges
+// [0, R] is cut into S segments with their own nodes (points of a segment use
+// only its nodes).  The interpolation error bound, 1e-15 of max |j_l|, is far
+// below the FP32 rounding of the GEMM operands.
+//
+// Kernels:
+//   k_mp_prep        per point: r, cos(theta), phi, real Y_lm (the f64
+//                    recurrence of spherical.rs:54-93) and w_i L_b(r_i)
+//   k_mp_moments     the GEMM, register-tiled SIMT, FP32 or FP64 operands,
+//                    split over points with f64 atomic accumulation
+//   k_mp_node_bessel j_0..j_{l_q}(q rho_b), the Miller recurrence of
+//                    spherical.rs:95-133 in f64
+//   k_mp_gram        per q: A^c_lm for each requested amplitude combination c
+//                    and 4 pi sum_{l <= l_q, m} A^c A^d
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.hpp"
+#include "ops.hpp"
+
+namespace crab {
+namespace {
+
+constexpr double kPiD = 3.14159265358979323846;
+constexpr int kMaxL = 64;
+constexpr int kMaxNodes = 64;       // Chebyshev nodes per radial segment (GEMM N tile)
+constexpr int kMaxSegments = 16;
+constexpr int kGemmM = 128;         // lm rows per GEMM tile
+constexpr int kPointAlign = 32;     // group padding (GEMM K step for FP32)
+constexpr int64_t kSplitK = 4096;   // points per GEMM work item
+
+// spherical.rs:201-203
+int adaptive_l(double q, double max_radius, int maximum) {
+  long v = (long)std::ceil(q * max_radius) + 8;
+  const long lo = std::min(maximum, 8);
+  if (v < lo) v = lo;
+  if (v > maximum) v = maximum;
+  return (int)v;
+}
+
+// spherical.rs:33-51
+std::vector<double> harmonic_norms(int L) {
+  std::vector<double> norms((size_t)(L + 1) * (L + 1), 0.0);
+  for (int l = 0; l <= L; ++l)
+    for (int m = 0; m <= l; ++m) {
+      double ratio = 1.0;
+      for (int k = l - m + 1; k <= l + m; ++k) ratio /= (double)k;
+      norms[(size_t)l * l + l + m] = std::sqrt(((double)(2 * l + 1) / (4.0 * kPiD)) * ratio);
+    }
+  return norms;
+}
+
+// Smallest node count whose Chebyshev interpolation of exp(i w s) on [-1, 1]
+// errs by less than 1e-15: the tail sum_{k >= n} 2 |J_k(w)| with
+// |J_k(w)| <= (e w / 2k)^k / sqrt(2 pi k).
+int nodes_needed(double w) {
+  int n = std::max(8, (int)std::ceil(w) + 8);
+  for (;; ++n) {
+    const double lb = n * std::log(std::exp(1.0) * std::max(w, 1e-300) / (2.0 * n)) - 0.5 * std::log(2.0 * kPiD * n);
+    if (w <= 0.0 || lb < std::log(1e-16)) return n;
+  }
+}
+
+struct RadialBasis {
+  int S = 1, nb = 8;
+  double R = 0.0;
+  std::vector<double> nodes;  // S * nb
+  std::vector<double> bary;   // nb (first-kind Chebyshev barycentric weights)
+};
+
+RadialBasis radial_basis(double R, double qmax) {
+  RadialBasis B;
+  B.R = R;
+  for (B.S = 1; B.S <= kMaxSegments; ++B.S) {
+    B.nb = nodes_needed(qmax * R / (2.0 * B.S));
+    if (B.nb <= kMaxNodes) break;
+  }
+  if (B.S > kMaxSegments)
+    throw Error(CRAB_EINVAL, "multipole radial range too wide for the q grid (q_max * r_max too large)");
+  B.nodes.resize((size_t)B.S * B.nb);
+  B.bary.resize(B.nb);
+  for (int b = 0; b < B.nb; ++b) {
+    const double th = (2.0 * b + 1.0) * kPiD / (2.0 * B.nb);
+    B.bary[b] = ((b & 1) ? -1.0 : 1.0) * std::sin(th);
+    for (int s = 0; s < B.S; ++s) {
+      const double a0 = R * s / B.S, a1 = R * (s + 1) / B.S;
+      B.nodes[(size_t)s * B.nb + b] = 0.5 * (a0 + a1) + 0.5 * (a1 - a0) * std::cos(th);
+    }
+  }
+  return B;
+}
+
+struct MpWork {
+  int32_t group, lm0;
+  int64_t k0, k1;
+};
+
+// ------------------------------------------------------------------ kernels
+
+// Per point: real harmonics (spherical.rs:54-93, 165-199) and the weighted
+// Lagrange basis of its radial segment.  pts: x, y, z (centred), w, r.
+template <typename E>
+__global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restrict__ seg, int64_t n_pad, int L,
+                          int lm_pad, int nb, const double* __restrict__ norms, const double* __restrict__ nodes,
+                          const double* __restrict__ bary, E* __restrict__ YT, E* __restrict__ WT) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pad) return;
+  const double px = pts[5 * i], py = pts[5 * i + 1], pz = pts[5 * i + 2], w = pts[5 * i + 3], r = pts[5 * i + 4];
+  double x, phi;
+  if (r < 1e-12) {
+    x = 1.0;
+    phi = 0.0;
+  } else {
+    x = fmin(fmax(__ddiv_rn(pz, r), -1.0), 1.0);
+    phi = atan2(py, px);
+  }
+  const double sin_theta = sqrt(fmax(__dadd_rn(1.0, -__dmul_rn(x, x)), 0.0));
+  double sin_phi, cos_phi;
+  sincos(phi, &sin_phi, &cos_phi);
+  const double sqrt2 = sqrt(2.0);
+  double sin_m = 0.0, cos_m = 1.0, pmm = 1.0;
+  auto emit = [&](int l, int m, double p) {
+    const int pos = l * l + l + m;
+    if (m == 0) {
+      YT[(int64_t)pos * n_pad + i] = (E)__dmul_rn(norms[pos], p);
+    } else {
+      const double v = __dmul_rn(__dmul_rn(sqrt2, norms[pos]), p);
+      YT[(int64_t)pos * n_pad + i] = (E)__dmul_rn(v, cos_m);
+      YT[(int64_t)(l * l + l - m) * n_pad + i] = (E)__dmul_rn(v, sin_m);
+    }
+  };
+  for (int m = 0; m <= L; ++m) {
+    if (m > 0) {
+      pmm = __dmul_rn(pmm, __dmul_rn(-(double)(2 * m - 1), sin_theta));
+      const double next_cos = __dadd_rn(__dmul_rn(cos_m, cos_phi), -__dmul_rn(sin_m, sin_phi));
+      sin_m = __dadd_rn(__dmul_rn(sin_m, cos_phi), __dmul_rn(cos_m, sin_phi));
+      cos_m = next_cos;
+    }
+    emit(m, m, pmm);
+    if (m == L) continue;
+    const double pm1 = __dmul_rn(__dmul_rn(x, (double)(2 * m + 1)), pmm);
+    emit(m + 1, m, pm1);
+    double prev = pmm, cur = pm1;
+    for (int l = m + 2; l <= L; ++l) {
+      const double num = __dadd_rn(__dmul_rn(__dmul_rn((double)(2 * l - 1), x), cur), -__dmul_rn((double)(l + m - 1), prev));
+      const double next = __ddiv_rn(num, (double)(l - m));
+      emit(l, m, next);
+      prev = cur;
+      cur = next;
+    }
+  }
+  for (int pos = (L + 1) * (L + 1); pos < lm_pad; ++pos) YT[(int64_t)pos * n_pad + i] = (E)0;
+  // Barycentric Lagrange basis at the segment's first-kind Chebyshev nodes.
+  const double* nd = nodes + (int64_t)seg[i] * nb;
+  int hit = -1;
+  double den = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    const double d = r - nd[b];
+    if (d == 0.0) hit = b;
+    else den += bary[b] / d;
+  }
+  for (int b = 0; b < kMaxNodes; ++b) {
+    double v = 0.0;
+    if (b < nb) {
+      if (hit >= 0) v = (b == hit) ? w : 0.0;
+      else v = w * ((bary[b] / (r - nd[b])) / den);
+    }
+    WT[(int64_t)b * n_pad + i] = (E)v;
+  }
+}
+
+// M[g][b][lm] += sum_{k in [k0, k1)} YT[lm][k] WT[b][k] for one 128 x 64 tile.
+// 256 threads, 8 x 4 outputs each; operands staged through shared memory in
+// 128-byte rows (32 floats or 16 doubles of K per step).
+template <typename E>
+__global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, const E* __restrict__ WT, int64_t n_pad,
+                                                    int lm_pad, const MpWork* __restrict__ work,
+                                                    double* __restrict__ M) {
+  constexpr int KS = 128 / sizeof(E);
+  constexpr int V = 16 / sizeof(E);
+  typedef typename std::conditional<sizeof(E) == 4, float4, double2>::type Vec;
+  __shared__ __align__(16) E As[KS][kGemmM + V];
+  __shared__ __align__(16) E Bs[KS][kMaxNodes + V];
+  const MpWork wk = work[blockIdx.x];
+  const int tid = threadIdx.x, tm = tid >> 4, tn = tid & 15;
+  E acc[8][4];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = (E)0;
+  for (int64_t k0 = wk.k0; k0 < wk.k1; k0 += KS) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {  // A: 128 rows x 8 vectors
+      const int idx = it * 256 + tid, row = idx >> 3, c = (idx & 7) * V;
+      const Vec v = *reinterpret_cast<const Vec*>(YT + (int64_t)(wk.lm0 + row) * n_pad + k0 + c);
+      const E* pv = reinterpret_cast<const E*>(&v);
+#pragma unroll
+      for (int j = 0; j < V; ++j) As[c + j][row] = pv[j];
+    }
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {  // B: 64 rows x 8 vectors
+      const int idx = it * 256 + tid, row = idx >> 3, c = (idx & 7) * V;
+      const Vec v = *reinterpret_cast<const Vec*>(WT + (int64_t)row * n_pad + k0 + c);
+      const E* pv = reinterpret_cast<const E*>(&v);
+#pragma unroll
+      for (int j = 0; j < V; ++j) Bs[c + j][row] = pv[j];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < KS; ++kk) {
+      E a[8], b[4];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a[j] = As[kk][tm * 8 + j];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tn * 4 + j];
+#pragma unroll
+      for (int x = 0; x < 8; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+    }
+    __syncthreads();
+  }
+  double* Mg = M + (int64_t)wk.group * kMaxNodes * lm_pad;
+#pragma unroll
+  for (int x = 0; x < 8; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      const double v = (double)acc[x][y];
+      if (v != 0.0) atomicAdd(Mg + (int64_t)(tn * 4 + y) * lm_pad + wk.lm0 + tm * 8 + x, v);
+    }
+}
+
+// j_0..j_{l_q}(q rho) at every node (spherical.rs:95-133, f64 as the
+// reference), zero for l_q < l <= L.  Jn[k][s*nb + b][l].
+__global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __restrict__ lq, int64_t nq,
+                                 const double* __restrict__ nodes, int n_nodes, int L, double* __restrict__ Jn) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nq * n_nodes) return;
+  const int64_t k = idx / n_nodes;
+  const int node = (int)(idx % n_nodes);
+  const int ql = lq[k];
+  const double x = q[k] * nodes[node];
+  double* out = Jn + idx * (L + 1);
+  for (int l = 0; l <= L; ++l) out[l] = 0.0;
+  if (fabs(x) < 1e-8) {
+    out[0] = 1.0;
+    return;
+  }
+  double s, c;
+  sincos(x, &s, &c);
+  if (ql == 0) {
+    out[0] = s / x;
+    return;
+  }
+  double work[kMaxL + 26];
+  const int start = ql + 24;
+  for (int l = 0; l < start + 2; ++l) work[l] = 0.0;
+  work[start] = 1.0;
+  for (int l = start; l >= 1; --l) {
+    work[l - 1] = __dadd_rn(__ddiv_rn(__dmul_rn((double)(2 * l + 1), work[l]), x), -work[l + 1]);
+    if (fabs(work[l - 1]) > 1e100)
+      for (int kk = l - 1; kk <= start + 1; ++kk) work[kk] *= 1e-100;
+  }
+  const double j0 = s / x;
+  const double j1 = __dadd_rn(s / (x * x), -(c / x));
+  const double scale = fabs(j0) >= fabs(j1) ? j0 / work[0] : j1 / work[1];
+  for (int l = 0; l <= ql; ++l) out[l] = work[l] * scale;
+}
+
+// One q per block: A^c_lm = sum_g amp[c][g][k] sum_b M[g][b][lm] Jn[k][seg_g*nb + b][l]
+// for l <= l_q, then 4 pi sum_lm A^c A^d for c <= d (order (0,0), (1,1),
+// (2,2), (0,1), (0,2), (1,2) for three combinations).
+template <int K>
+__global__ void __launch_bounds__(256) k_mp_gram(const double* __restrict__ M, const double* __restrict__ Jn,
+                                                 const int32_t* __restrict__ lq, const double* __restrict__ amp,
+                                                 const int32_t* __restrict__ gseg, int G, int nb, int n_nodes, int L,
+                                                 int lm_pad, int64_t nq, double* __restrict__ out) {
+  constexpr int P = K * (K + 1) / 2;
+  const int64_t k = blockIdx.x;
+  const int ql = lq[k];
+  const int nlm = (ql + 1) * (ql + 1);
+  const double* Jq = Jn + k * (int64_t)n_nodes * (L + 1);
+  double acc[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) acc[p] = 0.0;
+  for (int lm = threadIdx.x; lm < nlm; lm += blockDim.x) {
+    int l = (int)sqrt((double)lm);
+    while (l * l > lm) --l;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    double A[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) A[c] = 0.0;
+    for (int g = 0; g < G; ++g) {
+      const double* Mg = M + (int64_t)g * kMaxNodes * lm_pad + lm;
+      const double* J = Jq + (int64_t)gseg[g] * nb * (L + 1) + l;
+      double C = 0.0;
+      for (int b = 0; b < nb; ++b) C = fma(Mg[(int64_t)b * lm_pad], __ldg(J + b * (L + 1)), C);
+#pragma unroll
+      for (int c = 0; c < K; ++c) A[c] = fma(amp[((int64_t)c * G + g) * nq + k], C, A[c]);
+    }
+    int p = 0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[p++] += A[c] * A[c];
+#pragma unroll
+    for (int c = 0; c < K; ++c)
+#pragma unroll
+      for (int d = c + 1; d < K; ++d) acc[p++] += A[c] * A[d];
+  }
+  __shared__ double red[8][P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    double v = acc[p];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][p] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < P) {
+    double v = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[wi][threadIdx.x];
+    out[threadIdx.x * nq + k] = 4.0 * kPiD * v;
+  }
+}
+
+// ------------------------------------------------------------------ host
+
+struct MpInput {
+  const TypedAtoms* t;
+  double centre[3];
+  double rmax_lq;                 // radius for the per-q order (atoms, or atoms and sites)
+  std::vector<double> amp;        // K x T x nq amplitude combinations (no occupancy)
+  int K = 1;
+};
+
+// Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
+void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, double* out) {
+  const TypedAtoms& t = *in.t;
+  const int T = t.T, K = in.K, P = K * (K + 1) / 2;
+  const int64_t n = (int64_t)t.w.size();
+  std::fill(out, out + (size_t)P * nq, 0.0);
+  if (n == 0 || nq == 0) return;
+  // geometry relative to the structure centroid (spherical.rs:165-199)
+  std::vector<double> r(n);
+  double R = 0.0, qmax = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double dx = t.xyz[3 * i] - in.centre[0], dy = t.xyz[3 * i + 1] - in.centre[1],
+                 dz = t.xyz[3 * i + 2] - in.centre[2];
+    r[i] = std::sqrt(((0.0 + dx * dx) + dy * dy) + dz * dz);
+    R = std::max(R, r[i]);
+  }
+  for (int64_t k = 0; k < nq; ++k) qmax = std::max(qmax, q[k]);
+  R = R > 0.0 ? R * (1.0 + 1e-12) : 1.0;
+  const RadialBasis B = radial_basis(R, qmax);
+  const int S = B.S, nb = B.nb, G = T * S;
+  // group = type * S + segment; points sorted by group, padded per group
+  std::vector<int32_t> seg_of(n), group_of(n);
+  std::vector<int64_t> count(G, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    seg_of[i] = std::min(S - 1, (int)(r[i] / R * S));
+    group_of[i] = t.type[i] * S + seg_of[i];
+    ++count[group_of[i]];
+  }
+  std::vector<int64_t> begin(G + 1, 0);
+  for (int g = 0; g < G; ++g) begin[g + 1] = begin[g] + (count[g] + kPointAlign - 1) / kPointAlign * kPointAlign;
+  const int64_t n_pad = std::max<int64_t>(begin[G], kPointAlign);
+  std::vector<double> pts((size_t)5 * n_pad, 0.0);
+  std::vector<int32_t> seg(n_pad, 0);
+  std::vector<int64_t> fill(begin.begin(), begin.end() - 1);
+  for (int g = 0; g < G; ++g)
+    for (int64_t k = begin[g]; k < begin[g + 1]; ++k) seg[k] = g % S;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t k = fill[group_of[i]]++;
+    pts[5 * k] = t.xyz[3 * i] - in.centre[0];
+    pts[5 * k + 1] = t.xyz[3 * i + 1] - in.centre[1];
+    pts[5 * k + 2] = t.xyz[3 * i + 2] - in.centre[2];
+    pts[5 * k + 3] = t.w[i];
+    pts[5 * k + 4] = r[i];
+  }
+  const int lm_count = (L + 1) * (L + 1);
+  const int lm_pad = (lm_count + kGemmM - 1) / kGemmM * kGemmM;
+  std::vector<int32_t> lq(nq);
+  for (int64_t k = 0; k < nq; ++k) lq[k] = adaptive_l(q[k], in.rmax_lq, L);
+  std::vector<MpWork> work;
+  for (int g = 0; g < G; ++g)
+    for (int64_t k0 = begin[g]; k0 < begin[g + 1]; k0 += kSplitK)
+      for (int lm0 = 0; lm0 < lm_pad; lm0 += kGemmM)
+        work.push_back(MpWork{g, lm0, k0, std::min(begin[g + 1], k0 + kSplitK)});
+  std::vector<int32_t> gseg(G);
+  for (int g = 0; g < G; ++g) gseg[g] = g % S;
+  std::vector<double> ampg((size_t)K * G * nq);
+  for (int c = 0; c < K; ++c)
+    for (int g = 0; g < G; ++g)
+      std::memcpy(&ampg[((size_t)c * G + g) * nq], &in.amp[((size_t)c * T + g / S) * nq], sizeof(double) * nq);
+  const std::vector<double> norms = harmonic_norms(L);
+
+  cudaStream_t s = ctx->stream;
+  const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+  double* d_pts = (double*)ctx->dev("mp_pts", sizeof(double) * pts.size());
+  int32_t* d_seg = (int32_t*)ctx->dev("mp_seg", sizeof(int32_t) * n_pad);
+  double* d_norms = (double*)ctx->dev("mp_norms", sizeof(double) * norms.size());
+  double* d_nodes = (double*)ctx->dev("mp_nodes", sizeof(double) * B.nodes.size());
+  double* d_bary = (double*)ctx->dev("mp_bary", sizeof(double) * B.bary.size());
+  void* d_YT = ctx->dev("mp_Y", esz * (size_t)lm_pad * n_pad);
+  void* d_WT = ctx->dev("mp_W", esz * (size_t)kMaxNodes * n_pad);
+  MpWork* d_work = (MpWork*)ctx->dev("mp_work", sizeof(MpWork) * work.size());
+  double* d_M = (double*)ctx->dev("mp_M", sizeof(double) * (size_t)G * kMaxNodes * lm_pad);
+  double* d_q = (double*)ctx->dev("mp_q", sizeof(double) * nq);
+  int32_t* d_lq = (int32_t*)ctx->dev("mp_lq", sizeof(int32_t) * nq);
+  double* d_Jn = (double*)ctx->dev("mp_Jn", sizeof(double) * (size_t)nq * S * nb * (L + 1));
+  double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * ampg.size());
+  int32_t* d_gseg = (int32_t*)ctx->dev("mp_gseg", sizeof(int32_t) * G);
+  double* d_out = (double*)ctx->dev("mp_out", sizeof(double) * (size_t)P * nq);
+  copy_h2d(ctx, d_pts, pts.data(), sizeof(double) * pts.size(), s);
+  copy_h2d(ctx, d_seg, seg.data(), sizeof(int32_t) * n_pad, s);
+  copy_h2d(ctx, d_norms, norms.data(), sizeof(double) * norms.size(), s);
+  copy_h2d(ctx, d_nodes, B.nodes.data(), sizeof(double) * B.nodes.size(), s);
+  copy_h2d(ctx, d_bary, B.bary.data(), sizeof(double) * B.bary.size(), s);
+  copy_h2d(ctx, d_work, work.data(), sizeof(MpWork) * work.size(), s);
+  copy_h2d(ctx, d_q, q, sizeof(double) * nq, s);
+  copy_h2d(ctx, d_lq, lq.data(), sizeof(int32_t) * nq, s);
+  copy_h2d(ctx, d_amp, ampg.data(), sizeof(double) * ampg.size(), s);
+  copy_h2d(ctx, d_gseg, gseg.data(), sizeof(int32_t) * G, s);
+  CRAB_CUDA_CHECK(cudaMemsetAsync(d_M, 0, sizeof(double) * (size_t)G * kMaxNodes * lm_pad, s));
+
+  const unsigned prep_blocks = (unsigned)((n_pad + 127) / 128);
+  if (fp64) {
+    k_mp_prep<double><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
+                                                   (double*)d_YT, (double*)d_WT);
+    k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
+                                                                lm_pad, d_work, d_M);
+  } else {
+    k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
+                                                  (float*)d_YT, (float*)d_WT);
+    k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad, lm_pad,
+                                                               d_work, d_M);
+  }
+  const int n_nodes = S * nb;
+  const int64_t nbess = nq * n_nodes;
+  k_mp_node_bessel<<<(unsigned)((nbess + 127) / 128), 128, 0, s>>>(d_q, d_lq, nq, d_nodes, n_nodes, L, d_Jn);
+  if (K == 1)
+    k_mp_gram<1><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
+  else
+    k_mp_gram<3><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+  ctx->launches += 4;
+  copy_d2h(ctx, out, d_out, sizeof(double) * (size_t)P * nq, s);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+bool multipole_precision(int precision) {
+  if (precision == CRAB_PREC_FP64) return true;
+  if (precision == CRAB_PREC_FP32) return false;
+  throw Error(CRAB_EINVAL, "multipole precision must be CRAB_PREC_FP64 or CRAB_PREC_FP32");
+}
+
+void validate_multipole(const crab_struct* st, const double* q, int64_t nq, int l_max) {
+  require(st != nullptr, "structure is NULL");
+  require(nq >= 0 && (nq == 0 || q != nullptr), "q grid is NULL");
+  validate_q(q, nq);
+  require(l_max >= 0 && l_max <= kMaxL, "multipole l_max must be between 0 and 64");
+}
+
+// Per-type multipole amplitudes without occupancy (spherical.rs:205-231):
+// V, E, H [T][nq].  Hydration sites (element -1) carry the grid amplitude
+// rho/10 * V_voxel * f_water(q) in H.
+void multipole_tables(const TypedAtoms& t, const double* q, int64_t nq, const crab_solvent* s, bool implicit,
+                      double site_volume, std::vector<double>& V, std::vector<double>& E, std::vector<double>& H) {
+  const int T = t.T;
+  V.assign((size_t)T * nq, 0.0);
+  E.assign((size_t)T * nq, 0.0);
+  H.assign((size_t)T * nq, 0.0);
+  const bool grid = s && s->hydration_model != CRAB_HYD_ANALYTIC;
+  for (int a = 0; a < T; ++a)
+    for (int64_t k = 0; k < nq; ++k) {
+      const size_t o = (size_t)a * nq + k;
+      if (t.cls[a].element < 0) {
+        H[o] = s->bulk_density / 10.0 * site_volume * water_form_factor(q[k]);
+        continue;
+      }
+      if (!s) {
+        V[o] = form_factor(t.cls[a].element, t.cls[a].group, 1.0, implicit, q[k]);
+        continue;
+      }
+      double v, e, h;
+      multipole_class_amplitudes(t.cls[a], implicit, q[k], s->bulk_density, s->shell_thickness, &v, &e, &h);
+      V[o] = v;
+      E[o] = e;
+      H[o] = grid ? 0.0 : h;
+    }
+}
+
+// Atoms (and grid sites) with their amplitude tables, the centroid and the
+// radius that sets l_q.
+struct MpSolventSetup {
+  GridResult g;
+  TypedAtoms t;
+  std::vector<double> V, E, H;
+  double centre[3], rmax_lq;
+};
+
+void solvent_setup(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
+                   bool implicit, MpSolventSetup& u) {
+  const bool grid = s.hydration_model != CRAB_HYD_ANALYTIC;
+  if (grid) u.g = hydration_sites(ctx, st, s);
+  u.t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &u.g.sites : nullptr);
+  multipole_tables(u.t, q, nq, &s, implicit, u.g.voxel_volume, u.V, u.E, u.H);
+  double rmax;
+  centre_and_rmax(st, u.centre, &rmax);
+  u.rmax_lq = rmax;
+  if (grid) {  // spherical.rs:423-427, 489-493: the order also covers the sites
+    double rs = 0.0;
+    const size_t ns = u.g.sites.size() / 3;
+    for (size_t i = 0; i < ns; ++i) {
+      const double dx = u.g.sites[3 * i] - u.centre[0], dy = u.g.sites[3 * i + 1] - u.centre[1],
+                   dz = u.g.sites[3 * i + 2] - u.centre[2];
+      rs = std::max(rs, std::sqrt(((0.0 + dx * dx) + dy * dy) + dz * dz));
+    }
+    if (ns > 0) u.rmax_lq = std::max(rmax, rs);
+  }
+}
+
+}  // namespace
+
+void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                              bool implicit, int precision, double* out) {
+  validate_multipole(st, q, nq, l_max);
+  const bool fp64 = multipole_precision(precision);
+  if (st->n == 0) {
+    std::fill(out, out + nq, 0.0);
+    return;
+  }
+  TypedAtoms t = type_atoms(st, implicit, TermSet::Vacuum, nullptr);
+  MpInput in;
+  in.t = &t;
+  double rmax;
+  centre_and_rmax(st, in.centre, &rmax);
+  in.rmax_lq = rmax;
+  std::vector<double> V, E, H;
+  multipole_tables(t, q, nq, nullptr, implicit, 0.0, V, E, H);
+  in.amp = V;
+  in.K = 1;
+  multipole_run(ctx, in, q, nq, l_max, fp64, out);
+  for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
+}
+
+void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                                  const crab_solvent& s, bool implicit, int precision, double* out6) {
+  validate_multipole(st, q, nq, l_max);
+  validate_solvent(s);
+  const bool fp64 = multipole_precision(precision);
+  if (st->n == 0) {
+    std::fill(out6, out6 + 6 * nq, 0.0);
+    return;
+  }
+  MpSolventSetup u;
+  solvent_setup(ctx, st, q, nq, s, implicit, u);
+  MpInput in;
+  in.t = &u.t;
+  std::copy(u.centre, u.centre + 3, in.centre);
+  in.rmax_lq = u.rmax_lq;
+  in.K = 3;
+  in.amp.reserve(u.V.size() * 3);
+  in.amp.insert(in.amp.end(), u.V.begin(), u.V.end());
+  in.amp.insert(in.amp.end(), u.E.begin(), u.E.end());
+  in.amp.insert(in.amp.end(), u.H.begin(), u.H.end());
+  multipole_run(ctx, in, q, nq, l_max, fp64, out6);
+}
+
+void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
+                                      const crab_solvent& s, bool implicit, int precision, double* out) {
+  validate_multipole(st, q, nq, l_max);
+  validate_solvent(s);
+  const bool fp64 = multipole_precision(precision);
+  if (st->n == 0) {
+    std::fill(out, out + nq, 0.0);
+    return;
+  }
+  MpSolventSetup u;
+  solvent_setup(ctx, st, q, nq, s, implicit, u);
+  MpInput in;
+  in.t = &u.t;
+  std::copy(u.centre, u.centre + 3, in.centre);
+  in.rmax_lq = u.rmax_lq;
+  in.K = 1;
+  // spherical.rs:438-444, 453-462: f = v - G(q) e + c2 h per atom, c2 * amplitude per site
+  in.amp.resize(u.V.size());
+  for (int a = 0; a < u.t.T; ++a)
+    for (int64_t k = 0; k < nq; ++k) {
+      const size_t o = (size_t)a * nq + k;
+      in.amp[o] = u.V[o] - excluded_volume_scale(q[k], s.c1) * u.E[o] + s.c2 * u.H[o];
+    }
+  multipole_run(ctx, in, q, nq, l_max, fp64, out);
+  for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
+}
+
+}  // namespace crab
+
+using namespace crab;
+extern "C" {
+int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max, int implicit_hydrogen,
+                             int precision, double* out) {
+  if (!ctx || !st || (nq > 0 && !out)) return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() { multipole_intensity_impl(ctx, st, q, nq, l_max, implicit_hydrogen != 0, precision, out); });
+}
+int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                 const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6) {
+  if (!ctx || !st || !solvent || (nq > 0 && !out6)) return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() {
+    multipole_solvent_basis_impl(ctx, st, q, nq, l_max, *solvent, implicit_hydrogen != 0, precision, out6);
+  });
+}
+}
