@@ -50,6 +50,12 @@ Q = np.linspace(0.001, 0.5, 500)
 FLUSH_BYTES = 256 << 20
 
 
+
+def _variant_name(v: int) -> str:
+    """Autotuner variant code Q*16 + jb; jb >= 8 is the q-packed kernel with jb-8 chains."""
+    q, jb = int(v) // 16, int(v) % 16
+    return f"Q{q}xJ{jb - 8}pq" if jb >= 8 else f"Q{q}xJ{jb}"
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -319,7 +325,7 @@ def run_ours(args, rank, world, local):
     ntv = C.c_int32()
     eng.check(lib.crab_pair_plan_autotune(eng.handle, plan, C.byref(chosen), tv.ctypes.data_as(N.I32P),
                                           tms.ctypes.data_as(N.D), 16, C.byref(ntv)))
-    tuning = {f"Q{v // 16}xJ{v % 16}": round(float(t), 3) for v, t in zip(tv[:ntv.value], tms[:ntv.value])}
+    tuning = {_variant_name(v): round(float(t), 3) for v, t in zip(tv[:ntv.value], tms[:ntv.value])}
     pairq = lib.crab_pair_plan_pairq(plan)
     ns = len(sites)
     kernel_pairq = pairq - ns * (ns - 1) / 2.0 * len(Q)  # the lattice path sums the site–site pairs
@@ -410,7 +416,7 @@ def run_ours(args, rank, world, local):
             "config": {"workload": "debye pair sums per type pair, 20k-atom structure + adaptive 3 Å hydration "
                                    "sites, 500 q on [0.001, 0.5]",
                        "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_types": T, "n_q": len(Q),
-                       "kernel_variant": f"Q{chosen.value // 16}xJ{chosen.value % 16}", "autotune_ms": tuning,
+                       "kernel_variant": _variant_name(chosen.value), "autotune_ms": tuning,
                        "parallelism": f"independent structure per GPU x{world}",
                        "l2": "flushed before every step (256 MiB memset, outside the step events)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",

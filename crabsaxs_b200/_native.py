@@ -129,6 +129,7 @@ _SIGS = {
                                                 C.POINTER(P)]),
     "crab_pair_plan_run": (C.c_int, [P, P, C.c_int32, I64, D]),
     "crab_pair_plan_autotune": (C.c_int, [P, P, I32P, I32P, D, C.c_int32, I32P]),
+    "crab_pair_plan_select": (C.c_int, [P, P, C.c_int32]),
     "crab_pair_plan_read": (C.c_int, [P, P, D, D]),
     "crab_pair_plan_pairq": (C.c_double, [P]),
     "crab_pair_plan_destroy": (C.c_int, [P]),

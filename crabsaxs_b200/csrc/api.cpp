@@ -489,6 +489,11 @@ int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen
   });
 }
 
+int crab_pair_plan_select(crab_ctx* ctx, crab_pair_plan* plan, int32_t variant) {
+  if (!ctx || !plan) return CRAB_EINVAL;
+  GUARD(ctx, { pair_plan_select(ctx, *plan->plan, variant); });
+}
+
 double crab_pair_plan_pairq(const crab_pair_plan* plan) {
   if (!plan) return 0.0;
   const double n = (double)plan->plan->L.n;

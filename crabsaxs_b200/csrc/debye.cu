@@ -44,6 +44,8 @@ using namespace dev;
 
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
 constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 128};  // compiled q-block lengths
+// jb values at or above kPackedQ select the q-packed kernel with jb - kPackedQ chains.
+constexpr int kPackedQ = 8;
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
 template <int Q>
@@ -97,6 +99,55 @@ __device__ __forceinline__ void pair_setup(const float4& ai, const float4& aj, f
   else sincos_small(h, &sh, &ch);
   nl = -4.0f * sh * sh;
   d = 2.0f * sh * fmaf(s, sh, c0 * ch);
+}
+
+// Set-up for the q-packed recurrence: the two halves of each f32x2 register
+// follow the even and the odd q points of the block, so each half steps by
+// 2Δ (angle Δr, λ' = 4 sin²(Δr)).  S, C = sin, cos(q0 r) come from the
+// hardware sine/cosine after an explicit reduction by 2π when q0 r >= 1
+// (absolute error about 5e-7, uncorrelated between pairs), and from the
+// Taylor polynomials below 1 rad, where an absolute error would be a large
+// relative one and would add up coherently over pairs; s1, c1 = sin, cos(Δr) from short
+// polynomials when the plan's largest step angle is at most 0.25 rad
+// (wide == 0), else from the reduced polynomial seed.  Then:
+//   lane A: s = S,                   d = S - sin(q0 r - 2Δr) = 2 s1 cos(q0 r - Δr)
+//   lane B: s = sin(q0 r + Δr),      d = sin(q0 r + Δr) - sin(q0 r - Δr) = 2 s1 C.
+__device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj, float wj, const float4& qp, int wide,
+                                              unsigned long long& u2, unsigned long long& nl2,
+                                              unsigned long long& s2, unsigned long long& d2) {
+  const float dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
+  const float x = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-8f);
+  const float y0 = rsqrtf(x);
+  const float sq = x * y0;
+  const float hy = 0.5f * y0;
+  const float r = fmaf(fmaf(-sq, sq, x), hy, sq);
+  const float rinv = fmaf(fmaf(-sq, y0, 1.0f), hy, y0);
+  const float u = ai.w * wj * rinv;
+  const float phi = fmaf(qp.x, r, qp.y * r);
+  const float g = 2.0f * fmaf(qp.z, r, qp.w * r);  // Δr
+  float S, C, s1, c1;
+  if (phi < 1.0f) sincos_small(phi, &S, &C);  // relative accuracy where sin(q0 r) is small
+  else sincos_seed_hw(phi, &S, &C);
+  if (wide) {
+    sincos_seed(g, &s1, &c1);
+  } else {
+    // |g| <= 0.25: Taylor to g^7 for sin and g^6 for cos (truncation < 4e-10)
+    const float g2 = g * g;
+    float ps = fmaf(g2, -1.0f / 5040.0f, 1.0f / 120.0f);
+    ps = fmaf(g2, ps, -1.0f / 6.0f);
+    s1 = fmaf(g * g2, ps, g);
+    float pc = fmaf(g2, -1.0f / 720.0f, 1.0f / 24.0f);
+    pc = fmaf(g2, pc, -0.5f);
+    c1 = fmaf(g2, pc, 1.0f);
+  }
+  const float sB = fmaf(S, c1, C * s1);
+  const float dA = 2.0f * s1 * fmaf(C, c1, S * s1);
+  const float dB = 2.0f * s1 * C;
+  const float nl = -4.0f * s1 * s1;
+  u2 = pack2(u, u);
+  nl2 = pack2(nl, nl);
+  s2 = pack2(S, sB);
+  d2 = pack2(dA, dB);
 }
 
 // Work item: (i tile, first j tile, end j tile, q block); items are taken
@@ -178,8 +229,8 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
           const float wA = (diag && j + 2 * p <= tid) ? 0.0f : aA.w;
           const float wB = (diag && j + 2 * p + 1 <= tid) ? 0.0f : aB.w;
           float nlA, sA, dA, nlB, sB, dB;
-          pair_setup(ai, aA, wA, qp, wide, u[2 * p], nlA, sA, dA);
-          pair_setup(ai, aB, wB, qp, wide, u[2 * p + 1], nlB, sB, dB);
+          pair_setup(ai, aA, wA, qp, wide >= 2, u[2 * p], nlA, sA, dA);
+          pair_setup(ai, aB, wB, qp, wide >= 2, u[2 * p + 1], nlB, sB, dB);
           s2[p] = pack2(sA, sB);
           d2[p] = pack2(dA, dB);
           nl2[p] = pack2(nlA, nlB);
@@ -203,6 +254,129 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
       flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+    }
+  }
+}
+
+// The same work items with the q-packed recurrence: accumulators are f32x2
+// pairs (q points 2m, 2m+1), and JB j atoms run JB independent packed chains,
+// 3 packed instructions per chain and step (6 FP32 lane operations for 2
+// pair·q, as the j-packed form, but with JB chains in flight per warp).
+template <int Q>
+__device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2], float (*red)[Q], int ab, int qstart,
+                                              int qcount, int nq, double* __restrict__ partials) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 0; m < Q / 2; ++m) {
+    float a, b;
+    unpack2(acc2[m], a, b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      red[warp][2 * m] = a;
+      red[warp][2 * m + 1] = b;
+    }
+    acc2[m] = 0ull;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < qcount; k += kThreads) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += (double)red[w][k];
+    atomicAdd(&partials[(size_t)ab * nq + qstart + k], s);
+  }
+  __syncthreads();
+}
+
+template <int Q, int JB>
+__global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
+    k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
+                   int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
+                   int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
+                   const int64_t* __restrict__ work_out) {
+  static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
+  __shared__ __align__(16) float4 sj[2][kTile];
+  __shared__ float red[kThreads / 32][Q];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned phase_bits = 0u;
+  bool ok = true;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(next_work, 1);
+    __syncthreads();
+    const int w = s_item;
+    __syncthreads();
+    if (w >= n_work || !ok) break;
+    const int4 wk = work[w];
+    const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
+    double* __restrict__ out = partials + (work_out ? work_out[w] : 0);
+    const float4 ai = atoms[(size_t)it * kTile + tid];
+    const float4 qp = qpar[qb];
+    const int2 qr = qrange[qb];
+    const int ti = tile_type[it];
+    unsigned long long acc2[Q / 2];
+#pragma unroll
+    for (int m = 0; m < Q / 2; ++m) acc2[m] = 0ull;
+    int cur = tile_type[jt0];
+    if (tid == 0) {
+      mbar_expect_tx(&bar[0], kTile * sizeof(float4));
+      bulk_g2s(&sj[0][0], atoms + (size_t)jt0 * kTile, kTile * sizeof(float4), &bar[0]);
+    }
+    int buf = 0;
+    for (int jt = jt0; jt < jt1; ++jt) {
+      const int tj = tile_type[jt];
+      if (tj != cur) {
+        const int a = min(ti, cur), b = max(ti, cur);
+        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        cur = tj;
+      }
+      if (tid == 0 && jt + 1 < jt1) {
+        mbar_expect_tx(&bar[buf ^ 1], kTile * sizeof(float4));
+        bulk_g2s(&sj[buf ^ 1][0], atoms + (size_t)(jt + 1) * kTile, kTile * sizeof(float4), &bar[buf ^ 1]);
+      }
+      if (!mbar_wait(&bar[buf], (phase_bits >> buf) & 1u)) {
+        if (tid == 0) atomicExch(status, CRAB_ETIMEOUT);
+        ok = false;
+      }
+      phase_bits ^= 1u << buf;
+      if (!__syncthreads_and(ok)) { ok = false; break; }
+      const bool diag = (jt == it);
+#pragma unroll 1
+      for (int j = 0; j < kTile; j += JB) {
+        unsigned long long u2[JB], nl2[JB], s2[JB], d2[JB];
+#pragma unroll
+        for (int c = 0; c < JB; ++c) {
+          const float4 aj = sj[buf][j + c];
+          const float wj = (diag && j + c <= tid) ? 0.0f : aj.w;
+          pair_setup_pq(ai, aj, wj, qp, wide >= 1, u2[c], nl2[c], s2[c], d2[c]);
+        }
+#pragma unroll
+        for (int m = 0; m < Q / 2; ++m) {
+#pragma unroll
+          for (int c = 0; c < JB; ++c) {
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2[m]) : "l"(u2[c]), "l"(s2[c]));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2[c]) : "l"(nl2[c]), "l"(s2[c]));
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2[c]) : "l"(d2[c]));
+          }
+        }
+      }
+      __syncthreads();
+      buf ^= 1;
+    }
+    if (ok) {
+      const int a = min(ti, cur), b = max(ti, cur);
+      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
     }
   }
 }
@@ -312,6 +486,18 @@ void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const i
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
                                                      status, next_work, work_out);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int Q, int JB>
+void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
+                    int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
+                    int* status, int* next_work, const int64_t* work_out) {
+  int per_sm = 0;
+  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB>, kThreads, 0));
+  int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
+  k_pair_fp32_pq<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
+                                                        status, next_work, work_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -455,6 +641,23 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
   }
 }
 
+// Untuned choice of (Q, jb): the block length by a cost model (launched steps
+// of 3 FP32 ops each plus a per-pair seed of about 60 ops per block), and the
+// q-packed kernel with two chains where it is compiled for that length.
+int2 default_variant(const std::vector<double>& q) {
+  int bestQ = 64;
+  long best_cost = -1;
+  for (int Qc : kQBlocks) {
+    const long cost = (long)q_blocks(q, Qc).size() * (3 * Qc + 60);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      bestQ = Qc;
+    }
+  }
+  const bool packed = bestQ == 64 || bestQ == 96 || bestQ == 128;
+  return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
+}
+
 // (Re)build the q blocks and the work list of an FP32 plan for block length Q.
 void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   P.jb = jb;
@@ -474,7 +677,11 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
     qpar[b] = make_float4(q0h, (float)(q0 - (double)q0h), hh, (float)(half - (double)hh));
     max_half = std::max(max_half, std::fabs(half));
   }
-  P.wide = (max_half * (P.L.extent + 1.0) > 0.8) ? 1 : 0;
+  // largest half step angle h = Δr/2: above 0.8 rad both kernels seed the
+  // step by range reduction (2), above 0.125 rad only the q-packed one,
+  // whose step is 2h (1); otherwise both use short polynomials (0)
+  const double hmax = max_half * (P.L.extent + 1.0);
+  P.wide = hmax > 0.8 ? 2 : (hmax > 0.125 ? 1 : 0);
   std::vector<int4> work;
   if (P.segments.empty()) {
     work = make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile);
@@ -511,18 +718,8 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   }
   if (!fp64) {
     P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
-    // block length Q by a cost model: launched steps (3 FP32 ops each) plus
-    // a per-pair seed of about 60 ops per block
-    int bestQ = 64;
-    long best_cost = -1;
-    for (int Qc : kQBlocks) {
-      const long cost = (long)q_blocks(P->q, Qc).size() * (3 * Qc + 60);
-      if (best_cost < 0 || cost < best_cost) {
-        best_cost = cost;
-        bestQ = Qc;
-      }
-    }
-    configure_fp32(ctx, *P, bestQ, 2);
+    const int2 v = default_variant(P->q);
+    configure_fp32(ctx, *P, v.x, v.y);
   } else {
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
     const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8, P->L.n_tiles);
@@ -572,16 +769,8 @@ std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout
   cudaStream_t s = ctx->stream;
   if (nq == 0 || L.n_tiles == 0) return P;
   P->d_atoms = upload(ctx, P->owned, (const float4*)L.atoms.data(), (size_t)L.n_pad, s);
-  int bestQ = 64;
-  long best_cost = -1;
-  for (int Qc : kQBlocks) {
-    const long cost = (long)q_blocks(P->q, Qc).size() * (3 * Qc + 60);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      bestQ = Qc;
-    }
-  }
-  configure_fp32(ctx, *P, bestQ, 2);
+  const int2 v = default_variant(P->q);
+  configure_fp32(ctx, *P, v.x, v.y);
   P->d_tile_type = upload(ctx, P->owned, L.tile_type.data(), L.tile_type.size(), s);
   P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)(P->segments.size() - 1) * P->n_pairs * nq, s);
   P->d_status = upload<int>(ctx, P->owned, nullptr, 2, s);
@@ -620,8 +809,19 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH(128, 2)
     CRAB_LAUNCH(64, 4)
     CRAB_LAUNCH(96, 4)
-    if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
 #undef CRAB_LAUNCH
+#define CRAB_LAUNCH_PQ(QQ, JJ)                                                                                  \
+  if (P.Q == QQ && P.jb == JJ + kPackedQ) {                                                                      \
+    launch_fp32_pq<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange,  \
+                           nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);                           \
+    launched = true;                                                                                             \
+  }
+    CRAB_LAUNCH_PQ(64, 2)
+    CRAB_LAUNCH_PQ(96, 2)
+    CRAB_LAUNCH_PQ(128, 1)
+    CRAB_LAUNCH_PQ(128, 2)
+#undef CRAB_LAUNCH_PQ
+    if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
   }
   ctx->launches += 1;
   if (P.lattice.active) lattice_plan_launch(ctx, P, s);
@@ -743,10 +943,27 @@ void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_
 
 namespace crab {
 
+// Every (Q, jb) pair that pair_plan_launch can dispatch.
+static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2},
+                                     {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
+                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ}};
+
+void pair_plan_select(crab_ctx* ctx, PairPlan& P, int variant) {
+  require(!P.fp64, "the FP64 plan has a single kernel");
+  const int Q = variant / 16, jb = variant % 16;
+  bool known = false;
+  for (const auto& v : kLaunchable) known = known || (v[0] == Q && v[1] == jb);
+  require(known, "unknown kernel variant " + std::to_string(variant));
+  if (P.nq == 0 || P.L.n_tiles == 0) return;
+  configure_fp32(ctx, P, Q, jb);
+  CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+}
+
 int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out, int capacity, int* n_out) {
   if (n_out) *n_out = 0;
   if (P.fp64 || P.nq == 0 || P.L.n_tiles == 0) return P.Q;
-  static const int kVariants[][2] = {{64, 2}, {96, 2}, {128, 2}, {64, 4}, {96, 4}};
+  static const int kVariants[][2] = {{64, 2},  {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
+                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;

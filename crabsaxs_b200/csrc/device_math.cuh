@@ -41,8 +41,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
   return false;
 }
 
-// sin(h), cos(h) for |h| <= 0.8 by their Taylor series (error < 1e-11 before
-// rounding); used for the half-step angle h = Δr/2.
+// sin(h), cos(h) for |h| <= 1 by their Taylor series (error < 2e-10 before
+// rounding); used for the half-step angle h = Δr/2 and for small seeds.
 __device__ __forceinline__ void sincos_small(float h, float* sh, float* ch) {
   const float h2 = h * h;
   float ps = fmaf(h2, -1.0f / 39916800.0f, 1.0f / 362880.0f);
@@ -82,6 +82,16 @@ __device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
   const float cc = (qd & 1) ? sy : cy;
   *s = (qd & 2) ? -ss : ss;
   *c = ((qd + 1) & 2) ? -cc : cc;
+}
+
+// sin(x), cos(x) for 0 <= x < 2^22: reduction by 2π split into a 12-bit head
+// and a tail (k·head exact for k < 2^12 ... the product error stays below
+// ulp(x) for larger k), then the hardware sine and cosine on [-π, π].
+__device__ __forceinline__ void sincos_seed_hw(float x, float* s, float* c) {
+  const float k = rintf(x * 0x1.45f306p-3f);  // x/(2π)
+  float y = fmaf(-k, 0x1.92p+2f, x);          // 2π head (12 significant bits)
+  y = fmaf(-k, 0x1.fb54442ep-10f, y);         // 2π - head
+  __sincosf(y, s, c);
 }
 
 // Packed pair of FP32 values in one 64-bit register pair (Blackwell f32x2 ops).

@@ -204,6 +204,8 @@ void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_
 // Time each compiled kernel variant (q-block length Q, j atoms per iteration)
 // once on this plan and keep the fastest; returns Q*16 + JB.
 int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out, int capacity, int* n_out);
+// Fix the kernel variant (Q*16 + jb, as pair_plan_autotune reports it).
+void pair_plan_select(crab_ctx* ctx, PairPlan& P, int variant);
 double measure_fp32_peak(crab_ctx* ctx, double target_ms);
 
 // Quadratic form Σ_ij X_i Y_j sinc(q r_ij) for per-type amplitude tables

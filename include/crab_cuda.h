@@ -190,11 +190,16 @@ int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double
 int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int64_t flush_bytes, double* step_ms);
 /* Autotune: time every compiled kernel variant on this plan (q-block length Q
  * = q values one thread advances per pair between exact re-seeds, and JB = j
- * atoms per thread iteration) and keep the fastest.  *chosen = Q*16 + JB;
+ * atoms per thread iteration; JB >= 8 selects the q-packed kernel, whose f32x2
+ * registers hold two consecutive q points, with JB-8 independent chains) and
+ * keep the fastest.  *chosen = Q*16 + JB;
  * the first `capacity` variants and their times (ms) are written to
  * variants/ms (may be NULL), their count to *n_variants. */
 int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen, int32_t* variants, double* ms,
                             int32_t capacity, int32_t* n_variants);
+/* Fix the kernel variant of an FP32 plan (a code as crab_pair_plan_autotune
+ * reports it); CRAB_EINVAL for a variant that is not compiled. */
+int crab_pair_plan_select(crab_ctx* ctx, crab_pair_plan* plan, int32_t variant);
 /* Copy the partials of the last run to the host (layout of crab_debye_partials). */
 int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double* self_out);
 /* Pair·q evaluations of one run: (n(n-1)/2) * nq. */

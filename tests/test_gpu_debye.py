@@ -302,3 +302,44 @@ def test_lattice_plan_matches_fp64_config2(engine):
     err = np.abs(P - P64) / scale
     assert err[-1].max() <= 1e-12  # site–site row: exact lattice sums
     assert err.max() <= PARTIAL_ATOL
+
+
+# Every kernel variant the plan can dispatch (Q*16 + jb; jb >= 8: q-packed).
+ALL_VARIANTS = [8 * 16 + 2, 16 * 16 + 2, 32 * 16 + 2, 48 * 16 + 2, 64 * 16 + 2, 96 * 16 + 2, 128 * 16 + 2,
+                64 * 16 + 4, 96 * 16 + 4, 64 * 16 + 10, 96 * 16 + 10, 128 * 16 + 9, 128 * 16 + 10]
+
+
+@pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "wide"])
+def test_every_kernel_variant_matches_fp64(engine, qkind):
+    import ctypes as C
+
+    from crabsaxs_b200 import _native as N
+
+    T = 3
+    xyz, w, t = _random_typed(700, T, 11, radius=20.0)
+    t = t.astype(np.int32)
+    if qkind == "uniform":
+        q = np.linspace(0.001, 0.5, 333)
+    elif qkind == "nonuniform":
+        q = np.concatenate([np.linspace(0.0, 0.1, 57), np.linspace(0.102, 0.6, 141), [0.65, 0.7, 0.8]])
+    else:  # steps of about 0.05 Å⁻¹ over a 70 Å extent: the seed path for the step angle
+        q = np.linspace(0.01, 3.0, 61)
+    q = np.ascontiguousarray(q)
+    xyz = np.ascontiguousarray(xyz)
+    P64, _ = cs.debye_partials(xyz, w, t, T, q, fp64=True, engine=engine)
+    scale = _partials_scale(w, t, T)[:, None]
+    plan = C.c_void_p()
+    engine.check(N.lib.crab_pair_plan_create(engine.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
+                                             t.ctypes.data_as(N.I32P), len(w), T, q.ctypes.data_as(N.D), len(q),
+                                             C.byref(plan)))
+    try:
+        for v in ALL_VARIANTS:
+            engine.check(N.lib.crab_pair_plan_select(engine.handle, plan, v))
+            engine.check(N.lib.crab_pair_plan_run(engine.handle, plan, 1, 0, None))
+            P = np.empty((T * (T + 1) // 2, len(q)))
+            engine.check(N.lib.crab_pair_plan_read(engine.handle, plan, P.ctypes.data_as(N.D), None))
+            err = np.abs(P - P64) / scale
+            assert err.max() <= PARTIAL_ATOL, (v, err.max())
+        assert N.lib.crab_pair_plan_select(engine.handle, plan, 100 * 16 + 2) == N.EINVAL
+    finally:
+        N.lib.crab_pair_plan_destroy(plan)
