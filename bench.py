@@ -295,6 +295,63 @@ def ensemble_section(eng, rank):
             "reduced_chi2": float(best["reduced_chi2"]), "kl_reduced_chi2": float(best["kl_reduced_chi2"])}
 
 
+def multipole_section(eng, rank, fp32_peak):
+    """Config 3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50, FP32
+    moment GEMM.  Reports the call's wall and device time, the GEMM's FP32
+    fraction, the error against the FP64 device multipole (all q; precision)
+    and against FP64 Debye (every 50th q; truncation of the expansion at L),
+    and config 2's solvent curve by multipole (L = 30) for comparison with Debye."""
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import _native as N
+    from crabsaxs_b200 import synth
+
+    w = synth.CONFIG3
+    s = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
+    L = 50
+    cs.multipole_intensity(s, w.q, L, engine=eng)
+    walls, dev, gemm = [], [], []
+    tot, gm, fl = C.c_double(), C.c_double(), C.c_double()
+    for _ in range(5):
+        t0 = time.perf_counter()
+        f32 = cs.multipole_intensity(s, w.q, L, engine=eng)
+        walls.append((time.perf_counter() - t0) * 1e3)
+        eng.check(N.lib.crab_multipole_last_timing(eng.handle, C.byref(tot), C.byref(gm), C.byref(fl)))
+        dev.append(tot.value)
+        gemm.append(gm.value)
+    f64 = cs.multipole_intensity(s, w.q, L, precision=N.PREC_FP64, engine=eng)
+    rel = np.abs(f32 - f64) / np.abs(f64)
+    sub = np.arange(0, len(w.q), 50)
+    d64 = cs.debye_solvent_basis(s, w.q[sub], cs.SolventParams(), engine=eng, fp64=True)[0]
+    trunc = np.abs(f64[sub] - d64) / np.abs(d64)
+    # the contraction a direct per-(l, q) evaluation would do: 2 N sum_q (l_q+1)^2
+    c = s.xyz.mean(axis=0)
+    rmax = float(np.max(np.linalg.norm(s.xyz - c, axis=1)))
+    lq = np.clip(np.ceil(w.q * rmax) + 8, min(8, L), L)
+    direct_flop = 2.0 * s.atom_count * float(np.sum((lq + 1) ** 2))
+    gemm_ms = float(np.median(gemm))
+    # config 2 curve with the adaptive 3 Å grid by multipole, L = 30
+    s2 = synth.protein(synth.CONFIG2.seed, synth.CONFIG2.n_atoms, synth.CONFIG2.radius)
+    sp = cs.SolventParams(hydration_model=cs.HydrationModel.AdaptiveGrid, hydration_grid_spacing_angstrom=3.0)
+    opt = cs.ComputeOptions(method=cs.ScatteringMethod.Multipole, solvent=sp, multipole_l_max=30)
+    cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
+    c2_ms = (time.perf_counter() - t0) * 1e3 / 3
+    return {"workload": "multipole intensity, 100k atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50",
+            "wall_ms": float(np.median(walls)), "device_ms": float(np.median(dev)),
+            "moments_gemm": {"ms": gemm_ms, "flop": fl.value, "achieved_tflops": fl.value / (gemm_ms * 1e-3) / 1e12,
+                             "peak_tflops": fp32_peak, "bound": "fp32 (SIMT register-tiled GEMM)",
+                             "frac": fl.value / (gemm_ms * 1e-3) / 1e12 / fp32_peak},
+            "direct_contraction_flop": direct_flop,
+            "direct_equivalent_tflops": direct_flop / (float(np.median(dev)) * 1e-3) / 1e12,
+            "max_rel_err_vs_fp64_multipole": float(rel.max()),
+            "rms_rel_err_vs_fp64_multipole": float(np.sqrt(np.mean(rel**2))),
+            "max_rel_err_vs_fp64_debye_every_50th_q": float(trunc.max()),
+            "rms_rel_err_vs_fp64_debye_every_50th_q": float(np.sqrt(np.mean(trunc**2))),
+            "config2_multipole_l30_curve_ms": c2_ms}
+
+
 def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
@@ -407,6 +464,7 @@ def run_ours(args, rank, world, local):
                          f"{dt:.1f} s; f64 C++ restatement of solvent.rs debye_solvent_basis"}
 
     ens = None if args.no_ensemble else ensemble_section(eng, rank)
+    mp = None if args.no_multipole else multipole_section(eng, rank, peak.value)
 
     if rank == 0:
         line = {
@@ -426,6 +484,7 @@ def run_ours(args, rank, world, local):
                          "flop_per_unit": 4},
             "parity": {"max_rel_err_vs_fp64": max_rel, "c1": c1, "c2": c2},
             "ensemble": ens,
+            "multipole": mp,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,
@@ -449,6 +508,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-multipole", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

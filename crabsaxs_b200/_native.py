@@ -108,6 +108,7 @@ _SIGS = {
                                                        C.POINTER(I64), D, P]),
     "crab_multipole_intensity": (C.c_int, [P, P, D, I64, C.c_int, C.c_int, C.c_int, D]),
     "crab_multipole_solvent_basis": (C.c_int, [P, P, D, I64, C.c_int, C.POINTER(Solvent), C.c_int, C.c_int, D]),
+    "crab_multipole_last_timing": (C.c_int, [P, D, D, D]),
     "crab_fit": (C.c_int, [P, P, D, D, D, I64, C.POINTER(FitOpts), C.c_double, C.c_double,
                            C.POINTER(FitResult), D]),
     "crab_chi2_grad": (C.c_int, [P, P, D, D, D, I64, C.POINTER(Solvent), C.c_int, C.c_double, C.c_double, D, D, D]),
@@ -130,6 +131,7 @@ _SIGS = {
     "crab_pair_plan_run": (C.c_int, [P, P, C.c_int32, I64, D]),
     "crab_pair_plan_autotune": (C.c_int, [P, P, I32P, I32P, D, C.c_int32, I32P]),
     "crab_pair_plan_select": (C.c_int, [P, P, C.c_int32]),
+    "crab_ctx_set_pair_variant": (C.c_int, [P, C.c_int32]),
     "crab_pair_plan_read": (C.c_int, [P, P, D, D]),
     "crab_pair_plan_pairq": (C.c_double, [P]),
     "crab_pair_plan_destroy": (C.c_int, [P]),

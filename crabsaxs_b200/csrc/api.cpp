@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -14,6 +15,14 @@
 #include "ops.hpp"
 
 // ---------------------------------------------------------------- context
+
+bool crab::trace_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("CRAB_TRACE");
+    return v && std::atoi(v) > 0;
+  }();
+  return on;
+}
 
 void* crab_ctx::dev(const std::string& name, size_t bytes) {
   crab::DevBuf& b = bufs[name];
@@ -167,7 +176,11 @@ void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const cr
 Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,
                       const GridResult* lattice_sites) {
   Partials P;
-  Layout L = build_layout(t.xyz.data(), t.w.data(), t.type.data(), (int64_t)t.w.size(), t.T, fp64);
+  Layout L;
+  {
+    TraceScope tl("build_layout");
+    L = build_layout(t.xyz.data(), t.w.data(), t.type.data(), (int64_t)t.w.size(), t.T, fp64);
+  }
   LatticeSpec spec;
   if (lattice_sites) {
     spec.cells = lattice_sites->cells.data();
@@ -186,13 +199,20 @@ GridResult hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solv
 
 void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
                  bool implicit, double* out6, bool fp64) {
+  TraceScope trace("debye_basis");
   GridResult g;
   const bool grid = s.hydration_model != CRAB_HYD_ANALYTIC;
-  if (grid) g = hydration_sites(ctx, st, s);
-  TypedAtoms t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic,
-                            grid ? &g.sites : nullptr);
+  if (grid) {
+    TraceScope tg("hydration_sites");
+    g = hydration_sites(ctx, st, s);
+  }
+  TypedAtoms t;
   std::vector<double> V, E, H;
-  amplitude_tables(t, q, nq, &s, implicit, g.voxel_volume, V, E, H);
+  {
+    TraceScope tt("type_atoms+tables");
+    t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &g.sites : nullptr);
+    amplitude_tables(t, q, nq, &s, implicit, g.voxel_volume, V, E, H);
+  }
   Partials P = partials_for(ctx, t, q, nq, fp64, grid ? &g : nullptr);
   quadratic_terms(P, V.data(), V.data(), out6);
   quadratic_terms(P, E.data(), E.data(), out6 + nq);
@@ -486,6 +506,14 @@ int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen
     if (variants)
       for (int i = 0; i < n; ++i) variants[i] = v[i];
     if (n_variants) *n_variants = n;
+  });
+}
+
+int crab_ctx_set_pair_variant(crab_ctx* ctx, int32_t variant) {
+  if (!ctx) return CRAB_EINVAL;
+  GUARD(ctx, {
+    require(variant == 0 || pair_variant_known(variant), "unknown kernel variant " + std::to_string(variant));
+    ctx->pair_variant = variant;
   });
 }
 

@@ -104,12 +104,11 @@ __device__ __forceinline__ void pair_setup(const float4& ai, const float4& aj, f
 // Set-up for the q-packed recurrence: the two halves of each f32x2 register
 // follow the even and the odd q points of the block, so each half steps by
 // 2Δ (angle Δr, λ' = 4 sin²(Δr)).  S, C = sin, cos(q0 r) come from the
-// hardware sine/cosine after an explicit reduction by 2π when q0 r >= 1
-// (absolute error about 5e-7, uncorrelated between pairs), and from the
-// Taylor polynomials below 1 rad, where an absolute error would be a large
-// relative one and would add up coherently over pairs; s1, c1 = sin, cos(Δr) from short
-// polynomials when the plan's largest step angle is at most 0.25 rad
-// (wide == 0), else from the reduced polynomial seed.  Then:
+// reduced polynomial seed (within an ulp or two; the hardware sine, about
+// 5e-7 absolute, is not accurate enough: solvent curves cancel to a few
+// percent of their vacuum terms at high q and would carry its error 30-fold);
+// s1, c1 = sin, cos(Δr) from short polynomials when the plan's largest step
+// angle is at most 0.25 rad (wide == 0), else from the reduced seed.  Then:
 //   lane A: s = S,                   d = S - sin(q0 r - 2Δr) = 2 s1 cos(q0 r - Δr)
 //   lane B: s = sin(q0 r + Δr),      d = sin(q0 r + Δr) - sin(q0 r - Δr) = 2 s1 C.
 __device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj, float wj, const float4& qp, int wide,
@@ -126,8 +125,7 @@ __device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj
   const float phi = fmaf(qp.x, r, qp.y * r);
   const float g = 2.0f * fmaf(qp.z, r, qp.w * r);  // Δr
   float S, C, s1, c1;
-  if (phi < 1.0f) sincos_small(phi, &S, &C);  // relative accuracy where sin(q0 r) is small
-  else sincos_seed_hw(phi, &S, &C);
+  sincos_seed(phi, &S, &C);
   if (wide) {
     sincos_seed(g, &s1, &c1);
   } else {
@@ -643,7 +641,8 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
 
 // Untuned choice of (Q, jb): the block length by a cost model (launched steps
 // of 3 FP32 ops each plus a per-pair seed of about 60 ops per block), and the
-// q-packed kernel with two chains where it is compiled for that length.
+// q-packed kernel where it is compiled for that length (one chain at Q = 128,
+// two below, the fastest on the 20k-atom config-2 workload).
 int2 default_variant(const std::vector<double>& q) {
   int bestQ = 64;
   long best_cost = -1;
@@ -654,7 +653,8 @@ int2 default_variant(const std::vector<double>& q) {
       bestQ = Qc;
     }
   }
-  const bool packed = bestQ == 64 || bestQ == 96 || bestQ == 128;
+  if (bestQ == 128) return make_int2(128, 1 + kPackedQ);
+  const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
 
@@ -718,7 +718,8 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   }
   if (!fp64) {
     P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
-    const int2 v = default_variant(P->q);
+    const int2 v = ctx->pair_variant ? make_int2(ctx->pair_variant / 16, ctx->pair_variant % 16)
+                                      : default_variant(P->q);
     configure_fp32(ctx, *P, v.x, v.y);
   } else {
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
@@ -769,7 +770,8 @@ std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout
   cudaStream_t s = ctx->stream;
   if (nq == 0 || L.n_tiles == 0) return P;
   P->d_atoms = upload(ctx, P->owned, (const float4*)L.atoms.data(), (size_t)L.n_pad, s);
-  const int2 v = default_variant(P->q);
+  const int2 v = ctx->pair_variant ? make_int2(ctx->pair_variant / 16, ctx->pair_variant % 16)
+                                    : default_variant(P->q);
   configure_fp32(ctx, *P, v.x, v.y);
   P->d_tile_type = upload(ctx, P->owned, L.tile_type.data(), L.tile_type.size(), s);
   P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)(P->segments.size() - 1) * P->n_pairs * nq, s);
@@ -880,10 +882,19 @@ void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bo
   out.T = L.T;
   out.nq = nq;
   out.self = L.self_w2;
-  std::unique_ptr<PairPlan> P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice);
+  std::unique_ptr<PairPlan> P;
+  {
+    TraceScope tp("make_pair_plan");
+    P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice);
+  }
   out.pair.assign((size_t)P->n_pairs * nq, 0.0);
-  pair_plan_launch(ctx, *P, ctx->stream, !fp64);
-  pair_plan_fetch(ctx, *P, out.pair.data(), !fp64);
+  {
+    TraceScope tr("pair_launch+fetch");
+    pair_plan_launch(ctx, *P, ctx->stream, !fp64);
+    pair_plan_fetch(ctx, *P, out.pair.data(), !fp64);
+  }
+  TraceScope td("pair_plan_free");
+  P.reset();
 }
 
 void quadratic_terms(const Partials& P, const double* X, const double* Y, double* out) {
@@ -948,12 +959,17 @@ static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2
                                      {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
                                      {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ}};
 
-void pair_plan_select(crab_ctx* ctx, PairPlan& P, int variant) {
-  require(!P.fp64, "the FP64 plan has a single kernel");
+bool pair_variant_known(int variant) {
   const int Q = variant / 16, jb = variant % 16;
   bool known = false;
   for (const auto& v : kLaunchable) known = known || (v[0] == Q && v[1] == jb);
-  require(known, "unknown kernel variant " + std::to_string(variant));
+  return known;
+}
+
+void pair_plan_select(crab_ctx* ctx, PairPlan& P, int variant) {
+  require(!P.fp64, "the FP64 plan has a single kernel");
+  const int Q = variant / 16, jb = variant % 16;
+  require(pair_variant_known(variant), "unknown kernel variant " + std::to_string(variant));
   if (P.nq == 0 || P.L.n_tiles == 0) return;
   configure_fp32(ctx, P, Q, jb);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));

@@ -84,16 +84,6 @@ __device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
   *c = ((qd + 1) & 2) ? -cc : cc;
 }
 
-// sin(x), cos(x) for 0 <= x < 2^22: reduction by 2π split into a 12-bit head
-// and a tail (k·head exact for k < 2^12 ... the product error stays below
-// ulp(x) for larger k), then the hardware sine and cosine on [-π, π].
-__device__ __forceinline__ void sincos_seed_hw(float x, float* s, float* c) {
-  const float k = rintf(x * 0x1.45f306p-3f);  // x/(2π)
-  float y = fmaf(-k, 0x1.92p+2f, x);          // 2π head (12 significant bits)
-  y = fmaf(-k, 0x1.fb54442ep-10f, y);         // 2π - head
-  __sincosf(y, s, c);
-}
-
 // Packed pair of FP32 values in one 64-bit register pair (Blackwell f32x2 ops).
 __device__ __forceinline__ unsigned long long pack2(float x, float y) {
   unsigned long long r;

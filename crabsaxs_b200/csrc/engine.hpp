@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -34,6 +36,24 @@ inline void require(bool ok, const std::string& msg) {
   if (!ok) throw Error(CRAB_EINVAL, msg);
 }
 
+// Host-phase tracing: with CRAB_TRACE=1 in the environment every TraceScope
+// prints "[crab] <name> <ms>" to stderr when it closes (wall time of the
+// phase, including the stream synchronisations inside it).
+bool trace_enabled();
+struct TraceScope {
+  const char* name;
+  bool on;
+  std::chrono::steady_clock::time_point t0;
+  explicit TraceScope(const char* n) : name(n), on(trace_enabled()) {
+    if (on) t0 = std::chrono::steady_clock::now();
+  }
+  ~TraceScope() {
+    if (on)
+      std::fprintf(stderr, "[crab] %s %.3f ms\n", name,
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
+
 // Grow-only device buffer: one per named slot in the context, so repeated
 // calls reuse memory instead of allocating.
 struct DevBuf {
@@ -62,6 +82,10 @@ struct crab_ctx {
   int64_t h2d_bytes = 0, d2h_bytes = 0;
   double last_pair_ms = 0.0;
   double last_pair_q = 0.0;
+  // device times of the last multipole call: all its kernels, the moment
+  // GEMM alone, and the GEMM's algorithmic FLOP count
+  double last_mp_ms = 0.0, last_mp_gemm_ms = 0.0, last_mp_gemm_flop = 0.0;
+  int pair_variant = 0;  // kernel variant of plans built by one-shot calls (0: automatic)
 
   void* dev(const std::string& name, size_t bytes);
   void* host(const std::string& name, size_t bytes);
@@ -206,6 +230,8 @@ void pair_plan_run_timed(crab_ctx* ctx, PairPlan& P, int repeats, int64_t flush_
 int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out, int capacity, int* n_out);
 // Fix the kernel variant (Q*16 + jb, as pair_plan_autotune reports it).
 void pair_plan_select(crab_ctx* ctx, PairPlan& P, int variant);
+// True when `variant` (Q*16 + jb) names a compiled FP32 pair kernel.
+bool pair_variant_known(int variant);
 double measure_fp32_peak(crab_ctx* ctx, double target_ms);
 
 // Quadratic form Σ_ij X_i Y_j sinc(q r_ij) for per-type amplitude tables

@@ -349,6 +349,7 @@ struct MpInput {
 
 // Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
 void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, double* out) {
+  TraceScope trace("multipole_run");
   const TypedAtoms& t = *in.t;
   const int T = t.T, K = in.K, P = K * (K + 1) / 2;
   const int64_t n = (int64_t)t.w.size();
@@ -408,6 +409,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
       std::memcpy(&ampg[((size_t)c * G + g) * nq], &in.amp[((size_t)c * T + g / S) * nq], sizeof(double) * nq);
   const std::vector<double> norms = harmonic_norms(L);
 
+  TraceScope tdev("multipole_device");
   cudaStream_t s = ctx->stream;
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
   double* d_pts = (double*)ctx->dev("mp_pts", sizeof(double) * pts.size());
@@ -437,18 +439,31 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   copy_h2d(ctx, d_gseg, gseg.data(), sizeof(int32_t) * G, s);
   CRAB_CUDA_CHECK(cudaMemsetAsync(d_M, 0, sizeof(double) * (size_t)G * kMaxNodes * lm_pad, s));
 
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } ev_guard{ev};
+  for (int i = 0; i < 4; ++i) CRAB_CUDA_CHECK(cudaEventCreate(&ev[i]));
+  CRAB_CUDA_CHECK(cudaEventRecord(ev[0], s));
   const unsigned prep_blocks = (unsigned)((n_pad + 127) / 128);
   if (fp64) {
     k_mp_prep<double><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                    (double*)d_YT, (double*)d_WT);
+    CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
                                                                 lm_pad, d_work, d_M);
   } else {
     k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                   (float*)d_YT, (float*)d_WT);
+    CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad, lm_pad,
                                                                d_work, d_M);
   }
+  CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
   k_mp_node_bessel<<<(unsigned)((nbess + 127) / 128), 128, 0, s>>>(d_q, d_lq, nq, d_nodes, n_nodes, L, d_Jn);
@@ -457,9 +472,16 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   else
     k_mp_gram<3><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
+  CRAB_CUDA_CHECK(cudaEventRecord(ev[3], s));
   ctx->launches += 4;
   copy_d2h(ctx, out, d_out, sizeof(double) * (size_t)P * nq, s);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  float total_ms = 0.0f, gemm_ms = 0.0f;
+  CRAB_CUDA_CHECK(cudaEventElapsedTime(&total_ms, ev[0], ev[3]));
+  CRAB_CUDA_CHECK(cudaEventElapsedTime(&gemm_ms, ev[1], ev[2]));
+  ctx->last_mp_ms = total_ms;
+  ctx->last_mp_gemm_ms = gemm_ms;
+  ctx->last_mp_gemm_flop = 2.0 * (double)lm_count * nb * (double)n;  // useful rows, nodes and points
 }
 
 bool multipole_precision(int precision) {
@@ -616,6 +638,14 @@ int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, in
                              int precision, double* out) {
   if (!ctx || !st || (nq > 0 && !out)) return CRAB_EINVAL;
   return guarded_impl(ctx, [&]() { multipole_intensity_impl(ctx, st, q, nq, l_max, implicit_hydrogen != 0, precision, out); });
+}
+int crab_multipole_last_timing(crab_ctx* ctx, double* total_ms, double* moments_ms, double* moments_flop) {
+  if (!ctx) return CRAB_EINVAL;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  if (total_ms) *total_ms = ctx->last_mp_ms;
+  if (moments_ms) *moments_ms = ctx->last_mp_gemm_ms;
+  if (moments_flop) *moments_flop = ctx->last_mp_gemm_flop;
+  return CRAB_OK;
 }
 int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                                  const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6) {

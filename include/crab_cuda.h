@@ -197,6 +197,10 @@ int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int
  * variants/ms (may be NULL), their count to *n_variants. */
 int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen, int32_t* variants, double* ms,
                             int32_t capacity, int32_t* n_variants);
+/* Kernel variant used by the plans that one-shot calls (Debye curves, bases,
+ * partials, ensembles) build on this context: a code as
+ * crab_pair_plan_autotune reports it, or 0 for the automatic choice. */
+int crab_ctx_set_pair_variant(crab_ctx* ctx, int32_t variant);
 /* Fix the kernel variant of an FP32 plan (a code as crab_pair_plan_autotune
  * reports it); CRAB_EINVAL for a variant that is not compiled. */
 int crab_pair_plan_select(crab_ctx* ctx, crab_pair_plan* plan, int32_t variant);
@@ -256,6 +260,11 @@ int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing,
  * precision: CRAB_PREC_*; tensor-core GEMM per l for TF32/BF16 modes. */
 int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                              int implicit_hydrogen, int precision, double* out);
+/* Device time of the last multipole call on this context: all its kernels
+ * (total_ms), the moment GEMM alone (moments_ms) and that GEMM's algorithmic
+ * FLOP count, 2 * (L+1)^2 * nodes * points (moments_flop).  Any pointer may
+ * be NULL. */
+int crab_multipole_last_timing(crab_ctx* ctx, double* total_ms, double* moments_ms, double* moments_flop);
 /* multipole_solvent_basis (spherical.rs:474-565), out6 [6][nq]. */
 int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                                  const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6);

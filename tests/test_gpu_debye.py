@@ -343,3 +343,27 @@ def test_every_kernel_variant_matches_fp64(engine, qkind):
         assert N.lib.crab_pair_plan_select(engine.handle, plan, 100 * 16 + 2) == N.EINVAL
     finally:
         N.lib.crab_pair_plan_destroy(plan)
+
+
+def test_every_kernel_variant_keeps_solvent_curve_parity(engine):
+    """Curve-level check of every variant through the public solvent-basis call:
+    with the adaptive grid the solvent curve cancels to a few percent of its
+    vacuum term at high q, which magnifies any per-pair error of the kernel."""
+    from crabsaxs_b200 import _native as N
+    from crabsaxs_b200 import synth
+
+    s = synth.protein(61, 4000, 22.0)
+    q = np.linspace(0.001, 0.5, 240)
+    c1, c2 = 0.976, 0.6
+    sp = cs.SolventParams(c1=c1, c2=c2, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                          hydration_grid_spacing_angstrom=3.0)
+    i64 = cs.combine_solvent_basis(cs.debye_solvent_basis(s, q, sp, engine=engine, fp64=True), q, c1, c2)
+    try:
+        for v in ALL_VARIANTS:
+            engine.check(N.lib.crab_ctx_set_pair_variant(engine.handle, v))
+            i32 = cs.combine_solvent_basis(cs.debye_solvent_basis(s, q, sp, engine=engine), q, c1, c2)
+            err = float(np.max(np.abs(i32 - i64) / np.abs(i64)))
+            assert err <= INTENSITY_RTOL, (v, err)
+        assert N.lib.crab_ctx_set_pair_variant(engine.handle, 100 * 16 + 2) == N.EINVAL
+    finally:
+        engine.check(N.lib.crab_ctx_set_pair_variant(engine.handle, 0))
