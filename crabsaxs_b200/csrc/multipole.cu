@@ -31,6 +31,7 @@
 #include <cstring>
 #include <vector>
 
+#include "device_math.cuh"
 #include "engine.hpp"
 #include "ops.hpp"
 
@@ -246,6 +247,239 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
     }
 }
 
+// ---- tensor-core moment GEMM (tcgen05, TF32 operands split into terms) ----
+//
+// The same product M[g][b][lm] += sum_k YT[lm][k] WT[b][k] for one 128 x 64
+// tile, on the 5th-generation tensor cores: each FP32 operand x is split into
+// TF32 terms x = h + m + l (round-to-nearest TF32 of x, of x - h, of x - h - m)
+// and the tile accumulates the products whose order is at most 2^-22:
+//   S = 1: h h'                        (TF32, relative error ~5e-4)
+//   S = 2: h h' + h m' + m h'          (~1e-6)
+//   S = 3: + h l' + m m' + l h'        (~1e-10, better than FP32 FMA)
+// Operands are staged by all 256 threads (global float4 loads, split, 16-byte
+// shared stores) into the K-major no-swizzle core-matrix layout: element
+// (row r, k) of a 32-wide K stage sits at (r/8)*1024 + (k/4)*128 + (r%8)*16 +
+// (k%4)*4 bytes (8-row core matrices of 16-byte rows; LBO 128 B between the
+// K-adjacent core matrices, SBO 1024 B between 8-row groups).  Thread 0 issues
+// tcgen05.mma (M = 128 lm rows, N = 64 nodes, K = 8 points) into a TMEM
+// accumulator and commits each stage to an mbarrier; two stages alternate.
+// The epilogue reads TMEM with tcgen05.ld (warp w: lanes 32(w%4).., columns
+// 32(w/4)..) and adds the tile into the f64 moments.  Every mbarrier wait is
+// bounded; on expiry the kernel flags CRAB_ETIMEOUT, waits (bounded) for its
+// own MMAs and frees its TMEM before returning.
+constexpr int kTcK = 32;                    // points per stage
+constexpr int kTcThreads = 256;
+constexpr int kTcTmemCols = 256;            // two 64-column accumulators used (headroom for the N field)
+constexpr int kTcChunk = 1;                 // stages accumulated in TMEM before the f64 drain
+constexpr int kTcABytes = kGemmM * kTcK * 4;     // 16 KB
+constexpr int kTcBBytes = kMaxNodes * kTcK * 4;  // 8 KB
+// TF32, FP32 accumulate, K-major A and B, N = 64 (bits 17-22, N>>3), M = 128 (bits 24-28, M>>4)
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;   // leading (K) byte offset
+  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;  // stride (8-row group) byte offset
+  d |= (uint64_t)1 << 46;                         // descriptor version for sm_100
+  return d;                                       // base offset 0, no swizzle
+}
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t u;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+  return __uint_as_float(u);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Split 4 values into S TF32 terms and store each term's 16-byte chunk.
+template <int S>
+__device__ __forceinline__ void tc_store_split(unsigned char* base, int part_bytes, int off, float4 v) {
+  float x[4] = {v.x, v.y, v.z, v.w};
+  float t[3][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float h = tf32_rna(x[i]);
+    t[0][i] = h;
+    if (S >= 2) {
+      const float r = x[i] - h;
+      const float m = tf32_rna(r);
+      t[1][i] = m;
+      if (S >= 3) t[2][i] = tf32_rna(r - m);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < S; ++p)
+    *reinterpret_cast<float4*>(base + p * part_bytes + off) = make_float4(t[p][0], t[p][1], t[p][2], t[p][3]);
+}
+
+template <int S>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_mp_moments_tc(const float* __restrict__ YT, const float* __restrict__ WT, int64_t n_pad, int lm_pad,
+                    const MpWork* __restrict__ work, double* __restrict__ M, int* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  // stage st: S A terms at st*stage_bytes, then S B terms
+  constexpr int stage_bytes = S * (kTcABytes + kTcBBytes);
+  unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
+  // barriers: 0, 1 stage buffers free; 2, 3 chunk accumulators complete;
+  // 4 all MMAs complete (error path)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * stage_bytes + kTcBBytes);  // after a B-sized gap
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const MpWork wk = work[blockIdx.x];
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 5; ++b) dev::mbar_init(&bars[b], 1);
+    dev::fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
+  const int nk = (int)((wk.k1 - wk.k0) / kTcK);
+  const int n_chunks = (nk + kTcChunk - 1) / kTcChunk;
+  const int quarter = warp & 3, half = warp >> 2;
+  bool ok = true;
+  double acc[32];  // this thread's row (lm) and 32 of the 64 node columns, in f64
+#pragma unroll
+  for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+  // Add chunk c's TMEM accumulator (columns 64 (c % 2) ..) into acc once its
+  // MMAs are complete.  Collective over the CTA (uniform ok).
+  auto drain = [&](int c) {
+    if (!dev::mbar_wait(&bars[2 + (c & 1)], (unsigned)((c >> 1) & 1))) ok = false;
+    ok = __syncthreads_and(ok);
+    if (!ok) return;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int c16 = 0; c16 < 2; ++c16) {
+      float v[16];
+      const uint32_t col = (uint32_t)((c & 1) * 64 + half * 32 + c16 * 16);
+      tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + col, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  };
+  // register prefetch of a stage: A rows (4 float4 per thread), B rows (2)
+  float4 ra[4], rb[2];
+  auto fetch = [&](int s) {
+    const int64_t k0 = wk.k0 + (int64_t)s * kTcK;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
+      ra[it] = *reinterpret_cast<const float4*>(YT + (int64_t)(wk.lm0 + row) * n_pad + k0 + c4 * 4);
+    }
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
+      rb[it] = *reinterpret_cast<const float4*>(WT + (int64_t)row * n_pad + k0 + c4 * 4);
+    }
+  };
+  if (nk > 0) fetch(0);
+  int drained = 0;  // chunks added into acc
+  for (int s = 0; s < nk && ok; ++s) {
+    const int st = s & 1, chunk = s / kTcChunk, first = (s % kTcChunk) == 0;
+    const int last = (s % kTcChunk) == kTcChunk - 1 || s == nk - 1;
+    if (s >= 2 && !dev::mbar_wait(&bars[st], (unsigned)(((s - 2) >> 1) & 1))) ok = false;
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    unsigned char* sa = smem + st * stage_bytes;
+    unsigned char* sb = sa + S * kTcABytes;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
+      tc_store_split<S>(sa, kTcABytes, (row >> 3) * 1024 + c4 * 128 + (row & 7) * 16, ra[it]);
+    }
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
+      tc_store_split<S>(sb, kTcBBytes, (row >> 3) * 1024 + c4 * 128 + (row & 7) * 16, rb[it]);
+    }
+    if (s + 1 < nk) fetch(s + 1);  // global loads of the next stage overlap the MMAs of this one
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_base + st * stage_bytes, b0 = a0 + S * kTcABytes;
+      const uint32_t d = tmem + (uint32_t)((chunk & 1) * 64);
+      // (A term, B term) pairs of order <= 2^-22
+      constexpr int np = S == 1 ? 1 : (S == 2 ? 3 : 6);
+      const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+#pragma unroll
+      for (int kk = 0; kk < kTcK / 8; ++kk)
+#pragma unroll
+        for (int p = 0; p < np; ++p) {
+          const uint64_t ad = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 256);
+          const uint64_t bd = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 256);
+          tc_mma(d, ad, bd, (!first || kk || p) ? 1u : 0u);
+        }
+      tc_commit(&bars[st]);
+      if (last) tc_commit(&bars[2 + (chunk & 1)]);
+    }
+    // with the next chunk's first MMAs queued, add the previous chunk
+    if (first && chunk > 0) {
+      drain(chunk - 1);
+      ++drained;
+    }
+  }
+  if (ok && drained < n_chunks) drain(n_chunks - 1);
+  if (ok && nk > 0) {
+    const int row = quarter * 32 + lane;
+    double* Mg = M + (int64_t)wk.group * kMaxNodes * lm_pad + wk.lm0 + row;
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if (acc[i] != 0.0) atomicAdd(Mg + (int64_t)(half * 32 + i) * lm_pad, acc[i]);
+  }
+  if (!ok) {
+    // bounded wait for every MMA this CTA issued before freeing TMEM
+    if (tid == 0) {
+      tc_commit(&bars[4]);
+      atomicExch(status, CRAB_ETIMEOUT);
+    }
+    dev::mbar_wait(&bars[4], 0);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+}
+
+// Dynamic shared memory of one CTA; at least 80 KB so that at most two CTAs
+// (2 x 256 TMEM columns) share an SM and tcgen05.alloc never has to wait.
+template <int S>
+constexpr size_t tc_smem_bytes() {
+  const size_t need = 1024 /* alignment slack */ + 2 * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ + 64;
+  return need > 80 * 1024 ? need : 80 * 1024;
+}
+
 // j_0..j_{l_q}(q rho) at every node (spherical.rs:95-133, f64 as the
 // reference), zero for l_q < l <= L.  Jn[k][s*nb + b][l].
 __global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __restrict__ lq, int64_t nq,
@@ -348,7 +582,10 @@ struct MpInput {
 };
 
 // Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
-void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, double* out) {
+// tc_terms: 0 = SIMT GEMM (FP32 or FP64 operands), 1..3 = tensor-core GEMM
+// with that many TF32 terms per operand (FP32 operands).
+void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, int tc_terms,
+                   double* out) {
   TraceScope trace("multipole_run");
   const TypedAtoms& t = *in.t;
   const int T = t.T, K = in.K, P = K * (K + 1) / 2;
@@ -427,6 +664,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * ampg.size());
   int32_t* d_gseg = (int32_t*)ctx->dev("mp_gseg", sizeof(int32_t) * G);
   double* d_out = (double*)ctx->dev("mp_out", sizeof(double) * (size_t)P * nq);
+  int* d_status = (int*)ctx->dev("mp_status", sizeof(int));
   copy_h2d(ctx, d_pts, pts.data(), sizeof(double) * pts.size(), s);
   copy_h2d(ctx, d_seg, seg.data(), sizeof(int32_t) * n_pad, s);
   copy_h2d(ctx, d_norms, norms.data(), sizeof(double) * norms.size(), s);
@@ -437,6 +675,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   copy_h2d(ctx, d_lq, lq.data(), sizeof(int32_t) * nq, s);
   copy_h2d(ctx, d_amp, ampg.data(), sizeof(double) * ampg.size(), s);
   copy_h2d(ctx, d_gseg, gseg.data(), sizeof(int32_t) * G, s);
+  CRAB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
   CRAB_CUDA_CHECK(cudaMemsetAsync(d_M, 0, sizeof(double) * (size_t)G * kMaxNodes * lm_pad, s));
 
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -460,8 +699,22 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                   (float*)d_YT, (float*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
-    k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad, lm_pad,
-                                                               d_work, d_M);
+    if (tc_terms == 0) {
+      k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad,
+                                                                 lm_pad, d_work, d_M);
+    } else {
+#define CRAB_TC(SS)                                                                                               \
+  if (tc_terms == SS) {                                                                                           \
+    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_tc<SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                                         (int)tc_smem_bytes<SS>()));                                              \
+    k_mp_moments_tc<SS><<<(unsigned)work.size(), kTcThreads, tc_smem_bytes<SS>(), s>>>(                           \
+        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_M, d_status);                            \
+  }
+      CRAB_TC(1)
+      CRAB_TC(2)
+      CRAB_TC(3)
+#undef CRAB_TC
+    }
   }
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   const int n_nodes = S * nb;
@@ -475,7 +728,10 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   CRAB_CUDA_CHECK(cudaEventRecord(ev[3], s));
   ctx->launches += 4;
   copy_d2h(ctx, out, d_out, sizeof(double) * (size_t)P * nq, s);
+  int status = 0;
+  if (tc_terms) copy_d2h(ctx, &status, d_status, sizeof(int), s);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
   float total_ms = 0.0f, gemm_ms = 0.0f;
   CRAB_CUDA_CHECK(cudaEventElapsedTime(&total_ms, ev[0], ev[3]));
   CRAB_CUDA_CHECK(cudaEventElapsedTime(&gemm_ms, ev[1], ev[2]));
@@ -484,10 +740,21 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   ctx->last_mp_gemm_flop = 2.0 * (double)lm_count * nb * (double)n;  // useful rows, nodes and points
 }
 
-bool multipole_precision(int precision) {
-  if (precision == CRAB_PREC_FP64) return true;
-  if (precision == CRAB_PREC_FP32) return false;
-  throw Error(CRAB_EINVAL, "multipole precision must be CRAB_PREC_FP64 or CRAB_PREC_FP32");
+// (fp64 operands, tensor-core TF32 terms) of a precision mode.
+struct MpPrecision {
+  bool fp64;
+  int tc_terms;
+};
+MpPrecision multipole_precision(int precision) {
+  switch (precision) {
+    case CRAB_PREC_FP64: return {true, 0};
+    case CRAB_PREC_FP32: return {false, 0};
+    case CRAB_PREC_TF32: return {false, 1};
+    case CRAB_PREC_TF32_SPLIT: return {false, 2};
+    case CRAB_PREC_TF32_SPLIT3: return {false, 3};
+    default:
+      throw Error(CRAB_EINVAL, "multipole precision must be FP64, FP32, TF32, TF32_SPLIT or TF32_SPLIT3");
+  }
 }
 
 void validate_multipole(const crab_struct* st, const double* q, int64_t nq, int l_max) {
@@ -561,7 +828,7 @@ void solvent_setup(crab_ctx* ctx, const crab_struct* st, const double* q, int64_
 void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
                               bool implicit, int precision, double* out) {
   validate_multipole(st, q, nq, l_max);
-  const bool fp64 = multipole_precision(precision);
+  const MpPrecision mp = multipole_precision(precision);
   if (st->n == 0) {
     std::fill(out, out + nq, 0.0);
     return;
@@ -576,7 +843,7 @@ void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double
   multipole_tables(t, q, nq, nullptr, implicit, 0.0, V, E, H);
   in.amp = V;
   in.K = 1;
-  multipole_run(ctx, in, q, nq, l_max, fp64, out);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
 
@@ -584,7 +851,7 @@ void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const do
                                   const crab_solvent& s, bool implicit, int precision, double* out6) {
   validate_multipole(st, q, nq, l_max);
   validate_solvent(s);
-  const bool fp64 = multipole_precision(precision);
+  const MpPrecision mp = multipole_precision(precision);
   if (st->n == 0) {
     std::fill(out6, out6 + 6 * nq, 0.0);
     return;
@@ -600,14 +867,14 @@ void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const do
   in.amp.insert(in.amp.end(), u.V.begin(), u.V.end());
   in.amp.insert(in.amp.end(), u.E.begin(), u.E.end());
   in.amp.insert(in.amp.end(), u.H.begin(), u.H.end());
-  multipole_run(ctx, in, q, nq, l_max, fp64, out6);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out6);
 }
 
 void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
                                       const crab_solvent& s, bool implicit, int precision, double* out) {
   validate_multipole(st, q, nq, l_max);
   validate_solvent(s);
-  const bool fp64 = multipole_precision(precision);
+  const MpPrecision mp = multipole_precision(precision);
   if (st->n == 0) {
     std::fill(out, out + nq, 0.0);
     return;
@@ -626,7 +893,7 @@ void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, cons
       const size_t o = (size_t)a * nq + k;
       in.amp[o] = u.V[o] - excluded_volume_scale(q[k], s.c1) * u.E[o] + s.c2 * u.H[o];
     }
-  multipole_run(ctx, in, q, nq, l_max, fp64, out);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
 

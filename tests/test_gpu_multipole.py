@@ -163,3 +163,43 @@ def test_empty_structure_and_invalid_arguments(engine):
         cs.multipole_intensity(s, q, 16, precision=N.PREC_BF16, engine=engine)
     with pytest.raises(cs.InvalidInput):
         cs.multipole_intensity(s, np.array([0.1, -0.2]), 16, engine=engine)
+
+
+# Tensor-core moment GEMM (tcgen05): TF32 operands split into 1, 2 or 3 terms.
+TC_MODES = [(N.PREC_TF32_SPLIT3, FP32_RTOL), (N.PREC_TF32_SPLIT, FP32_RTOL), (N.PREC_TF32, 5e-3)]
+
+
+@pytest.mark.parametrize("prec,tol", TC_MODES)
+def test_tensor_core_moments_match_oracle(engine, prec, tol):
+    xyz, el = helix96()
+    s = cs.Structure(xyz, el)
+    q = np.concatenate([[0.0], np.arange(1, 101) * 0.005])
+    ref = O.multipole_intensity(_oracle_atoms(s), q, 32)
+    got = cs.multipole_intensity(s, q, 32, precision=prec, engine=engine)
+    assert _rel(got, ref) <= tol
+    big = synth.protein(32, 3000, 20.0)
+    q2 = np.linspace(0.001, 0.5, 150)
+    ref2 = O.multipole_intensity(_oracle_atoms(big), q2, 30)
+    got2 = cs.multipole_intensity(big, q2, 30, precision=prec, engine=engine)
+    assert _rel(got2, ref2) <= tol
+
+
+def test_tensor_core_split3_matches_fp64_on_config3(engine):
+    """100,000 atoms, 1000 q, L = 50: the three-term TF32 GEMM against the FP64
+    device path (tighter than FP32: 2e-6), and the solvent basis on a grid."""
+    w = synth.CONFIG3
+    s = synth.protein(w.seed, w.n_atoms, w.radius)
+    got = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_TF32_SPLIT3, engine=engine)
+    ref = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_FP64, engine=engine)
+    assert _rel(got, ref) <= 2e-6
+    s2 = synth.protein(36, 2000, 16.0)
+    q = np.linspace(0.01, 0.5, 80)
+    p = cs.SolventParams(c1=1.01, c2=0.9, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                         hydration_grid_spacing_angstrom=3.0)
+    b64 = cs.multipole_solvent_basis(s2, q, 28, p, precision=N.PREC_FP64, engine=engine)
+    btc = cs.multipole_solvent_basis(s2, q, 28, p, precision=N.PREC_TF32_SPLIT3, engine=engine)
+    for k in range(6):
+        assert np.max(np.abs(btc[k] - b64[k])) / np.max(np.abs(b64[k])) <= 1e-6, k
+    i64 = cs.combine_solvent_basis(b64, q, p.c1, p.c2)
+    itc = cs.combine_solvent_basis(btc, q, p.c1, p.c2)
+    assert _rel(itc, i64) <= FP32_RTOL
