@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ETIMEOUT", 5:
 
 HYD_ANALYTIC, HYD_GRID, HYD_ADAPTIVE = 0, 1, 2
 METHOD_AUTO, METHOD_DEBYE, METHOD_MULTIPOLE = 0, 1, 2
-PREC_FP64, PREC_TF32, PREC_BF16, PREC_BF16_SPLIT, PREC_TF32_SPLIT, PREC_FP32, PREC_TF32_SPLIT3 = 0, 1, 2, 3, 4, 5, 6
+PREC_FP64, PREC_TF32, PREC_BF16, PREC_BF16_SPLIT, PREC_TF32_SPLIT, PREC_FP32 = 0, 1, 2, 3, 4, 5
 SCALE_FIT, SCALE_FIXED = 0, 1
 BG_FIT, BG_FIXED_ZERO, BG_FIXED = 0, 1, 2
 

@@ -95,5 +95,21 @@ __device__ __forceinline__ void unpack2(unsigned long long v, float& x, float& y
 }
 
 
+// Bounded spin on an mbarrier phase with the non-suspending test_wait (for
+// waits expected to be short, where a suspended try_wait would oversleep).
+__device__ __forceinline__ bool mbar_spin(uint64_t* bar, unsigned phase) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (int it = 0; it < (1 << 26); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 }  // namespace dev
 }  // namespace crab

@@ -45,6 +45,7 @@ constexpr int kMaxSegments = 16;
 constexpr int kGemmM = 128;         // lm rows per GEMM tile
 constexpr int kPointAlign = 32;     // group padding (GEMM K step for FP32)
 constexpr int64_t kSplitK = 4096;   // points per GEMM work item
+constexpr int kTileElems = kGemmM * kMaxNodes;  // one partial tile
 
 // spherical.rs:201-203
 int adaptive_l(double q, double max_radius, int maximum) {
@@ -114,6 +115,13 @@ struct MpWork {
 
 // ------------------------------------------------------------------ kernels
 
+// Operand layout of the moment GEMM: rows (lm or node) by points, blocked by
+// 32 points so that a 32-point stage of a row tile is one contiguous block:
+// element (row, k) at ((k / 32) * rows + row) * 32 + k % 32.
+__host__ __device__ __forceinline__ int64_t mp_blocked(int row, int64_t k, int rows) {
+  return ((k >> 5) * rows + row) * 32 + (k & 31);
+}
+
 // Per point: real harmonics (spherical.rs:54-93, 165-199) and the weighted
 // Lagrange basis of its radial segment.  pts: x, y, z (centred), w, r.
 template <typename E>
@@ -139,11 +147,11 @@ __global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restr
   auto emit = [&](int l, int m, double p) {
     const int pos = l * l + l + m;
     if (m == 0) {
-      YT[(int64_t)pos * n_pad + i] = (E)__dmul_rn(norms[pos], p);
+      YT[mp_blocked(pos, i, lm_pad)] = (E)__dmul_rn(norms[pos], p);
     } else {
       const double v = __dmul_rn(__dmul_rn(sqrt2, norms[pos]), p);
-      YT[(int64_t)pos * n_pad + i] = (E)__dmul_rn(v, cos_m);
-      YT[(int64_t)(l * l + l - m) * n_pad + i] = (E)__dmul_rn(v, sin_m);
+      YT[mp_blocked(pos, i, lm_pad)] = (E)__dmul_rn(v, cos_m);
+      YT[mp_blocked(l * l + l - m, i, lm_pad)] = (E)__dmul_rn(v, sin_m);
     }
   };
   for (int m = 0; m <= L; ++m) {
@@ -166,7 +174,7 @@ __global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restr
       cur = next;
     }
   }
-  for (int pos = (L + 1) * (L + 1); pos < lm_pad; ++pos) YT[(int64_t)pos * n_pad + i] = (E)0;
+  for (int pos = (L + 1) * (L + 1); pos < lm_pad; ++pos) YT[mp_blocked(pos, i, lm_pad)] = (E)0;
   // Barycentric Lagrange basis at the segment's first-kind Chebyshev nodes.
   const double* nd = nodes + (int64_t)seg[i] * nb;
   int hit = -1;
@@ -182,17 +190,18 @@ __global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restr
       if (hit >= 0) v = (b == hit) ? w : 0.0;
       else v = w * ((bary[b] / (r - nd[b])) / den);
     }
-    WT[(int64_t)b * n_pad + i] = (E)v;
+    WT[mp_blocked(b, i, kMaxNodes)] = (E)v;
   }
 }
 
-// M[g][b][lm] += sum_{k in [k0, k1)} YT[lm][k] WT[b][k] for one 128 x 64 tile.
+// Partial tile of work item w: part[w][b][r] = sum_{k in [k0, k1)} YT[lm0 + r][k] WT[b][k]
+// (128 lm rows x 64 nodes, plain stores; k_mp_reduce sums the point splits).
 // 256 threads, 8 x 4 outputs each; operands staged through shared memory in
 // 128-byte rows (32 floats or 16 doubles of K per step).
 template <typename E>
 __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, const E* __restrict__ WT, int64_t n_pad,
                                                     int lm_pad, const MpWork* __restrict__ work,
-                                                    double* __restrict__ M) {
+                                                    double* __restrict__ part) {
   constexpr int KS = 128 / sizeof(E);
   constexpr int V = 16 / sizeof(E);
   typedef typename std::conditional<sizeof(E) == 4, float4, double2>::type Vec;
@@ -209,7 +218,7 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 #pragma unroll
     for (int it = 0; it < 4; ++it) {  // A: 128 rows x 8 vectors
       const int idx = it * 256 + tid, row = idx >> 3, c = (idx & 7) * V;
-      const Vec v = *reinterpret_cast<const Vec*>(YT + (int64_t)(wk.lm0 + row) * n_pad + k0 + c);
+      const Vec v = *reinterpret_cast<const Vec*>(YT + mp_blocked(wk.lm0 + row, k0 + c, lm_pad));
       const E* pv = reinterpret_cast<const E*>(&v);
 #pragma unroll
       for (int j = 0; j < V; ++j) As[c + j][row] = pv[j];
@@ -217,7 +226,7 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 #pragma unroll
     for (int it = 0; it < 2; ++it) {  // B: 64 rows x 8 vectors
       const int idx = it * 256 + tid, row = idx >> 3, c = (idx & 7) * V;
-      const Vec v = *reinterpret_cast<const Vec*>(WT + (int64_t)row * n_pad + k0 + c);
+      const Vec v = *reinterpret_cast<const Vec*>(WT + mp_blocked(row, k0 + c, kMaxNodes));
       const E* pv = reinterpret_cast<const E*>(&v);
 #pragma unroll
       for (int j = 0; j < V; ++j) Bs[c + j][row] = pv[j];
@@ -237,51 +246,56 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
     }
     __syncthreads();
   }
-  double* Mg = M + (int64_t)wk.group * kMaxNodes * lm_pad;
+  double* tile = part + (int64_t)blockIdx.x * kTileElems;
 #pragma unroll
   for (int x = 0; x < 8; ++x)
 #pragma unroll
-    for (int y = 0; y < 4; ++y) {
-      const double v = (double)acc[x][y];
-      if (v != 0.0) atomicAdd(Mg + (int64_t)(tn * 4 + y) * lm_pad + wk.lm0 + tm * 8 + x, v);
-    }
+    for (int y = 0; y < 4; ++y) tile[(tn * 4 + y) * kGemmM + tm * 8 + x] = (double)acc[x][y];
 }
 
 // ---- tensor-core moment GEMM (tcgen05, TF32 operands split into terms) ----
 //
 // The same product M[g][b][lm] += sum_k YT[lm][k] WT[b][k] for one 128 x 64
-// tile, on the 5th-generation tensor cores: each FP32 operand x is split into
-// TF32 terms x = h + m + l (round-to-nearest TF32 of x, of x - h, of x - h - m)
-// and the tile accumulates the products whose order is at most 2^-22:
-//   S = 1: h h'                        (TF32, relative error ~5e-4)
-//   S = 2: h h' + h m' + m h'          (~1e-6)
-//   S = 3: + h l' + m m' + l h'        (~1e-10, better than FP32 FMA)
-// Operands are staged by all 256 threads (global float4 loads, split, 16-byte
-// shared stores) into the K-major no-swizzle core-matrix layout: element
-// (row r, k) of a 32-wide K stage sits at (r/8)*1024 + (k/4)*128 + (r%8)*16 +
-// (k%4)*4 bytes (8-row core matrices of 16-byte rows; LBO 128 B between the
-// K-adjacent core matrices, SBO 1024 B between 8-row groups).  Thread 0 issues
-// tcgen05.mma (M = 128 lm rows, N = 64 nodes, K = 8 points) into a TMEM
-// accumulator and commits each stage to an mbarrier; two stages alternate.
-// The epilogue reads TMEM with tcgen05.ld (warp w: lanes 32(w%4).., columns
-// 32(w/4)..) and adds the tile into the f64 moments.  Every mbarrier wait is
-// bounded; on expiry the kernel flags CRAB_ETIMEOUT, waits (bounded) for its
-// own MMAs and frees its TMEM before returning.
+// tile, on the 5th-generation tensor cores.  Each FP32 operand x is split
+// into TF32 terms (h = x rounded to TF32, m = x - h rounded to TF32):
+//   S = 1: h h'                  (TF32, relative error ~5e-4)
+//   S = 2: h h' + h m' + m h'    (relative error ~5e-7)
+// The S = 2 error is set by the tensor core's FP32 accumulation, which rounds
+// toward zero (about 2^-24 of the accumulator per MMA); a third TF32 term
+// would not lower it.  To keep that bias small the TMEM accumulator covers one
+// 32-point stage only and is then drained into f64 registers.
+// Data path per stage: every thread copies its six 16-byte chunks of the
+// FP32 tiles (A: 128 lm rows x 32 points, B: 64 nodes x 32) from global
+// memory with cp.async into a private slot of a 3-deep ring, three stages
+// ahead; it reads them back, splits them and stores the terms in the K-major
+// 128-byte-swizzled layout: row r of a term tile is the 128-byte line at
+// (r/8)*1024 + (r%8)*128, its 16-byte chunk c at position c ^ (r%8)
+// (SBO 1024 B).  Thread 0 issues tcgen05.mma (M = 128, N = 64, K = 8; the K
+// step advances the descriptor start by 32 B) into the stage's TMEM
+// accumulator and commits it to the stage's mbarrier.  Term buffers and
+// accumulators are three deep: stage s is drained during stage s + 2, so the
+// MMAs of a stage have two stages of staging work to complete behind.  Every
+// mbarrier wait is bounded; on expiry the kernel flags CRAB_ETIMEOUT, waits
+// (bounded) for its own MMAs and frees its TMEM before returning.
 constexpr int kTcK = 32;                    // points per stage
 constexpr int kTcThreads = 256;
-constexpr int kTcTmemCols = 256;            // two 64-column accumulators used (headroom for the N field)
-constexpr int kTcChunk = 1;                 // stages accumulated in TMEM before the f64 drain
+constexpr int kTcDepth = 3;                 // term buffers and TMEM accumulators
+constexpr int kTcTmemCols = 256;            // three 64-column accumulators used
+constexpr int kTcRing = 3;                  // raw FP32 stages in flight per thread
+constexpr int kTcChunks = 6;                // 16-byte chunks per thread per stage (4 of A, 2 of B)
 constexpr int kTcABytes = kGemmM * kTcK * 4;     // 16 KB
 constexpr int kTcBBytes = kMaxNodes * kTcK * 4;  // 8 KB
+constexpr int kTcRingBytes = kTcRing * kTcThreads * kTcChunks * 16;  // 72 KB
 // TF32, FP32 accumulate, K-major A and B, N = 64 (bits 17-22, N>>3), M = 128 (bits 24-28, M>>4)
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;   // leading (K) byte offset
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
   d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;  // stride (8-row group) byte offset
   d |= (uint64_t)1 << 46;                         // descriptor version for sm_100
-  return d;                                       // base offset 0, no swizzle
+  d |= (uint64_t)2 << 61;                         // 128-byte swizzle
+  return d;
 }
 __device__ __forceinline__ float tf32_rna(float x) {
   uint32_t u;
@@ -311,40 +325,50 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Split 4 values into S TF32 terms and store each term's 16-byte chunk.
 template <int S>
 __device__ __forceinline__ void tc_store_split(unsigned char* base, int part_bytes, int off, float4 v) {
-  float x[4] = {v.x, v.y, v.z, v.w};
-  float t[3][4];
+  const float x[4] = {v.x, v.y, v.z, v.w};
+  float t[2][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const float h = tf32_rna(x[i]);
-    t[0][i] = h;
-    if (S >= 2) {
-      const float r = x[i] - h;
-      const float m = tf32_rna(r);
-      t[1][i] = m;
-      if (S >= 3) t[2][i] = tf32_rna(r - m);
-    }
+    t[0][i] = tf32_rna(x[i]);
+    if (S >= 2) t[1][i] = tf32_rna(x[i] - t[0][i]);
   }
 #pragma unroll
   for (int p = 0; p < S; ++p)
     *reinterpret_cast<float4*>(base + p * part_bytes + off) = make_float4(t[p][0], t[p][1], t[p][2], t[p][3]);
 }
 
+// Chunk c of this thread in a stage: rows of A (c < 4) or B, 16-byte column c4.
+__device__ __forceinline__ void tc_chunk(int c, int tid, int& row, int& c4) {
+  const int idx = (c < 4 ? c : c - 4) * kTcThreads + tid;
+  row = idx >> 3;
+  c4 = idx & 7;
+}
+
 template <int S>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_mp_moments_tc(const float* __restrict__ YT, const float* __restrict__ WT, int64_t n_pad, int lm_pad,
-                    const MpWork* __restrict__ work, double* __restrict__ M, int* __restrict__ status) {
+                    const MpWork* __restrict__ work, double* __restrict__ part, int* __restrict__ status) {
+  static_assert(S == 1 || S == 2, "one or two TF32 terms");
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  // stage st: S A terms at st*stage_bytes, then S B terms
-  constexpr int stage_bytes = S * (kTcABytes + kTcBBytes);
+  // term buffers: slot d holds S A terms then S B terms; then the raw ring
+  constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);
   unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
-  // barriers: 0, 1 stage buffers free; 2, 3 chunk accumulators complete;
-  // 4 all MMAs complete (error path)
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * stage_bytes + kTcBBytes);  // after a B-sized gap
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  unsigned char* ring = smem + kTcDepth * slot_bytes + kTcBBytes;  // after a B-sized gap
+  // barriers: 0..2 stage MMAs complete (per slot); 3 all MMAs complete (error path)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kTcRingBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kTcDepth + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const MpWork wk = work[blockIdx.x];
   if (warp == 0) {
@@ -354,7 +378,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int b = 0; b < 5; ++b) dev::mbar_init(&bars[b], 1);
+    for (int b = 0; b <= kTcDepth; ++b) dev::mbar_init(&bars[b], 1);
     dev::fence_mbar_init();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -362,109 +386,104 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
+  const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
   const int nk = (int)((wk.k1 - wk.k0) / kTcK);
-  const int n_chunks = (nk + kTcChunk - 1) / kTcChunk;
   const int quarter = warp & 3, half = warp >> 2;
   bool ok = true;
   double acc[32];  // this thread's row (lm) and 32 of the 64 node columns, in f64
 #pragma unroll
   for (int i = 0; i < 32; ++i) acc[i] = 0.0;
-  // Add chunk c's TMEM accumulator (columns 64 (c % 2) ..) into acc once its
-  // MMAs are complete.  Collective over the CTA (uniform ok).
-  auto drain = [&](int c) {
-    if (!dev::mbar_wait(&bars[2 + (c & 1)], (unsigned)((c >> 1) & 1))) ok = false;
+  // Add stage s's TMEM accumulator into acc once its MMAs are complete; this
+  // also frees slot s % kTcDepth.  Collective over the CTA (uniform ok).
+  auto drain = [&](int s) {
+    const int d = s % kTcDepth;
+    if (!dev::mbar_spin(&bars[d], (unsigned)((s / kTcDepth) & 1))) ok = false;
     ok = __syncthreads_and(ok);
     if (!ok) return;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
     for (int c16 = 0; c16 < 2; ++c16) {
       float v[16];
-      const uint32_t col = (uint32_t)((c & 1) * 64 + half * 32 + c16 * 16);
+      const uint32_t col = (uint32_t)(d * 64 + half * 32 + c16 * 16);
       tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + col, v);
 #pragma unroll
       for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   };
-  // register prefetch of a stage: A rows (4 float4 per thread), B rows (2)
-  float4 ra[4], rb[2];
-  auto fetch = [&](int s) {
-    const int64_t k0 = wk.k0 + (int64_t)s * kTcK;
+  // this thread's chunks of stage s into ring slot s % kTcRing
+  auto issue = [&](int s) {
+    if (s < nk) {
+      const int64_t k0 = wk.k0 + (int64_t)s * kTcK;
+      const uint32_t slot = ring_base + (uint32_t)(((s % kTcRing) * kTcThreads + tid) * kTcChunks * 16);
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
-      ra[it] = *reinterpret_cast<const float4*>(YT + (int64_t)(wk.lm0 + row) * n_pad + k0 + c4 * 4);
+      for (int c = 0; c < kTcChunks; ++c) {
+        int row, c4;
+        tc_chunk(c, tid, row, c4);
+        const float* src = c < 4 ? YT + mp_blocked(wk.lm0 + row, k0 + c4 * 4, lm_pad)
+                                 : WT + mp_blocked(row, k0 + c4 * 4, kMaxNodes);
+        cp_async16(slot + c * 16, src);
+      }
     }
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
-      rb[it] = *reinterpret_cast<const float4*>(WT + (int64_t)row * n_pad + k0 + c4 * 4);
-    }
+    cp_async_commit();  // one group per stage, empty past the end
   };
-  if (nk > 0) fetch(0);
-  int drained = 0;  // chunks added into acc
+#pragma unroll
+  for (int s = 0; s < kTcRing; ++s) issue(s);
   for (int s = 0; s < nk && ok; ++s) {
-    const int st = s & 1, chunk = s / kTcChunk, first = (s % kTcChunk) == 0;
-    const int last = (s % kTcChunk) == kTcChunk - 1 || s == nk - 1;
-    if (s >= 2 && !dev::mbar_wait(&bars[st], (unsigned)(((s - 2) >> 1) & 1))) ok = false;
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    unsigned char* sa = smem + st * stage_bytes;
+    const int d = s % kTcDepth;
+    cp_async_wait<kTcRing - 1>();  // this thread's chunks of stage s have landed
+    const float4* mine = reinterpret_cast<const float4*>(ring + ((s % kTcRing) * kTcThreads + tid) * kTcChunks * 16);
+    float4 raw[kTcChunks];
+#pragma unroll
+    for (int c = 0; c < kTcChunks; ++c) raw[c] = mine[c];
+    issue(s + kTcRing);  // the slot just read is refilled three stages ahead
+    // slot d was last used by stage s - 3, drained during stage s - 1
+    unsigned char* sa = smem + d * slot_bytes;
     unsigned char* sb = sa + S * kTcABytes;
 #pragma unroll
-    for (int it = 0; it < 4; ++it) {
-      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
-      tc_store_split<S>(sa, kTcABytes, (row >> 3) * 1024 + c4 * 128 + (row & 7) * 16, ra[it]);
+    for (int c = 0; c < kTcChunks; ++c) {
+      int row, c4;
+      tc_chunk(c, tid, row, c4);
+      const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c4 ^ (row & 7)) << 4);
+      if (c < 4) tc_store_split<S>(sa, kTcABytes, off, raw[c]);
+      else tc_store_split<S>(sb, kTcBBytes, off, raw[c]);
     }
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-      const int idx = it * kTcThreads + tid, row = idx >> 3, c4 = idx & 7;
-      tc_store_split<S>(sb, kTcBBytes, (row >> 3) * 1024 + c4 * 128 + (row & 7) * 16, rb[it]);
-    }
-    if (s + 1 < nk) fetch(s + 1);  // global loads of the next stage overlap the MMAs of this one
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_base + st * stage_bytes, b0 = a0 + S * kTcABytes;
-      const uint32_t d = tmem + (uint32_t)((chunk & 1) * 64);
-      // (A term, B term) pairs of order <= 2^-22
-      constexpr int np = S == 1 ? 1 : (S == 2 ? 3 : 6);
-      const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+      const uint32_t a0 = smem_base + d * slot_bytes, b0 = a0 + S * kTcABytes;
+      const uint32_t acc_cols = tmem + (uint32_t)(d * 64);
+      // (A term, B term) pairs: hh', hm', mh'
+      constexpr int np = S == 1 ? 1 : 3;
+      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
 #pragma unroll
       for (int kk = 0; kk < kTcK / 8; ++kk)
 #pragma unroll
         for (int p = 0; p < np; ++p) {
-          const uint64_t ad = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 256);
-          const uint64_t bd = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 256);
-          tc_mma(d, ad, bd, (!first || kk || p) ? 1u : 0u);
+          const uint64_t ad = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32);
+          const uint64_t bd = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32);
+          tc_mma(acc_cols, ad, bd, (kk || p) ? 1u : 0u);
         }
-      tc_commit(&bars[st]);
-      if (last) tc_commit(&bars[2 + (chunk & 1)]);
+      tc_commit(&bars[d]);
     }
-    // with the next chunk's first MMAs queued, add the previous chunk
-    if (first && chunk > 0) {
-      drain(chunk - 1);
-      ++drained;
-    }
+    if (s >= 2) drain(s - 2);  // two stages back: its MMAs had this stage's staging to finish
   }
-  if (ok && drained < n_chunks) drain(n_chunks - 1);
+  if (ok && nk >= 2) drain(nk - 2);
+  if (ok && nk >= 1) drain(nk - 1);
+  cp_async_wait<0>();  // no copy may land after the CTA exits
   if (ok && nk > 0) {
-    const int row = quarter * 32 + lane;
-    double* Mg = M + (int64_t)wk.group * kMaxNodes * lm_pad + wk.lm0 + row;
+    double* tile = part + (int64_t)blockIdx.x * kTileElems + quarter * 32 + lane;
 #pragma unroll
-    for (int i = 0; i < 32; ++i)
-      if (acc[i] != 0.0) atomicAdd(Mg + (int64_t)(half * 32 + i) * lm_pad, acc[i]);
+    for (int i = 0; i < 32; ++i) tile[(half * 32 + i) * kGemmM] = acc[i];
   }
   if (!ok) {
     // bounded wait for every MMA this CTA issued before freeing TMEM
     if (tid == 0) {
-      tc_commit(&bars[4]);
+      tc_commit(&bars[kTcDepth]);
       atomicExch(status, CRAB_ETIMEOUT);
     }
-    dev::mbar_wait(&bars[4], 0);
+    dev::mbar_spin(&bars[kTcDepth], 0);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -472,12 +491,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
 }
 
-// Dynamic shared memory of one CTA; at least 80 KB so that at most two CTAs
-// (2 x 256 TMEM columns) share an SM and tcgen05.alloc never has to wait.
+// Dynamic shared memory of one CTA (one CTA per SM: the 256 TMEM columns
+// always fit and tcgen05.alloc never waits).
 template <int S>
 constexpr size_t tc_smem_bytes() {
-  const size_t need = 1024 /* alignment slack */ + 2 * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ + 64;
-  return need > 80 * 1024 ? need : 80 * 1024;
+  return 1024 /* alignment slack */ + kTcDepth * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ +
+         kTcRingBytes + 64;
+}
+
+// M[g][b][t*128 + r] = sum over the point splits of group g of the partial
+// tiles of lm tile t; one block per (group, lm tile), in a fixed order.
+__global__ void __launch_bounds__(256) k_mp_reduce(const double* __restrict__ part, const int32_t* __restrict__ gfirst,
+                                                   const int32_t* __restrict__ gsplits, int n_lmt, int lm_pad,
+                                                   double* __restrict__ M) {
+  const int g = blockIdx.x / n_lmt, t = blockIdx.x % n_lmt;
+  const int first = gfirst[g], n = gsplits[g];
+  for (int e = threadIdx.x; e < kTileElems; e += blockDim.x) {
+    double v = 0.0;
+    for (int k = 0; k < n; ++k) v += part[(int64_t)(first + k * n_lmt + t) * kTileElems + e];
+    M[((int64_t)g * kMaxNodes + e / kGemmM) * lm_pad + t * kGemmM + e % kGemmM] = v;
+  }
 }
 
 // j_0..j_{l_q}(q rho) at every node (spherical.rs:95-133, f64 as the
@@ -582,7 +615,7 @@ struct MpInput {
 };
 
 // Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
-// tc_terms: 0 = SIMT GEMM (FP32 or FP64 operands), 1..3 = tensor-core GEMM
+// tc_terms: 0 = SIMT GEMM (FP32 or FP64 operands), 1..2 = tensor-core GEMM
 // with that many TF32 terms per operand (FP32 operands).
 void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, int tc_terms,
                    double* out) {
@@ -633,11 +666,17 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const int lm_pad = (lm_count + kGemmM - 1) / kGemmM * kGemmM;
   std::vector<int32_t> lq(nq);
   for (int64_t k = 0; k < nq; ++k) lq[k] = adaptive_l(q[k], in.rmax_lq, L);
+  // work items: group, then point split, then lm tile (k_mp_reduce relies on this order)
+  const int n_lmt = lm_pad / kGemmM;
   std::vector<MpWork> work;
-  for (int g = 0; g < G; ++g)
-    for (int64_t k0 = begin[g]; k0 < begin[g + 1]; k0 += kSplitK)
+  std::vector<int32_t> gfirst(G), gsplits(G);
+  for (int g = 0; g < G; ++g) {
+    gfirst[g] = (int32_t)work.size();
+    gsplits[g] = 0;
+    for (int64_t k0 = begin[g]; k0 < begin[g + 1]; k0 += kSplitK, ++gsplits[g])
       for (int lm0 = 0; lm0 < lm_pad; lm0 += kGemmM)
         work.push_back(MpWork{g, lm0, k0, std::min(begin[g + 1], k0 + kSplitK)});
+  }
   std::vector<int32_t> gseg(G);
   for (int g = 0; g < G; ++g) gseg[g] = g % S;
   std::vector<double> ampg((size_t)K * G * nq);
@@ -658,6 +697,9 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   void* d_WT = ctx->dev("mp_W", esz * (size_t)kMaxNodes * n_pad);
   MpWork* d_work = (MpWork*)ctx->dev("mp_work", sizeof(MpWork) * work.size());
   double* d_M = (double*)ctx->dev("mp_M", sizeof(double) * (size_t)G * kMaxNodes * lm_pad);
+  double* d_part = (double*)ctx->dev("mp_part", sizeof(double) * (size_t)kTileElems * work.size());
+  int32_t* d_gfirst = (int32_t*)ctx->dev("mp_gfirst", sizeof(int32_t) * G);
+  int32_t* d_gsplits = (int32_t*)ctx->dev("mp_gsplits", sizeof(int32_t) * G);
   double* d_q = (double*)ctx->dev("mp_q", sizeof(double) * nq);
   int32_t* d_lq = (int32_t*)ctx->dev("mp_lq", sizeof(int32_t) * nq);
   double* d_Jn = (double*)ctx->dev("mp_Jn", sizeof(double) * (size_t)nq * S * nb * (L + 1));
@@ -676,7 +718,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   copy_h2d(ctx, d_amp, ampg.data(), sizeof(double) * ampg.size(), s);
   copy_h2d(ctx, d_gseg, gseg.data(), sizeof(int32_t) * G, s);
   CRAB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
-  CRAB_CUDA_CHECK(cudaMemsetAsync(d_M, 0, sizeof(double) * (size_t)G * kMaxNodes * lm_pad, s));
+  copy_h2d(ctx, d_gfirst, gfirst.data(), sizeof(int32_t) * G, s);
+  copy_h2d(ctx, d_gsplits, gsplits.data(), sizeof(int32_t) * G, s);
 
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   struct EvGuard {
@@ -694,28 +737,28 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
                                                    (double*)d_YT, (double*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
-                                                                lm_pad, d_work, d_M);
+                                                                lm_pad, d_work, d_part);
   } else {
     k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                   (float*)d_YT, (float*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     if (tc_terms == 0) {
       k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad,
-                                                                 lm_pad, d_work, d_M);
+                                                                 lm_pad, d_work, d_part);
     } else {
 #define CRAB_TC(SS)                                                                                               \
   if (tc_terms == SS) {                                                                                           \
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_tc<SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                          (int)tc_smem_bytes<SS>()));                                              \
     k_mp_moments_tc<SS><<<(unsigned)work.size(), kTcThreads, tc_smem_bytes<SS>(), s>>>(                           \
-        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_M, d_status);                            \
+        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_part, d_status);                            \
   }
       CRAB_TC(1)
       CRAB_TC(2)
-      CRAB_TC(3)
 #undef CRAB_TC
     }
   }
+  k_mp_reduce<<<(unsigned)(G * n_lmt), 256, 0, s>>>(d_part, d_gfirst, d_gsplits, n_lmt, lm_pad, d_M);
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
@@ -726,7 +769,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     k_mp_gram<3><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
   CRAB_CUDA_CHECK(cudaEventRecord(ev[3], s));
-  ctx->launches += 4;
+  ctx->launches += 5;
   copy_d2h(ctx, out, d_out, sizeof(double) * (size_t)P * nq, s);
   int status = 0;
   if (tc_terms) copy_d2h(ctx, &status, d_status, sizeof(int), s);
@@ -751,9 +794,8 @@ MpPrecision multipole_precision(int precision) {
     case CRAB_PREC_FP32: return {false, 0};
     case CRAB_PREC_TF32: return {false, 1};
     case CRAB_PREC_TF32_SPLIT: return {false, 2};
-    case CRAB_PREC_TF32_SPLIT3: return {false, 3};
     default:
-      throw Error(CRAB_EINVAL, "multipole precision must be FP64, FP32, TF32, TF32_SPLIT or TF32_SPLIT3");
+      throw Error(CRAB_EINVAL, "multipole precision must be FP64, FP32, TF32 or TF32_SPLIT");
   }
 }
 

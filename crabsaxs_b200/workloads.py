@@ -1,7 +1,7 @@
 """Named benchmark workloads, run a fixed number of times (for profilers).
 
     python -m crabsaxs_b200.workloads debye-config2 [--variant V] [--repeats N]
-    python -m crabsaxs_b200.workloads multipole-config3 [--precision fp32|fp64] [--repeats N]
+    python -m crabsaxs_b200.workloads multipole-config3 [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
     python -m crabsaxs_b200.workloads gradient-config4 [--repeats N]
 
 debye-config2: the 20,000-atom synthetic protein plus its adaptive 3 Å
@@ -56,7 +56,7 @@ def debye_config2(engine: cs.Engine, variant: int | None, repeats: int) -> str:
 def multipole_config3(engine: cs.Engine, precision: str, repeats: int) -> str:
     w = synth.CONFIG3
     s = synth.protein(w.seed, w.n_atoms, w.radius)
-    prec = N.PREC_FP64 if precision == "fp64" else N.PREC_FP32
+    prec = {"fp64": N.PREC_FP64, "fp32": N.PREC_FP32, "tf32": N.PREC_TF32, "tf32x2": N.PREC_TF32_SPLIT}[precision]
     wall = []
     for _ in range(repeats):
         t0 = time.perf_counter()
@@ -82,7 +82,7 @@ def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
     ap.add_argument("workload", choices=["debye-config2", "multipole-config3", "gradient-config4"])
     ap.add_argument("--variant", type=int, default=None)
-    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="fp32")
     ap.add_argument("--repeats", type=int, default=2)
     a = ap.parse_args(argv)
     engine = cs.Engine.default(0)

@@ -60,7 +60,7 @@ enum { CRAB_HYD_ANALYTIC = 0, CRAB_HYD_GRID = 1, CRAB_HYD_ADAPTIVE = 2 };
 enum { CRAB_METHOD_AUTO = 0, CRAB_METHOD_DEBYE = 1, CRAB_METHOD_MULTIPOLE = 2 };
 /* Multipole GEMM precision. */
 enum { CRAB_PREC_FP64 = 0, CRAB_PREC_TF32 = 1, CRAB_PREC_BF16 = 2, CRAB_PREC_BF16_SPLIT = 3, CRAB_PREC_TF32_SPLIT = 4,
-       CRAB_PREC_FP32 = 5, CRAB_PREC_TF32_SPLIT3 = 6 };
+       CRAB_PREC_FP32 = 5 };
 /* fit.rs:30-47 modes. */
 enum { CRAB_SCALE_FIT = 0, CRAB_SCALE_FIXED = 1 };
 enum { CRAB_BG_FIT = 0, CRAB_BG_FIXED_ZERO = 1, CRAB_BG_FIXED = 2 };
