@@ -124,10 +124,13 @@ __host__ __device__ __forceinline__ int64_t mp_blocked(int row, int64_t k, int r
 
 // Per point: real harmonics (spherical.rs:54-93, 165-199) and the weighted
 // Lagrange basis of its radial segment.  pts: x, y, z (centred), w, r.
+// The recurrence divides by (l - m) as the reference does, here as a product
+// with the f64 reciprocal inv[l - m] (at most one ulp apart per step).
 template <typename E>
 __global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restrict__ seg, int64_t n_pad, int L,
                           int lm_pad, int nb, const double* __restrict__ norms, const double* __restrict__ nodes,
-                          const double* __restrict__ bary, E* __restrict__ YT, E* __restrict__ WT) {
+                          const double* __restrict__ bary, const double* __restrict__ inv, E* __restrict__ YT,
+                          E* __restrict__ WT) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pad) return;
   const double px = pts[5 * i], py = pts[5 * i + 1], pz = pts[5 * i + 2], w = pts[5 * i + 3], r = pts[5 * i + 4];
@@ -168,7 +171,7 @@ __global__ void k_mp_prep(const double* __restrict__ pts, const int32_t* __restr
     double prev = pmm, cur = pm1;
     for (int l = m + 2; l <= L; ++l) {
       const double num = __dadd_rn(__dmul_rn(__dmul_rn((double)(2 * l - 1), x), cur), -__dmul_rn((double)(l + m - 1), prev));
-      const double next = __ddiv_rn(num, (double)(l - m));
+      const double next = __dmul_rn(num, inv[l - m]);
       emit(l, m, next);
       prev = cur;
       cur = next;
@@ -550,57 +553,105 @@ __global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __
   for (int l = 0; l <= ql; ++l) out[l] = work[l] * scale;
 }
 
-// One q per block: A^c_lm = sum_g amp[c][g][k] sum_b M[g][b][lm] Jn[k][seg_g*nb + b][l]
-// for l <= l_q, then 4 pi sum_lm A^c A^d for c <= d (order (0,0), (1,1),
-// (2,2), (0,1), (0,2), (1,2) for three combinations).
+// One block per kGramQ consecutive q.  The node values j_l(q rho_b) of the
+// block's q for a window of l (all l whose values fit kGramSmem) are staged in
+// shared memory, then every thread takes lm rows of the window:
+//   A^c_lm(q) = sum_g amp[c][t(g)][q] sum_b M[g][b][lm] j_l(q rho_{seg(g), b})
+// and 4 pi sum_{l <= l_q, m} A^c A^d accumulates per q for c <= d (order
+// (0,0), (1,1), (2,2), (0,1), (0,2), (1,2) for three combinations).  Each M
+// element is read once per block of q.
+constexpr int kGramQ = 4;
+constexpr size_t kGramSmem = 96 * 1024;
 template <int K>
 __global__ void __launch_bounds__(256) k_mp_gram(const double* __restrict__ M, const double* __restrict__ Jn,
                                                  const int32_t* __restrict__ lq, const double* __restrict__ amp,
-                                                 const int32_t* __restrict__ gseg, int G, int nb, int n_nodes, int L,
-                                                 int lm_pad, int64_t nq, double* __restrict__ out) {
+                                                 int T, int S, int nb, int n_nodes, int L, int lm_pad, int64_t nq,
+                                                 int l_window, double* __restrict__ out) {
   constexpr int P = K * (K + 1) / 2;
-  const int64_t k = blockIdx.x;
-  const int ql = lq[k];
-  const int nlm = (ql + 1) * (ql + 1);
-  const double* Jq = Jn + k * (int64_t)n_nodes * (L + 1);
-  double acc[P];
-#pragma unroll
-  for (int p = 0; p < P; ++p) acc[p] = 0.0;
-  for (int lm = threadIdx.x; lm < nlm; lm += blockDim.x) {
-    int l = (int)sqrt((double)lm);
-    while (l * l > lm) --l;
-    while ((l + 1) * (l + 1) <= lm) ++l;
-    double A[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) A[c] = 0.0;
-    for (int g = 0; g < G; ++g) {
-      const double* Mg = M + (int64_t)g * kMaxNodes * lm_pad + lm;
-      const double* J = Jq + (int64_t)gseg[g] * nb * (L + 1) + l;
-      double C = 0.0;
-      for (int b = 0; b < nb; ++b) C = fma(Mg[(int64_t)b * lm_pad], __ldg(J + b * (L + 1)), C);
-#pragma unroll
-      for (int c = 0; c < K; ++c) A[c] = fma(amp[((int64_t)c * G + g) * nq + k], C, A[c]);
-    }
-    int p = 0;
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[p++] += A[c] * A[c];
-#pragma unroll
-    for (int c = 0; c < K; ++c)
-#pragma unroll
-      for (int d = c + 1; d < K; ++d) acc[p++] += A[c] * A[d];
-  }
-  __shared__ double red[8][P];
-#pragma unroll
-  for (int p = 0; p < P; ++p) {
-    double v = acc[p];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][p] = v;
+  extern __shared__ double gram_smem[];
+  double* amps = gram_smem;                      // [K][T][kGramQ]
+  double* Js = gram_smem + K * T * kGramQ;       // [l - l0][node][kGramQ]
+  __shared__ int lqs[kGramQ];
+  __shared__ double red[8][P * kGramQ];
+  const int64_t q0 = (int64_t)blockIdx.x * kGramQ;
+  const int nqb = (int)min((int64_t)kGramQ, nq - q0);
+  const int tid = threadIdx.x;
+  if (tid < kGramQ) lqs[tid] = tid < nqb ? lq[q0 + tid] : -1;
+  for (int idx = tid; idx < K * T * kGramQ; idx += blockDim.x) {
+    const int qi = idx % kGramQ, ct = idx / kGramQ;
+    amps[idx] = qi < nqb ? amp[(int64_t)ct * nq + q0 + qi] : 0.0;
   }
   __syncthreads();
-  if (threadIdx.x < P) {
+  int lmax = -1;
+  for (int qi = 0; qi < kGramQ; ++qi) lmax = max(lmax, lqs[qi]);
+  const int G = T * S;
+  double acc[P][kGramQ];
+#pragma unroll
+  for (int p = 0; p < P; ++p)
+#pragma unroll
+    for (int qi = 0; qi < kGramQ; ++qi) acc[p][qi] = 0.0;
+  for (int l0 = 0; l0 <= lmax; l0 += l_window) {
+    const int l1 = min(lmax + 1, l0 + l_window);
+    __syncthreads();
+    for (int idx = tid; idx < (l1 - l0) * n_nodes * kGramQ; idx += blockDim.x) {
+      const int qi = idx % kGramQ, node = (idx / kGramQ) % n_nodes, dl = idx / (kGramQ * n_nodes);
+      Js[idx] = qi < nqb ? Jn[((q0 + qi) * n_nodes + node) * (int64_t)(L + 1) + l0 + dl] : 0.0;
+    }
+    __syncthreads();
+    for (int lm = l0 * l0 + tid; lm < l1 * l1; lm += blockDim.x) {
+      int l = (int)sqrt((double)lm);
+      while (l * l > lm) --l;
+      while ((l + 1) * (l + 1) <= lm) ++l;
+      const double* Jl = Js + (l - l0) * n_nodes * kGramQ;
+      double A[K][kGramQ];
+#pragma unroll
+      for (int c = 0; c < K; ++c)
+#pragma unroll
+        for (int qi = 0; qi < kGramQ; ++qi) A[c][qi] = 0.0;
+      for (int g = 0; g < G; ++g) {
+        const double* Mg = M + (int64_t)g * kMaxNodes * lm_pad + lm;
+        const double* Jg = Jl + (g % S) * nb * kGramQ;
+        double C[kGramQ];
+#pragma unroll
+        for (int qi = 0; qi < kGramQ; ++qi) C[qi] = 0.0;
+        for (int b = 0; b < nb; ++b) {
+          const double mv = Mg[(int64_t)b * lm_pad];
+#pragma unroll
+          for (int qi = 0; qi < kGramQ; ++qi) C[qi] = fma(mv, Jg[b * kGramQ + qi], C[qi]);
+        }
+        const int t = g / S;
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+#pragma unroll
+          for (int qi = 0; qi < kGramQ; ++qi) A[c][qi] = fma(amps[(c * T + t) * kGramQ + qi], C[qi], A[c][qi]);
+      }
+#pragma unroll
+      for (int qi = 0; qi < kGramQ; ++qi) {
+        if (l > lqs[qi]) continue;
+        int p = 0;
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[p++][qi] += A[c][qi] * A[c][qi];
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+#pragma unroll
+          for (int d = c + 1; d < K; ++d) acc[p++][qi] += A[c][qi] * A[d][qi];
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < P; ++p)
+#pragma unroll
+    for (int qi = 0; qi < kGramQ; ++qi) {
+      double v = acc[p][qi];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((tid & 31) == 0) red[tid >> 5][p * kGramQ + qi] = v;
+    }
+  __syncthreads();
+  if (tid < P * kGramQ) {
+    const int p = tid / kGramQ, qi = tid % kGramQ;
     double v = 0.0;
-    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[wi][threadIdx.x];
-    out[threadIdx.x * nq + k] = 4.0 * kPiD * v;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[wi][tid];
+    if (qi < nqb) out[p * nq + q0 + qi] = 4.0 * kPiD * v;
   }
 }
 
@@ -677,13 +728,9 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
       for (int lm0 = 0; lm0 < lm_pad; lm0 += kGemmM)
         work.push_back(MpWork{g, lm0, k0, std::min(begin[g + 1], k0 + kSplitK)});
   }
-  std::vector<int32_t> gseg(G);
-  for (int g = 0; g < G; ++g) gseg[g] = g % S;
-  std::vector<double> ampg((size_t)K * G * nq);
-  for (int c = 0; c < K; ++c)
-    for (int g = 0; g < G; ++g)
-      std::memcpy(&ampg[((size_t)c * G + g) * nq], &in.amp[((size_t)c * T + g / S) * nq], sizeof(double) * nq);
   const std::vector<double> norms = harmonic_norms(L);
+  std::vector<double> inv(L + 2, 0.0);
+  for (int k = 1; k <= L + 1; ++k) inv[k] = 1.0 / (double)k;
 
   TraceScope tdev("multipole_device");
   cudaStream_t s = ctx->stream;
@@ -691,6 +738,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_pts = (double*)ctx->dev("mp_pts", sizeof(double) * pts.size());
   int32_t* d_seg = (int32_t*)ctx->dev("mp_seg", sizeof(int32_t) * n_pad);
   double* d_norms = (double*)ctx->dev("mp_norms", sizeof(double) * norms.size());
+  double* d_inv = (double*)ctx->dev("mp_inv", sizeof(double) * inv.size());
   double* d_nodes = (double*)ctx->dev("mp_nodes", sizeof(double) * B.nodes.size());
   double* d_bary = (double*)ctx->dev("mp_bary", sizeof(double) * B.bary.size());
   void* d_YT = ctx->dev("mp_Y", esz * (size_t)lm_pad * n_pad);
@@ -703,20 +751,19 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_q = (double*)ctx->dev("mp_q", sizeof(double) * nq);
   int32_t* d_lq = (int32_t*)ctx->dev("mp_lq", sizeof(int32_t) * nq);
   double* d_Jn = (double*)ctx->dev("mp_Jn", sizeof(double) * (size_t)nq * S * nb * (L + 1));
-  double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * ampg.size());
-  int32_t* d_gseg = (int32_t*)ctx->dev("mp_gseg", sizeof(int32_t) * G);
+  double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * in.amp.size());
   double* d_out = (double*)ctx->dev("mp_out", sizeof(double) * (size_t)P * nq);
   int* d_status = (int*)ctx->dev("mp_status", sizeof(int));
   copy_h2d(ctx, d_pts, pts.data(), sizeof(double) * pts.size(), s);
   copy_h2d(ctx, d_seg, seg.data(), sizeof(int32_t) * n_pad, s);
   copy_h2d(ctx, d_norms, norms.data(), sizeof(double) * norms.size(), s);
+  copy_h2d(ctx, d_inv, inv.data(), sizeof(double) * inv.size(), s);
   copy_h2d(ctx, d_nodes, B.nodes.data(), sizeof(double) * B.nodes.size(), s);
   copy_h2d(ctx, d_bary, B.bary.data(), sizeof(double) * B.bary.size(), s);
   copy_h2d(ctx, d_work, work.data(), sizeof(MpWork) * work.size(), s);
   copy_h2d(ctx, d_q, q, sizeof(double) * nq, s);
   copy_h2d(ctx, d_lq, lq.data(), sizeof(int32_t) * nq, s);
-  copy_h2d(ctx, d_amp, ampg.data(), sizeof(double) * ampg.size(), s);
-  copy_h2d(ctx, d_gseg, gseg.data(), sizeof(int32_t) * G, s);
+  copy_h2d(ctx, d_amp, in.amp.data(), sizeof(double) * in.amp.size(), s);
   CRAB_CUDA_CHECK(cudaMemsetAsync(d_status, 0, sizeof(int), s));
   copy_h2d(ctx, d_gfirst, gfirst.data(), sizeof(int32_t) * G, s);
   copy_h2d(ctx, d_gsplits, gsplits.data(), sizeof(int32_t) * G, s);
@@ -734,13 +781,13 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const unsigned prep_blocks = (unsigned)((n_pad + 127) / 128);
   if (fp64) {
     k_mp_prep<double><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
-                                                   (double*)d_YT, (double*)d_WT);
+                                                   d_inv, (double*)d_YT, (double*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
                                                                 lm_pad, d_work, d_part);
   } else {
     k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
-                                                  (float*)d_YT, (float*)d_WT);
+                                                  d_inv, (float*)d_YT, (float*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
     if (tc_terms == 0) {
       k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad,
@@ -763,10 +810,21 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
   k_mp_node_bessel<<<(unsigned)((nbess + 127) / 128), 128, 0, s>>>(d_q, d_lq, nq, d_nodes, n_nodes, L, d_Jn);
-  if (K == 1)
-    k_mp_gram<1><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
-  else
-    k_mp_gram<3><<<(unsigned)nq, 256, 0, s>>>(d_M, d_Jn, d_lq, d_amp, d_gseg, G, nb, n_nodes, L, lm_pad, nq, d_out);
+  const size_t amp_bytes = sizeof(double) * (size_t)K * T * kGramQ;
+  const size_t per_l = sizeof(double) * (size_t)n_nodes * kGramQ;
+  require(amp_bytes + per_l <= kGramSmem, "multipole: too many scattering types or radial nodes");
+  const int l_window = (int)std::min<size_t>((size_t)L + 1, (kGramSmem - amp_bytes) / per_l);
+  const size_t gram_smem = amp_bytes + per_l * (size_t)l_window;
+  const unsigned gram_blocks = (unsigned)((nq + kGramQ - 1) / kGramQ);
+  if (K == 1) {
+    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
+    k_mp_gram<1><<<gram_blocks, 256, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, T, S, nb, n_nodes, L, lm_pad, nq,
+                                                      l_window, d_out);
+  } else {
+    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
+    k_mp_gram<3><<<gram_blocks, 256, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, T, S, nb, n_nodes, L, lm_pad, nq,
+                                                      l_window, d_out);
+  }
   CRAB_CUDA_CHECK(cudaGetLastError());
   CRAB_CUDA_CHECK(cudaEventRecord(ev[3], s));
   ctx->launches += 5;
