@@ -296,11 +296,13 @@ def ensemble_section(eng, rank):
 
 
 def multipole_section(eng, rank, fp32_peak):
-    """Config 3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50, FP32
-    moment GEMM.  Reports the call's wall and device time, the GEMM's FP32
-    fraction, the error against the FP64 device multipole (all q; precision)
-    and against FP64 Debye (every 50th q; truncation of the expansion at L),
-    and config 2's solvent curve by multipole (L = 30) for comparison with Debye."""
+    """Config 3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.  The
+    default path runs the moment GEMM on tcgen05 tensor cores (TF32 hi+lo, 3
+    products per K step); the FP32 SIMT GEMM is timed beside it.  Reports the
+    call's wall and device time, each GEMM against its peak, the error against
+    the FP64 device multipole (all q; precision) and against FP64 Debye (every
+    50th q; truncation of the expansion at L), and config 2's solvent curve by
+    multipole (L = 30) for comparison with Debye."""
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
     from crabsaxs_b200 import synth
@@ -308,18 +310,25 @@ def multipole_section(eng, rank, fp32_peak):
     w = synth.CONFIG3
     s = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
     L = 50
-    cs.multipole_intensity(s, w.q, L, engine=eng)
-    walls, dev, gemm = [], [], []
     tot, gm, fl = C.c_double(), C.c_double(), C.c_double()
-    for _ in range(5):
-        t0 = time.perf_counter()
-        f32 = cs.multipole_intensity(s, w.q, L, engine=eng)
-        walls.append((time.perf_counter() - t0) * 1e3)
-        eng.check(N.lib.crab_multipole_last_timing(eng.handle, C.byref(tot), C.byref(gm), C.byref(fl)))
-        dev.append(tot.value)
-        gemm.append(gm.value)
+
+    def timed(prec):
+        cs.multipole_intensity(s, w.q, L, precision=prec, engine=eng)
+        walls, dev, gemm = [], [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            out = cs.multipole_intensity(s, w.q, L, precision=prec, engine=eng)
+            walls.append((time.perf_counter() - t0) * 1e3)
+            eng.check(N.lib.crab_multipole_last_timing(eng.handle, C.byref(tot), C.byref(gm), C.byref(fl)))
+            dev.append(tot.value)
+            gemm.append(gm.value)
+        return out, float(np.median(walls)), float(np.median(dev)), float(np.median(gemm)), fl.value
+
+    tc, tc_wall, tc_dev, tc_gemm, flop = timed(N.PREC_TF32_SPLIT)
+    f32, f32_wall, f32_dev, f32_gemm, _ = timed(N.PREC_FP32)
     f64 = cs.multipole_intensity(s, w.q, L, precision=N.PREC_FP64, engine=eng)
-    rel = np.abs(f32 - f64) / np.abs(f64)
+    rel = np.abs(tc - f64) / np.abs(f64)
+    rel32 = np.abs(f32 - f64) / np.abs(f64)
     sub = np.arange(0, len(w.q), 50)
     d64 = cs.debye_solvent_basis(s, w.q[sub], cs.SolventParams(), engine=eng, fp64=True)[0]
     trunc = np.abs(f64[sub] - d64) / np.abs(d64)
@@ -328,7 +337,12 @@ def multipole_section(eng, rank, fp32_peak):
     rmax = float(np.max(np.linalg.norm(s.xyz - c, axis=1)))
     lq = np.clip(np.ceil(w.q * rmax) + 8, min(8, L), L)
     direct_flop = 2.0 * s.atom_count * float(np.sum((lq + 1) ** 2))
-    gemm_ms = float(np.median(gemm))
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    tf32_peak = 0.5 * float(peaks.get("bf16_tflops", 1590.0))  # dense TF32 runs at half the BF16 rate
     # config 2 curve with the adaptive 3 Å grid by multipole, L = 30
     s2 = synth.protein(synth.CONFIG2.seed, synth.CONFIG2.n_atoms, synth.CONFIG2.radius)
     sp = cs.SolventParams(hydration_model=cs.HydrationModel.AdaptiveGrid, hydration_grid_spacing_angstrom=3.0)
@@ -339,14 +353,21 @@ def multipole_section(eng, rank, fp32_peak):
         cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
     c2_ms = (time.perf_counter() - t0) * 1e3 / 3
     return {"workload": "multipole intensity, 100k atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50",
-            "wall_ms": float(np.median(walls)), "device_ms": float(np.median(dev)),
-            "moments_gemm": {"ms": gemm_ms, "flop": fl.value, "achieved_tflops": fl.value / (gemm_ms * 1e-3) / 1e12,
-                             "peak_tflops": fp32_peak, "bound": "fp32 (SIMT register-tiled GEMM)",
-                             "frac": fl.value / (gemm_ms * 1e-3) / 1e12 / fp32_peak},
+            "precision": "TF32 hi+lo on tcgen05 (default)", "wall_ms": tc_wall, "device_ms": tc_dev,
+            "moments_gemm_tensor": {
+                "ms": tc_gemm, "useful_flop": flop, "tensor_flop": 3.0 * flop,
+                "achieved_tflops": 3.0 * flop / (tc_gemm * 1e-3) / 1e12, "peak_tflops": tf32_peak,
+                "peak_source": "0.5 x bf16_tflops of MEASURED_PEAKS.json (dense TF32 = half the BF16 rate)",
+                "frac": 3.0 * flop / (tc_gemm * 1e-3) / 1e12 / tf32_peak,
+                "note": "3 TF32 products per K step (h h', h m', m h'); includes the split reduction"},
+            "moments_gemm_fp32_simt": {"ms": f32_gemm, "achieved_tflops": flop / (f32_gemm * 1e-3) / 1e12,
+                                       "peak_tflops": fp32_peak, "frac": flop / (f32_gemm * 1e-3) / 1e12 / fp32_peak,
+                                       "device_ms": f32_dev, "wall_ms": f32_wall},
             "direct_contraction_flop": direct_flop,
-            "direct_equivalent_tflops": direct_flop / (float(np.median(dev)) * 1e-3) / 1e12,
+            "direct_equivalent_tflops": direct_flop / (tc_dev * 1e-3) / 1e12,
             "max_rel_err_vs_fp64_multipole": float(rel.max()),
             "rms_rel_err_vs_fp64_multipole": float(np.sqrt(np.mean(rel**2))),
+            "fp32_simt_max_rel_err_vs_fp64_multipole": float(rel32.max()),
             "max_rel_err_vs_fp64_debye_every_50th_q": float(trunc.max()),
             "rms_rel_err_vs_fp64_debye_every_50th_q": float(np.sqrt(np.mean(trunc**2))),
             "config2_multipole_l30_curve_ms": c2_ms}

@@ -380,7 +380,7 @@ def solvent_corrected_intensity(structure, q, params: SolventParams, implicit_hy
 
 
 def multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: bool = True,
-                        precision: int = N.PREC_FP32, engine: Optional[Engine] = None) -> np.ndarray:
+                        precision: int = N.PREC_TF32_SPLIT, engine: Optional[Engine] = None) -> np.ndarray:
     """spherical.rs:266-403."""
     eng = engine or Engine.default()
     qa = _f64(q)
@@ -391,7 +391,7 @@ def multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: 
 
 
 def multipole_solvent_basis(structure: Structure, q, l_max: int, params: SolventParams,
-                            implicit_hydrogen: bool = True, precision: int = N.PREC_FP32,
+                            implicit_hydrogen: bool = True, precision: int = N.PREC_TF32_SPLIT,
                             engine: Optional[Engine] = None) -> np.ndarray:
     """spherical.rs:474-565."""
     eng = engine or Engine.default()

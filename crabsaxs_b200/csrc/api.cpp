@@ -581,8 +581,8 @@ int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t 
         combine_basis(q, nq, b.data(), opt->solvent.c1, opt->solvent.c2, out);
       }
     } else {
-      if (!opt->has_solvent) multipole_intensity_impl(ctx, st, q, nq, l_max, implicit, CRAB_PREC_FP32, out);
-      else multipole_solvent_intensity_impl(ctx, st, q, nq, l_max, opt->solvent, implicit, CRAB_PREC_FP32, out);
+      if (!opt->has_solvent) multipole_intensity_impl(ctx, st, q, nq, l_max, implicit, CRAB_PREC_TF32_SPLIT, out);
+      else multipole_solvent_intensity_impl(ctx, st, q, nq, l_max, opt->solvent, implicit, CRAB_PREC_TF32_SPLIT, out);
     }
     if (method_used) *method_used = method;
   });

@@ -258,37 +258,50 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 
 // ---- tensor-core moment GEMM (tcgen05, TF32 operands split into terms) ----
 //
-// The same product M[g][b][lm] += sum_k YT[lm][k] WT[b][k] for one 128 x 64
-// tile, on the 5th-generation tensor cores.  Each FP32 operand x is split
-// into TF32 terms (h = x rounded to TF32, m = x - h rounded to TF32):
+// The same product part[w] = YT-tile . WT-tile^T (128 lm rows x 64 nodes over
+// the item's points) on the 5th-generation tensor cores.  Each FP32 operand x
+// is split into TF32 terms (h = x rounded to TF32, m = x - h rounded to TF32):
 //   S = 1: h h'                  (TF32, relative error ~5e-4)
 //   S = 2: h h' + h m' + m h'    (relative error ~5e-7)
 // The S = 2 error is set by the tensor core's FP32 accumulation, which rounds
-// toward zero (about 2^-24 of the accumulator per MMA); a third TF32 term
-// would not lower it.  To keep that bias small the TMEM accumulator covers one
-// 32-point stage only and is then drained into f64 registers.
-// Data path per stage: every thread copies its six 16-byte chunks of the
-// FP32 tiles (A: 128 lm rows x 32 points, B: 64 nodes x 32) from global
-// memory with cp.async into a private slot of a 3-deep ring, three stages
-// ahead; it reads them back, splits them and stores the terms in the K-major
-// 128-byte-swizzled layout: row r of a term tile is the 128-byte line at
-// (r/8)*1024 + (r%8)*128, its 16-byte chunk c at position c ^ (r%8)
-// (SBO 1024 B).  Thread 0 issues tcgen05.mma (M = 128, N = 64, K = 8; the K
-// step advances the descriptor start by 32 B) into the stage's TMEM
-// accumulator and commits it to the stage's mbarrier.  Term buffers and
-// accumulators are three deep: stage s is drained during stage s + 2, so the
-// MMAs of a stage have two stages of staging work to complete behind.  Every
-// mbarrier wait is bounded; on expiry the kernel flags CRAB_ETIMEOUT, waits
-// (bounded) for its own MMAs and frees its TMEM before returning.
+// toward zero (about 2^-24 of the accumulator per MMA), so a TMEM accumulator
+// covers one 32-point stage only and is then drained into f64 registers.
+//
+// Warp-specialised pipeline (17 warps):
+//  * producers, warps 0-7: each thread copies its six 16-byte chunks of a
+//    stage's FP32 tiles (A: 128 rows x 32 points, B: 64 x 32; point-blocked,
+//    so each tile is contiguous) with cp.async into a private slot of a
+//    3-deep ring, reads them back, waits until term slot d is empty, stores
+//    the S TF32 terms in the K-major 128-byte-swizzled layout (row r at
+//    (r/8)*1024 + (r%8)*128, 16-byte chunk c at position c ^ (r%8)), fences
+//    the generic-proxy writes for the tensor core and arrives on full[d];
+//  * MMA issuer, warp 8 lane 0: waits full[d] and accfree[a], issues
+//    tcgen05.mma (M = 128, N = 64, K = 8, descriptor start +32 B per K step)
+//    into TMEM accumulator a and commits to empty[d] and accfull[a];
+//  * drainers, warps 9-16: wait accfull[a], read their lane quarter (warp % 4)
+//    and 32 of the 64 columns with tcgen05.ld, add them into f64 registers and
+//    arrive on accfree[a]; at the end they store the f64 tile.
+// Three term slots, four accumulators.  Every wait is bounded: a role whose
+// wait runs out stops, the others run out in turn, and the CTA flags
+// CRAB_ETIMEOUT, waits (bounded) for its own MMAs and frees its TMEM.
 constexpr int kTcK = 32;                    // points per stage
-constexpr int kTcThreads = 256;
-constexpr int kTcDepth = 3;                 // term buffers and TMEM accumulators
-constexpr int kTcTmemCols = 256;            // three 64-column accumulators used
-constexpr int kTcRing = 3;                  // raw FP32 stages in flight per thread
-constexpr int kTcChunks = 6;                // 16-byte chunks per thread per stage (4 of A, 2 of B)
+constexpr int kTcProducers = 256;           // warps 0-7
+constexpr int kTcMmaWarp = 8;
+constexpr int kTcDrainers = 256;            // warps 9-16
+constexpr int kTcThreads = kTcProducers + 32 + kTcDrainers;
+constexpr int kTcSlots = 3;                 // term buffers
+constexpr int kTcAccs = 4;                  // 64-column TMEM accumulators
+constexpr int kTcTmemCols = 256;
+constexpr int kTcRing = 3;                  // raw FP32 stages in flight per producer
+constexpr int kTcChunks = 6;                // 16-byte chunks per producer per stage (4 of A, 2 of B)
+constexpr int kTcAChunks = 4;
+static_assert(kTcAChunks * kTcProducers * 4 == kGemmM * kTcK, "A tile chunks");
+static_assert((kTcChunks - kTcAChunks) * kTcProducers * 4 == kMaxNodes * kTcK, "B tile chunks");
+static_assert(kTcThreads % 32 == 0 && kTcProducers == 32 * kTcMmaWarp, "warp roles");
 constexpr int kTcABytes = kGemmM * kTcK * 4;     // 16 KB
 constexpr int kTcBBytes = kMaxNodes * kTcK * 4;  // 8 KB
-constexpr int kTcRingBytes = kTcRing * kTcThreads * kTcChunks * 16;  // 72 KB
+constexpr int kTcRingBytes = kTcRing * kTcProducers * kTcChunks * 16;  // 72 KB
+constexpr int kTcBars = 2 * kTcSlots + 2 * kTcAccs + 1;
 // TF32, FP32 accumulate, K-major A and B, N = 64 (bits 17-22, N>>3), M = 128 (bits 24-28, M>>4)
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -300,10 +313,12 @@ __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
   d |= (uint64_t)2 << 61;                         // 128-byte swizzle
   return d;
 }
+// x rounded to the nearest TF32 value (ties away from zero): add half of the
+// last kept bit (bit 13) to the magnitude bits and clear the 13 dropped bits;
+// a carry into the exponent is the correct rounding.  Integer ALU work
+// instead of a conversion instruction on the narrower XU pipe.
 __device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t u;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-  return __uint_as_float(u);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -315,6 +330,10 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, ui
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
 }
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
@@ -352,9 +371,10 @@ __device__ __forceinline__ void tc_store_split(unsigned char* base, int part_byt
     *reinterpret_cast<float4*>(base + p * part_bytes + off) = make_float4(t[p][0], t[p][1], t[p][2], t[p][3]);
 }
 
-// Chunk c of this thread in a stage: rows of A (c < 4) or B, 16-byte column c4.
-__device__ __forceinline__ void tc_chunk(int c, int tid, int& row, int& c4) {
-  const int idx = (c < 4 ? c : c - 4) * kTcThreads + tid;
+// Chunk c of producer thread t in a stage: A rows for c < kTcAChunks, B rows
+// after; 16-byte column c4 of the row.
+__device__ __forceinline__ void tc_chunk(int c, int t, int& row, int& c4) {
+  const int idx = (c < kTcAChunks ? c : c - kTcAChunks) * kTcProducers + t;
   row = idx >> 3;
   c4 = idx & 7;
 }
@@ -365,13 +385,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const MpWork* __restrict__ work, double* __restrict__ part, int* __restrict__ status) {
   static_assert(S == 1 || S == 2, "one or two TF32 terms");
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  // term buffers: slot d holds S A terms then S B terms; then the raw ring
-  constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);
+  constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);  // S A terms, then S B terms
   unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
-  unsigned char* ring = smem + kTcDepth * slot_bytes + kTcBBytes;  // after a B-sized gap
-  // barriers: 0..2 stage MMAs complete (per slot); 3 all MMAs complete (error path)
+  unsigned char* ring = smem + kTcSlots * slot_bytes + kTcBBytes;  // after a B-sized gap
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kTcRingBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kTcDepth + 1);
+  uint64_t* full = bars;                      // [kTcSlots], one arrival per producer
+  uint64_t* empty = bars + kTcSlots;          // [kTcSlots], MMA commit
+  uint64_t* accfull = bars + 2 * kTcSlots;    // [kTcAccs], MMA commit
+  uint64_t* accfree = accfull + kTcAccs;      // [kTcAccs], one arrival per drainer
+  uint64_t* done = accfree + kTcAccs;         // error path: all MMAs complete
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kTcBars);
+  __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const MpWork wk = work[blockIdx.x];
   if (warp == 0) {
@@ -381,114 +405,138 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    for (int b = 0; b <= kTcDepth; ++b) dev::mbar_init(&bars[b], 1);
+    for (int d = 0; d < kTcSlots; ++d) {
+      dev::mbar_init(&full[d], kTcProducers);
+      dev::mbar_init(&empty[d], 1);
+    }
+    for (int a = 0; a < kTcAccs; ++a) {
+      dev::mbar_init(&accfull[a], 1);
+      dev::mbar_init(&accfree[a], kTcDrainers);
+    }
+    dev::mbar_init(done, 1);
     dev::fence_mbar_init();
+    s_fail = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
-  const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
   const int nk = (int)((wk.k1 - wk.k0) / kTcK);
-  const int quarter = warp & 3, half = warp >> 2;
+  const int64_t kb0 = wk.k0 >> 5;  // first 32-point block of the item
   bool ok = true;
-  double acc[32];  // this thread's row (lm) and 32 of the 64 node columns, in f64
+  // set when a role gave up; the others stop at their next wait
+  auto failed = [&]() { return *((volatile int*)&s_fail) != 0; };
+
+  if (warp < kTcMmaWarp) {
+    // ---------------- producers
+    const int t = tid;
+    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
+    auto issue = [&](int s) {
+      if (s < nk) {
+        const uint32_t slot = ring_base + (uint32_t)(((s % kTcRing) * kTcProducers + t) * kTcChunks * 16);
+        const float* a_blk = YT + ((kb0 + s) * lm_pad + wk.lm0) * 32;
+        const float* b_blk = WT + (kb0 + s) * kMaxNodes * 32;
 #pragma unroll
-  for (int i = 0; i < 32; ++i) acc[i] = 0.0;
-  // Add stage s's TMEM accumulator into acc once its MMAs are complete; this
-  // also frees slot s % kTcDepth.  Collective over the CTA (uniform ok).
-  auto drain = [&](int s) {
-    const int d = s % kTcDepth;
-    if (!dev::mbar_spin(&bars[d], (unsigned)((s / kTcDepth) & 1))) ok = false;
-    ok = __syncthreads_and(ok);
-    if (!ok) return;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int c = 0; c < kTcChunks; ++c) {
+          int row, c4;
+          tc_chunk(c, t, row, c4);
+          cp_async16(slot + c * 16, (c < kTcAChunks ? a_blk : b_blk) + row * 32 + c4 * 4);
+        }
+      }
+      cp_async_commit();  // one group per stage, empty past the end
+    };
 #pragma unroll
-    for (int c16 = 0; c16 < 2; ++c16) {
-      float v[16];
-      const uint32_t col = (uint32_t)(d * 64 + half * 32 + c16 * 16);
-      tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + col, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  };
-  // this thread's chunks of stage s into ring slot s % kTcRing
-  auto issue = [&](int s) {
-    if (s < nk) {
-      const int64_t k0 = wk.k0 + (int64_t)s * kTcK;
-      const uint32_t slot = ring_base + (uint32_t)(((s % kTcRing) * kTcThreads + tid) * kTcChunks * 16);
+    for (int s = 0; s < kTcRing; ++s) issue(s);
+    for (int s = 0; s < nk; ++s) {
+      const int d = s % kTcSlots;
+      cp_async_wait<kTcRing - 1>();  // this thread's chunks of stage s have landed
+      const float4* mine = reinterpret_cast<const float4*>(ring + ((s % kTcRing) * kTcProducers + t) * kTcChunks * 16);
+      if (s >= kTcSlots && (failed() || !dev::mbar_spin(&empty[d], (unsigned)((s / kTcSlots - 1) & 1)))) {
+        ok = false;
+        break;
+      }
+      unsigned char* sa = smem + d * slot_bytes;
+      unsigned char* sb = sa + S * kTcABytes;
 #pragma unroll
       for (int c = 0; c < kTcChunks; ++c) {
         int row, c4;
-        tc_chunk(c, tid, row, c4);
-        const float* src = c < 4 ? YT + mp_blocked(wk.lm0 + row, k0 + c4 * 4, lm_pad)
-                                 : WT + mp_blocked(row, k0 + c4 * 4, kMaxNodes);
-        cp_async16(slot + c * 16, src);
+        tc_chunk(c, t, row, c4);
+        const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c4 ^ (row & 7)) << 4);
+        const float4 raw = mine[c];
+        if (c < kTcAChunks) tc_store_split<S>(sa, kTcABytes, off, raw);
+        else tc_store_split<S>(sb, kTcBBytes, off, raw);
+      }
+      issue(s + kTcRing);  // the ring slot just read is refilled kTcRing stages ahead
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&full[d]);
+    }
+    cp_async_wait<0>();  // no copy may land after the CTA exits
+  } else if (warp == kTcMmaWarp) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
+      constexpr int np = S == 1 ? 1 : 3;  // (A term, B term): hh', hm', mh'
+      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+      for (int s = 0; s < nk; ++s) {
+        const int d = s % kTcSlots, a = s % kTcAccs;
+        if (failed() || !dev::mbar_spin(&full[d], (unsigned)((s / kTcSlots) & 1)) ||
+            (s >= kTcAccs && !dev::mbar_spin(&accfree[a], (unsigned)((s / kTcAccs - 1) & 1)))) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_base + d * slot_bytes, b0 = a0 + S * kTcABytes;
+        const uint32_t acc_cols = tmem + (uint32_t)(a * 64);
+#pragma unroll
+        for (int kk = 0; kk < kTcK / 8; ++kk)
+#pragma unroll
+          for (int p = 0; p < np; ++p)
+            tc_mma(acc_cols, tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32),
+                   tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32), (kk || p) ? 1u : 0u);
+        tc_commit(&empty[d]);
+        tc_commit(&accfull[a]);
       }
     }
-    cp_async_commit();  // one group per stage, empty past the end
-  };
+  } else {
+    // ---------------- drainers
+    const int quarter = warp & 3, half = (warp - kTcMmaWarp - 1) >> 2;
+    double acc[32];  // this thread's lm row and 32 of the 64 node columns
 #pragma unroll
-  for (int s = 0; s < kTcRing; ++s) issue(s);
-  for (int s = 0; s < nk && ok; ++s) {
-    const int d = s % kTcDepth;
-    cp_async_wait<kTcRing - 1>();  // this thread's chunks of stage s have landed
-    const float4* mine = reinterpret_cast<const float4*>(ring + ((s % kTcRing) * kTcThreads + tid) * kTcChunks * 16);
-    float4 raw[kTcChunks];
-#pragma unroll
-    for (int c = 0; c < kTcChunks; ++c) raw[c] = mine[c];
-    issue(s + kTcRing);  // the slot just read is refilled three stages ahead
-    // slot d was last used by stage s - 3, drained during stage s - 1
-    unsigned char* sa = smem + d * slot_bytes;
-    unsigned char* sb = sa + S * kTcABytes;
-#pragma unroll
-    for (int c = 0; c < kTcChunks; ++c) {
-      int row, c4;
-      tc_chunk(c, tid, row, c4);
-      const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c4 ^ (row & 7)) << 4);
-      if (c < 4) tc_store_split<S>(sa, kTcABytes, off, raw[c]);
-      else tc_store_split<S>(sb, kTcBBytes, off, raw[c]);
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+    for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+    for (int s = 0; s < nk; ++s) {
+      const int a = s % kTcAccs;
+      if (failed() || !dev::mbar_spin(&accfull[a], (unsigned)((s / kTcAccs) & 1))) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_base + d * slot_bytes, b0 = a0 + S * kTcABytes;
-      const uint32_t acc_cols = tmem + (uint32_t)(d * 64);
-      // (A term, B term) pairs: hh', hm', mh'
-      constexpr int np = S == 1 ? 1 : 3;
-      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
 #pragma unroll
-      for (int kk = 0; kk < kTcK / 8; ++kk)
+      for (int c16 = 0; c16 < 2; ++c16) {
+        float v[16];
+        tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + half * 32 + c16 * 16), v);
 #pragma unroll
-        for (int p = 0; p < np; ++p) {
-          const uint64_t ad = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32);
-          const uint64_t bd = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32);
-          tc_mma(acc_cols, ad, bd, (kk || p) ? 1u : 0u);
-        }
-      tc_commit(&bars[d]);
+        for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&accfree[a]);
     }
-    if (s >= 2) drain(s - 2);  // two stages back: its MMAs had this stage's staging to finish
-  }
-  if (ok && nk >= 2) drain(nk - 2);
-  if (ok && nk >= 1) drain(nk - 1);
-  cp_async_wait<0>();  // no copy may land after the CTA exits
-  if (ok && nk > 0) {
-    double* tile = part + (int64_t)blockIdx.x * kTileElems + quarter * 32 + lane;
+    if (ok) {
+      double* tile = part + (int64_t)blockIdx.x * kTileElems + quarter * 32 + lane;
 #pragma unroll
-    for (int i = 0; i < 32; ++i) tile[(half * 32 + i) * kGemmM] = acc[i];
+      for (int i = 0; i < 32; ++i) tile[(half * 32 + i) * kGemmM] = acc[i];
+    }
   }
-  if (!ok) {
+  if (!ok) atomicExch(&s_fail, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (s_fail) {
     // bounded wait for every MMA this CTA issued before freeing TMEM
-    if (tid == 0) {
-      tc_commit(&bars[kTcDepth]);
+    if (tid == kTcMmaWarp * 32) {
+      tc_commit(done);
       atomicExch(status, CRAB_ETIMEOUT);
     }
-    dev::mbar_spin(&bars[kTcDepth], 0);
+    dev::mbar_spin(done, 0);
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
@@ -498,8 +546,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // always fit and tcgen05.alloc never waits).
 template <int S>
 constexpr size_t tc_smem_bytes() {
-  return 1024 /* alignment slack */ + kTcDepth * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ +
-         kTcRingBytes + 64;
+  return 1024 /* alignment slack */ + kTcSlots * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ +
+         kTcRingBytes + sizeof(uint64_t) * kTcBars + 16;
 }
 
 // M[g][b][t*128 + r] = sum over the point splits of group g of the partial

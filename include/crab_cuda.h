@@ -257,7 +257,14 @@ int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing,
 
 /* ---- multipole engine ------------------------------------------------- */
 /* multipole_intensity (spherical.rs:266-403) with per-q adaptive order.
- * precision: CRAB_PREC_*; tensor-core GEMM per l for TF32/BF16 modes. */
+ * precision of the moment GEMM (j_l interpolated at Chebyshev nodes in r, so
+ * the expansion is one GEMM [(L+1)^2 x N] x [N x nodes]):
+ *   CRAB_PREC_FP64        f64 SIMT (device reference, 1e-9 of the oracle)
+ *   CRAB_PREC_FP32        FP32 SIMT (about 4e-7)
+ *   CRAB_PREC_TF32_SPLIT  tcgen05 tensor cores, TF32 hi+lo terms (about 5e-7;
+ *                         the compute_curve default)
+ *   CRAB_PREC_TF32        tcgen05, single TF32 term (about 1e-3)
+ * BF16 modes return CRAB_EINVAL. */
 int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                              int implicit_hydrogen, int precision, double* out);
 /* Device time of the last multipole call on this context: all its kernels
