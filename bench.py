@@ -52,9 +52,12 @@ FLUSH_BYTES = 256 << 20
 
 
 def _variant_name(v: int) -> str:
-    """Autotuner variant code Q*16 + jb; jb >= 8 is the q-packed kernel with jb-8 chains."""
+    """Autotuner variant code Q*16 + jb; jb >= 8 is the q-packed kernel with (jb-8) % 4 chains,
+    jb >= 12 its build for three CTAs per SM."""
     q, jb = int(v) // 16, int(v) % 16
-    return f"Q{q}xJ{jb - 8}pq" if jb >= 8 else f"Q{q}xJ{jb}"
+    if jb < 8:
+        return f"Q{q}xJ{jb}"
+    return f"Q{q}xJ{(jb - 8) % 4}pq" + ("-3cta" if jb >= 12 else "")
 
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))

@@ -44,8 +44,10 @@ using namespace dev;
 
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
 constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 128};  // compiled q-block lengths
-// jb values at or above kPackedQ select the q-packed kernel with jb - kPackedQ chains.
+// jb values at or above kPackedQ select the q-packed kernel with
+// (jb - kPackedQ) % kDenser chains; + kDenser asks for 3 CTAs per SM.
 constexpr int kPackedQ = 8;
+constexpr int kDenser = 4;
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
 template <int Q>
@@ -289,8 +291,8 @@ __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2],
   __syncthreads();
 }
 
-template <int Q, int JB>
-__global__ void __launch_bounds__(kThreads, Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))
+template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))>
+__global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                    int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
                    int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
@@ -487,14 +489,14 @@ void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const i
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
-template <int Q, int JB>
+template <int Q, int JB, int OCC>
 void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                     int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
                     int* status, int* next_work, const int64_t* work_out) {
   int per_sm = 0;
-  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB>, kThreads, 0));
+  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
-  k_pair_fp32_pq<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
+  k_pair_fp32_pq<Q, JB, OCC><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
                                                         status, next_work, work_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
@@ -641,8 +643,9 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
 
 // Untuned choice of (Q, jb): the block length by a cost model (launched steps
 // of 3 FP32 ops each plus a per-pair seed of about 60 ops per block), and the
-// q-packed kernel where it is compiled for that length (one chain at Q = 128,
-// two below, the fastest on the 20k-atom config-2 workload).
+// q-packed kernel where it is compiled for that length (one chain and three
+// CTAs per SM at Q = 128, two chains below: the fastest on the 20k-atom
+// config-2 workload).
 int2 default_variant(const std::vector<double>& q) {
   int bestQ = 64;
   long best_cost = -1;
@@ -653,7 +656,7 @@ int2 default_variant(const std::vector<double>& q) {
       bestQ = Qc;
     }
   }
-  if (bestQ == 128) return make_int2(128, 1 + kPackedQ);
+  if (bestQ == 128) return make_int2(128, 1 + kPackedQ + kDenser);
   const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
@@ -812,16 +815,17 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH(64, 4)
     CRAB_LAUNCH(96, 4)
 #undef CRAB_LAUNCH
-#define CRAB_LAUNCH_PQ(QQ, JJ)                                                                                  \
-  if (P.Q == QQ && P.jb == JJ + kPackedQ) {                                                                      \
-    launch_fp32_pq<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange,  \
-                           nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);                           \
+#define CRAB_LAUNCH_PQ(QQ, JJ, OO, CODE)                                                                        \
+  if (P.Q == QQ && P.jb == CODE) {                                                                               \
+    launch_fp32_pq<QQ, JJ, OO>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,          \
+                               P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);           \
     launched = true;                                                                                             \
   }
-    CRAB_LAUNCH_PQ(64, 2)
-    CRAB_LAUNCH_PQ(96, 2)
-    CRAB_LAUNCH_PQ(128, 1)
-    CRAB_LAUNCH_PQ(128, 2)
+    CRAB_LAUNCH_PQ(64, 2, 4, 2 + kPackedQ)
+    CRAB_LAUNCH_PQ(96, 2, 3, 2 + kPackedQ)
+    CRAB_LAUNCH_PQ(128, 1, 2, 1 + kPackedQ)
+    CRAB_LAUNCH_PQ(128, 2, 2, 2 + kPackedQ)
+    CRAB_LAUNCH_PQ(128, 1, 3, 1 + kPackedQ + kDenser)
 #undef CRAB_LAUNCH_PQ
     if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
   }
@@ -957,7 +961,8 @@ namespace crab {
 // Every (Q, jb) pair that pair_plan_launch can dispatch.
 static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2},
                                      {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
-                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ}};
+                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
+                                     {128, 1 + kPackedQ + kDenser}};
 
 bool pair_variant_known(int variant) {
   const int Q = variant / 16, jb = variant % 16;
@@ -979,7 +984,8 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out
   if (n_out) *n_out = 0;
   if (P.fp64 || P.nq == 0 || P.L.n_tiles == 0) return P.Q;
   static const int kVariants[][2] = {{64, 2},  {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
-                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ}};
+                                     {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
+                                     {128, 1 + kPackedQ + kDenser}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;

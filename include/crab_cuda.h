@@ -191,7 +191,8 @@ int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int
 /* Autotune: time every compiled kernel variant on this plan (q-block length Q
  * = q values one thread advances per pair between exact re-seeds, and JB = j
  * atoms per thread iteration; JB >= 8 selects the q-packed kernel, whose f32x2
- * registers hold two consecutive q points, with JB-8 independent chains) and
+ * registers hold two consecutive q points, with (JB-8) % 4 independent chains,
+ * built for three CTAs per SM when JB >= 12) and
  * keep the fastest.  *chosen = Q*16 + JB;
  * the first `capacity` variants and their times (ms) are written to
  * variants/ms (may be NULL), their count to *n_variants. */
