@@ -376,6 +376,41 @@ def multipole_section(eng, rank, fp32_peak):
             "config2_multipole_l30_curve_ms": c2_ms}
 
 
+def grid_and_gradient_section(eng, rank):
+    """Hydration grid of config 2 (adaptive, 3 Å spacing; bit-exact against the
+    oracle in the tests) and chi^2 with its full adjoint gradient on config 4
+    (5,000 atoms, 100 q): wall time per public call, median of 5 after a warm-up."""
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import synth
+
+    def med(fn, n=5):
+        fn()
+        ts = []
+        for _ in range(n):
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return float(np.median(ts))
+
+    s2 = synth.protein(synth.CONFIG2.seed + 1000 * rank, synth.CONFIG2.n_atoms, synth.CONFIG2.radius)
+    sites, _ = cs.hydration_grid_adaptive(s2, 3.0, engine=eng)
+    grid_ms = med(lambda: cs.hydration_grid_adaptive(s2, 3.0, engine=eng))
+    ext = cs.hydration_grid_exterior(s2, engine=eng)[0]
+    ext_ms = med(lambda: cs.hydration_grid_exterior(s2, engine=eng))
+    w = synth.CONFIG4
+    s4 = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
+    y = cs.compute_curve(s4, w.q, cs.ComputeOptions(method=cs.ScatteringMethod.Debye,
+                                                    solvent=cs.SolventParams())).intensity
+    sigma = 0.01 * y
+    grad_ms = med(lambda: cs.chi2_grad(s4, w.q, 1.01 * y, sigma, cs.SolventParams(), 1.0, 0.0, engine=eng))
+    pairq = s4.atom_count * (s4.atom_count - 1) / 2.0 * len(w.q)
+    return {"adaptive_grid_config2": {"ms": grid_ms, "sites": int(len(sites)), "atoms": s2.atom_count},
+            "exterior_grid_config2": {"ms": ext_ms, "sites": int(len(ext))},
+            "chi2_grad_config4": {"ms": grad_ms, "atoms": s4.atom_count, "n_q": len(w.q),
+                                  "pair_q_per_s": 2.0 * pairq / (grad_ms * 1e-3),
+                                  "note": "ordered pairs (i, j) and (j, i): 2 * N(N-1)/2 * nq per call"}}
+
+
 def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
@@ -489,6 +524,7 @@ def run_ours(args, rank, world, local):
 
     ens = None if args.no_ensemble else ensemble_section(eng, rank)
     mp = None if args.no_multipole else multipole_section(eng, rank, peak.value)
+    aux = None if args.no_multipole else grid_and_gradient_section(eng, rank)
 
     if rank == 0:
         line = {
@@ -509,6 +545,7 @@ def run_ours(args, rank, world, local):
             "parity": {"max_rel_err_vs_fp64": max_rel, "c1": c1, "c2": c2},
             "ensemble": ens,
             "multipole": mp,
+            "grids_and_gradient": aux,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,

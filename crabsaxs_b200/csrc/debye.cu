@@ -502,10 +502,9 @@ void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, cons
 }
 
 template <class T>
-T* upload(crab_ctx* ctx, std::vector<void*>& owned, const T* src, size_t count, cudaStream_t s) {
-  void* p = nullptr;
-  CRAB_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-  owned.push_back(p);
+T* upload(crab_ctx* ctx, PairPlan& P, std::vector<void*>& list, const char* name, const T* src, size_t count,
+          cudaStream_t s) {
+  void* p = plan_alloc(ctx, P, list, name, std::max<size_t>(count, 1) * sizeof(T));
   if (count && src) copy_h2d(ctx, p, src, count * sizeof(T), s);
   return (T*)p;
 }
@@ -534,8 +533,10 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
     rmax = std::max(rmax, std::sqrt(r2));
   }
   L.extent = 2.0 * rmax;
-  // order: type, then Morton code of the centred position
-  std::vector<uint64_t> key(n);
+  // order: type, then the 30-bit Morton code of the centred position, ties by
+  // input index (a counting sort by type, then a stable LSD radix sort of the
+  // Morton codes within each type, three 10-bit digits)
+  std::vector<uint32_t> key(n);
   for (int64_t i = 0; i < n; ++i) {
     uint32_t m = 0;
     for (int d = 0; d < 3; ++d) {
@@ -543,13 +544,26 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
       double cell = std::floor((xyz[3 * i + d] - c[d] - lo[d]) / span * 1024.0);
       m |= morton10((uint32_t)std::min(1023.0, std::max(0.0, cell))) << d;
     }
-    key[i] = ((uint64_t)(uint32_t)type[i] << 32) | m;
+    key[i] = m;
   }
-  std::vector<int64_t> order(n);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
   std::vector<int64_t> count(T, 0);
   for (int64_t i = 0; i < n; ++i) count[type[i]]++;
+  std::vector<int64_t> order(n), tmp(n), tstart(T + 1, 0);
+  for (int t = 0; t < T; ++t) tstart[t + 1] = tstart[t] + count[t];
+  {
+    std::vector<int64_t> pos(tstart.begin(), tstart.end() - 1);
+    for (int64_t i = 0; i < n; ++i) order[pos[type[i]]++] = i;
+  }
+  for (int t = 0; t < T; ++t) {
+    const int64_t a = tstart[t], b = tstart[t + 1];
+    for (int shift = 0; shift < 30; shift += 10) {
+      int64_t digit[1025] = {0};
+      for (int64_t k = a; k < b; ++k) digit[((key[order[k]] >> shift) & 1023u) + 1]++;
+      for (int d = 0; d < 1024; ++d) digit[d + 1] += digit[d];
+      for (int64_t k = a; k < b; ++k) tmp[a + digit[(key[order[k]] >> shift) & 1023u]++] = order[k];
+      std::copy(tmp.begin() + a, tmp.begin() + b, order.begin() + a);
+    }
+  }
   int64_t n_pad = 0;
   for (int t = 0; t < T; ++t) n_pad += (count[t] + kTile - 1) / kTile * kTile;
   L.n_pad = n_pad;
@@ -691,17 +705,18 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   } else {
     std::vector<int64_t> out;
     make_work_segments(P, P.n_qblocks, 8, work, out);
-    P.d_work_out = upload(ctx, P.qcfg, out.data(), out.size(), ctx->stream);
+    P.d_work_out = upload(ctx, P, P.qcfg, "work_out", out.data(), out.size(), ctx->stream);
   }
   P.n_work = (int)work.size();
-  P.d_work = upload(ctx, P.qcfg, work.data(), work.size(), ctx->stream);
-  P.d_qpar = upload(ctx, P.qcfg, qpar.data(), qpar.size(), ctx->stream);
-  P.d_qrange = upload(ctx, P.qcfg, qrange.data(), qrange.size(), ctx->stream);
+  P.d_work = upload(ctx, P, P.qcfg, "work", work.data(), work.size(), ctx->stream);
+  P.d_qpar = upload(ctx, P, P.qcfg, "qpar", qpar.data(), qpar.size(), ctx->stream);
+  P.d_qrange = upload(ctx, P, P.qcfg, "qrange", qrange.data(), qrange.size(), ctx->stream);
 }
 
 std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
-                                         const LatticeSpec* lattice) {
+                                         const LatticeSpec* lattice, bool pooled) {
   std::unique_ptr<PairPlan> P(new PairPlan());
+  P->pooled = pooled;
   P->L = std::move(L);
   P->fp64 = fp64;
   P->nq = nq;
@@ -720,7 +735,7 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
     P->lattice_first_tile = first;
   }
   if (!fp64) {
-    P->d_atoms = upload(ctx, P->owned, (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
+    P->d_atoms = upload(ctx, *P, P->owned, "atoms", (const float4*)P->L.atoms.data(), (size_t)P->L.n_pad, s);
     const int2 v = ctx->pair_variant ? make_int2(ctx->pair_variant / 16, ctx->pair_variant % 16)
                                       : default_variant(P->q);
     configure_fp32(ctx, *P, v.x, v.y);
@@ -728,13 +743,13 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
     const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8, P->L.n_tiles);
     P->n_work = (int)work.size();
-    P->d_atoms64 = upload(ctx, P->owned, (const double4*)P->L.atoms64.data(), (size_t)P->L.n_pad, s);
-    P->d_work = upload(ctx, P->owned, work.data(), work.size(), s);
-    P->d_q = upload(ctx, P->owned, q, (size_t)nq, s);
+    P->d_atoms64 = upload(ctx, *P, P->owned, "atoms64", (const double4*)P->L.atoms64.data(), (size_t)P->L.n_pad, s);
+    P->d_work = upload(ctx, *P, P->owned, "work64", work.data(), work.size(), s);
+    P->d_q = upload(ctx, *P, P->owned, "q", q, (size_t)nq, s);
   }
-  P->d_tile_type = upload(ctx, P->owned, P->L.tile_type.data(), P->L.tile_type.size(), s);
-  P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)P->n_pairs * nq, s);
-  P->d_status = upload<int>(ctx, P->owned, nullptr, 2, s);
+  P->d_tile_type = upload(ctx, *P, P->owned, "tile_type", P->L.tile_type.data(), P->L.tile_type.size(), s);
+  P->d_out = upload<double>(ctx, *P, P->owned, "out", nullptr, (size_t)P->n_pairs * nq, s);
+  P->d_status = upload<int>(ctx, *P, P->owned, "status", nullptr, 2, s);
   P->d_next = P->d_status + 1;
   if (lattice) lattice_plan_init(ctx, *P, lattice->cells, lattice->m, lattice->spacing);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -772,13 +787,13 @@ std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout
   P->lattice_first_tile = L.n_tiles;
   cudaStream_t s = ctx->stream;
   if (nq == 0 || L.n_tiles == 0) return P;
-  P->d_atoms = upload(ctx, P->owned, (const float4*)L.atoms.data(), (size_t)L.n_pad, s);
+  P->d_atoms = upload(ctx, *P, P->owned, "atoms", (const float4*)L.atoms.data(), (size_t)L.n_pad, s);
   const int2 v = ctx->pair_variant ? make_int2(ctx->pair_variant / 16, ctx->pair_variant % 16)
                                     : default_variant(P->q);
   configure_fp32(ctx, *P, v.x, v.y);
-  P->d_tile_type = upload(ctx, P->owned, L.tile_type.data(), L.tile_type.size(), s);
-  P->d_out = upload<double>(ctx, P->owned, nullptr, (size_t)(P->segments.size() - 1) * P->n_pairs * nq, s);
-  P->d_status = upload<int>(ctx, P->owned, nullptr, 2, s);
+  P->d_tile_type = upload(ctx, *P, P->owned, "tile_type", L.tile_type.data(), L.tile_type.size(), s);
+  P->d_out = upload<double>(ctx, *P, P->owned, "out", nullptr, (size_t)(P->segments.size() - 1) * P->n_pairs * nq, s);
+  P->d_status = upload<int>(ctx, *P, P->owned, "status", nullptr, 2, s);
   P->d_next = P->d_status + 1;
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   return P;
@@ -889,7 +904,7 @@ void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bo
   std::unique_ptr<PairPlan> P;
   {
     TraceScope tp("make_pair_plan");
-    P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice);
+    P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice, true);  // lives inside this call
   }
   out.pair.assign((size_t)P->n_pairs * nq, 0.0);
   {

@@ -186,6 +186,7 @@ struct PairPlan {
   int n_pairs = 0, Q = 0, jb = 2, n_qblocks = 0, n_work = 0, wide = 0;
   std::vector<void*> owned;
   std::vector<void*> qcfg;  // q-block and work-list buffers (rebuilt when Q changes)
+  bool pooled = false;      // buffers from the context pool (a plan that lives inside one call)
   float4* d_atoms = nullptr;
   double4* d_atoms64 = nullptr;
   int* d_tile_type = nullptr;
@@ -202,6 +203,18 @@ struct PairPlan {
   LatticePart lattice;
   ~PairPlan();
 };
+
+// Device memory of a pair plan: its own cudaMalloc, freed with the plan, or
+// for a pooled plan the context's grow-only buffer of that name (no
+// allocation once the pool is large enough).
+inline void* plan_alloc(crab_ctx* ctx, PairPlan& P, std::vector<void*>& list, const char* name, size_t bytes) {
+  bytes = bytes ? bytes : 1;
+  if (P.pooled) return ctx->dev(std::string("pair.") + name, bytes);
+  void* p = nullptr;
+  CRAB_CUDA_CHECK(cudaMalloc(&p, bytes));
+  list.push_back(p);
+  return p;
+}
 // Lattice description of the last type (hydration sites on a voxel grid):
 // cells are the sites' integer voxel indices (3 per site, in any order).
 struct LatticeSpec {
@@ -213,7 +226,7 @@ void lattice_plan_init(crab_ctx* ctx, PairPlan& P, const int32_t* cells, int64_t
 void lattice_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s);
 bool q_grid_uniform(const double* q, int64_t nq);
 std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
-                                         const LatticeSpec* lattice = nullptr);
+                                         const LatticeSpec* lattice = nullptr, bool pooled = false);
 // Enqueue the pair kernel on stream s (device time recorded when timed).
 void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed);
 // Copy back and convert raw sums to P_ab(q) (divide by q; exact q = 0).

@@ -102,21 +102,13 @@ void lattice_plan_init(crab_ctx* ctx, PairPlan& P, const int32_t* cells, int64_t
   }
   std::vector<int4> c4(std::max<int64_t>(m, 1));
   for (int64_t i = 0; i < m; ++i) c4[i] = make_int4(cells[3 * i], cells[3 * i + 1], cells[3 * i + 2], 0);
-  void* p = nullptr;
-  CRAB_CUDA_CHECK(cudaMalloc(&p, c4.size() * sizeof(int4)));
-  P.owned.push_back(p);
-  Lp.d_cells = (int4*)p;
+  Lp.d_cells = (int4*)plan_alloc(ctx, P, P.owned, "lattice_cells", c4.size() * sizeof(int4));
   copy_h2d(ctx, Lp.d_cells, c4.data(), (size_t)m * sizeof(int4), ctx->stream);
-  CRAB_CUDA_CHECK(cudaMalloc(&p, (size_t)Lp.bins * sizeof(unsigned long long)));
-  P.owned.push_back(p);
-  Lp.d_hist = (unsigned long long*)p;
-  CRAB_CUDA_CHECK(cudaMalloc(&p, (size_t)std::max<int64_t>(P.nq, 1) * sizeof(double)));
-  P.owned.push_back(p);
-  Lp.d_out = (double*)p;
+  Lp.d_hist = (unsigned long long*)plan_alloc(ctx, P, P.owned, "lattice_hist",
+                                               (size_t)Lp.bins * sizeof(unsigned long long));
+  Lp.d_out = (double*)plan_alloc(ctx, P, P.owned, "lattice_out", (size_t)std::max<int64_t>(P.nq, 1) * sizeof(double));
   if (!P.d_q) {
-    CRAB_CUDA_CHECK(cudaMalloc(&p, (size_t)std::max<int64_t>(P.nq, 1) * sizeof(double)));
-    P.owned.push_back(p);
-    P.d_q = (double*)p;
+    P.d_q = (double*)plan_alloc(ctx, P, P.owned, "lattice_q", (size_t)std::max<int64_t>(P.nq, 1) * sizeof(double));
     copy_h2d(ctx, P.d_q, P.q.data(), (size_t)P.nq * sizeof(double), ctx->stream);
   }
   Lp.active = true;
