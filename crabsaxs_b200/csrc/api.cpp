@@ -24,6 +24,30 @@ bool crab::trace_enabled() {
   return on;
 }
 
+namespace {
+thread_local crab::TraceScope* g_trace_top = nullptr;
+}
+
+crab::TraceScope::TraceScope(const char* n) : name(n), on(trace_enabled()), parent(nullptr) {
+  if (!on) return;
+  t0 = std::chrono::steady_clock::now();
+  parent = g_trace_top;
+  g_trace_top = this;
+}
+
+crab::TraceScope::~TraceScope() {
+  if (!on) return;
+  std::fprintf(stderr, "[crab] %s %.3f ms\n", name,
+               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  g_trace_top = parent;
+}
+
+void crab::trace_mark(const char* name) {
+  if (!trace_enabled() || !g_trace_top) return;
+  std::fprintf(stderr, "[crab] %s: %s at %.3f ms\n", g_trace_top->name, name,
+               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_trace_top->t0).count());
+}
+
 void* crab_ctx::dev(const std::string& name, size_t bytes) {
   crab::DevBuf& b = bufs[name];
   if (b.bytes < bytes || !b.ptr) {
@@ -105,10 +129,13 @@ static bool excluded_zero(const AtomClass& c, bool implicit) {
 }
 
 TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites) {
+  // Classes are (element 0..14, united-atom group -1..13), numbered in
+  // (element, group) order; a direct 15 x 15 table replaces a map lookup per atom.
   TypedAtoms t;
-  std::map<AtomClass, int> index;
+  constexpr int kE = CRAB_EL_OTHER + 1, kG = 15;
+  int present[kE][kG] = {};
   std::vector<int64_t> keep;
-  std::vector<AtomClass> cls_of;
+  keep.reserve(st->n);
   for (int64_t i = 0; i < st->n; ++i) {
     const AtomClass c{st->elem[i], implicit ? (int)st->group[i] : -1};
     bool drop = false;
@@ -116,29 +143,31 @@ TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const 
     else if (need == TermSet::SolventGrid) drop = vacuum_zero(c, implicit) && excluded_zero(c, implicit);
     if (drop) continue;
     keep.push_back(i);
-    cls_of.push_back(c);
-    index[c] = 0;
+    present[c.element][c.group + 1] = 1;
   }
+  int index[kE][kG];
   int next = 0;
-  for (auto& kv : index) {
-    kv.second = next++;
-    t.cls.push_back(kv.first);
-  }
+  for (int e = 0; e < kE; ++e)
+    for (int g = 0; g < kG; ++g) {
+      index[e][g] = present[e][g] ? next++ : -1;
+      if (present[e][g]) t.cls.push_back(AtomClass{e, g - 1});
+    }
   const int64_t ns = sites ? (int64_t)sites->size() / 3 : 0;
   if (sites) t.cls.push_back(AtomClass{-1, -1});
-  t.xyz.resize(3 * (keep.size() + ns));
-  t.w.resize(keep.size() + ns);
-  t.type.resize(keep.size() + ns);
-  t.src.assign(keep.size() + ns, -1);
-  for (size_t k = 0; k < keep.size(); ++k) {
+  const size_t nk = keep.size();
+  t.xyz.resize(3 * (nk + ns));
+  t.w.resize(nk + ns);
+  t.type.resize(nk + ns);
+  t.src.assign(nk + ns, -1);
+  for (size_t k = 0; k < nk; ++k) {
     const int64_t i = keep[k];
     for (int d = 0; d < 3; ++d) t.xyz[3 * k + d] = st->xyz[3 * i + d];
     t.w[k] = st->occ[i];
-    t.type[k] = index[cls_of[k]];
+    t.type[k] = index[st->elem[i]][(implicit ? (int)st->group[i] : -1) + 1];
     t.src[k] = i;
   }
   for (int64_t s = 0; s < ns; ++s) {
-    const size_t k = keep.size() + s;
+    const size_t k = nk + s;
     for (int d = 0; d < 3; ++d) t.xyz[3 * k + d] = (*sites)[3 * s + d];
     t.w[k] = 1.0;
     t.type[k] = next;

@@ -40,18 +40,16 @@ inline void require(bool ok, const std::string& msg) {
 // prints "[crab] <name> <ms>" to stderr when it closes (wall time of the
 // phase, including the stream synchronisations inside it).
 bool trace_enabled();
+// Prints the wall time since the innermost open TraceScope started (a split
+// inside a phase).
+void trace_mark(const char* name);
 struct TraceScope {
   const char* name;
   bool on;
   std::chrono::steady_clock::time_point t0;
-  explicit TraceScope(const char* n) : name(n), on(trace_enabled()) {
-    if (on) t0 = std::chrono::steady_clock::now();
-  }
-  ~TraceScope() {
-    if (on)
-      std::fprintf(stderr, "[crab] %s %.3f ms\n", name,
-                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-  }
+  TraceScope* parent;
+  explicit TraceScope(const char* n);
+  ~TraceScope();
 };
 
 // Grow-only device buffer: one per named slot in the context, so repeated

@@ -780,6 +780,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   std::vector<double> inv(L + 2, 0.0);
   for (int k = 1; k <= L + 1; ++k) inv[k] = 1.0 / (double)k;
 
+  trace_mark("mp_host_prep");
   TraceScope tdev("multipole_device");
   cudaStream_t s = ctx->stream;
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
@@ -981,14 +982,19 @@ void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double
     std::fill(out, out + nq, 0.0);
     return;
   }
-  TypedAtoms t = type_atoms(st, implicit, TermSet::Vacuum, nullptr);
+  TraceScope trace("multipole_intensity");
+  TypedAtoms t;
   MpInput in;
-  in.t = &t;
-  double rmax;
-  centre_and_rmax(st, in.centre, &rmax);
-  in.rmax_lq = rmax;
   std::vector<double> V, E, H;
-  multipole_tables(t, q, nq, nullptr, implicit, 0.0, V, E, H);
+  {
+    TraceScope tt("mp_type_atoms+tables");
+    t = type_atoms(st, implicit, TermSet::Vacuum, nullptr);
+    in.t = &t;
+    double rmax;
+    centre_and_rmax(st, in.centre, &rmax);
+    in.rmax_lq = rmax;
+    multipole_tables(t, q, nq, nullptr, implicit, 0.0, V, E, H);
+  }
   in.amp = V;
   in.K = 1;
   multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
