@@ -82,7 +82,7 @@ def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
     ap.add_argument("workload", choices=["debye-config2", "multipole-config3", "gradient-config4"])
     ap.add_argument("--variant", type=int, default=None)
-    ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="fp32")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
     ap.add_argument("--repeats", type=int, default=2)
     a = ap.parse_args(argv)
     engine = cs.Engine.default(0)
