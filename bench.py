@@ -505,8 +505,11 @@ def run_ours(args, rank, world, local):
     eng.reset_stats()
     dist.barrier()
     t0 = time.perf_counter()
+    e2e_steps = []
     for _ in range(args.steps):
+        ts = time.perf_counter()
         e2e_step()
+        e2e_steps.append((time.perf_counter() - ts) * 1e3)
     e2e_s = time.perf_counter() - t0
     dist.barrier()
     e2e_launches, _, _ = eng.stats()
@@ -549,7 +552,8 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,
-                    "ms_per_step": 1e3 * e2e_s / args.steps},
+                    "ms_per_step": 1e3 * e2e_s / args.steps,
+                    "step_ms_min_median_max": [min(e2e_steps), float(np.median(e2e_steps)), max(e2e_steps)]},
             "gpu_launches": int(launches),
             "e2e_gpu_launches": int(e2e_launches),
             "clocks": clocks.summary(),
