@@ -839,3 +839,72 @@ def reweight_curves(names: Sequence[str], curves, experimental: ExperimentalCurv
                                                               fo.solvent.c2),
                                 res.chi2, res.reduced_chi2, res.kl_divergence, res.effective_sample_size,
                                 res.iterations, bool(res.converged))
+
+
+# ---------------------------------------------------------------- coordinate P(r)
+@dataclass
+class PrOptions:
+    """metrics.rs:15-29: bins of the coordinate P(r) (raised to at least 16);
+    max_r only bounds the experimental transform, which is not on this path."""
+    bins: int = 160
+    max_r: Optional[float] = None
+
+
+@dataclass
+class PairDistribution:
+    """metrics.rs:31-37; rg / dmax are None where the reference has None."""
+    r: np.ndarray
+    p: np.ndarray
+    rg: Optional[float]
+    dmax: Optional[float]
+
+
+@dataclass
+class CoordinateFeatures:
+    """metrics.rs:60-65."""
+    rg: float
+    dmax: float
+    p_r: PairDistribution
+
+
+def coordinate_features(structure: Structure, options: Optional[PrOptions] = None,
+                        engine: Optional[Engine] = None) -> CoordinateFeatures:
+    """metrics.rs:236-270: scattering-weighted Rg, Dmax and normalised P(r)."""
+    eng = engine or Engine.default()
+    o = options or PrOptions()
+    m = max(int(o.bins), 16)
+    r, p = np.empty(m), np.empty(m)
+    rg, dmax, prg, pdm = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    used = C.c_int64()
+    eng.check(N.lib.crab_coordinate_features(eng.handle, structure.handle(eng), int(o.bins), C.byref(rg),
+                                             C.byref(dmax), _dp(r), _dp(p), C.byref(used), C.byref(prg),
+                                             C.byref(pdm)))
+    k = used.value
+
+    def opt(x):
+        return None if math.isnan(x) else x
+
+    return CoordinateFeatures(rg.value, dmax.value,
+                              PairDistribution(r[:k].copy(), p[:k].copy(), opt(prg.value), opt(pdm.value)))
+
+
+def pair_distance_histogram(xyz, w, bins: int, engine: Optional[Engine] = None):
+    """metrics.rs:475-522 before normalisation: (dmax, weighted histogram [bins])."""
+    eng = engine or Engine.default()
+    x = _f64(xyz).reshape(-1, 3)
+    ww = _f64(w)
+    if len(ww) != x.shape[0]:
+        raise InvalidInput("one weight per atom")
+    hist = np.empty(max(int(bins), 0))
+    dmax = C.c_double()
+    eng.check(N.lib.crab_pair_distance_histogram(eng.handle, _dp(x), _dp(ww), x.shape[0], int(bins),
+                                                 C.byref(dmax), _dp(hist)))
+    return dmax.value, hist
+
+
+def pr_last_timing(engine: Optional[Engine] = None):
+    """Device ms of the last P(r) call (all kernels, histogram kernel) and its pair count."""
+    eng = engine or Engine.default()
+    t, h, n = C.c_double(), C.c_double(), C.c_double()
+    eng.check(N.lib.crab_pr_last_timing(eng.handle, C.byref(t), C.byref(h), C.byref(n)))
+    return t.value, h.value, n.value

@@ -84,6 +84,9 @@ struct crab_ctx {
   // GEMM alone, and the GEMM's algorithmic FLOP count
   double last_mp_ms = 0.0, last_mp_gemm_ms = 0.0, last_mp_gemm_flop = 0.0;
   int pair_variant = 0;  // kernel variant of plans built by one-shot calls (0: automatic)
+  // device times of the last pair-distance histogram: all its kernels, the
+  // histogram kernel alone, and the pairs it binned
+  double last_pr_ms = 0.0, last_pr_hist_ms = 0.0, last_pr_pairs = 0.0;
 
   void* dev(const std::string& name, size_t bytes);
   void* host(const std::string& name, size_t bytes);
@@ -275,3 +278,15 @@ struct crab_struct {
   std::vector<int8_t> elem;
   std::vector<int8_t> group;
 };
+
+namespace crab {
+// ---------------------------------------------------------------- coordinate P(r)
+// Weighted pair-distance histogram (metrics.rs:475-522): returns dmax and
+// fills hist[bins] with Σ w_i w_j per bin; dmax 0 and hist zero when every
+// pair distance is zero.
+double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w, int64_t n, int64_t bins,
+                               double* hist);
+// metrics.rs:236-270 coordinate_features (see crab_coordinate_features).
+void coordinate_features(crab_ctx* ctx, const crab_struct* st, int64_t bins, double* rg, double* dmax, double* r,
+                         double* p, int64_t* m, double* pr_rg, double* pr_dmax);
+}  // namespace crab

@@ -3,6 +3,7 @@
     python -m crabsaxs_b200.workloads debye-config2 [--variant V] [--repeats N]
     python -m crabsaxs_b200.workloads multipole-config3 [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
     python -m crabsaxs_b200.workloads gradient-config4 [--repeats N]
+    python -m crabsaxs_b200.workloads pr-config3 [--bins B] [--repeats N]
 
 debye-config2: the 20,000-atom synthetic protein plus its adaptive 3 Å
 hydration sites, 500 q on [0.001, 0.5], one lattice pair plan (atoms by the
@@ -11,6 +12,8 @@ FP32 recurrence kernel, site-site pairs by the exact lattice histogram),
 plan's untuned choice).
 multipole-config3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.
 gradient-config4: 5,000 atoms (R 28 Å), 100 q, chi^2 and its full gradient.
+pr-config3: coordinate features (Rg, Dmax, P(r) with 160 bins) of the
+100,000-atom structure of multipole-config3.
 Each prints one line with its device or wall times.
 """
 from __future__ import annotations
@@ -78,9 +81,25 @@ def gradient_config4(engine: cs.Engine, repeats: int) -> str:
     return f"gradient-config4 wall_ms={np.round(wall, 3).tolist()}"
 
 
+def pr_config3(engine: cs.Engine, bins: int, repeats: int) -> str:
+    w = synth.CONFIG3
+    s = synth.protein(w.seed, w.n_atoms, w.radius)
+    wall, dev, hist = [], [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        cs.coordinate_features(s, cs.PrOptions(bins=bins), engine=engine)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        total_ms, hist_ms, pairs = cs.pr_last_timing(engine)
+        dev.append(total_ms)
+        hist.append(hist_ms)
+    return (f"pr-config3 bins={bins} pairs={pairs:.6g} wall_ms={np.round(wall, 3).tolist()} "
+            f"device_ms={np.round(dev, 3).tolist()} histogram_ms={np.round(hist, 3).tolist()}")
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
-    ap.add_argument("workload", choices=["debye-config2", "multipole-config3", "gradient-config4"])
+    ap.add_argument("workload", choices=["debye-config2", "multipole-config3", "gradient-config4", "pr-config3"])
+    ap.add_argument("--bins", type=int, default=160)
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
     ap.add_argument("--repeats", type=int, default=2)
@@ -90,6 +109,8 @@ def main(argv=None) -> None:
         print(debye_config2(engine, a.variant, a.repeats))
     elif a.workload == "multipole-config3":
         print(multipole_config3(engine, a.precision, a.repeats))
+    elif a.workload == "pr-config3":
+        print(pr_config3(engine, a.bins, a.repeats))
     else:
         print(gradient_config4(engine, a.repeats))
 

@@ -21,6 +21,7 @@
  *                                 (behind SaxsFitter::fit analysis.rs:76-87 and SaxsScorer::score analysis.rs:156-177)
  *   crab_ensemble_fit             src/ensemble.rs:127-299   EnsembleFitter::fit / fit_core
  *   crab_reweight_curves          src/reweight.rs:84-154    reweight_curves
+ *   crab_coordinate_features      src/metrics.rs:236-270    coordinate_features (P(r): metrics.rs:475-583)
  *
  * Status codes map onto crabSAXS's SaxsError (src/error.rs:4-25):
  *   CRAB_EINVAL -> SaxsError::InvalidInput, CRAB_ENOTCONV -> FitDidNotConverge,
@@ -362,6 +363,33 @@ int crab_ensemble_plan_score(crab_ctx* ctx, crab_ensemble_plan* plan, const doub
                              double* elapsed_ms, double* best_fit, double* weights, double* grad_w,
                              double* kl_weights, double* reweight_out);
 int crab_ensemble_plan_destroy(crab_ensemble_plan* plan);
+
+/* ---- coordinate pair-distance distribution -------------------------------- */
+/* Weighted pair-distance histogram, coordinate_pr before normalisation
+ * (metrics.rs:475-522).  dmax is the square root of the largest squared pair
+ * distance dx*dx + dy*dy + dz*dz (f64, as the reference computes it); pair
+ * i < j adds w_i*w_j to hist[min(floor(r_ij / step), bins - 1)], step =
+ * dmax / bins.  The bin of every pair is the reference's, bit for bit; the
+ * sums differ from the reference's only by f64 summation order.  xyz (n*3) and
+ * w (n) are host arrays, bins in [1, 16777216], coordinates finite and below
+ * 1e100 in magnitude.  When every pair distance is zero (n < 2 included)
+ * *dmax = 0 and hist is all zero. */
+int crab_pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w, int64_t n, int64_t bins,
+                                 double* dmax, double* hist);
+/* coordinate_features (metrics.rs:236-270) with PrOptions::bins = bins:
+ * weights |form_factor_for_atom(atom, implicit hydrogens, q = 0)| floored at
+ * 1e-6, Rg about the weighted centre (rg), the largest pair distance (dmax),
+ * and the normalised P(r) of max(bins, 16) bins (normalize_distribution,
+ * metrics.rs:550-583): r and p receive *m values (*m = 1 for the reference's
+ * single-point results: all atoms at one position, or a non-positive area);
+ * pr_rg and pr_dmax are the distribution's Rg and Dmax, NaN for None.
+ * r and p must hold max(bins, 16) values.  Empty structure: CRAB_EINVAL. */
+int crab_coordinate_features(crab_ctx* ctx, crab_struct* st, int64_t bins, double* rg, double* dmax, double* r,
+                             double* p, int64_t* m, double* pr_rg, double* pr_dmax);
+/* Device time of the last pair-distance histogram on this context: all its
+ * kernels (dmax pass, bin edges, histogram), the histogram kernel alone, and
+ * the number of pairs n(n-1)/2.  Any pointer may be NULL. */
+int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs);
 
 /* ---- synthetic inputs (no counterpart in the reference) ----------------- */
 /* Seeded protein-like structure: Cα-style self-avoiding walk (3.8 Å steps,

@@ -60,6 +60,9 @@ _SIGS = {
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "orc_chi2_grad": (C.c_int, [I64, D, I32, I32, D, C.c_int, I64, D, D, D, C.c_double, C.c_double, C.c_double,
                                 C.c_double, C.c_double, C.c_double, D, D, D]),
+    "orc_pair_distance_histogram": (C.c_double, [I64, D, D, I64, D]),
+    "orc_normalize_distribution": (C.c_int, [I64, D, D, D, D]),
+    "orc_coordinate_features": (C.c_int, [I64, D, I32, I32, D, I64, D, D, D, D, C.POINTER(I64), D, D]),
 }
 for _n, (_r, _a) in _SIGS.items():
     _f = getattr(lib, _n)
@@ -265,3 +268,26 @@ def chi2_grad(a: Atoms, q, y, sigma, c1, c2, scale, background, thickness=3.0, d
                       _d(yy), _d(ss), c1, c2, thickness, density, scale, background, C.byref(chi),
                       None if gx is None else _d(gx), _d(gp))
     return chi.value, gx, gp
+
+
+def pair_distance_histogram(xyz, w, bins):
+    """metrics.rs:475-522: (dmax, raw weighted histogram of `bins` bins)."""
+    x, ww = _f64(xyz).reshape(-1, 3), _f64(w)
+    hist = np.empty(bins)
+    dmax = lib.orc_pair_distance_histogram(x.shape[0], _d(x), _d(ww), bins, _d(hist))
+    return dmax, hist
+
+
+def coordinate_features(a: Atoms, bins=160):
+    """metrics.rs:236-270: dict(rg, dmax, r, p, pr_rg, pr_dmax); None fields as NaN."""
+    m = max(int(bins), 16)
+    r, p = np.empty(m), np.empty(m)
+    rg, dmax, prg, pdm = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    used = C.c_int64()
+    rc = lib.orc_coordinate_features(a.n, _d(a.xyz), _i(a.element), _i(a.group), _d(a.occ), int(bins),
+                                     C.byref(rg), C.byref(dmax), _d(r), _d(p), C.byref(used), C.byref(prg),
+                                     C.byref(pdm))
+    if rc:
+        raise ValueError("coordinate features require a non-empty structure")
+    k = used.value
+    return dict(rg=rg.value, dmax=dmax.value, r=r[:k].copy(), p=p[:k].copy(), pr_rg=prg.value, pr_dmax=pdm.value)

@@ -1177,3 +1177,119 @@ ORC_API int orc_chi2_grad(int64_t n, const double* xyz, const int* elem, const i
   }
   return 0;
 }
+
+// ---------------------------------------------------------------- coordinate P(r)
+namespace {
+
+// metrics.rs:535-541 squared_distance: dx*dx + dy*dy + dz*dz, left to right.
+inline double squared_distance(const double* a, const double* b) {
+  const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// `(distance / step).floor() as usize` clamped to bins-1 (metrics.rs:515-516);
+// Rust's float-to-usize cast saturates and maps NaN to 0.
+inline int64_t pr_bin_index(double distance, double step, int64_t bins) {
+  const double v = std::floor(distance / step);
+  if (!(v >= 0.0)) return 0;
+  if (v >= (double)bins) return bins - 1;
+  return std::min<int64_t>((int64_t)v, bins - 1);
+}
+
+}  // namespace
+
+// metrics.rs:475-522 coordinate_pr up to the raw histogram: the maximum
+// squared pair distance (f64::max fold, which skips NaN), step = dmax/bins,
+// and per 64-row chunk a histogram of w_left*w_right over right > left,
+// the chunks added in order.  Returns dmax; hist (bins values) is zero when
+// every pair distance is zero (the reference returns early there).
+ORC_API double orc_pair_distance_histogram(int64_t n, const double* xyz, const double* w, int64_t bins, double* hist) {
+  double dmax2 = 0.0;
+#pragma omp parallel for reduction(max : dmax2) schedule(dynamic, 64)
+  for (int64_t l = 0; l < n; ++l) {
+    double m = 0.0;
+    for (int64_t r = l + 1; r < n; ++r) m = std::fmax(m, squared_distance(xyz + 3 * l, xyz + 3 * r));
+    dmax2 = std::fmax(dmax2, m);
+  }
+  for (int64_t k = 0; k < bins; ++k) hist[k] = 0.0;
+  if (dmax2 <= 0.0) return 0.0;
+  const double dmax = std::sqrt(dmax2);
+  const double step = dmax / (double)bins;
+  const int64_t kChunk = 64;
+  const int64_t n_chunks = (n + kChunk - 1) / kChunk;
+  std::vector<double> part((size_t)n_chunks * bins, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t c = 0; c < n_chunks; ++c) {
+    double* h = part.data() + (size_t)c * bins;
+    const int64_t end = std::min(n, (c + 1) * kChunk);
+    for (int64_t l = c * kChunk; l < end; ++l)
+      for (int64_t r = l + 1; r < n; ++r) {
+        const double d = std::sqrt(squared_distance(xyz + 3 * l, xyz + 3 * r));
+        h[pr_bin_index(d, step, bins)] += w[l] * w[r];
+      }
+  }
+  for (int64_t c = 0; c < n_chunks; ++c)
+    for (int64_t k = 0; k < bins; ++k) hist[k] += part[(size_t)c * bins + k];
+  return dmax;
+}
+
+// metrics.rs:550-583 normalize_distribution on (r, p) in place: trapezoid
+// area to 1, rg = sqrt(max(moment/2, 0)) from the trapezoid of r^2 p, dmax =
+// r at the last p above 1% of the maximum.  Returns 0 when the area is not
+// finite and positive (the reference's None); rg / dmax are NaN for None.
+ORC_API int orc_normalize_distribution(int64_t m, const double* r, double* p, double* rg, double* dmax) {
+  if (m <= 0) return 0;
+  double area = 0.0;
+  for (int64_t i = 0; i + 1 < m; ++i) area += 0.5 * (r[i + 1] - r[i]) * (p[i] + p[i + 1]);
+  if (!std::isfinite(area) || area <= 0.0) return 0;
+  for (int64_t i = 0; i < m; ++i) p[i] /= area;
+  double moment = 0.0;
+  for (int64_t i = 0; i + 1 < m; ++i)
+    moment += 0.5 * (r[i + 1] - r[i]) * (r[i] * r[i] * p[i] + r[i + 1] * r[i + 1] * p[i + 1]);
+  const double g = std::sqrt(std::fmax(moment / 2.0, 0.0));
+  *rg = std::isfinite(g) ? g : NAN;
+  double maximum = 0.0;
+  for (int64_t i = 0; i < m; ++i) maximum = std::fmax(maximum, p[i]);
+  *dmax = NAN;
+  for (int64_t i = m - 1; i >= 0; --i)
+    if (p[i] > maximum * 0.01) { *dmax = r[i]; break; }
+  return 1;
+}
+
+// metrics.rs:236-270 coordinate_features with metrics.rs:523-533: weights
+// |form_factor_for_atom(atom, implicit = true, q = 0)| floored at 1e-6, the
+// weighted centre and Rg, then coordinate_pr with max(bins, 16) bins.
+// r_out / p_out hold max(bins, 16) values; *m_out is the length used (1 for
+// the reference's single-point fallbacks).  Returns -1 for an empty structure.
+ORC_API int orc_coordinate_features(int64_t n, const double* xyz, const int* elem, const int* group,
+                                    const double* occ, int64_t bins, double* rg, double* dmax, double* r_out,
+                                    double* p_out, int64_t* m_out, double* pr_rg, double* pr_dmax) {
+  if (n <= 0) return -1;
+  bins = std::max<int64_t>(bins, 16);
+  std::vector<double> w(n);
+  for (int64_t i = 0; i < n; ++i) w[i] = std::fmax(std::fabs(form_factor(elem[i], group[i], occ[i], true, 0.0)), 1e-6);
+  double total = 0.0;
+  for (int64_t i = 0; i < n; ++i) total += w[i];
+  double c[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) c[d] = c[d] + xyz[3 * i + d] * w[i];
+  for (int d = 0; d < 3; ++d) c[d] = c[d] / total;
+  double acc = 0.0;
+  for (int64_t i = 0; i < n; ++i)
+    acc += w[i] * norm2(xyz[3 * i] - c[0], xyz[3 * i + 1] - c[1], xyz[3 * i + 2] - c[2]);
+  *rg = std::sqrt(acc / total);
+  std::vector<double> hist(bins);
+  const double dm = orc_pair_distance_histogram(n, xyz, w.data(), bins, hist.data());
+  *dmax = dm;
+  if (dm <= 0.0) {  // metrics.rs:489-498
+    r_out[0] = 0.0; p_out[0] = 1.0; *m_out = 1; *pr_rg = 0.0; *pr_dmax = 0.0;
+    return 0;
+  }
+  const double step = dm / (double)bins;
+  for (int64_t k = 0; k < bins; ++k) { r_out[k] = ((double)k + 0.5) * step; p_out[k] = hist[k]; }
+  *m_out = bins;
+  if (!orc_normalize_distribution(bins, r_out, p_out, pr_rg, pr_dmax)) {  // metrics.rs:527-532
+    r_out[0] = step * 0.5; p_out[0] = 1.0; *m_out = 1; *pr_rg = 0.0; *pr_dmax = dm;
+  }
+  return 0;
+}

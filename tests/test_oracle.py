@@ -309,3 +309,53 @@ def test_chi2_gradient_matches_central_differences():
         cm = O.chi2_grad(a, q, y, sigma, c1m, c2m, sm, bm, want_xyz=False)[0]
         fd = (cp - cm) / (2 * h)
         assert abs(gp[k] - fd) <= 1e-5 * max(abs(fd), 1e-6), (k, gp[k], fd)
+
+
+def _two_carbons_4a():  # metrics.rs:651-677: C at the origin and at 4 Å
+    return O.Atoms(np.array([[0.0, 0.0, 0.0], [4.0, 0.0, 0.0]]), np.array([C, C]))
+
+
+def test_coordinate_features_report_pair_distance():  # metrics.rs:678-684
+    f = O.coordinate_features(_two_carbons_4a())
+    assert abs(f["dmax"] - 4.0) < 1e-12
+    assert f["rg"] > 1.0
+    assert len(f["p"]) > 0
+
+
+def test_two_atom_distribution_closed_form():
+    """One pair at exactly dmax lands in the last bin (the bins-1 cap); the
+    trapezoid area is step/2 * p_last, so p_last = 2/step, the distribution's
+    Rg is r_last/sqrt(2) and its Dmax is r_last (metrics.rs:550-583)."""
+    f = O.coordinate_features(_two_carbons_4a(), bins=160)
+    step = 4.0 / 160
+    r_last = 159.5 * step
+    assert f["rg"] == 2.0 and f["dmax"] == 4.0
+    assert np.count_nonzero(f["p"]) == 1 and f["p"][-1] == pytest.approx(2.0 / step, rel=1e-15)
+    assert f["pr_rg"] == pytest.approx(r_last / math.sqrt(2.0), rel=1e-15)
+    assert f["pr_dmax"] == r_last
+
+
+def test_coordinate_pr_single_point_results():  # metrics.rs:489-498
+    same = O.Atoms(np.tile([1.0, 2.0, 3.0], (5, 1)), np.full(5, C))
+    f = O.coordinate_features(same)
+    assert f["dmax"] == 0.0 and list(f["r"]) == [0.0] and list(f["p"]) == [1.0]
+    assert f["pr_rg"] == 0.0 and f["pr_dmax"] == 0.0
+    with pytest.raises(ValueError):
+        O.coordinate_features(O.Atoms(np.zeros((0, 3)), np.zeros(0, dtype=int)))
+
+
+def test_coordinate_pr_bins_on_exact_edges():
+    """17 atoms on a line at integer positions with 16 bins: step = 1, so every
+    distance k falls exactly on the lower edge of bin k; distance 16 is capped
+    into bin 15 (metrics.rs:515-516)."""
+    xyz = np.zeros((17, 3))
+    xyz[:, 0] = np.arange(17)
+    dmax, hist = O.pair_distance_histogram(xyz, np.ones(17), 16)
+    expected = np.array([0.0] + [17.0 - k for k in range(1, 16)])
+    expected[15] += 1.0
+    assert dmax == 16.0 and np.array_equal(hist, expected)
+
+
+def test_coordinate_pr_bins_floor_at_sixteen():  # metrics.rs:268: options.bins.max(16)
+    f = O.coordinate_features(_two_carbons_4a(), bins=3)
+    assert len(f["p"]) == 16
