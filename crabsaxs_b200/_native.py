@@ -127,7 +127,7 @@ _SIGS = {
     "crab_synth_protein": (C.c_int, [C.c_uint64, I64, C.c_double, D, I8P]),
     "crab_pair_distance_histogram": (C.c_int, [P, D, D, I64, I64, D, D]),
     "crab_coordinate_features": (C.c_int, [P, P, I64, D, D, D, D, C.POINTER(I64), D, D]),
-    "crab_pr_last_timing": (C.c_int, [P, D, D, D]),
+    "crab_pr_last_timing": (C.c_int, [P, D, D, D, C.POINTER(C.c_int32)]),
     "crab_pair_plan_create": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, C.POINTER(P)]),
     "crab_pair_plan_create_lattice": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, I32P, I64, C.c_double,
                                                 C.POINTER(P)]),

@@ -903,8 +903,9 @@ def pair_distance_histogram(xyz, w, bins: int, engine: Optional[Engine] = None):
 
 
 def pr_last_timing(engine: Optional[Engine] = None):
-    """Device ms of the last P(r) call (all kernels, histogram kernel) and its pair count."""
+    """Device ms of the last P(r) call (all kernels, histogram kernel), its pair
+    count and accumulation mode (0 class counts, 1 shared f64, 2 device-memory f64)."""
     eng = engine or Engine.default()
-    t, h, n = C.c_double(), C.c_double(), C.c_double()
-    eng.check(N.lib.crab_pr_last_timing(eng.handle, C.byref(t), C.byref(h), C.byref(n)))
-    return t.value, h.value, n.value
+    t, h, n, m = C.c_double(), C.c_double(), C.c_double(), C.c_int32()
+    eng.check(N.lib.crab_pr_last_timing(eng.handle, C.byref(t), C.byref(h), C.byref(n), C.byref(m)))
+    return t.value, h.value, n.value, m.value

@@ -87,6 +87,7 @@ struct crab_ctx {
   // device times of the last pair-distance histogram: all its kernels, the
   // histogram kernel alone, and the pairs it binned
   double last_pr_ms = 0.0, last_pr_hist_ms = 0.0, last_pr_pairs = 0.0;
+  int last_pr_mode = -1;  // 0 class counts, 1 per-warp f64 shared, 2 f64 rows in device memory
 
   void* dev(const std::string& name, size_t bytes);
   void* host(const std::string& name, size_t bytes);

@@ -11,19 +11,28 @@
 //   k_pr_edges   per bin k the smallest f64 d2 that the reference's
 //                floor(sqrt(d2) / step) maps to k or above: a binary search
 //                over the bit patterns of non-negative doubles, with the same
-//                IEEE-rounded sqrt and division.  The bin of a pair is then
-//                the number of edges at or below its d2: bit-exact, with no
-//                square root or division per pair
-//   k_pr_hist    per pair: d2 in f64 with the reference's operation order (no
-//                fused multiply-add), a bin estimate from centred FP32
-//                coordinates, corrected against the exact edges, and the f64
-//                product w_i*w_j added to a per-warp shared histogram
-//   k_pr_reduce  the per-block rows summed in block order
+//                IEEE-rounded sqrt and division.  A pair's bin is the number
+//                of edges at or below its d2
+//   k_pr_hist    per pair the bin coordinate x = r / step from centred FP32
+//                coordinates.  When x is farther than a proven error bound
+//                delta from every integer, floor(x) is the reference's bin;
+//                otherwise (about 2*delta of the pairs) d2 is computed in f64
+//                with the reference's operation order (no fused multiply-add)
+//                and placed against the exact edges.
+//                Accumulation: when the atoms carry few distinct weights the
+//                tiles are grouped by weight class and each block counts pairs
+//                per class pair in u32 shared counters (flushed to u64 global
+//                counts); otherwise each warp adds the f64 product w_i*w_j to
+//                its own shared histogram
+//   k_pr_combine hist[k] = Σ over class pairs (in order) of count * w_a * w_b
+//   k_pr_reduce  (weighted mode) the per-block rows summed in block order
 //
-// Atoms are the spatially ordered 128-atom tiles of build_layout (one type).
-// A warp's 32 i atoms are every fourth slot of the tile, so the distances of
-// one j atom to them spread over many bins and the shared atomics rarely
-// collide.
+// Atoms are the spatially ordered 128-atom tiles of build_layout.  Each block
+// takes a contiguous run of the upper-triangle tile pairs (column-major), so
+// its j tile stays staged across consecutive items and its class pair rarely
+// changes.  A warp's 32 i atoms are every fourth slot of the tile, so the
+// distances of one j atom to them spread over many bins and the shared
+// atomics rarely collide.
 
 #include <cuda_runtime.h>
 
@@ -31,6 +40,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 
 #include "engine.hpp"
 #include "ops.hpp"
@@ -38,14 +48,21 @@
 namespace crab {
 namespace {
 
-constexpr int kPrThreads = kTile;              // one i atom per thread
-constexpr size_t kPrDynSmem = 96 * 1024;       // edges + per-warp histograms
+constexpr int kPrThreads = kTile;         // one i atom per thread
+constexpr size_t kPrDynSmem = 96 * 1024;  // edges + histograms
 constexpr int64_t kPrMaxBins = 1 << 24;
+constexpr int kPrMaxClasses = 64;                 // weight classes for integer counting
+constexpr size_t kPrMaxCountBytes = 256u << 20;   // u64 counts [class pairs][bins]
+constexpr int kPrFlushItems = 1 << 19;            // u32 counters: at most 4096 pairs per warp per item
+
+enum PrMode { kPrCounts = 0, kPrWeighted = 1, kPrWeightedGlobal = 2 };
 
 struct PrParams {
   double step;
   float inv_step;
+  float delta;     // bound on |x_fp32 - x_exact| in bins; FLT_MAX: always exact
   int degenerate;  // every pair distance is zero: no histogram
+  int pad;
 };
 
 __device__ __forceinline__ double pr_sqdist(const double4& a, const double4& b) {
@@ -62,9 +79,15 @@ __device__ __forceinline__ void pr_tri_decode(int64_t w, int& a, int& b) {
   a = (int)(w - bb * (bb + 1) / 2);
 }
 
+__device__ __forceinline__ int pr_pair_index(int a, int b, int T) {
+  if (a > b) { const int t = a; a = b; b = t; }
+  return a * T - a * (a - 1) / 2 + (b - a);
+}
+
+// tiles[t] = (weight class, real atoms in the tile); real atoms come first.
 __global__ void __launch_bounds__(kPrThreads)
-    k_pr_dmax(const double4* __restrict__ pos, int64_t n, int n_tiles, const double4* __restrict__ sphere,
-              double lower, unsigned long long* __restrict__ out) {
+    k_pr_dmax(const double4* __restrict__ pos, const int2* __restrict__ tiles, int n_tiles,
+              const double4* __restrict__ sphere, double lower, unsigned long long* __restrict__ out) {
   __shared__ double4 sj[kPrThreads];
   __shared__ double red[kPrThreads / 32];
   double best = 0.0;
@@ -76,15 +99,13 @@ __global__ void __launch_bounds__(kPrThreads)
     const double cx = sa.x - sb.x, cy = sa.y - sb.y, cz = sa.z - sb.z;
     const double ub = (sqrt(cx * cx + cy * cy + cz * cz) + sa.w + sb.w) * (1.0 + 1e-9);
     if (ub * ub < lower) continue;  // uniform over the block: no pair here reaches the bound
-    const int64_t j0 = (int64_t)b * kPrThreads;
+    const int na = tiles[a].y, nb = tiles[b].y;
     __syncthreads();
-    if (j0 + threadIdx.x < n) sj[threadIdx.x] = pos[j0 + threadIdx.x];
+    if ((int)threadIdx.x < nb) sj[threadIdx.x] = pos[(int64_t)b * kPrThreads + threadIdx.x];
     __syncthreads();
-    const int64_t i = (int64_t)a * kPrThreads + threadIdx.x;
-    if (i < n) {
-      const double4 pi = pos[i];
-      const int jn = (int)(n - j0 < (int64_t)kPrThreads ? n - j0 : (int64_t)kPrThreads);
-      for (int j = 0; j < jn; ++j) best = fmax(best, pr_sqdist(pi, sj[j]));
+    if ((int)threadIdx.x < na) {
+      const double4 pi = pos[(int64_t)a * kPrThreads + threadIdx.x];
+      for (int j = 0; j < nb; ++j) best = fmax(best, pr_sqdist(pi, sj[j]));
     }
   }
   for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -106,8 +127,16 @@ __device__ __forceinline__ int64_t pr_bin_of(double d2, double step, int64_t bin
   return (int64_t)v < bins - 1 ? (int64_t)v : bins - 1;
 }
 
-__global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, int64_t bins, double* __restrict__ edges,
-                           PrParams* __restrict__ par) {
+// radius: the largest distance of an atom from the centre of the FP32
+// coordinates.  The FP32 bin coordinate x = fl(fl(d2f * rsqrtf(d2f)) * inv_step)
+// differs from sqrt(d2) / step by at most
+//   (sqrt(3) * 2^-23 * radius + 10.5 * 2^-24 * d) / step
+// (coordinate rounding to float, the difference, the sum of squares, the
+// 2-ulp rsqrtf, the product and the rounded reciprocal step); delta is four
+// times that with d <= dmax = bins * step.  Above 2^20 bins every pair takes
+// the exact path.
+__global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, int64_t bins, double radius,
+                           double* __restrict__ edges, PrParams* __restrict__ par) {
   const double dmax2 = __longlong_as_double((long long)*dmax2_bits);
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (!(dmax2 > 0.0)) {
@@ -118,6 +147,9 @@ __global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, in
   if (k == 0) {
     par->step = step;
     par->inv_step = (float)fmin(1.0 / step, (double)FLT_MAX);
+    const double bound = (1.7320508075688772 * 0x1p-23 * radius / step + 10.5 * 0x1p-24 * (double)(bins + 1));
+    par->delta = bins > (1 << 20) ? FLT_MAX : (float)fmin(4.0 * bound, 0.25);
+    if (4.0 * bound > 0.25) par->delta = FLT_MAX;
     par->degenerate = 0;
   }
   if (k > bins) return;
@@ -133,67 +165,139 @@ __global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, in
   edges[k] = __longlong_as_double((long long)hi);
 }
 
-template <bool kShared>
+// Shared layout: kPrCounts: edges[bins + 1] (f64), then copies x u32[bins];
+// kPrWeighted: edges, then copies x f64[bins]; kPrWeightedGlobal: no dynamic
+// shared memory (edges and the block's row in device memory).
+template <int kMode>
 __global__ void __launch_bounds__(kPrThreads)
-    k_pr_hist(const double4* __restrict__ pos, const float4* __restrict__ pos32, int64_t n, int n_tiles,
-              const double* __restrict__ edges, const PrParams* __restrict__ par, int bins, int copies,
+    k_pr_hist(const double4* __restrict__ pos, const float4* __restrict__ pos32, const int2* __restrict__ tiles,
+              int n_tiles, int n_types, int64_t chunk, const double* __restrict__ edges,
+              const PrParams* __restrict__ par, int bins, int copies, unsigned long long* __restrict__ counts,
               double* __restrict__ rows) {
-  extern __shared__ double pr_dyn[];  // kShared: edges[bins + 1], then copies x hist[bins]
+  extern __shared__ double pr_dyn[];
   __shared__ double4 sj[kPrThreads];
   __shared__ float4 sj32[kPrThreads];
   if (par->degenerate) return;
-  const float inv_step = par->inv_step;
+  const float inv_step = par->inv_step, delta = par->delta;
+  const bool always_exact = !(delta < 1.0f);
+  const float top = (float)bins - 0.5f;  // nearest integer >= bins: bin bins - 1
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double* E;
-  double* H;
-  if constexpr (kShared) {
-    E = pr_dyn;
-    H = pr_dyn + (bins + 1) + (size_t)(warp % copies) * bins;
-    for (int k = threadIdx.x; k <= bins; k += kPrThreads) pr_dyn[k] = edges[k];
-    for (int k = threadIdx.x; k < copies * bins; k += kPrThreads) pr_dyn[bins + 1 + k] = 0.0;
-  } else {
-    E = edges;
-    H = rows + (size_t)blockIdx.x * bins;  // zeroed by the host
-  }
   const int si = lane * 4 + warp;  // this thread's slot in the i tile
+  const double* E = kMode == kPrWeightedGlobal ? edges : pr_dyn;
+  unsigned* Hc = reinterpret_cast<unsigned*>(pr_dyn + bins + 1);
+  double* Hw = kMode == kPrWeightedGlobal ? rows + (size_t)blockIdx.x * bins : pr_dyn + bins + 1;
+  if constexpr (kMode != kPrWeightedGlobal) {
+    for (int k = threadIdx.x; k <= bins; k += kPrThreads) pr_dyn[k] = edges[k];
+    if constexpr (kMode == kPrCounts)
+      for (int k = threadIdx.x; k < copies * bins; k += kPrThreads) Hc[k] = 0u;
+    else
+      for (int k = threadIdx.x; k < copies * bins; k += kPrThreads) Hw[k] = 0.0;
+  }
+  unsigned* myc = Hc + (size_t)(warp % copies) * bins;
+  double* myw = kMode == kPrWeightedGlobal ? Hw : Hw + (size_t)(warp % copies) * bins;
+
   const int64_t n_work = (int64_t)n_tiles * (n_tiles + 1) / 2;
-  for (int64_t w = blockIdx.x; w < n_work; w += gridDim.x) {
-    int a, b;
-    pr_tri_decode(w, a, b);
-    const int64_t j0 = (int64_t)b * kPrThreads;
+  int64_t w = (int64_t)blockIdx.x * chunk;
+  const int64_t w_end = min(w + chunk, n_work);
+  int a = 0, b = 0;
+  if (w < w_end) pr_tri_decode(w, a, b);
+  int cur_b = -1, cur_pair = -1, since = 0;
+
+  auto flush_counts = [&]() {
     __syncthreads();
-    if (j0 + threadIdx.x < n) {
-      sj[threadIdx.x] = pos[j0 + threadIdx.x];
-      sj32[threadIdx.x] = pos32[j0 + threadIdx.x];
+    for (int k = threadIdx.x; k < bins; k += kPrThreads) {
+      unsigned long long s = 0ull;
+      for (int c = 0; c < copies; ++c) {
+        s += Hc[(size_t)c * bins + k];
+        Hc[(size_t)c * bins + k] = 0u;
+      }
+      if (s) atomicAdd(&counts[(size_t)cur_pair * bins + k], s);
     }
     __syncthreads();
-    const int64_t i = (int64_t)a * kPrThreads + si;
-    if (i >= n) continue;
-    const double4 pi = pos[i];
-    const float4 fi = pos32[i];
-    const int jn = (int)(n - j0 < (int64_t)kPrThreads ? n - j0 : (int64_t)kPrThreads);
-    for (int j = (a == b) ? si + 1 : 0; j < jn; ++j) {
-      const double4 pj = sj[j];
-      const float4 fj = sj32[j];
-      const double d2 = pr_sqdist(pi, pj);
-      const float fx = fi.x - fj.x, fy = fi.y - fj.y, fz = fi.z - fj.z;
-      const float d2f = fx * fx + fy * fy + fz * fz;
-      const float r = d2f * rsqrtf(fmaxf(d2f, 1e-30f));
-      int e = min((int)(r * inv_step), bins - 1);
-      e = max(e, 0);
-      while (e + 1 < bins && d2 >= E[e + 1]) ++e;
-      while (e > 0 && d2 < E[e]) --e;
-      atomicAdd(&H[e], pi.w * pj.w);
+  };
+
+  for (; w < w_end; ++w) {
+    const int2 ta = tiles[a], tb = tiles[b];
+    if constexpr (kMode == kPrCounts) {
+      const int pair = pr_pair_index(ta.x, tb.x, n_types);
+      if (pair != cur_pair || since == kPrFlushItems) {
+        if (cur_pair >= 0) flush_counts();
+        cur_pair = pair;
+        since = 0;
+      }
+      ++since;
+    }
+    if (b != cur_b) {
+      __syncthreads();
+      if ((int)threadIdx.x < tb.y) {
+        sj[threadIdx.x] = pos[(int64_t)b * kPrThreads + threadIdx.x];
+        sj32[threadIdx.x] = pos32[(int64_t)b * kPrThreads + threadIdx.x];
+      }
+      __syncthreads();
+      cur_b = b;
+    }
+    if (si < ta.y) {
+      const int64_t gi = (int64_t)a * kPrThreads + si;
+      const float4 fi = pos32[gi];
+      double wi = 0.0;
+      if constexpr (kMode != kPrCounts) wi = pos[gi].w;
+      for (int j = (a == b) ? si + 1 : 0; j < tb.y; ++j) {
+        const float4 fj = sj32[j];
+        const float fx = fi.x - fj.x, fy = fi.y - fj.y, fz = fi.z - fj.z;
+        const float d2f = fx * fx + fy * fy + fz * fz;
+        const float x = d2f * rsqrtf(fmaxf(d2f, 1e-30f)) * inv_step;
+        int e;
+        bool exact = always_exact;
+        if (!always_exact) {
+          const float t = x + 12582912.0f;  // 1.5 * 2^23: rounds x to the nearest integer
+          const float k = t - 12582912.0f;
+          const int ki = __float_as_int(t) - 0x4B400000;
+          if (fabsf(x - k) >= delta) e = ki - (k > x ? 1 : 0);  // no edge within reach: floor(x)
+          else if (k < 0.5f) e = 0;                             // next to 0: floor is 0
+          else if (k > top) e = bins - 1;                        // at or past bins: the last bin
+          else {
+            e = ki;
+            exact = true;
+          }
+        }
+        if (exact) {
+          if (always_exact) e = (int)fminf(fmaxf(x, 0.0f), (float)(bins - 1));
+          e = min(max(e, 0), bins - 1);
+          const double d2 = pr_sqdist(pos[gi], sj[j]);
+          while (e + 1 < bins && d2 >= E[e + 1]) ++e;
+          while (e > 0 && d2 < E[e]) --e;
+        }
+        e = min(e, bins - 1);
+        if constexpr (kMode == kPrCounts) atomicAdd(&myc[e], 1u);
+        else atomicAdd(&myw[e], wi * sj[j].w);
+      }
+    }
+    if (++a > b) {
+      a = 0;
+      ++b;
     }
   }
-  if constexpr (kShared) {
+  if constexpr (kMode == kPrCounts) {
+    if (cur_pair >= 0) flush_counts();
+  } else if constexpr (kMode == kPrWeighted) {
     __syncthreads();
     for (int k = threadIdx.x; k < bins; k += kPrThreads) {
       double s = 0.0;
-      for (int c = 0; c < copies; ++c) s += pr_dyn[bins + 1 + (size_t)c * bins + k];
+      for (int c = 0; c < copies; ++c) s += Hw[(size_t)c * bins + k];
       rows[(size_t)blockIdx.x * bins + k] = s;
     }
   }
+}
+
+// hist[k] = Σ_pairs counts[pair][k] * wprod[pair], pairs in order.
+__global__ void k_pr_combine(const unsigned long long* __restrict__ counts, const double* __restrict__ wprod,
+                             int n_pairs, int bins, const PrParams* __restrict__ par, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= bins) return;
+  double s = 0.0;
+  if (!par->degenerate)
+    for (int p = 0; p < n_pairs; ++p) s += (double)counts[(size_t)p * bins + k] * wprod[p];
+  out[k] = s;
 }
 
 __global__ void k_pr_reduce(const double* __restrict__ rows, int n_rows, int bins, const PrParams* __restrict__ par,
@@ -211,6 +315,14 @@ inline double host_sqdist(const double* a, const double* b) {
   return dx * dx + dy * dy + dz * dz;
 }
 
+template <int kMode>
+int pr_blocks_per_sm(size_t dyn) {
+  if (dyn) CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pr_hist<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  int per_sm = 0;
+  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_hist<kMode>, kPrThreads, dyn));
+  return std::max(per_sm, 1);
+}
+
 }  // namespace
 
 double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w, int64_t n, int64_t bins,
@@ -223,6 +335,7 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   for (int64_t i = 0; i < n; ++i) require(std::isfinite(w[i]), "weights must be finite");
   std::fill(hist, hist + bins, 0.0);
   ctx->last_pr_ms = ctx->last_pr_hist_ms = 0.0;
+  ctx->last_pr_mode = -1;
   ctx->last_pr_pairs = (double)n * (double)(n > 0 ? n - 1 : 0) * 0.5;
   if (n < 2) return 0.0;
 
@@ -240,21 +353,55 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   }
   const double lower = host_sqdist(xyz + 3 * p0, xyz + 3 * p1);
 
+  // weight classes: distinct weight values (bit patterns), when there are few
   std::vector<int32_t> type(n, 0);
+  std::vector<double> class_w;
+  {
+    std::unordered_map<uint64_t, int> ids;
+    for (int64_t i = 0; i < n && (int)class_w.size() <= kPrMaxClasses; ++i) {
+      uint64_t key;
+      std::memcpy(&key, &w[i], sizeof key);
+      auto it = ids.find(key);
+      if (it == ids.end()) {
+        it = ids.emplace(key, (int)class_w.size()).first;
+        class_w.push_back(w[i]);
+      }
+      type[i] = it->second;
+    }
+  }
+  const int T = (int)class_w.size();
+  const int n_pairs = T * (T + 1) / 2;
+  const size_t edge_bytes = (size_t)(bins + 1) * sizeof(double);
+  int mode = kPrWeightedGlobal, copies = 1;
+  if (T <= kPrMaxClasses && (size_t)n_pairs * bins * 8 <= kPrMaxCountBytes &&
+      edge_bytes + (size_t)bins * 4 <= kPrDynSmem) {
+    mode = kPrCounts;
+    copies = (int)std::min<size_t>(kPrThreads / 32, (kPrDynSmem - edge_bytes) / ((size_t)bins * 4));
+  } else if (edge_bytes + (size_t)bins * 8 <= kPrDynSmem) {
+    mode = kPrWeighted;
+    copies = (int)std::min<size_t>(kPrThreads / 32, (kPrDynSmem - edge_bytes) / ((size_t)bins * 8));
+  }
+  if (mode != kPrCounts) std::fill(type.begin(), type.end(), 0);
   Layout L;
   {
     TraceScope t2("pr.layout");
-    L = build_layout(xyz, w, type.data(), n, 1, false);
+    L = build_layout(xyz, w, type.data(), n, mode == kPrCounts ? T : 1, false);
   }
   const int n_tiles = L.n_tiles;
   const int64_t n_pad = L.n_pad;
+  double radius = 0.0;  // of the centred FP32 coordinates
   cudaStream_t s = ctx->stream;
   auto* h_pos = (double4*)ctx->host("pr.pos", (size_t)n_pad * sizeof(double4));
   auto* h_sph = (double4*)ctx->host("pr.sphere", (size_t)n_tiles * sizeof(double4));
+  auto* h_tiles = (int2*)ctx->host("pr.tiles", (size_t)n_tiles * sizeof(int2));
   for (int64_t k = 0; k < n_pad; ++k) {
     const int64_t src = L.source[k];
     h_pos[k] = src >= 0 ? make_double4(xyz[3 * src], xyz[3 * src + 1], xyz[3 * src + 2], w[src])
                         : make_double4(0.0, 0.0, 0.0, 0.0);
+    if (src >= 0) {
+      const float* f = &L.atoms[4 * k];
+      radius = std::max(radius, std::sqrt((double)f[0] * f[0] + (double)f[1] * f[1] + (double)f[2] * f[2]));
+    }
   }
   for (int t = 0; t < n_tiles; ++t) {
     double c[3] = {0.0, 0.0, 0.0}, mag = 0.0;
@@ -271,44 +418,60 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
     }
     // inflated past the rounding of the centre and of every distance above
     h_sph[t] = make_double4(c[0], c[1], c[2], std::sqrt(r2) * (1.0 + 1e-12) + mag * 1e-12);
+    h_tiles[t] = make_int2(L.tile_type[t], cnt);
   }
+  radius = radius * (1.0 + 1e-6) + 1e-30;
 
   auto* d_pos = (double4*)ctx->dev("pr.pos", (size_t)n_pad * sizeof(double4));
   auto* d_pos32 = (float4*)ctx->dev("pr.pos32", (size_t)n_pad * sizeof(float4));
   auto* d_sph = (double4*)ctx->dev("pr.sphere", (size_t)n_tiles * sizeof(double4));
-  auto* d_edges = (double*)ctx->dev("pr.edges", (size_t)(bins + 1) * sizeof(double));
+  auto* d_tiles = (int2*)ctx->dev("pr.tiles", (size_t)n_tiles * sizeof(int2));
+  auto* d_edges = (double*)ctx->dev("pr.edges", edge_bytes);
   auto* d_out = (double*)ctx->dev("pr.out", (size_t)bins * sizeof(double));
-  // PrParams and the dmax bits share one small buffer
-  auto* d_misc = (char*)ctx->dev("pr.misc", 64);
+  // the dmax bits, PrParams and the class-pair weight products share one buffer
+  auto* d_misc = (char*)ctx->dev("pr.misc", 64 + (size_t)n_pairs * sizeof(double));
   auto* d_dmax2 = (unsigned long long*)d_misc;
   auto* d_par = (PrParams*)(d_misc + 16);
+  auto* d_wprod = (double*)(d_misc + 64);
   copy_h2d(ctx, d_pos, h_pos, (size_t)n_pad * sizeof(double4), s);
   copy_h2d(ctx, d_pos32, L.atoms.data(), (size_t)n_pad * sizeof(float4), s);
   copy_h2d(ctx, d_sph, h_sph, (size_t)n_tiles * sizeof(double4), s);
+  copy_h2d(ctx, d_tiles, h_tiles, (size_t)n_tiles * sizeof(int2), s);
   CRAB_CUDA_CHECK(cudaMemsetAsync(d_misc, 0, 64, s));
+  if (mode == kPrCounts) {
+    auto* h_wprod = (double*)ctx->host("pr.wprod", (size_t)n_pairs * sizeof(double));
+    for (int a = 0; a < T; ++a)
+      for (int b = a; b < T; ++b) h_wprod[pair_index(a, b, T)] = class_w[a] * class_w[b];
+    copy_h2d(ctx, d_wprod, h_wprod, (size_t)n_pairs * sizeof(double), s);
+  }
 
   const int ibins = (int)bins;
-  const size_t per_copy = (size_t)bins * sizeof(double);
-  const size_t edge_bytes = (size_t)(bins + 1) * sizeof(double);
-  int copies = 0;
-  if (edge_bytes + per_copy <= kPrDynSmem)
-    copies = (int)std::min<size_t>(kPrThreads / 32, (kPrDynSmem - edge_bytes) / per_copy);
-  const bool shared_hist = copies > 0;
-  const size_t dyn = shared_hist ? edge_bytes + (size_t)copies * per_copy : 0;
-  int per_sm = 0;
-  if (shared_hist) {
-    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pr_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_hist<true>, kPrThreads, dyn));
+  size_t dyn = 0;
+  int per_sm = 1;
+  if (mode == kPrCounts) {
+    dyn = edge_bytes + (size_t)copies * bins * 4;
+    per_sm = pr_blocks_per_sm<kPrCounts>(dyn);
+  } else if (mode == kPrWeighted) {
+    dyn = edge_bytes + (size_t)copies * bins * 8;
+    per_sm = pr_blocks_per_sm<kPrWeighted>(dyn);
   } else {
-    CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_hist<false>, kPrThreads, 0));
+    per_sm = pr_blocks_per_sm<kPrWeightedGlobal>(0);
   }
   const int64_t n_work = (int64_t)n_tiles * (n_tiles + 1) / 2;
-  // one histogram row per block, at most 256 MB of rows (huge bin counts run fewer blocks)
-  const int64_t max_rows = std::max<int64_t>(1, (int64_t)(256u << 20) / (int64_t)per_copy);
-  const int grid = (int)std::max<int64_t>(
-      1, std::min({(int64_t)ctx->sm_count * std::max(per_sm, 1), n_work, max_rows}));
-  auto* d_rows = (double*)ctx->dev("pr.rows", (size_t)grid * per_copy);
-  if (!shared_hist) CRAB_CUDA_CHECK(cudaMemsetAsync(d_rows, 0, (size_t)grid * per_copy, s));
+  // weighted modes keep one f64 row per block: at most 256 MB of rows
+  const int64_t max_rows = mode == kPrCounts ? INT64_MAX : std::max<int64_t>(1, (int64_t)(256u << 20) / (bins * 8));
+  const int64_t grid0 = std::max<int64_t>(1, std::min({(int64_t)ctx->sm_count * per_sm, n_work, max_rows}));
+  const int64_t chunk = (n_work + grid0 - 1) / grid0;
+  const int grid = (int)((n_work + chunk - 1) / chunk);
+  unsigned long long* d_counts = nullptr;
+  double* d_rows = nullptr;
+  if (mode == kPrCounts) {
+    d_counts = (unsigned long long*)ctx->dev("pr.counts", (size_t)n_pairs * bins * 8);
+    CRAB_CUDA_CHECK(cudaMemsetAsync(d_counts, 0, (size_t)n_pairs * bins * 8, s));
+  } else {
+    d_rows = (double*)ctx->dev("pr.rows", (size_t)grid * bins * 8);
+    if (mode == kPrWeightedGlobal) CRAB_CUDA_CHECK(cudaMemsetAsync(d_rows, 0, (size_t)grid * bins * 8, s));
+  }
 
   cudaEvent_t ev[3];
   for (auto& e : ev) CRAB_CUDA_CHECK(cudaEventCreate(&e));
@@ -316,18 +479,26 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   int dgrid = 0;
   CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dgrid, k_pr_dmax, kPrThreads, 0));
   dgrid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sm_count * std::max(dgrid, 1), n_work));
-  k_pr_dmax<<<dgrid, kPrThreads, 0, s>>>(d_pos, n, n_tiles, d_sph, lower, d_dmax2);
+  k_pr_dmax<<<dgrid, kPrThreads, 0, s>>>(d_pos, d_tiles, n_tiles, d_sph, lower, d_dmax2);
   CRAB_CUDA_CHECK(cudaGetLastError());
-  k_pr_edges<<<(unsigned)((bins + 1 + 127) / 128), 128, 0, s>>>(d_dmax2, bins, d_edges, d_par);
+  k_pr_edges<<<(unsigned)((bins + 1 + 127) / 128), 128, 0, s>>>(d_dmax2, bins, radius, d_edges, d_par);
   CRAB_CUDA_CHECK(cudaGetLastError());
   CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
-  if (shared_hist)
-    k_pr_hist<true><<<grid, kPrThreads, dyn, s>>>(d_pos, d_pos32, n, n_tiles, d_edges, d_par, ibins, copies, d_rows);
+  if (mode == kPrCounts)
+    k_pr_hist<kPrCounts><<<grid, kPrThreads, dyn, s>>>(d_pos, d_pos32, d_tiles, n_tiles, T, chunk, d_edges, d_par,
+                                                        ibins, copies, d_counts, nullptr);
+  else if (mode == kPrWeighted)
+    k_pr_hist<kPrWeighted><<<grid, kPrThreads, dyn, s>>>(d_pos, d_pos32, d_tiles, n_tiles, 1, chunk, d_edges, d_par,
+                                                          ibins, copies, nullptr, d_rows);
   else
-    k_pr_hist<false><<<grid, kPrThreads, 0, s>>>(d_pos, d_pos32, n, n_tiles, d_edges, d_par, ibins, 1, d_rows);
+    k_pr_hist<kPrWeightedGlobal><<<grid, kPrThreads, 0, s>>>(d_pos, d_pos32, d_tiles, n_tiles, 1, chunk, d_edges,
+                                                              d_par, ibins, 1, nullptr, d_rows);
   CRAB_CUDA_CHECK(cudaGetLastError());
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
-  k_pr_reduce<<<(ibins + 127) / 128, 128, 0, s>>>(d_rows, grid, ibins, d_par, d_out);
+  if (mode == kPrCounts)
+    k_pr_combine<<<(ibins + 127) / 128, 128, 0, s>>>(d_counts, d_wprod, n_pairs, ibins, d_par, d_out);
+  else
+    k_pr_reduce<<<(ibins + 127) / 128, 128, 0, s>>>(d_rows, grid, ibins, d_par, d_out);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 4;
   auto* h_misc = (char*)ctx->host("pr.misc", 64);
@@ -340,6 +511,7 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   for (auto& e : ev) cudaEventDestroy(e);
   ctx->last_pr_ms = t_all;
   ctx->last_pr_hist_ms = t_hist;
+  ctx->last_pr_mode = mode;
   unsigned long long bits;
   std::memcpy(&bits, h_misc, sizeof bits);
   double dmax2;
@@ -440,12 +612,13 @@ int crab_coordinate_features(crab_ctx* ctx, crab_struct* st, int64_t bins, doubl
   return guarded_impl(ctx, [&]() { coordinate_features(ctx, st, bins, rg, dmax, r, p, m, pr_rg, pr_dmax); });
 }
 
-int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs) {
+int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs, int32_t* mode) {
   if (!ctx) return CRAB_EINVAL;
   std::lock_guard<std::mutex> g(ctx->mu);
   if (total_ms) *total_ms = ctx->last_pr_ms;
   if (histogram_ms) *histogram_ms = ctx->last_pr_hist_ms;
   if (pairs) *pairs = ctx->last_pr_pairs;
+  if (mode) *mode = ctx->last_pr_mode;
   return CRAB_OK;
 }
 

@@ -89,10 +89,10 @@ def pr_config3(engine: cs.Engine, bins: int, repeats: int) -> str:
         t0 = time.perf_counter()
         cs.coordinate_features(s, cs.PrOptions(bins=bins), engine=engine)
         wall.append((time.perf_counter() - t0) * 1e3)
-        total_ms, hist_ms, pairs = cs.pr_last_timing(engine)
+        total_ms, hist_ms, pairs, mode = cs.pr_last_timing(engine)
         dev.append(total_ms)
         hist.append(hist_ms)
-    return (f"pr-config3 bins={bins} pairs={pairs:.6g} wall_ms={np.round(wall, 3).tolist()} "
+    return (f"pr-config3 bins={bins} mode={mode} pairs={pairs:.6g} wall_ms={np.round(wall, 3).tolist()} "
             f"device_ms={np.round(dev, 3).tolist()} histogram_ms={np.round(hist, 3).tolist()}")
 
 

@@ -387,9 +387,15 @@ int crab_pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double*
 int crab_coordinate_features(crab_ctx* ctx, crab_struct* st, int64_t bins, double* rg, double* dmax, double* r,
                              double* p, int64_t* m, double* pr_rg, double* pr_dmax);
 /* Device time of the last pair-distance histogram on this context: all its
- * kernels (dmax pass, bin edges, histogram), the histogram kernel alone, and
- * the number of pairs n(n-1)/2.  Any pointer may be NULL. */
-int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs);
+ * kernels (dmax pass, bin edges, histogram), the histogram kernel alone, the
+ * number of pairs n(n-1)/2, and how the histogram was accumulated (mode):
+ *   0  integer pair counts per class pair (at most 64 distinct weights),
+ *      combined as count * w_a * w_b: deterministic
+ *   1  f64 products w_i*w_j into per-warp shared-memory histograms
+ *   2  as 1, into one row per block in device memory (many bins)
+ *  -1  no histogram kernel ran (fewer than two atoms).
+ * Any pointer may be NULL. */
+int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs, int32_t* mode);
 
 /* ---- synthetic inputs (no counterpart in the reference) ----------------- */
 /* Seeded protein-like structure: Cα-style self-avoiding walk (3.8 Å steps,

@@ -64,12 +64,42 @@ def test_groups_occupancy_and_hydrogen_floor(engine):
     _check_features(s, 200, engine)
 
 
+def _mode(engine):
+    return cs.pr_last_timing(engine)[3]
+
+
 def test_unit_weight_bins_are_exact(engine):
+    """Unit weights: one weight class, integer pair counts (mode 0)."""
     s = synth.protein(17, 3000, 20.0)
     for bins in (16, 160, 4096):
         dmax, hist = cs.pair_distance_histogram(s.xyz, np.ones(len(s.xyz)), bins, engine=engine)
+        assert _mode(engine) == 0
         rd, rh = O.pair_distance_histogram(s.xyz, np.ones(len(s.xyz)), bins)
         assert dmax == rd and np.array_equal(hist, rh), bins
+
+
+def test_integer_weight_bins_are_exact_in_the_f64_mode(engine):
+    """100 distinct integer weights exceed the 64 weight classes, so the
+    products go through the per-warp f64 histograms (mode 1); integer sums
+    below 2^53 are exact in any order, so the bins must equal the oracle's."""
+    s = synth.protein(18, 2800, 19.0)
+    w = 1.0 + (np.arange(len(s.xyz)) % 100)
+    for bins in (16, 160, 3000):
+        dmax, hist = cs.pair_distance_histogram(s.xyz, w, bins, engine=engine)
+        assert _mode(engine) == 1
+        rd, rh = O.pair_distance_histogram(s.xyz, w, bins)
+        assert dmax == rd and np.array_equal(hist, rh), bins
+
+
+def test_several_weight_classes_count_exactly(engine):
+    """A few distinct weights: per-class-pair counts (mode 0) combined as
+    count * w_a * w_b against the oracle's pair-by-pair sums."""
+    s = synth.protein(19, 2000, 16.0)
+    w = np.array([1.0, 6.5, 7.25, 8.0, 16.125])[np.arange(len(s.xyz)) % 5]
+    dmax, hist = cs.pair_distance_histogram(s.xyz, w, 160, engine=engine)
+    assert _mode(engine) == 0
+    rd, rh = O.pair_distance_histogram(s.xyz, w, 160)
+    assert dmax == rd and np.array_equal(hist, rh)
 
 
 def test_pairs_on_exact_bin_edges(engine):
@@ -90,17 +120,25 @@ def test_pairs_on_exact_bin_edges(engine):
 
 
 def test_many_bins_use_the_global_histogram(engine):
-    """Above ~6,000 bins the per-warp histograms no longer fit in shared
-    memory and each block accumulates into its own row in device memory."""
+    """Above ~6,000 bins (f64) or ~8,000 (counts) the histograms no longer fit
+    in shared memory and each block accumulates into its own row in device
+    memory (mode 2).  20,000 bins still take the FP32 fast path with a wide
+    edge margin; above 75,000 bins the margin reaches a quarter bin and every
+    pair takes the exact f64 path; above 2^20 bins as well."""
     s = synth.protein(23, 1200, 13.0)
     w = np.random.default_rng(2).uniform(1.0, 16.0, len(s.xyz))
     dmax, hist = cs.pair_distance_histogram(s.xyz, w, 20000, engine=engine)
+    assert _mode(engine) == 2
     rd, rh = O.pair_distance_histogram(s.xyz, w, 20000)
     assert dmax == rd
     assert np.max(np.abs(hist - rh)) <= SUM_RTOL * np.max(rh)
-    d1, h1 = cs.pair_distance_histogram(s.xyz, np.ones(len(s.xyz)), 20000, engine=engine)
-    r1 = O.pair_distance_histogram(s.xyz, np.ones(len(s.xyz)), 20000)[1]
-    assert np.array_equal(h1, r1)
+    small = synth.protein(24, 300, 8.0)
+    for atoms, bins in ((s, 20000), (s, 100000), (small, 1_200_000)):
+        n = len(atoms.xyz)
+        d1, h1 = cs.pair_distance_histogram(atoms.xyz, np.ones(n), bins, engine=engine)
+        assert _mode(engine) == 2
+        r1 = O.pair_distance_histogram(atoms.xyz, np.ones(n), bins)[1]
+        assert np.array_equal(h1, r1), bins
 
 
 def test_single_point_and_invalid_inputs(engine):  # metrics.rs:241-244, 489-498
@@ -120,9 +158,16 @@ def test_single_point_and_invalid_inputs(engine):  # metrics.rs:241-244, 489-498
 
 
 def test_large_structure_matches_oracle(engine):
-    """30,000 atoms (4.5e8 pairs): weighted P(r) against the oracle."""
+    """30,000 atoms (4.5e8 pairs): P(r) against the oracle, with the element
+    weights (class counts) and with random per-atom weights (f64 mode)."""
     s = synth.protein(29, 30000, 40.0)
     _check_features(s, 160, engine)
+    assert _mode(engine) == 0
+    w = np.random.default_rng(4).uniform(0.5, 9.0, len(s.xyz))
+    dmax, hist = cs.pair_distance_histogram(s.xyz, w, 160, engine=engine)
+    assert _mode(engine) == 1
+    rd, rh = O.pair_distance_histogram(s.xyz, w, 160)
+    assert dmax == rd and np.max(np.abs(hist - rh)) <= SUM_RTOL * np.max(rh)
 
 
 def test_config3_size_properties(engine):
@@ -141,5 +186,5 @@ def test_config3_size_properties(engine):
     ext = s.xyz[np.concatenate([np.argmin(s.xyz, 0), np.argmax(s.xyz, 0)])]
     dd = ext[:, None, :] - ext[None, :, :]
     assert dmax >= math.sqrt(np.max(np.sum(dd * dd, -1))) - 1e-9
-    total_ms, hist_ms, pairs = cs.pr_last_timing(engine)
-    assert pairs == n * (n - 1) / 2 and 0.0 < hist_ms <= total_ms
+    total_ms, hist_ms, pairs, mode = cs.pr_last_timing(engine)
+    assert pairs == n * (n - 1) / 2 and 0.0 < hist_ms <= total_ms and mode == 1
