@@ -411,6 +411,43 @@ def grid_and_gradient_section(eng, rank):
                                   "note": "ordered pairs (i, j) and (j, i): 2 * N(N-1)/2 * nq per call"}}
 
 
+def pr_section(eng, rank, with_cpu):
+    """Coordinate features (metrics.rs:236-270): Rg, Dmax and the 160-bin P(r)
+    of config 3's 100,000-atom structure (5e9 pairs).  Wall time of the public
+    call and device time of its kernels, median of 5 after a warm-up; the CPU
+    baseline is the oracle (the reference's 64-row-chunk loop, OpenMP on every
+    host core) on a seeded 20,000-atom subset."""
+    import crabsaxs_b200 as cs
+    import oracle as O
+    from crabsaxs_b200 import synth
+
+    w = synth.CONFIG3
+    s = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
+    cs.coordinate_features(s, engine=eng)
+    walls, dev, hist = [], [], []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        cs.coordinate_features(s, engine=eng)
+        walls.append((time.perf_counter() - t0) * 1e3)
+        total_ms, hist_ms, pairs, mode = cs.pr_last_timing(eng)
+        dev.append(total_ms)
+        hist.append(hist_ms)
+    out = {"atoms": s.atom_count, "bins": 160, "pairs": pairs, "wall_ms": float(np.median(walls)),
+           "device_ms": float(np.median(dev)), "histogram_kernel_ms": float(np.median(hist)),
+           "pairs_per_s": pairs / (float(np.median(hist)) * 1e-3),
+           "accumulation": {0: "class-pair counts", 1: "f64 per warp", 2: "f64 rows"}.get(mode, "none")}
+    if with_cpu and rank == 0:
+        idx = np.sort(np.random.default_rng(0).choice(s.atom_count, 20000, replace=False))
+        a = O.Atoms(s.xyz[idx], s.element[idx], s.group[idx], s.occupancy[idx])
+        t0 = time.perf_counter()
+        O.coordinate_features(a, 160)
+        dt = time.perf_counter() - t0
+        sub_pairs = 20000 * 19999 / 2.0
+        out["cpu_baseline"] = {"value": sub_pairs / dt, "unit": "pairs/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": "seeded 20,000-atom subset, 160 bins", "seconds": dt}
+    return out
+
+
 def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
@@ -528,6 +565,7 @@ def run_ours(args, rank, world, local):
     ens = None if args.no_ensemble else ensemble_section(eng, rank)
     mp = None if args.no_multipole else multipole_section(eng, rank, peak.value)
     aux = None if args.no_multipole else grid_and_gradient_section(eng, rank)
+    pr = None if args.no_multipole else pr_section(eng, rank, not args.no_cpu_baseline)
 
     if rank == 0:
         line = {
@@ -549,6 +587,7 @@ def run_ours(args, rank, world, local):
             "ensemble": ens,
             "multipole": mp,
             "grids_and_gradient": aux,
+            "coordinate_pr": pr,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,

@@ -535,35 +535,44 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
   L.extent = 2.0 * rmax;
   // order: type, then the 30-bit Morton code of the centred position, ties by
   // input index (a counting sort by type, then a stable LSD radix sort of the
-  // Morton codes within each type, three 10-bit digits)
-  std::vector<uint32_t> key(n);
-  for (int64_t i = 0; i < n; ++i) {
-    uint32_t m = 0;
-    for (int d = 0; d < 3; ++d) {
-      double span = std::max(hi[d] - lo[d], 1e-9);
-      double cell = std::floor((xyz[3 * i + d] - c[d] - lo[d]) / span * 1024.0);
-      m |= morton10((uint32_t)std::min(1023.0, std::max(0.0, cell))) << d;
-    }
-    key[i] = m;
-  }
+  // packed (Morton code, index) words within each type, three 10-bit digits)
+  require(n < ((int64_t)1 << 32), "at most 2^32 - 1 atoms per pair problem");
+  static const std::vector<uint32_t> spread = [] {
+    std::vector<uint32_t> t(1024);
+    for (uint32_t v = 0; v < 1024; ++v) t[v] = morton10(v);
+    return t;
+  }();
+  double scale[3];
+  for (int d = 0; d < 3; ++d) scale[d] = 1024.0 / std::max(hi[d] - lo[d], 1e-9);
   std::vector<int64_t> count(T, 0);
   for (int64_t i = 0; i < n; ++i) count[type[i]]++;
-  std::vector<int64_t> order(n), tmp(n), tstart(T + 1, 0);
+  std::vector<int64_t> tstart(T + 1, 0);
   for (int t = 0; t < T; ++t) tstart[t + 1] = tstart[t] + count[t];
+  std::vector<uint64_t> word(n), tmp(n);
   {
     std::vector<int64_t> pos(tstart.begin(), tstart.end() - 1);
-    for (int64_t i = 0; i < n; ++i) order[pos[type[i]]++] = i;
+    for (int64_t i = 0; i < n; ++i) {
+      uint32_t m = 0;
+      for (int d = 0; d < 3; ++d) {
+        const double cell = (xyz[3 * i + d] - c[d] - lo[d]) * scale[d];
+        const int ci = cell <= 0.0 ? 0 : (cell >= 1023.0 ? 1023 : (int)cell);
+        m |= spread[ci] << d;
+      }
+      word[pos[type[i]]++] = ((uint64_t)m << 32) | (uint64_t)i;
+    }
   }
   for (int t = 0; t < T; ++t) {
     const int64_t a = tstart[t], b = tstart[t + 1];
-    for (int shift = 0; shift < 30; shift += 10) {
+    for (int shift = 32; shift < 62; shift += 10) {
       int64_t digit[1025] = {0};
-      for (int64_t k = a; k < b; ++k) digit[((key[order[k]] >> shift) & 1023u) + 1]++;
+      for (int64_t k = a; k < b; ++k) digit[((word[k] >> shift) & 1023u) + 1]++;
       for (int d = 0; d < 1024; ++d) digit[d + 1] += digit[d];
-      for (int64_t k = a; k < b; ++k) tmp[a + digit[(key[order[k]] >> shift) & 1023u]++] = order[k];
-      std::copy(tmp.begin() + a, tmp.begin() + b, order.begin() + a);
+      for (int64_t k = a; k < b; ++k) tmp[a + digit[(word[k] >> shift) & 1023u]++] = word[k];
+      std::copy(tmp.begin() + a, tmp.begin() + b, word.begin() + a);
     }
   }
+  std::vector<int64_t> order(n);
+  for (int64_t k = 0; k < n; ++k) order[k] = (int64_t)(word[k] & 0xffffffffu);
   int64_t n_pad = 0;
   for (int t = 0; t < T; ++t) n_pad += (count[t] + kTile - 1) / kTile * kTile;
   L.n_pad = n_pad;

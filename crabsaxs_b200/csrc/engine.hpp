@@ -35,6 +35,11 @@ struct Error : std::runtime_error {
 inline void require(bool ok, const std::string& msg) {
   if (!ok) throw Error(CRAB_EINVAL, msg);
 }
+// Literal messages: no std::string is built unless the check fails (these
+// checks run once per atom).
+inline void require(bool ok, const char* msg) {
+  if (!ok) throw Error(CRAB_EINVAL, msg);
+}
 
 // Host-phase tracing: with CRAB_TRACE=1 in the environment every TraceScope
 // prints "[crab] <name> <ms>" to stderr when it closes (wall time of the

@@ -14,11 +14,14 @@
 //                IEEE-rounded sqrt and division.  A pair's bin is the number
 //                of edges at or below its d2
 //   k_pr_hist    per pair the bin coordinate x = r / step from centred FP32
-//                coordinates.  When x is farther than a proven error bound
-//                delta from every integer, floor(x) is the reference's bin;
-//                otherwise (about 2*delta of the pairs) d2 is computed in f64
-//                with the reference's operation order (no fused multiply-add)
-//                and placed against the exact edges.
+//                coordinates scaled by 1/step.  When x is farther than a
+//                proven error bound delta from every integer, floor(x) is the
+//                reference's bin; otherwise (about 2*delta of the pairs) d2 is
+//                computed in f64 with the reference's operation order (no
+//                fused multiply-add) and placed against the exact edges.  In
+//                full tiles the near-edge pairs are marked in a 32-bit mask
+//                and placed after each 32-pair chunk, so the chunk itself has
+//                no branches.
 //                Accumulation: when the atoms carry few distinct weights the
 //                tiles are grouped by weight class and each block counts pairs
 //                per class pair in u32 shared counters (flushed to u64 global
@@ -40,7 +43,6 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
-#include <unordered_map>
 
 #include "engine.hpp"
 #include "ops.hpp"
@@ -128,13 +130,15 @@ __device__ __forceinline__ int64_t pr_bin_of(double d2, double step, int64_t bin
 }
 
 // radius: the largest distance of an atom from the centre of the FP32
-// coordinates.  The FP32 bin coordinate x = fl(fl(d2f * rsqrtf(d2f)) * inv_step)
-// differs from sqrt(d2) / step by at most
-//   (sqrt(3) * 2^-23 * radius + 10.5 * 2^-24 * d) / step
-// (coordinate rounding to float, the difference, the sum of squares, the
-// 2-ulp rsqrtf, the product and the rounded reciprocal step); delta is four
-// times that with d <= dmax = bins * step.  Above 2^20 bins every pair takes
-// the exact path.
+// coordinates.  The kernel scales the FP32 coordinates by inv_step = fl(1/step)
+// when it stages them and takes x = sqrt.approx(d2f) in bins.  With
+// R = radius / step and d = sqrt(d2) / step, x differs from d by at most
+//   sqrt(3) * 2^-22 * R + 11.5 * 2^-24 * d
+// (per coordinate the rounding to float and the scaling, 2 * 2^-24 * R each
+// side of the difference; the difference, the sum of squares, a 4-ulp
+// sqrt.approx and the rounded reciprocal step relative to d).  delta is four
+// times that with d <= bins + 1; when delta would exceed a quarter bin, or
+// above 2^20 bins, every pair takes the exact path.
 __global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, int64_t bins, double radius,
                            double* __restrict__ edges, PrParams* __restrict__ par) {
   const double dmax2 = __longlong_as_double((long long)*dmax2_bits);
@@ -147,7 +151,7 @@ __global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, in
   if (k == 0) {
     par->step = step;
     par->inv_step = (float)fmin(1.0 / step, (double)FLT_MAX);
-    const double bound = (1.7320508075688772 * 0x1p-23 * radius / step + 10.5 * 0x1p-24 * (double)(bins + 1));
+    const double bound = (1.7320508075688772 * 0x1p-22 * radius / step + 11.5 * 0x1p-24 * (double)(bins + 1));
     par->delta = bins > (1 << 20) ? FLT_MAX : (float)fmin(4.0 * bound, 0.25);
     if (4.0 * bound > 0.25) par->delta = FLT_MAX;
     par->degenerate = 0;
@@ -165,11 +169,46 @@ __global__ void k_pr_edges(const unsigned long long* __restrict__ dmax2_bits, in
   edges[k] = __longlong_as_double((long long)hi);
 }
 
+__device__ __forceinline__ float pr_sqrt_approx(float v) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+// Bin coordinate of a pair from FP32 coordinates already in bins.
+__device__ __forceinline__ float pr_bin_coord(const float4& fi, const float4& fj) {
+  const float fx = fi.x - fj.x, fy = fi.y - fj.y, fz = fi.z - fj.z;
+  return pr_sqrt_approx(fx * fx + fy * fy + fz * fz);
+}
+
+// The reference's bin of a pair from its exact f64 d2, starting the search at
+// the FP32 estimate x.
+__device__ __forceinline__ int pr_exact_bin(const double4& pi, const double4& pj, float x, const double* E, int bins) {
+  int e = (int)fminf(fmaxf(x, 0.0f), (float)(bins - 1));
+  const double d2 = pr_sqdist(pi, pj);
+  while (e + 1 < bins && d2 >= E[e + 1]) ++e;
+  while (e > 0 && d2 < E[e]) --e;
+  return e;
+}
+
+constexpr float kPrMagic = 12582912.0f;  // 1.5 * 2^23: x + kPrMagic holds floor(x) in its low bits
+constexpr int kPrMagicBits = 0x4B400000;
+
+template <int kMode>
+struct PrAcc {
+  unsigned* c;  // kPrCounts
+  double* w;    // weighted modes
+  __device__ __forceinline__ void add(int e, double wij) const {
+    if constexpr (kMode == kPrCounts) atomicAdd(&c[e], 1u);
+    else atomicAdd(&w[e], wij);
+  }
+};
+
 // Shared layout: kPrCounts: edges[bins + 1] (f64), then copies x u32[bins];
 // kPrWeighted: edges, then copies x f64[bins]; kPrWeightedGlobal: no dynamic
 // shared memory (edges and the block's row in device memory).
 template <int kMode>
-__global__ void __launch_bounds__(kPrThreads)
+__global__ void __launch_bounds__(kPrThreads, 8)
     k_pr_hist(const double4* __restrict__ pos, const float4* __restrict__ pos32, const int2* __restrict__ tiles,
               int n_tiles, int n_types, int64_t chunk, const double* __restrict__ edges,
               const PrParams* __restrict__ par, int bins, int copies, unsigned long long* __restrict__ counts,
@@ -178,9 +217,10 @@ __global__ void __launch_bounds__(kPrThreads)
   __shared__ double4 sj[kPrThreads];
   __shared__ float4 sj32[kPrThreads];
   if (par->degenerate) return;
-  const float inv_step = par->inv_step, delta = par->delta;
-  const bool always_exact = !(delta < 1.0f);
-  const float top = (float)bins - 0.5f;  // nearest integer >= bins: bin bins - 1
+  const float inv_step = par->inv_step;
+  // a pair is near an edge when its fractional bin coordinate is within delta
+  // of 0 or 1: |frac - 0.5| > 0.5 - delta (always, when delta is FLT_MAX)
+  const float near_edge = 0.5f - par->delta;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int si = lane * 4 + warp;  // this thread's slot in the i tile
   const double* E = kMode == kPrWeightedGlobal ? edges : pr_dyn;
@@ -193,8 +233,10 @@ __global__ void __launch_bounds__(kPrThreads)
     else
       for (int k = threadIdx.x; k < copies * bins; k += kPrThreads) Hw[k] = 0.0;
   }
-  unsigned* myc = Hc + (size_t)(warp % copies) * bins;
-  double* myw = kMode == kPrWeightedGlobal ? Hw : Hw + (size_t)(warp % copies) * bins;
+  PrAcc<kMode> acc;
+  acc.c = Hc + (size_t)(warp % copies) * bins;
+  acc.w = kMode == kPrWeightedGlobal ? Hw : Hw + (size_t)(warp % copies) * bins;
+  const int top = kPrMagicBits + bins - 1;  // floor(x) capped at bins - 1, in magic bits
 
   const int64_t n_work = (int64_t)n_tiles * (n_tiles + 1) / 2;
   int64_t w = (int64_t)blockIdx.x * chunk;
@@ -206,12 +248,12 @@ __global__ void __launch_bounds__(kPrThreads)
   auto flush_counts = [&]() {
     __syncthreads();
     for (int k = threadIdx.x; k < bins; k += kPrThreads) {
-      unsigned long long s = 0ull;
+      unsigned long long sum = 0ull;
       for (int c = 0; c < copies; ++c) {
-        s += Hc[(size_t)c * bins + k];
+        sum += Hc[(size_t)c * bins + k];
         Hc[(size_t)c * bins + k] = 0u;
       }
-      if (s) atomicAdd(&counts[(size_t)cur_pair * bins + k], s);
+      if (sum) atomicAdd(&counts[(size_t)cur_pair * bins + k], sum);
     }
     __syncthreads();
   };
@@ -230,46 +272,54 @@ __global__ void __launch_bounds__(kPrThreads)
     if (b != cur_b) {
       __syncthreads();
       if ((int)threadIdx.x < tb.y) {
-        sj[threadIdx.x] = pos[(int64_t)b * kPrThreads + threadIdx.x];
-        sj32[threadIdx.x] = pos32[(int64_t)b * kPrThreads + threadIdx.x];
+        const int64_t g = (int64_t)b * kPrThreads + threadIdx.x;
+        const float4 f = pos32[g];
+        sj[threadIdx.x] = pos[g];
+        sj32[threadIdx.x] = make_float4(f.x * inv_step, f.y * inv_step, f.z * inv_step, 0.0f);
       }
       __syncthreads();
       cur_b = b;
     }
     if (si < ta.y) {
       const int64_t gi = (int64_t)a * kPrThreads + si;
-      const float4 fi = pos32[gi];
+      float4 fi = pos32[gi];
+      fi = make_float4(fi.x * inv_step, fi.y * inv_step, fi.z * inv_step, 0.0f);
       double wi = 0.0;
       if constexpr (kMode != kPrCounts) wi = pos[gi].w;
-      for (int j = (a == b) ? si + 1 : 0; j < tb.y; ++j) {
-        const float4 fj = sj32[j];
-        const float fx = fi.x - fj.x, fy = fi.y - fj.y, fz = fi.z - fj.z;
-        const float d2f = fx * fx + fy * fy + fz * fz;
-        const float x = d2f * rsqrtf(fmaxf(d2f, 1e-30f)) * inv_step;
-        int e;
-        bool exact = always_exact;
-        if (!always_exact) {
-          const float t = x + 12582912.0f;  // 1.5 * 2^23: rounds x to the nearest integer
-          const float k = t - 12582912.0f;
-          const int ki = __float_as_int(t) - 0x4B400000;
-          if (fabsf(x - k) >= delta) e = ki - (k > x ? 1 : 0);  // no edge within reach: floor(x)
-          else if (k < 0.5f) e = 0;                             // next to 0: floor is 0
-          else if (k > top) e = bins - 1;                        // at or past bins: the last bin
-          else {
-            e = ki;
-            exact = true;
+      if (a != b && tb.y == kPrThreads) {
+        // full off-diagonal tile: 32 pairs per chunk without branches; pairs
+        // near an edge are marked and placed exactly after the chunk
+#pragma unroll 1
+        for (int jc = 0; jc < kPrThreads; jc += 32) {
+          unsigned marked = 0u;
+#pragma unroll
+          for (int jj = 0; jj < 32; ++jj) {
+            const float x = pr_bin_coord(fi, sj32[jc + jj]);
+            const float t = __fadd_rd(x, kPrMagic);
+            const float frac = x - (t - kPrMagic);
+            const bool edge = fabsf(frac - 0.5f) > near_edge;
+            marked |= (edge ? 1u : 0u) << jj;
+            const int e = min(__float_as_int(t), top) - kPrMagicBits;
+            if (!edge) acc.add(e, kMode == kPrCounts ? 0.0 : wi * sj[jc + jj].w);
+          }
+          while (marked) {
+            const int j = jc + __ffs(marked) - 1;
+            marked &= marked - 1u;
+            const double4 pj = sj[j];
+            acc.add(pr_exact_bin(pos[gi], pj, pr_bin_coord(fi, sj32[j]), E, bins), wi * pj.w);
           }
         }
-        if (exact) {
-          if (always_exact) e = (int)fminf(fmaxf(x, 0.0f), (float)(bins - 1));
-          e = min(max(e, 0), bins - 1);
-          const double d2 = pr_sqdist(pos[gi], sj[j]);
-          while (e + 1 < bins && d2 >= E[e + 1]) ++e;
-          while (e > 0 && d2 < E[e]) --e;
+      } else {
+        for (int j = (a == b) ? si + 1 : 0; j < tb.y; ++j) {
+          const float x = pr_bin_coord(fi, sj32[j]);
+          const float t = __fadd_rd(x, kPrMagic);
+          const float frac = x - (t - kPrMagic);
+          const double4 pj = sj[j];
+          int e;
+          if (fabsf(frac - 0.5f) > near_edge) e = pr_exact_bin(pos[gi], pj, x, E, bins);
+          else e = min(__float_as_int(t), top) - kPrMagicBits;
+          acc.add(e, wi * pj.w);
         }
-        e = min(e, bins - 1);
-        if constexpr (kMode == kPrCounts) atomicAdd(&myc[e], 1u);
-        else atomicAdd(&myw[e], wi * sj[j].w);
       }
     }
     if (++a > b) {
@@ -282,9 +332,9 @@ __global__ void __launch_bounds__(kPrThreads)
   } else if constexpr (kMode == kPrWeighted) {
     __syncthreads();
     for (int k = threadIdx.x; k < bins; k += kPrThreads) {
-      double s = 0.0;
-      for (int c = 0; c < copies; ++c) s += Hw[(size_t)c * bins + k];
-      rows[(size_t)blockIdx.x * bins + k] = s;
+      double sum = 0.0;
+      for (int c = 0; c < copies; ++c) sum += Hw[(size_t)c * bins + k];
+      rows[(size_t)blockIdx.x * bins + k] = sum;
     }
   }
 }
@@ -352,24 +402,33 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
     if (d > best) { best = d; p1 = i; }
   }
   const double lower = host_sqdist(xyz + 3 * p0, xyz + 3 * p1);
+  trace_mark("pr.lower_bound");
 
   // weight classes: distinct weight values (bit patterns), when there are few
   std::vector<int32_t> type(n, 0);
   std::vector<double> class_w;
   {
-    std::unordered_map<uint64_t, int> ids;
+    // open addressing over the weight bit patterns; the table holds at most
+    // kPrMaxClasses + 1 keys, so it never fills
+    constexpr int kSlots = 256;
+    uint64_t keys[kSlots];
+    int ids[kSlots];
+    std::fill(ids, ids + kSlots, -1);
     for (int64_t i = 0; i < n && (int)class_w.size() <= kPrMaxClasses; ++i) {
       uint64_t key;
       std::memcpy(&key, &w[i], sizeof key);
-      auto it = ids.find(key);
-      if (it == ids.end()) {
-        it = ids.emplace(key, (int)class_w.size()).first;
+      uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 56);
+      while (ids[h] >= 0 && keys[h] != key) h = (h + 1) & (kSlots - 1);
+      if (ids[h] < 0) {
+        keys[h] = key;
+        ids[h] = (int)class_w.size();
         class_w.push_back(w[i]);
       }
-      type[i] = it->second;
+      type[i] = ids[h];
     }
   }
   const int T = (int)class_w.size();
+  trace_mark("pr.classes");
   const int n_pairs = T * (T + 1) / 2;
   const size_t edge_bytes = (size_t)(bins + 1) * sizeof(double);
   int mode = kPrWeightedGlobal, copies = 1;
@@ -421,6 +480,7 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
     h_tiles[t] = make_int2(L.tile_type[t], cnt);
   }
   radius = radius * (1.0 + 1e-6) + 1e-30;
+  trace_mark("pr.pack");
 
   auto* d_pos = (double4*)ctx->dev("pr.pos", (size_t)n_pad * sizeof(double4));
   auto* d_pos32 = (float4*)ctx->dev("pr.pos32", (size_t)n_pad * sizeof(float4));
@@ -445,6 +505,7 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
     copy_h2d(ctx, d_wprod, h_wprod, (size_t)n_pairs * sizeof(double), s);
   }
 
+  trace_mark("pr.upload");
   const int ibins = (int)bins;
   size_t dyn = 0;
   int per_sm = 1;
@@ -504,7 +565,9 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   auto* h_misc = (char*)ctx->host("pr.misc", 64);
   copy_d2h(ctx, h_misc, d_misc, 64, s);
   copy_d2h(ctx, hist, d_out, (size_t)bins * sizeof(double), s);
+  trace_mark("pr.launch");
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  trace_mark("pr.device");
   float t_all = 0.f, t_hist = 0.f;
   CRAB_CUDA_CHECK(cudaEventElapsedTime(&t_hist, ev[1], ev[2]));
   CRAB_CUDA_CHECK(cudaEventElapsedTime(&t_all, ev[0], ev[2]));
@@ -561,9 +624,20 @@ void coordinate_features(crab_ctx* ctx, const crab_struct* st, int64_t bins, dou
   const int64_t n = st->n;
   const double* xyz = st->xyz.data();
   // metrics.rs:245-266: |form factor at q = 0| with implicit hydrogens, floored at 1e-6
+  // the form factor at q = 0 once per (element, group); occupancy scales it as
+  // form_factor_for_atom does (formfactor.rs:425-439)
   std::vector<double> w(n);
-  for (int64_t i = 0; i < n; ++i)
-    w[i] = std::fmax(std::fabs(form_factor(st->elem[i], st->group[i], st->occ[i], true, 0.0)), 1e-6);
+  double ff0[CRAB_EL_OTHER + 1][15];
+  bool have[CRAB_EL_OTHER + 1][15] = {};
+  for (int64_t i = 0; i < n; ++i) {
+    const int el = st->elem[i], g = st->group[i] + 1;
+    if (!have[el][g]) {
+      ff0[el][g] = form_factor(el, g - 1, 1.0, true, 0.0);
+      have[el][g] = true;
+    }
+    const double f = (el == CRAB_EL_H) ? 0.0 : st->occ[i] * ff0[el][g];
+    w[i] = std::fmax(std::fabs(f), 1e-6);
+  }
   double total = 0.0;
   for (int64_t i = 0; i < n; ++i) total += w[i];
   double c[3] = {0.0, 0.0, 0.0};
