@@ -448,6 +448,55 @@ def pr_section(eng, rank, with_cpu):
     return out
 
 
+def _pdb_text(s):
+    """PDB ATOM records of a synthetic structure (residue SYN, six atoms per residue)."""
+    sym = {1: "C", 2: "N", 3: "O", 4: "S"}
+    lines = []
+    for i, (p, e) in enumerate(zip(s.xyz, s.element)):
+        el = sym[int(e)]
+        name = f"{el}{i % 6}"
+        lines.append(f"ATOM  {(i + 1) % 100000:>5} {name:<4} SYN {chr(65 + i // 60000)}{(i // 6) % 10000:>4}    "
+                     f"{p[0]:>8.3f}{p[1]:>8.3f}{p[2]:>8.3f}{1.0:>6.2f}{10.0:>6.2f}          {el:>2}")
+    return ("\n".join(lines) + "\nEND\n").encode()
+
+
+def ingest_section(rank, with_cpu):
+    """Structure ingest (structure.rs:209-327): the config-3 structure as
+    100,000 PDB ATOM records parsed by crab_parse_structure with the default
+    options, median of 5; the CPU baseline is the Python restatement of the
+    reference's reader and policies on the first 10,000 records."""
+    import ctypes as C
+
+    import crabsaxs_b200 as cs
+    from crabsaxs_b200 import _native as N
+    from crabsaxs_b200 import synth
+
+    w = synth.CONFIG3
+    text = _pdb_text(synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius))
+    o = cs.ParseOptions().to_c()
+    ts, n = [], 0
+    for _ in range(6):
+        p = C.c_void_p()
+        t0 = time.perf_counter()
+        if N.lib.crab_parse_structure(text, len(text), N.FORMAT_PDB, C.byref(o), C.byref(p)) != N.OK:
+            raise RuntimeError(N.lib.crab_parse_last_error().decode())
+        ts.append(time.perf_counter() - t0)
+        n = int(N.lib.crab_parsed_atom_count(p))
+        N.lib.crab_parsed_destroy(p)
+    ms = 1e3 * float(np.median(ts[1:]))
+    out = {"atoms": n, "bytes": len(text), "ms": ms, "atoms_per_s": n / (ms * 1e-3)}
+    if with_cpu and rank == 0:
+        from oracle import structure as OS
+
+        sub = b"\n".join(text.split(b"\n")[:10000]).decode() + "\n"
+        t0 = time.perf_counter()
+        k = len(OS.parse(sub, OS.Options()))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k / dt, "unit": "atoms/s", "cores": 1, "kind": "port",
+                               "sample": "first 10,000 records, Python restatement of structure.rs + pdbtbx reading"}
+    return out
+
+
 def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
@@ -566,6 +615,7 @@ def run_ours(args, rank, world, local):
     mp = None if args.no_multipole else multipole_section(eng, rank, peak.value)
     aux = None if args.no_multipole else grid_and_gradient_section(eng, rank)
     pr = None if args.no_multipole else pr_section(eng, rank, not args.no_cpu_baseline)
+    ingest = None if args.no_multipole else ingest_section(rank, not args.no_cpu_baseline)
 
     if rank == 0:
         line = {
@@ -588,6 +638,7 @@ def run_ours(args, rank, world, local):
             "multipole": mp,
             "grids_and_gradient": aux,
             "coordinate_pr": pr,
+            "structure_ingest": ingest,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d.value // args.steps,
                     "d2h_bytes_per_step": d2h.value // args.steps,

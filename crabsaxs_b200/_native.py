@@ -15,15 +15,25 @@ if not LIB_PATH.exists():
     raise ImportError(f"{LIB_PATH} is missing: build it with `python crabsaxs_b200/build.py`")
 lib = C.CDLL(str(LIB_PATH))
 
-OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENOTCONV, ECAPACITY, ENODEVICE = range(8)
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENOTCONV, ECAPACITY, ENODEVICE, EPARSE, EELEMENT, EIO = range(11)
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENOTCONV", 6: "ECAPACITY",
-                7: "ENODEVICE"}
+                7: "ENODEVICE", 8: "EPARSE", 9: "EELEMENT", 10: "EIO"}
+FORMAT_AUTO, FORMAT_PDB, FORMAT_MMCIF = 0, 1, 2
+ALTLOC_HIGHEST, ALTLOC_FIRST, ALTLOC_ALL = 0, 1, 2
+OCC_REPORTED, OCC_SELECTED_FULL = 0, 1
 
 HYD_ANALYTIC, HYD_GRID, HYD_ADAPTIVE = 0, 1, 2
 METHOD_AUTO, METHOD_DEBYE, METHOD_MULTIPOLE = 0, 1, 2
 PREC_FP64, PREC_TF32, PREC_BF16, PREC_BF16_SPLIT, PREC_TF32_SPLIT, PREC_FP32 = 0, 1, 2, 3, 4, 5
 SCALE_FIT, SCALE_FIXED = 0, 1
 BG_FIT, BG_FIXED_ZERO, BG_FIXED = 0, 1, 2
+
+
+class ParseOpts(C.Structure):
+    _fields_ = [("include_hetatm", C.c_int32), ("include_waters", C.c_int32), ("include_glycans", C.c_int32),
+                ("model_index", C.c_int32), ("allow_unknown_elements", C.c_int32),
+                ("occupancy_policy", C.c_int32), ("altloc_policy", C.c_int32), ("n_chains", C.c_int32),
+                ("chains", C.POINTER(C.c_char_p))]
 
 
 class Solvent(C.Structure):
@@ -126,6 +136,19 @@ _SIGS = {
                                        C.POINTER(ReweightResult)]),
     "crab_synth_protein": (C.c_int, [C.c_uint64, I64, C.c_double, D, I8P]),
     "crab_pair_distance_histogram": (C.c_int, [P, D, D, I64, I64, D, D]),
+    "crab_parse_options_default": (None, [C.POINTER(ParseOpts)]),
+    "crab_parse_last_error": (C.c_char_p, []),
+    "crab_parse_structure": (C.c_int, [C.c_char_p, I64, C.c_int32, C.POINTER(ParseOpts), C.POINTER(P)]),
+    "crab_parse_model_count": (C.c_int, [C.c_char_p, I64, C.c_int32, C.POINTER(C.c_int32)]),
+    "crab_read_structure_file": (C.c_int, [C.c_char_p, C.POINTER(ParseOpts), C.POINTER(P)]),
+    "crab_parsed_atom_count": (I64, [P]),
+    "crab_parsed_arrays": (C.c_int, [P, D, D, I8P, I8P, I8P, C.POINTER(I64)]),
+    "crab_parsed_atom_name": (C.c_char_p, [P, I64]),
+    "crab_parsed_residue_name": (C.c_char_p, [P, I64]),
+    "crab_parsed_chain_id": (C.c_char_p, [P, I64]),
+    "crab_parsed_strings": (C.c_int, [P, C.c_int32, C.c_char_p, I64, C.POINTER(I64)]),
+    "crab_parsed_destroy": (C.c_int, [P]),
+    "crab_structure_from_parsed": (C.c_int, [P, P, C.POINTER(P)]),
     "crab_coordinate_features": (C.c_int, [P, P, I64, D, D, D, D, C.POINTER(I64), D, D]),
     "crab_pr_last_timing": (C.c_int, [P, D, D, D, C.POINTER(C.c_int32)]),
     "crab_pair_plan_create": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, C.POINTER(P)]),

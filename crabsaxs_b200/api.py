@@ -12,9 +12,11 @@ the GPU; this module only marshals arrays.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import enum
 import math
 import threading
+from pathlib import Path
 from dataclasses import dataclass, field, replace
 from typing import Optional, Sequence
 
@@ -36,6 +38,14 @@ class FitDidNotConverge(SaxsError):
     pass
 
 
+class StructureParse(SaxsError):
+    """error.rs: failed to parse structure file."""
+
+
+class UnsupportedElement(SaxsError):
+    """error.rs: unsupported element."""
+
+
 class Other(SaxsError):
     pass
 
@@ -49,6 +59,12 @@ def _raise(status: int, ctx: Optional[C.c_void_p] = None) -> None:
         raise InvalidInput(msg or name)
     if status == N.ENOTCONV:
         raise FitDidNotConverge(msg or name)
+    if status == N.EPARSE:
+        raise StructureParse(msg or name)
+    if status == N.EELEMENT:
+        raise UnsupportedElement(msg or name)
+    if status == N.EIO:
+        raise OSError(msg or name)
     raise Other(f"{name}: {msg}")
 
 
@@ -167,6 +183,71 @@ class Structure:
         grp = np.array([united_atom_group(a.residue_name, a.atom_name) for a in atoms], dtype=np.int8)
         return cls(xyz, el, occ, grp)
 
+    @classmethod
+    def from_pdb_file(cls, path, options: Optional["ParseOptions"] = None) -> "Structure":
+        """structure.rs:205-207 / 209-327: PDB or mmCIF by extension."""
+        p = C.c_void_p()
+        o = (options or ParseOptions()).to_c()
+        _parse_check(N.lib.crab_read_structure_file(str(path).encode(), C.byref(o), C.byref(p)))
+        return cls._from_parsed(p)
+
+    from_pdb_file_with_options = from_pdb_file
+
+    @classmethod
+    def from_text(cls, text, options: Optional["ParseOptions"] = None, fmt: int = N.FORMAT_AUTO) -> "Structure":
+        """The same on PDB or mmCIF text (format detected unless given)."""
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        p = C.c_void_p()
+        o = (options or ParseOptions()).to_c()
+        _parse_check(N.lib.crab_parse_structure(data, len(data), fmt, C.byref(o), C.byref(p)))
+        return cls._from_parsed(p)
+
+    @classmethod
+    def from_pdb_file_models_with_options(cls, path, options: Optional["ParseOptions"] = None) -> list["Structure"]:
+        """structure.rs:330-345: every model of the file, in order."""
+        data = Path(path).read_bytes()
+        fmt = N.FORMAT_MMCIF if str(path).lower().endswith((".cif", ".mmcif")) else N.FORMAT_PDB
+        n = C.c_int32()
+        _parse_check(N.lib.crab_parse_model_count(data, len(data), fmt, C.byref(n)))
+        base = options or ParseOptions()
+        out = []
+        for k in range(max(n.value, 1)):
+            o = dataclasses.replace(base, model_index=k)
+            out.append(cls.from_text(data, o, fmt))
+        return out
+
+    @classmethod
+    def _from_parsed(cls, p: C.c_void_p) -> "Structure":
+        try:
+            n = int(N.lib.crab_parsed_atom_count(p))
+            xyz = np.empty((n, 3))
+            occ = np.empty(n)
+            el = np.empty(n, dtype=np.int8)
+            grp = np.empty(n, dtype=np.int8)
+            het = np.empty(n, dtype=np.int8)
+            rid = np.empty(n, dtype=np.int64)
+            N.lib.crab_parsed_arrays(p, _dp(xyz), _dp(occ), el.ctypes.data_as(N.I8P), grp.ctypes.data_as(N.I8P),
+                                     het.ctypes.data_as(N.I8P), rid.ctypes.data_as(C.POINTER(C.c_int64)))
+            s = cls(xyz, el, occ, grp)
+            s.is_hetatm = het.astype(bool)
+            s.residue_id = rid
+            s.atom_name, s.residue_name, s.chain_id = (_parsed_strings(p, k, n) for k in range(3))
+            return s
+        finally:
+            N.lib.crab_parsed_destroy(p)
+
+    @property
+    def atoms(self) -> list[Atom]:
+        """Per-atom records (structure.rs:151-160); names only for parsed structures."""
+        n = self.atom_count
+        names = getattr(self, "atom_name", [""] * n)
+        res = getattr(self, "residue_name", [""] * n)
+        chains = getattr(self, "chain_id", [""] * n)
+        het = getattr(self, "is_hetatm", np.zeros(n, dtype=bool))
+        rid = getattr(self, "residue_id", np.zeros(n, dtype=np.int64))
+        return [Atom(tuple(self.xyz[i]), Element(int(self.element[i])), float(self.occupancy[i]), bool(het[i]),
+                     names[i], res[i], chains[i], int(rid[i])) for i in range(n)]
+
     @property
     def atom_count(self) -> int:
         return int(self.xyz.shape[0])
@@ -195,6 +276,76 @@ class Structure:
             self.release()
         except Exception:
             pass
+
+
+class AltlocPolicy(enum.IntEnum):
+    """structure.rs:14-21."""
+    Highest = N.ALTLOC_HIGHEST
+    First = N.ALTLOC_FIRST
+    All = N.ALTLOC_ALL
+
+
+class OccupancyPolicy(enum.IntEnum):
+    """structure.rs:167-175."""
+    Reported = N.OCC_REPORTED
+    SelectedConformerFull = N.OCC_SELECTED_FULL
+
+
+@dataclass
+class ParseOptions:
+    """structure.rs:177-201 with its defaults."""
+    include_hetatm: bool = False
+    include_waters: bool = False
+    include_glycans: bool = True
+    model_index: int = 0
+    allow_unknown_elements: bool = False
+    occupancy_policy: OccupancyPolicy = OccupancyPolicy.Reported
+    altloc_policy: AltlocPolicy = AltlocPolicy.Highest
+    chains: Optional[list] = None
+
+    def to_c(self) -> N.ParseOpts:
+        o = N.ParseOpts()
+        N.lib.crab_parse_options_default(C.byref(o))
+        o.include_hetatm = int(self.include_hetatm)
+        o.include_waters = int(self.include_waters)
+        o.include_glycans = int(self.include_glycans)
+        o.model_index = int(self.model_index)
+        o.allow_unknown_elements = int(self.allow_unknown_elements)
+        o.occupancy_policy = int(self.occupancy_policy)
+        o.altloc_policy = int(self.altloc_policy)
+        if self.chains:
+            arr = (C.c_char_p * len(self.chains))(*[c.encode() for c in self.chains])
+            o._chains_keep = arr
+            o.n_chains = len(self.chains)
+            o.chains = C.cast(arr, C.POINTER(C.c_char_p))
+        return o
+
+
+def _parsed_strings(p: C.c_void_p, which: int, n: int) -> list:
+    size = C.c_int64()
+    N.lib.crab_parsed_strings(p, which, None, 0, C.byref(size))
+    buf = C.create_string_buffer(max(size.value, 1))
+    N.lib.crab_parsed_strings(p, which, buf, size.value, C.byref(size))
+    return buf.raw[:size.value].decode().split("\n")[:n]
+
+
+def _parse_check(status: int) -> None:
+    if status != N.OK:
+        msg = (N.lib.crab_parse_last_error() or b"").decode()
+        _raise_parse(status, msg)
+
+
+def _raise_parse(status: int, msg: str) -> None:
+    name = N.STATUS_NAMES.get(status, str(status))
+    if status == N.EPARSE:
+        raise StructureParse(msg or name)
+    if status == N.EELEMENT:
+        raise UnsupportedElement(msg or name)
+    if status == N.EIO:
+        raise OSError(msg or name)
+    if status == N.EINVAL:
+        raise InvalidInput(msg or name)
+    raise Other(f"{name}: {msg}")
 
 
 # ---------------------------------------------------------------- options

@@ -22,10 +22,13 @@
  *   crab_ensemble_fit             src/ensemble.rs:127-299   EnsembleFitter::fit / fit_core
  *   crab_reweight_curves          src/reweight.rs:84-154    reweight_curves
  *   crab_coordinate_features      src/metrics.rs:236-270    coordinate_features (P(r): metrics.rs:475-583)
+ *   crab_parse_structure          src/structure.rs:205-345  Structure::from_pdb_file(_with_options / _models_with_options)
  *
  * Status codes map onto crabSAXS's SaxsError (src/error.rs:4-25):
  *   CRAB_EINVAL -> SaxsError::InvalidInput, CRAB_ENOTCONV -> FitDidNotConverge,
- *   every other non-zero code -> SaxsError::Other (message from crab_ctx_last_error).
+ *   CRAB_EPARSE -> StructureParse, CRAB_EELEMENT -> UnsupportedElement, CRAB_EIO -> Io,
+ *   every other non-zero code -> SaxsError::Other (message from crab_ctx_last_error;
+ *   crab_parse_last_error for the ingest calls).
  *
  * Threading: a context serialises its own calls with an internal mutex; use
  * one context per host thread for concurrency (rayon workers in the reference
@@ -48,6 +51,9 @@ extern "C" {
 #define CRAB_ENOTCONV 5     /* fit did not converge (SaxsError::FitDidNotConverge) */
 #define CRAB_ECAPACITY 6    /* caller buffer too small (two-call size query) */
 #define CRAB_ENODEVICE 7    /* no CUDA device / extension not usable */
+#define CRAB_EPARSE 8       /* malformed structure text (SaxsError::StructureParse) */
+#define CRAB_EELEMENT 9     /* element without coefficients (SaxsError::UnsupportedElement) */
+#define CRAB_EIO 10         /* file could not be read (SaxsError::Io) */
 
 /* Element codes, in crabSAXS's `Element` order (src/structure.rs:90-106). */
 enum {
@@ -396,6 +402,65 @@ int crab_coordinate_features(crab_ctx* ctx, crab_struct* st, int64_t bins, doubl
  *  -1  no histogram kernel ran (fewer than two atoms).
  * Any pointer may be NULL. */
 int crab_pr_last_timing(crab_ctx* ctx, double* total_ms, double* histogram_ms, double* pairs, int32_t* mode);
+
+/* ---- structure ingest (host only; no context or GPU needed) -------------- */
+/* ParseOptions (structure.rs:168-201) and its defaults: HETATM records off,
+ * waters off, glycans on, model 0, unknown elements rejected, reported
+ * occupancy, highest-occupancy altloc, every chain. */
+#define CRAB_FORMAT_AUTO 0   /* mmCIF when the text starts with data_ or has _atom_site., else PDB */
+#define CRAB_FORMAT_PDB 1
+#define CRAB_FORMAT_MMCIF 2
+#define CRAB_ALTLOC_HIGHEST 0 /* AltlocPolicy::Highest (the last of equal maxima, as Iterator::max_by) */
+#define CRAB_ALTLOC_FIRST 1
+#define CRAB_ALTLOC_ALL 2
+#define CRAB_OCC_REPORTED 0   /* OccupancyPolicy::Reported */
+#define CRAB_OCC_SELECTED_FULL 1
+typedef struct crab_parse_options {
+  int32_t include_hetatm;
+  int32_t include_waters;
+  int32_t include_glycans;
+  int32_t model_index;          /* 0-based */
+  int32_t allow_unknown_elements;
+  int32_t occupancy_policy;     /* CRAB_OCC_* */
+  int32_t altloc_policy;        /* CRAB_ALTLOC_* */
+  int32_t n_chains;             /* 0: every chain */
+  const char* const* chains;    /* n_chains chain ids to keep */
+} crab_parse_options;
+typedef struct crab_parsed crab_parsed;
+void crab_parse_options_default(crab_parse_options* options);
+/* Message of the last failed parse call on this thread. */
+const char* crab_parse_last_error(void);
+/* Structure::from_pdb_file_with_options (structure.rs:209-327) on PDB or
+ * mmCIF text: model selection, chain/HETATM/water/glycan filters, element
+ * from the element column else the atom name (structure.rs:109-127),
+ * alternate-location and occupancy policies, atoms sorted by (chain, residue
+ * number, atom name).  Malformed numbers or a missing model: CRAB_EPARSE;
+ * an unknown element without allow_unknown_elements: CRAB_EELEMENT. */
+int crab_parse_structure(const char* text, int64_t len, int32_t format, const crab_parse_options* options,
+                         crab_parsed** out);
+/* Models in the text (Structure::from_pdb_file_models_with_options reads
+ * model_index 0 .. n-1). */
+int crab_parse_model_count(const char* text, int64_t len, int32_t format, int32_t* n_models);
+/* The same from a file; the format follows the extension (.cif/.mmcif: mmCIF,
+ * else PDB), as the reference's reader does. Unreadable file: CRAB_EIO. */
+int crab_read_structure_file(const char* path, const crab_parse_options* options, crab_parsed** out);
+int64_t crab_parsed_atom_count(const crab_parsed* parsed);
+/* Atom fields (structure.rs:151-160): xyz n*3, occupancy, element (CRAB_EL_*),
+ * united-atom group of (residue name, atom name) (formfactor.rs:357-417; -1
+ * none), HETATM flag, residue number.  Any pointer may be NULL. */
+int crab_parsed_arrays(const crab_parsed* parsed, double* xyz, double* occupancy, int8_t* element, int8_t* group,
+                       int8_t* hetatm, int64_t* residue_id);
+/* Names of atom i, valid until crab_parsed_destroy; NULL out of range. */
+const char* crab_parsed_atom_name(const crab_parsed* parsed, int64_t i);
+const char* crab_parsed_residue_name(const crab_parsed* parsed, int64_t i);
+const char* crab_parsed_chain_id(const crab_parsed* parsed, int64_t i);
+/* Every atom's name (which = 0), residue name (1) or chain id (2), each
+ * followed by a newline; *len receives the byte count.  buf NULL: size query;
+ * cap too small: CRAB_ECAPACITY. */
+int crab_parsed_strings(const crab_parsed* parsed, int32_t which, char* buf, int64_t cap, int64_t* len);
+int crab_parsed_destroy(crab_parsed* parsed);
+/* crab_structure_create from a parsed structure. */
+int crab_structure_from_parsed(crab_ctx* ctx, const crab_parsed* parsed, crab_struct** out);
 
 /* ---- synthetic inputs (no counterpart in the reference) ----------------- */
 /* Seeded protein-like structure: Cα-style self-avoiding walk (3.8 Å steps,
