@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import re
@@ -589,6 +590,8 @@ def run_ours(args, rank, world, local):
     for _ in range(args.warmup):
         e2e_step()
     eng.reset_stats()
+    gc.collect()
+    gc.disable()  # no collector pauses inside the timed steps
     dist.barrier()
     t0 = time.perf_counter()
     e2e_steps = []
@@ -597,6 +600,7 @@ def run_ours(args, rank, world, local):
         e2e_step()
         e2e_steps.append((time.perf_counter() - ts) * 1e3)
     e2e_s = time.perf_counter() - t0
+    gc.enable()
     dist.barrier()
     e2e_launches, _, _ = eng.stats()
     h2d, d2h = C.c_int64(), C.c_int64()
