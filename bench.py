@@ -242,7 +242,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def ensemble_section(eng, rank):
+def ensemble_section(eng, rank, with_cpu=False):
     """Config 5: 256 conformers (log-uniform 2k-40k atoms), 300 q, the 25 (c1, c2)
     candidates of ensemble.rs:302-315.  Batched: one CUDA graph per scoring pass
     (pair sums of all conformers, 25x256 curves, per-candidate simplex weights,
@@ -290,16 +290,29 @@ def ensemble_section(eng, rank):
         err = max(err, float(np.max(np.abs(bc[j] - i64) / i64)), float(np.max(np.abs(plain[i] - i64) / i64)))
     pairq = sum(c.atom_count * (c.atom_count - 1) / 2.0 for c in confs) * len(q)
     best = runs[-1]
+    cpu = None
+    if with_cpu and rank == 0:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        for i in order[:4]:
+            cc = confs[i]
+            O.debye_solvent_basis(O.Atoms(cc.xyz, cc.element, cc.group, cc.occupancy), q, c1, c2)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 4 / dt, "unit": "curves/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"the 4 smallest conformers ({', '.join(str(confs[i].atom_count) for i in order[:4])} atoms), "
+                         f"one f64 Debye solvent evaluation per curve as the reference's per-candidate "
+                         f"compute_curve does, {dt:.1f} s"}
     return {"curves_per_s": n_curves / (graph_ms * 1e-3), "plain_gpu_curves_per_s": len(confs) / plain_s,
             "speedup_vs_plain": (n_curves / (graph_ms * 1e-3)) / (len(confs) / plain_s),
             "graph_ms": graph_ms, "conformers": len(confs), "candidates": len(cand), "n_q": len(q),
             "atoms": int(sum(c.atom_count for c in confs)), "pair_q_per_pass": pairq,
             "pair_q_per_s": pairq / (graph_ms * 1e-3), "kernels_per_pass": int(launches // 3),
-            "max_rel_err_vs_fp64": err, "best_candidate": [float(best["c1"]), float(best["c2"])],
+            "max_rel_err_vs_fp64": err, "best_candidate": [float(best["c1"]), float(best["c2"])], "cpu_baseline": cpu,
             "reduced_chi2": float(best["reduced_chi2"]), "kl_reduced_chi2": float(best["kl_reduced_chi2"])}
 
 
-def multipole_section(eng, rank, fp32_peak):
+def multipole_section(eng, rank, fp32_peak, with_cpu=False):
     """Config 3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.  The
     default path runs the moment GEMM on tcgen05 tensor cores (TF32 hi+lo, 3
     products per K step); the FP32 SIMT GEMM is timed beside it.  Reports the
@@ -356,7 +369,21 @@ def multipole_section(eng, rank, fp32_peak):
     for _ in range(3):
         cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
     c2_ms = (time.perf_counter() - t0) * 1e3 / 3
+    cpu = None
+    if with_cpu and rank == 0:
+        import oracle as O
+
+        sub_q = w.q[::100]
+        a = O.Atoms(s.xyz, s.element, s.group, s.occupancy)
+        t0 = time.perf_counter()
+        O.multipole_intensity(a, sub_q, L)
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sub_q) / dt, "unit": "q/s", "cores": min(os.cpu_count() or 1, len(sub_q)), "kind": "port",
+               "sample": f"every 100th q ({len(sub_q)} of {len(w.q)}) of the same 100k-atom curve, f64 restatement "
+                         f"of spherical.rs multipole_intensity, {dt:.1f} s",
+               "gpu_q_per_s_wall": len(w.q) / (tc_wall * 1e-3)}
     return {"workload": "multipole intensity, 100k atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50",
+            "cpu_baseline": cpu,
             "precision": "TF32 hi+lo on tcgen05 (default)", "wall_ms": tc_wall, "device_ms": tc_dev,
             "moments_gemm_tensor": {
                 "ms": tc_gemm, "useful_flop": flop, "tensor_flop": 3.0 * flop,
@@ -615,8 +642,8 @@ def run_ours(args, rank, world, local):
                "sample": f"same structure + its {mm - N_ATOMS} sites, {nq} of 500 q values (one per thread), "
                          f"{dt:.1f} s; f64 C++ restatement of solvent.rs debye_solvent_basis"}
 
-    ens = None if args.no_ensemble else ensemble_section(eng, rank)
-    mp = None if args.no_multipole else multipole_section(eng, rank, peak.value)
+    ens = None if args.no_ensemble else ensemble_section(eng, rank, not args.no_cpu_baseline)
+    mp = None if args.no_multipole else multipole_section(eng, rank, peak.value, not args.no_cpu_baseline)
     aux = None if args.no_multipole else grid_and_gradient_section(eng, rank)
     pr = None if args.no_multipole else pr_section(eng, rank, not args.no_cpu_baseline)
     ingest = None if args.no_multipole else ingest_section(rank, not args.no_cpu_baseline)
