@@ -570,12 +570,13 @@ __global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __
                                  const double* __restrict__ nodes, int n_nodes, int L, double* __restrict__ Jn) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nq * n_nodes) return;
-  const int64_t k = idx / n_nodes;
-  const int node = (int)(idx % n_nodes);
+  const int64_t k = idx % nq;  // q fastest: the stores of one l are contiguous across threads
+  const int node = (int)(idx / nq);
   const int ql = lq[k];
   const double x = q[k] * nodes[node];
-  double* out = Jn + idx * (L + 1);
-  for (int l = 0; l <= L; ++l) out[l] = 0.0;
+  const int64_t stride = (int64_t)n_nodes * nq;  // Jn is [l][node][q]
+  double* out = Jn + (int64_t)node * nq + k;
+  for (int l = 0; l <= L; ++l) out[l * stride] = 0.0;
   if (fabs(x) < 1e-8) {
     out[0] = 1.0;
     return;
@@ -598,109 +599,138 @@ __global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __
   const double j0 = s / x;
   const double j1 = __dadd_rn(s / (x * x), -(c / x));
   const double scale = fabs(j0) >= fabs(j1) ? j0 / work[0] : j1 / work[1];
-  for (int l = 0; l <= ql; ++l) out[l] = work[l] * scale;
+  for (int l = 0; l <= ql; ++l) out[l * stride] = work[l] * scale;
 }
 
-// One block per kGramQ consecutive q.  The node values j_l(q rho_b) of the
-// block's q for a window of l (all l whose values fit kGramSmem) are staged in
-// shared memory, then every thread takes lm rows of the window:
-//   A^c_lm(q) = sum_g amp[c][t(g)][q] sum_b M[g][b][lm] j_l(q rho_{seg(g), b})
+// The q pass.  For every q and amplitude combination c
+//   A^c_lm(q) = sum_t amp[c][t][q] sum_s sum_b M[t*S+s][b][lm] j_l(q rho_{s,b})
 // and 4 pi sum_{l <= l_q, m} A^c A^d accumulates per q for c <= d (order
-// (0,0), (1,1), (2,2), (0,1), (0,2), (1,2) for three combinations).  Each M
-// element is read once per block of q.
-constexpr int kGramQ = 4;
-constexpr size_t kGramSmem = 96 * 1024;
+// (0,0), (1,1), (2,2), (0,1), (0,2), (1,2) for three combinations).
+// k_mp_gram: one block per (l, chunk of 32 m, chunk of 128 q).  Each warp
+// owns 4 m and each lane 4 q (lane + 32 j), so one thread keeps a 4 x 4 tile
+// of the contraction over the radial nodes in registers; the block's moments
+// (per group) and node values (per segment) are staged in shared memory,
+// where a warp's moment loads are broadcasts and its node-value loads are
+// contiguous.  Each block writes its partial sums per (combination, q);
+// k_mp_gram_reduce adds the rows in (l, m) order (deterministic).
+constexpr int kGramM = 32, kGramQ = 128, kGramThreads = 256;
+
 template <int K>
-__global__ void __launch_bounds__(256) k_mp_gram(const double* __restrict__ M, const double* __restrict__ Jn,
-                                                 const int32_t* __restrict__ lq, const double* __restrict__ amp,
-                                                 int T, int S, int nb, int n_nodes, int L, int lm_pad, int64_t nq,
-                                                 int l_window, double* __restrict__ out) {
+__global__ void __launch_bounds__(kGramThreads)
+    k_mp_gram(const double* __restrict__ M, const double* __restrict__ Jn, const int32_t* __restrict__ lq,
+              const double* __restrict__ amp, const int2* __restrict__ rows, int T, int S, int nb, int n_nodes,
+              int lm_pad, int64_t nq, double* __restrict__ part) {
   constexpr int P = K * (K + 1) / 2;
   extern __shared__ double gram_smem[];
-  double* amps = gram_smem;                      // [K][T][kGramQ]
-  double* Js = gram_smem + K * T * kGramQ;       // [l - l0][node][kGramQ]
-  __shared__ int lqs[kGramQ];
-  __shared__ double red[8][P * kGramQ];
-  const int64_t q0 = (int64_t)blockIdx.x * kGramQ;
-  const int nqb = (int)min((int64_t)kGramQ, nq - q0);
-  const int tid = threadIdx.x;
-  if (tid < kGramQ) lqs[tid] = tid < nqb ? lq[q0 + tid] : -1;
-  for (int idx = tid; idx < K * T * kGramQ; idx += blockDim.x) {
-    const int qi = idx % kGramQ, ct = idx / kGramQ;
-    amps[idx] = qi < nqb ? amp[(int64_t)ct * nq + q0 + qi] : 0.0;
-  }
-  __syncthreads();
-  int lmax = -1;
-  for (int qi = 0; qi < kGramQ; ++qi) lmax = max(lmax, lqs[qi]);
-  const int G = T * S;
-  double acc[P][kGramQ];
+  double* Js = gram_smem;                               // [nb][kGramQ] node values of one segment
+  double* Ms = gram_smem + (size_t)kMaxNodes * kGramQ;  // [nb][kGramM] moments of one group
+  const int2 row = rows[blockIdx.x];
+  const int l = row.x, m0 = row.y;
+  const int nm = min(kGramM, 2 * l + 1 - m0);
+  const int64_t q0 = (int64_t)blockIdx.y * kGramQ;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t jrow = (int64_t)l * n_nodes;
+  double A[K][4][4];
 #pragma unroll
-  for (int p = 0; p < P; ++p)
+  for (int c = 0; c < K; ++c)
 #pragma unroll
-    for (int qi = 0; qi < kGramQ; ++qi) acc[p][qi] = 0.0;
-  for (int l0 = 0; l0 <= lmax; l0 += l_window) {
-    const int l1 = min(lmax + 1, l0 + l_window);
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) A[c][i][j] = 0.0;
+  for (int sg = 0; sg < S; ++sg) {
     __syncthreads();
-    for (int idx = tid; idx < (l1 - l0) * n_nodes * kGramQ; idx += blockDim.x) {
-      const int qi = idx % kGramQ, node = (idx / kGramQ) % n_nodes, dl = idx / (kGramQ * n_nodes);
-      Js[idx] = qi < nqb ? Jn[((q0 + qi) * n_nodes + node) * (int64_t)(L + 1) + l0 + dl] : 0.0;
+    for (int idx = threadIdx.x; idx < nb * kGramQ; idx += kGramThreads) {
+      const int b = idx / kGramQ, ql = idx % kGramQ;
+      const int64_t q = q0 + ql;
+      Js[idx] = q < nq ? Jn[(jrow + sg * nb + b) * nq + q] : 0.0;
     }
-    __syncthreads();
-    for (int lm = l0 * l0 + tid; lm < l1 * l1; lm += blockDim.x) {
-      int l = (int)sqrt((double)lm);
-      while (l * l > lm) --l;
-      while ((l + 1) * (l + 1) <= lm) ++l;
-      const double* Jl = Js + (l - l0) * n_nodes * kGramQ;
-      double A[K][kGramQ];
+    for (int t = 0; t < T; ++t) {
+      const int g = t * S + sg;
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < nb * kGramM; idx += kGramThreads) {
+        const int b = idx / kGramM, mi = idx % kGramM;
+        Ms[idx] = mi < nm ? M[((int64_t)g * kMaxNodes + b) * lm_pad + l * l + m0 + mi] : 0.0;
+      }
+      __syncthreads();
+      double C[4][4];
 #pragma unroll
-      for (int c = 0; c < K; ++c)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int qi = 0; qi < kGramQ; ++qi) A[c][qi] = 0.0;
-      for (int g = 0; g < G; ++g) {
-        const double* Mg = M + (int64_t)g * kMaxNodes * lm_pad + lm;
-        const double* Jg = Jl + (g % S) * nb * kGramQ;
-        double C[kGramQ];
+        for (int j = 0; j < 4; ++j) C[i][j] = 0.0;
+      const double* mrow = Ms + warp * 4;
+      const double* jcol = Js + lane;
+#pragma unroll 2
+      for (int b = 0; b < nb; ++b) {
+        double mv[4], jv[4];
 #pragma unroll
-        for (int qi = 0; qi < kGramQ; ++qi) C[qi] = 0.0;
-        for (int b = 0; b < nb; ++b) {
-          const double mv = Mg[(int64_t)b * lm_pad];
+        for (int i = 0; i < 4; ++i) mv[i] = mrow[b * kGramM + i];
 #pragma unroll
-          for (int qi = 0; qi < kGramQ; ++qi) C[qi] = fma(mv, Jg[b * kGramQ + qi], C[qi]);
+        for (int j = 0; j < 4; ++j) jv[j] = jcol[b * kGramQ + 32 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) C[i][j] = fma(mv[i], jv[j], C[i][j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t q = q0 + lane + 32 * j;
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const double a = q < nq ? amp[((int64_t)c * T + t) * nq + q] : 0.0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) A[c][i][j] = fma(a, C[i][j], A[c][i][j]);
         }
-        const int t = g / S;
-#pragma unroll
-        for (int c = 0; c < K; ++c)
-#pragma unroll
-          for (int qi = 0; qi < kGramQ; ++qi) A[c][qi] = fma(amps[(c * T + t) * kGramQ + qi], C[qi], A[c][qi]);
-      }
-#pragma unroll
-      for (int qi = 0; qi < kGramQ; ++qi) {
-        if (l > lqs[qi]) continue;
-        int p = 0;
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[p++][qi] += A[c][qi] * A[c][qi];
-#pragma unroll
-        for (int c = 0; c < K; ++c)
-#pragma unroll
-          for (int d = c + 1; d < K; ++d) acc[p++][qi] += A[c][qi] * A[d][qi];
       }
     }
   }
+  double acc[P][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t q = q0 + lane + 32 * j;
+    const bool on = q < nq && l <= lq[q];
+    int p = 0;
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      double v = 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v = fma(A[c][i][j], A[c][i][j], v);
+      acc[p++][j] = on ? v : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < K; ++c)
+#pragma unroll
+      for (int d = c + 1; d < K; ++d) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v = fma(A[c][i][j], A[d][i][j], v);
+        acc[p++][j] = on ? v : 0.0;
+      }
+  }
+  __syncthreads();
+  double* red = gram_smem;  // [warp][P][kGramQ], over the node values (no longer needed)
 #pragma unroll
   for (int p = 0; p < P; ++p)
 #pragma unroll
-    for (int qi = 0; qi < kGramQ; ++qi) {
-      double v = acc[p][qi];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if ((tid & 31) == 0) red[tid >> 5][p * kGramQ + qi] = v;
-    }
+    for (int j = 0; j < 4; ++j) red[(warp * P + p) * kGramQ + lane + 32 * j] = acc[p][j];
   __syncthreads();
-  if (tid < P * kGramQ) {
-    const int p = tid / kGramQ, qi = tid % kGramQ;
+  for (int idx = threadIdx.x; idx < P * kGramQ; idx += kGramThreads) {
+    const int p = idx / kGramQ, ql = idx % kGramQ;
     double v = 0.0;
-    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[wi][tid];
-    if (qi < nqb) out[p * nq + q0 + qi] = 4.0 * kPiD * v;
+    for (int w = 0; w < kGramThreads / 32; ++w) v += red[(w * P + p) * kGramQ + ql];
+    const int64_t q = q0 + ql;
+    if (q < nq) part[((int64_t)blockIdx.x * P + p) * nq + q] = v;
   }
+}
+
+__global__ void k_mp_gram_reduce(const double* __restrict__ part, int n_rows, int P, int64_t nq,
+                                 double* __restrict__ out) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)P * nq) return;
+  const int p = (int)(idx / nq);
+  const int64_t q = idx % nq;
+  double v = 0.0;
+  for (int r = 0; r < n_rows; ++r) v += part[((int64_t)r * P + p) * nq + q];
+  out[(int64_t)p * nq + q] = 4.0 * kPiD * v;
 }
 
 // ------------------------------------------------------------------ host
@@ -859,20 +889,28 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
   k_mp_node_bessel<<<(unsigned)((nbess + 127) / 128), 128, 0, s>>>(d_q, d_lq, nq, d_nodes, n_nodes, L, d_Jn);
-  const size_t amp_bytes = sizeof(double) * (size_t)K * T * kGramQ;
-  const size_t per_l = sizeof(double) * (size_t)n_nodes * kGramQ;
-  require(amp_bytes + per_l <= kGramSmem, "multipole: too many scattering types or radial nodes");
-  const int l_window = (int)std::min<size_t>((size_t)L + 1, (kGramSmem - amp_bytes) / per_l);
-  const size_t gram_smem = amp_bytes + per_l * (size_t)l_window;
-  const unsigned gram_blocks = (unsigned)((nq + kGramQ - 1) / kGramQ);
-  if (K == 1) {
-    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
-    k_mp_gram<1><<<gram_blocks, 256, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, T, S, nb, n_nodes, L, lm_pad, nq,
-                                                      l_window, d_out);
-  } else {
-    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
-    k_mp_gram<3><<<gram_blocks, 256, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, T, S, nb, n_nodes, L, lm_pad, nq,
-                                                      l_window, d_out);
+  {
+    std::vector<int2> rows;
+    for (int l = 0; l <= L; ++l)
+      for (int m0 = 0; m0 < 2 * l + 1; m0 += kGramM) rows.push_back(make_int2(l, m0));
+    auto* d_rows = (int2*)ctx->dev("mp_gram_rows", sizeof(int2) * rows.size());
+    copy_h2d(ctx, d_rows, rows.data(), sizeof(int2) * rows.size(), s);
+    auto* d_gpart = (double*)ctx->dev("mp_gram_part", sizeof(double) * rows.size() * (size_t)P * nq);
+    const size_t gram_smem = sizeof(double) * (size_t)kMaxNodes * (kGramQ + kGramM);
+    const dim3 grid((unsigned)rows.size(), (unsigned)((nq + kGramQ - 1) / kGramQ));
+    if (K == 1) {
+      CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
+      k_mp_gram<1><<<grid, kGramThreads, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, d_rows, T, S, nb, n_nodes, lm_pad,
+                                                          nq, d_gpart);
+    } else {
+      CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_gram<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem));
+      k_mp_gram<3><<<grid, kGramThreads, gram_smem, s>>>(d_M, d_Jn, d_lq, d_amp, d_rows, T, S, nb, n_nodes, lm_pad,
+                                                          nq, d_gpart);
+    }
+    CRAB_CUDA_CHECK(cudaGetLastError());
+    k_mp_gram_reduce<<<(unsigned)(((int64_t)P * nq + 255) / 256), 256, 0, s>>>(d_gpart, (int)rows.size(), P, nq,
+                                                                                d_out);
+    ctx->launches += 1;
   }
   CRAB_CUDA_CHECK(cudaGetLastError());
   CRAB_CUDA_CHECK(cudaEventRecord(ev[3], s));
