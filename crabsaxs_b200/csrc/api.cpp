@@ -130,47 +130,60 @@ static bool excluded_zero(const AtomClass& c, bool implicit) {
 
 TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites) {
   // Classes are (element 0..14, united-atom group -1..13), numbered in
-  // (element, group) order; a direct 15 x 15 table replaces a map lookup per atom.
+  // (element, group) order; a direct 15 x 15 table replaces a map lookup per
+  // atom.  Pass 1 finds the classes present and the kept count; pass 2 fills.
   TypedAtoms t;
   constexpr int kE = CRAB_EL_OTHER + 1, kG = 15;
-  int present[kE][kG] = {};
-  std::vector<int64_t> keep;
-  keep.reserve(st->n);
-  for (int64_t i = 0; i < st->n; ++i) {
-    const AtomClass c{st->elem[i], implicit ? (int)st->group[i] : -1};
-    bool drop = false;
-    if (need == TermSet::Vacuum) drop = vacuum_zero(c, implicit);
-    else if (need == TermSet::SolventGrid) drop = vacuum_zero(c, implicit) && excluded_zero(c, implicit);
-    if (drop) continue;
-    keep.push_back(i);
-    present[c.element][c.group + 1] = 1;
-  }
-  int index[kE][kG];
-  int next = 0;
+  bool drop[kE][kG];
   for (int e = 0; e < kE; ++e)
     for (int g = 0; g < kG; ++g) {
-      index[e][g] = present[e][g] ? next++ : -1;
-      if (present[e][g]) t.cls.push_back(AtomClass{e, g - 1});
+      const AtomClass c{e, implicit ? g - 1 : -1};
+      bool d = false;
+      if (need == TermSet::Vacuum) d = vacuum_zero(c, implicit);
+      else if (need == TermSet::SolventGrid) d = vacuum_zero(c, implicit) && excluded_zero(c, implicit);
+      drop[e][g] = d;
+    }
+  int64_t present[kE][kG] = {};
+  const int8_t* el = st->elem.data();
+  const int8_t* gr = st->group.data();
+  for (int64_t i = 0; i < st->n; ++i) ++present[el[i]][(implicit ? (int)gr[i] : -1) + 1];
+  int index[kE][kG];
+  int next = 0;
+  int64_t nk = 0;
+  for (int e = 0; e < kE; ++e)
+    for (int g = 0; g < kG; ++g) {
+      const bool used = present[e][g] > 0 && !drop[e][g];
+      index[e][g] = used ? next++ : -1;
+      if (used) {
+        t.cls.push_back(AtomClass{e, g - 1});
+        nk += present[e][g];
+      }
     }
   const int64_t ns = sites ? (int64_t)sites->size() / 3 : 0;
   if (sites) t.cls.push_back(AtomClass{-1, -1});
-  const size_t nk = keep.size();
-  t.xyz.resize(3 * (nk + ns));
-  t.w.resize(nk + ns);
-  t.type.resize(nk + ns);
-  t.src.assign(nk + ns, -1);
-  for (size_t k = 0; k < nk; ++k) {
-    const int64_t i = keep[k];
-    for (int d = 0; d < 3; ++d) t.xyz[3 * k + d] = st->xyz[3 * i + d];
-    t.w[k] = st->occ[i];
-    t.type[k] = index[st->elem[i]][(implicit ? (int)st->group[i] : -1) + 1];
+  t.xyz.resize(3 * (size_t)(nk + ns));
+  t.w.resize((size_t)(nk + ns));
+  t.type.resize((size_t)(nk + ns));
+  t.src.resize((size_t)(nk + ns));
+  const double* xyz = st->xyz.data();
+  const double* occ = st->occ.data();
+  int64_t k = 0;
+  for (int64_t i = 0; i < st->n; ++i) {
+    const int ty = index[el[i]][(implicit ? (int)gr[i] : -1) + 1];
+    if (ty < 0) continue;
+    t.xyz[3 * k] = xyz[3 * i];
+    t.xyz[3 * k + 1] = xyz[3 * i + 1];
+    t.xyz[3 * k + 2] = xyz[3 * i + 2];
+    t.w[k] = occ[i];
+    t.type[k] = ty;
     t.src[k] = i;
+    ++k;
   }
-  for (int64_t s = 0; s < ns; ++s) {
-    const size_t k = nk + s;
+  for (int64_t s = 0; s < ns; ++s, ++k) {
     for (int d = 0; d < 3; ++d) t.xyz[3 * k + d] = (*sites)[3 * s + d];
     t.w[k] = 1.0;
     t.type[k] = next;
+    t.src[k] = -1;
   }
   t.T = (int)t.cls.size();
   return t;

@@ -778,11 +778,19 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   std::vector<int64_t> begin(G + 1, 0);
   for (int g = 0; g < G; ++g) begin[g + 1] = begin[g] + (count[g] + kPointAlign - 1) / kPointAlign * kPointAlign;
   const int64_t n_pad = std::max<int64_t>(begin[G], kPointAlign);
-  std::vector<double> pts((size_t)5 * n_pad, 0.0);
-  std::vector<int32_t> seg(n_pad, 0);
+  // points are built in the context's pinned staging buffers (reused across
+  // calls, uploaded asynchronously); padding slots are zeroed explicitly
+  auto* pts = (double*)ctx->host("mp_pts", sizeof(double) * 5 * (size_t)n_pad);
+  auto* seg = (int32_t*)ctx->host("mp_seg", sizeof(int32_t) * (size_t)n_pad);
   std::vector<int64_t> fill(begin.begin(), begin.end() - 1);
-  for (int g = 0; g < G; ++g)
+  for (int g = 0; g < G; ++g) {
     for (int64_t k = begin[g]; k < begin[g + 1]; ++k) seg[k] = g % S;
+    std::fill(pts + 5 * (begin[g] + count[g]), pts + 5 * begin[g + 1], 0.0);
+  }
+  if (begin[G] < n_pad) {  // no points at all: one zero tile
+    std::fill(pts + 5 * begin[G], pts + 5 * n_pad, 0.0);
+    std::fill(seg + begin[G], seg + n_pad, 0);
+  }
   for (int64_t i = 0; i < n; ++i) {
     const int64_t k = fill[group_of[i]]++;
     pts[5 * k] = t.xyz[3 * i] - in.centre[0];
@@ -814,7 +822,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   TraceScope tdev("multipole_device");
   cudaStream_t s = ctx->stream;
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
-  double* d_pts = (double*)ctx->dev("mp_pts", sizeof(double) * pts.size());
+  double* d_pts = (double*)ctx->dev("mp_pts", sizeof(double) * 5 * (size_t)n_pad);
   int32_t* d_seg = (int32_t*)ctx->dev("mp_seg", sizeof(int32_t) * n_pad);
   double* d_norms = (double*)ctx->dev("mp_norms", sizeof(double) * norms.size());
   double* d_inv = (double*)ctx->dev("mp_inv", sizeof(double) * inv.size());
@@ -833,8 +841,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * in.amp.size());
   double* d_out = (double*)ctx->dev("mp_out", sizeof(double) * (size_t)P * nq);
   int* d_status = (int*)ctx->dev("mp_status", sizeof(int));
-  copy_h2d(ctx, d_pts, pts.data(), sizeof(double) * pts.size(), s);
-  copy_h2d(ctx, d_seg, seg.data(), sizeof(int32_t) * n_pad, s);
+  copy_h2d(ctx, d_pts, pts, sizeof(double) * 5 * (size_t)n_pad, s);
+  copy_h2d(ctx, d_seg, seg, sizeof(int32_t) * n_pad, s);
   copy_h2d(ctx, d_norms, norms.data(), sizeof(double) * norms.size(), s);
   copy_h2d(ctx, d_inv, inv.data(), sizeof(double) * inv.size(), s);
   copy_h2d(ctx, d_nodes, B.nodes.data(), sizeof(double) * B.nodes.size(), s);
