@@ -552,20 +552,26 @@ constexpr size_t tc_smem_bytes() {
 
 // M[g][b][t*128 + r] = sum over the point splits of group g of the partial
 // tiles of lm tile t; one block per (group, lm tile), in a fixed order.
+// One CTA per (group, lm tile, 1/kReduceSplit of the tile's elements).
+constexpr int kReduceSplit = 8;
+static_assert(kTileElems % kReduceSplit == 0, "reduce split");
 __global__ void __launch_bounds__(256) k_mp_reduce(const double* __restrict__ part, const int32_t* __restrict__ gfirst,
                                                    const int32_t* __restrict__ gsplits, int n_lmt, int lm_pad,
                                                    double* __restrict__ M) {
   const int g = blockIdx.x / n_lmt, t = blockIdx.x % n_lmt;
   const int first = gfirst[g], n = gsplits[g];
-  for (int e = threadIdx.x; e < kTileElems; e += blockDim.x) {
+  constexpr int kPer = kTileElems / kReduceSplit;
+  const int e0 = blockIdx.y * kPer;
+  for (int e = e0 + threadIdx.x; e < e0 + kPer; e += blockDim.x) {
     double v = 0.0;
+#pragma unroll 4
     for (int k = 0; k < n; ++k) v += part[(int64_t)(first + k * n_lmt + t) * kTileElems + e];
     M[((int64_t)g * kMaxNodes + e / kGemmM) * lm_pad + t * kGemmM + e % kGemmM] = v;
   }
 }
 
 // j_0..j_{l_q}(q rho) at every node (spherical.rs:95-133, f64 as the
-// reference), zero for l_q < l <= L.  Jn[k][s*nb + b][l].
+// reference), zero for l_q < l <= L.  Jn[l][s*nb + b][k].
 __global__ void k_mp_node_bessel(const double* __restrict__ q, const int32_t* __restrict__ lq, int64_t nq,
                                  const double* __restrict__ nodes, int n_nodes, int L, double* __restrict__ Jn) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -722,15 +728,25 @@ __global__ void __launch_bounds__(kGramThreads)
   }
 }
 
-__global__ void k_mp_gram_reduce(const double* __restrict__ part, int n_rows, int P, int64_t nq,
-                                 double* __restrict__ out) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)P * nq) return;
-  const int p = (int)(idx / nq);
-  const int64_t q = idx % nq;
+// 32 (combination, q) outputs per CTA; thread row y sums the rows r = y, y + 8,
+// ... in order, then row 0 adds the eight partial sums in order.
+__global__ void __launch_bounds__(256) k_mp_gram_reduce(const double* __restrict__ part, int n_rows, int P,
+                                                        int64_t nq, double* __restrict__ out) {
+  __shared__ double red[8][32];
+  const int64_t idx = (int64_t)blockIdx.x * 32 + threadIdx.x;
+  const bool on = idx < (int64_t)P * nq;
+  const int p = on ? (int)(idx / nq) : 0;
+  const int64_t q = on ? idx % nq : 0;
   double v = 0.0;
-  for (int r = 0; r < n_rows; ++r) v += part[((int64_t)r * P + p) * nq + q];
-  out[(int64_t)p * nq + q] = 4.0 * kPiD * v;
+  if (on)
+    for (int r = threadIdx.y; r < n_rows; r += 8) v += part[((int64_t)r * P + p) * nq + q];
+  red[threadIdx.y][threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.y == 0 && on) {
+    double sum = 0.0;
+    for (int y = 0; y < 8; ++y) sum += red[y][threadIdx.x];
+    out[(int64_t)p * nq + q] = 4.0 * kPiD * sum;
+  }
 }
 
 // ------------------------------------------------------------------ host
@@ -892,7 +908,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
 #undef CRAB_TC
     }
   }
-  k_mp_reduce<<<(unsigned)(G * n_lmt), 256, 0, s>>>(d_part, d_gfirst, d_gsplits, n_lmt, lm_pad, d_M);
+  k_mp_reduce<<<dim3((unsigned)(G * n_lmt), kReduceSplit), 256, 0, s>>>(d_part, d_gfirst, d_gsplits, n_lmt, lm_pad,
+                                                                         d_M);
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
@@ -916,8 +933,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
                                                           nq, d_gpart);
     }
     CRAB_CUDA_CHECK(cudaGetLastError());
-    k_mp_gram_reduce<<<(unsigned)(((int64_t)P * nq + 255) / 256), 256, 0, s>>>(d_gpart, (int)rows.size(), P, nq,
-                                                                                d_out);
+    k_mp_gram_reduce<<<(unsigned)(((int64_t)P * nq + 31) / 32), dim3(32, 8), 0, s>>>(d_gpart, (int)rows.size(), P,
+                                                                                       nq, d_out);
     ctx->launches += 1;
   }
   CRAB_CUDA_CHECK(cudaGetLastError());
