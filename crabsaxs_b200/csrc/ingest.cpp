@@ -127,6 +127,40 @@ int64_t integer(const std::string& s, const char* what, int64_t line_no) {
   return (int64_t)v;
 }
 
+// Columns from..to of a line as a fixed-point decimal, without building a
+// string (the same exact fast path as number()); anything else goes through
+// number() and its strtod fallback.
+double column_number(const char* line, size_t n, size_t from, size_t to, const char* what, int64_t line_no) {
+  static const double kPow10[] = {1e0, 1e1, 1e2, 1e3, 1e4, 1e5, 1e6, 1e7, 1e8, 1e9, 1e10, 1e11, 1e12, 1e13, 1e14, 1e15};
+  size_t a = from - 1, b = n < to ? n : to;
+  if (n < from) b = a;
+  while (a < b && line[a] == ' ') ++a;
+  while (b > a && line[b - 1] == ' ') --b;
+  size_t i = a;
+  bool neg = false;
+  if (i < b && (line[i] == '-' || line[i] == '+')) neg = line[i++] == '-';
+  uint64_t m = 0;
+  int digits = 0, frac = -1;
+  bool ok = i < b;
+  for (; i < b && ok; ++i) {
+    const char c = line[i];
+    if (c >= '0' && c <= '9') {
+      m = m * 10 + (uint64_t)(c - '0');
+      ++digits;
+      if (frac >= 0) ++frac;
+    } else if (c == '.' && frac < 0) {
+      frac = 0;
+    } else {
+      ok = false;
+    }
+  }
+  if (ok && digits > 0 && digits <= 15) {
+    const double v = (double)m / kPow10[frac > 0 ? frac : 0];
+    return neg ? -v : v;
+  }
+  return number(field(line, n, from, to), what, line_no);
+}
+
 // PDB fixed columns (wwPDB format 3.3): ATOM/HETATM 1-6, name 13-16, altLoc 17,
 // resName 18-20, chainID 22, resSeq 23-26, iCode 27, x 31-38, y 39-46,
 // z 47-54, occupancy 55-60, element 77-78.  Models are MODEL ... ENDMDL.
@@ -146,14 +180,19 @@ std::vector<std::vector<Record>> read_pdb(const char* text, int64_t len) {
       const size_t k = std::strlen(tag);
       return n >= k && std::memcmp(line, tag, k) == 0;
     };
-    if (starts("MODEL")) {
+    // a new model reserves for the rest of the text at about 81 bytes a record
+    auto new_model = [&]() {
       models.emplace_back();
+      models.back().reserve((size_t)(end - p) / 81 + 16);
+    };
+    if (starts("MODEL")) {
+      new_model();
       continue;
     }
     const bool het = starts("HETATM");
     const bool atom = !het && starts("ATOM") && (n == 4 || line[4] == ' ');
     if (!atom && !het) continue;
-    if (models.empty()) models.emplace_back();  // records outside MODEL/ENDMDL join the current model
+    if (models.empty()) new_model();  // records outside MODEL/ENDMDL join the current model
     Record r;
     r.hetatm = het;
     r.name = field(line, n, 13, 16);
@@ -162,11 +201,12 @@ std::vector<std::vector<Record>> read_pdb(const char* text, int64_t len) {
     r.chain = field(line, n, 22, 22);
     r.resseq = integer(field(line, n, 23, 26), "residue number", line_no);
     r.icode = field(line, n, 27, 27);
-    r.x = number(field(line, n, 31, 38), "x coordinate", line_no);
-    r.y = number(field(line, n, 39, 46), "y coordinate", line_no);
-    r.z = number(field(line, n, 47, 54), "z coordinate", line_no);
-    const std::string o = field(line, n, 55, 60);
-    r.occ = o.empty() ? 1.0 : number(o, "occupancy", line_no);
+    r.x = column_number(line, n, 31, 38, "x coordinate", line_no);
+    r.y = column_number(line, n, 39, 46, "y coordinate", line_no);
+    r.z = column_number(line, n, 47, 54, "z coordinate", line_no);
+    bool blank_occ = true;
+    for (size_t k = 54; k < 60 && k < n; ++k) blank_occ = blank_occ && line[k] == ' ';
+    r.occ = blank_occ ? 1.0 : column_number(line, n, 55, 60, "occupancy", line_no);
     r.element = field(line, n, 77, 78);
     if (r.name.empty()) fail(CRAB_EPARSE, "line " + std::to_string(line_no) + ": missing atom name");
     models.back().push_back(std::move(r));
