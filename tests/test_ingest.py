@@ -276,3 +276,48 @@ def test_parsed_structure_scatters_like_its_arrays(engine):
     finally:
         N.lib.crab_parsed_destroy(parsed)
     assert np.array_equal(out, ref)
+
+
+SMALL_PDB = """HEADER    crabSAXS two atom scattering fixture
+ATOM      1  C1  TST A   1       0.000   0.000   0.000  1.00 10.00           C
+ATOM      2  C2  TST A   1       2.000   0.000   0.000  1.00 10.00           C
+END
+"""  # examples/data/small.pdb
+
+
+@pytest.mark.gpu
+def test_compute_curve_for_example_structure_is_well_formed(engine):  # tests/end_to_end.rs:3-10
+    """The two-atom fixture read by the PDB reader, then the vacuum Debye
+    curve on 100 q: finite, non-negative, and the oracle's within 1e-5."""
+    import oracle as O
+
+    s = cs.Structure.from_text(SMALL_PDB)
+    q = np.arange(100) * 0.005
+    got = cs.debye_intensity(s, q, engine=engine)
+    assert len(got) == len(q) and np.all(np.isfinite(got)) and np.all(got >= 0.0)
+    ref = O.debye_intensity(O.Atoms(s.xyz, s.element, s.group, s.occupancy), q)
+    assert np.max(np.abs(got - ref) / ref) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_calc_of_the_example_structure_with_adaptive_hydration(engine):  # tests/end_to_end.rs:12-49
+    """What `calc small.pdb --qmin 0.01 --qmax 0.05 --qstep 0.01 --method auto
+    --hydration adaptive-grid --c1 1.0 --c2 0.02` computes (4 Å grid, the
+    CLI's spacing): a grid hydration model sends Auto to the multipole
+    (scattering.rs:145-151) with l_max = clamp(ceil(q_max R) + 8, 8, 64)
+    (scattering.rs:168-175); five finite values, the oracle's within 1e-5."""
+    import math
+
+    import oracle as O
+
+    s = cs.Structure.from_text(SMALL_PDB)
+    q = np.array([0.01, 0.02, 0.03, 0.04, 0.05])
+    sp = cs.SolventParams(c1=1.0, c2=0.02, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                          hydration_grid_spacing_angstrom=4.0)
+    got = cs.compute_curve(s, q, cs.ComputeOptions(solvent=sp), engine=engine)
+    assert got.method == "Multipole" and len(got.intensity) == 5 and np.all(np.isfinite(got.intensity))
+    r = float(np.max(np.linalg.norm(s.xyz - s.xyz.mean(axis=0), axis=1)))
+    l_max = min(max(math.ceil(q.max() * r) + 8, 8), 64)
+    a = O.Atoms(s.xyz, s.element, s.group, s.occupancy)
+    ref = O.multipole_solvent_intensity(a, q, l_max, c1=1.0, c2=0.02, model=2, spacing=4.0)
+    assert np.max(np.abs(got.intensity - ref) / np.abs(ref)) <= 1e-5
