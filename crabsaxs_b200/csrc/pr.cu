@@ -237,6 +237,10 @@ __global__ void __launch_bounds__(kPrThreads, 8)
   acc.c = Hc + (size_t)(warp % copies) * bins;
   acc.w = kMode == kPrWeightedGlobal ? Hw : Hw + (size_t)(warp % copies) * bins;
   const int top = kPrMagicBits + bins - 1;  // floor(x) capped at bins - 1, in magic bits
+  // shared address of this warp's counter 0 less 4 * kPrMagicBits (32-bit
+  // wrap-around), so that adding 4 * (kPrMagicBits + k) gives counter k
+  const unsigned cbase =
+      kMode == kPrCounts ? (unsigned)__cvta_generic_to_shared(acc.c) - ((unsigned)kPrMagicBits << 2) : 0u;
 
   const int64_t n_work = (int64_t)n_tiles * (n_tiles + 1) / 2;
   int64_t w = (int64_t)blockIdx.x * chunk;
@@ -299,8 +303,15 @@ __global__ void __launch_bounds__(kPrThreads, 8)
             const float frac = x - (t - kPrMagic);
             const bool edge = fabsf(frac - 0.5f) > near_edge;
             marked |= (edge ? 1u : 0u) << jj;
-            const int e = min(__float_as_int(t), top) - kPrMagicBits;
-            if (!edge) acc.add(e, kMode == kPrCounts ? 0.0 : wi * sj[jc + jj].w);
+            if constexpr (kMode == kPrCounts) {
+              // t's bits are kPrMagicBits + floor(x): the counter's shared address
+              // comes from one shift and add on the offset base
+              const unsigned addr = cbase + ((unsigned)min(__float_as_int(t), top) << 2);
+              if (!edge) asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr) : "memory");
+            } else {
+              const int e = min(__float_as_int(t), top) - kPrMagicBits;
+              if (!edge) acc.add(e, wi * sj[jc + jj].w);
+            }
           }
           while (marked) {
             const int j = jc + __ffs(marked) - 1;
