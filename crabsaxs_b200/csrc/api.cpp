@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -401,8 +402,10 @@ int crab_structure_create(crab_ctx* ctx, const double* xyz, const double* occupa
       require(element[i] >= 0 && element[i] <= CRAB_EL_OTHER, "unknown element code");
       require(group[i] >= -1 && group[i] <= 13, "unknown united-atom group code");
     }
+    static std::atomic<uint64_t> next_serial{1};
     crab_struct* st = new crab_struct();
     st->ctx = ctx;
+    st->serial = next_serial.fetch_add(1);
     st->n = n;
     st->xyz.assign(xyz, xyz + 3 * n);
     st->occ.assign(occupancy, occupancy + n);
@@ -630,31 +633,54 @@ int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t 
   });
 }
 
-static int grid_entry(crab_ctx* ctx, crab_struct* st, double* sites, int64_t capacity, int64_t* m, double* volume,
-                      const std::function<GridResult()>& build) {
+// Two-call protocol: a size query (sites == NULL) builds the grid, leaves
+// the sites on the device and keeps the result in the context; the fill call
+// with the same structure and options copies those sites straight into the
+// caller's buffer instead of building the grid again.  Structures are
+// immutable, so the serial and the options identify the result; the device
+// sites stay valid until the context builds another grid.
+static int grid_entry(crab_ctx* ctx, crab_struct* st, int kind, double o0, double o1, double o2, double* sites,
+                      int64_t capacity, int64_t* m, double* volume, const std::function<GridResult()>& build) {
   if (!ctx || !st || !m) return CRAB_EINVAL;
   GUARD(ctx, {
-    GridResult g = build();
-    const int64_t count = (int64_t)g.sites.size() / 3;
+    const double option[3] = {o0, o1, o2};
+    GridMemo* memo = ctx->grid_memo.get();
+    const bool hit = memo && memo->serial == st->serial && memo->kind == kind &&
+                     std::memcmp(memo->option, option, sizeof(option)) == 0 &&
+                     (memo->result.m == 0 || memo->result.build == ctx->grid_builds);
+    if (!hit) {
+      ctx->grid_memo.reset();
+      auto fresh = std::make_shared<GridMemo>();
+      fresh->result = build();
+      fresh->serial = st->serial;
+      fresh->kind = kind;
+      std::memcpy(fresh->option, option, sizeof(option));
+      ctx->grid_memo = fresh;
+    }
+    const GridResult& g = ctx->grid_memo->result;
+    const int64_t count = g.m;
     *m = count;
     if (volume) *volume = g.voxel_volume;
     if (sites) {
       if (capacity < count) throw Error(CRAB_ECAPACITY, "site buffer too small");
-      std::copy(g.sites.begin(), g.sites.end(), sites);
+      copy_d2h(ctx, sites, g.d_sites, (size_t)count * 3 * sizeof(double), ctx->stream);
+      CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+      ctx->grid_memo.reset();
+      trim_grid_pool(ctx);
     }
   });
 }
 
 int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing, double clearance, double padding,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume) {
-  return grid_entry(ctx, st, sites, capacity, m, voxel_volume,
-                    [&]() { return adaptive_grid_device(ctx, st->xyz.data(), st->n, spacing, clearance, padding); });
+  return grid_entry(ctx, st, 0, spacing, clearance, padding, sites, capacity, m, voxel_volume,
+                    [&]() { return adaptive_grid_device(ctx, st->xyz.data(), st->n, spacing, clearance, padding, false); });
 }
 
 int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing, double probe, double thickness,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume) {
-  return grid_entry(ctx, st, sites, capacity, m, voxel_volume, [&]() {
-    return exterior_grid_device(ctx, st->xyz.data(), st->elem.data(), st->n, spacing, probe, thickness);
+  return grid_entry(ctx, st, 1, spacing, probe, thickness, sites, capacity, m, voxel_volume, [&]() {
+    return exterior_grid_device(ctx, st->xyz.data(), st->elem.data(), st->n, spacing, probe, thickness, false);
   });
 }
 

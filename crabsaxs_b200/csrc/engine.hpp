@@ -72,6 +72,10 @@ struct HostBuf {
 
 }  // namespace crab
 
+namespace crab {
+struct GridMemo;
+}
+
 struct crab_ctx {
   int device = 0;
   int sm_count = 148;
@@ -93,6 +97,11 @@ struct crab_ctx {
   // histogram kernel alone, and the pairs it binned
   double last_pr_ms = 0.0, last_pr_hist_ms = 0.0, last_pr_pairs = 0.0;
   int last_pr_mode = -1;  // 0 class counts, 1 per-warp f64 shared, 2 f64 rows in device memory
+
+  // Site list of the last hydration-grid size query (sites == NULL), kept
+  // for the fill call that follows it with the same structure and options.
+  std::shared_ptr<crab::GridMemo> grid_memo;
+  uint64_t grid_builds = 0;  // hydration-grid builds on this context (each reuses the "grid." device slots)
 
   void* dev(const std::string& name, size_t bytes);
   void* host(const std::string& name, size_t bytes);
@@ -264,20 +273,38 @@ inline int pair_index(int a, int b, int T) {
 
 // ---------------------------------------------------------------- hydration grids
 struct GridResult {
-  std::vector<double> sites;   // 3 per site, z→y→x order
-  std::vector<int32_t> cells;  // 3 voxel indices per site
+  std::vector<double> sites;   // 3 per site, z→y→x order (built with to_host)
+  std::vector<int32_t> cells;  // 3 voxel indices per site (built with to_host)
   double spacing = 0.0;
   double voxel_volume = 0.0;
+  int64_t m = 0;                   // number of sites
+  const double* d_sites = nullptr;  // the sites on the device, valid until the context's next grid build
+  uint64_t build = 0;               // crab_ctx::grid_builds of the build that made this result
 };
+// Key of a grid build: structure serial, grid kind (0 adaptive, 1 exterior)
+// and the three options bit for bit.  The result's device sites are valid
+// while result.build equals the context's grid_builds.
+struct GridMemo {
+  uint64_t serial = 0;
+  int kind = -1;
+  double option[3] = {0.0, 0.0, 0.0};
+  GridResult result;
+};
+// With to_host false only m and d_sites are filled: the host vectors stay
+// empty (the caller copies the sites itself before the next grid build).
 GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, double spacing, double clearance,
-                                double padding);
+                                double padding, bool to_host = true);
 GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* elem, int64_t n, double spacing,
-                                double probe, double thickness);
+                                double probe, double thickness, bool to_host = true);
+// Releases "grid." device slots above the keep size (after a caller copied
+// out the sites of a build made without to_host).
+void trim_grid_pool(crab_ctx* ctx);
 
 }  // namespace crab
 
 struct crab_struct {
   crab_ctx* ctx = nullptr;
+  uint64_t serial = 0;  // unique per structure in the process; the arrays never change after creation
   int64_t n = 0;
   std::vector<double> xyz;
   std::vector<double> occ;

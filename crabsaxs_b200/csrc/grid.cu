@@ -180,8 +180,20 @@ __global__ void k_seed_boundary(uint8_t* __restrict__ s, Box b) {
   }
 }
 
-// axis 0: lines along x (one per (y,z)); 1: along y; 2: along z.
-__global__ void k_sweep(uint8_t* __restrict__ s, Box b, int axis, int* __restrict__ changed) {
+// Voxels of a line a thread loads before it carries the label through them:
+// one memory latency per batch instead of one per voxel.
+constexpr int kSweepBatch = 16;
+// Sweep rounds enqueued between two reads of the change flag by the host.
+constexpr int kRoundsPerSync = 6;
+
+// One thread per line; axis 0: lines along x (one per (y,z)); 1: along y;
+// 2: along z.  A forward and a backward pass each carry the exterior label
+// through runs of unknown voxels.  Lines of one axis are disjoint, so threads
+// never touch the same voxel.  The round returns at once when the previous
+// round changed nothing (*prev_changed == 0): the fixed point is reached.
+__global__ void k_sweep(uint8_t* __restrict__ s, Box b, int axis, const int* __restrict__ prev_changed,
+                        int* __restrict__ changed) {
+  if (prev_changed && *prev_changed == 0) return;
   const uint64_t nx = b.n[0], ny = b.n[1], nz = b.n[2];
   uint64_t lines, len, stride;
   if (axis == 0) { lines = ny * nz; len = nx; stride = 1; }
@@ -193,44 +205,82 @@ __global__ void k_sweep(uint8_t* __restrict__ s, Box b, int axis, int* __restric
   if (axis == 0) start = l * nx;                       // l = z*ny + y
   else if (axis == 1) start = (l / nx) * nx * ny + (l % nx);  // l = z*nx + x
   else start = l;                                       // l = y*nx + x
+  uint8_t* line = s + start;
   int any = 0;
   bool carry = false;
-  for (uint64_t i = 0; i < len; ++i) {
-    uint8_t& v = s[start + i * stride];
-    if (v == 2) carry = true;
-    else if (v == 0) { if (carry) { v = 2; any = 1; } }
-    else carry = false;
+  // voxels past either end read as molecular (1): never written, stop the carry
+  for (uint64_t i0 = 0; i0 < len; i0 += kSweepBatch) {
+    uint8_t v[kSweepBatch];
+#pragma unroll
+    for (int k = 0; k < kSweepBatch; ++k) v[k] = i0 + k < len ? line[(i0 + k) * stride] : (uint8_t)1;
+#pragma unroll
+    for (int k = 0; k < kSweepBatch; ++k) {
+      if (v[k] == 2) carry = true;
+      else if (v[k] == 0) {
+        if (carry) {
+          line[(i0 + k) * stride] = 2;
+          any = 1;
+        }
+      } else carry = false;
+    }
   }
   carry = false;
-  for (uint64_t i = len; i-- > 0;) {
-    uint8_t& v = s[start + i * stride];
-    if (v == 2) carry = true;
-    else if (v == 0) { if (carry) { v = 2; any = 1; } }
-    else carry = false;
+  for (uint64_t e = len; e > 0;) {
+    const uint64_t i0 = e - 1;  // this batch covers i0, i0 - 1, ..., down to index 0 at most
+    uint8_t v[kSweepBatch];
+#pragma unroll
+    for (int k = 0; k < kSweepBatch; ++k) v[k] = (uint64_t)k <= i0 ? line[(i0 - k) * stride] : (uint8_t)1;
+#pragma unroll
+    for (int k = 0; k < kSweepBatch; ++k) {
+      if (v[k] == 2) carry = true;
+      else if (v[k] == 0) {
+        if (carry) {
+          line[(i0 - k) * stride] = 2;
+          any = 1;
+        }
+      } else carry = false;
+    }
+    e = e > (uint64_t)kSweepBatch ? e - kSweepBatch : 0;
   }
   if (any) atomicOr(changed, 1);
 }
 
-struct Scratch {
-  std::vector<void*> owned;
-  ~Scratch() {
-    for (void* p : owned) cudaFree(p);
+// Grid buffers live in the context's pool ("grid." slots), so repeated calls
+// allocate nothing.  A slot above kGridKeepBytes (a box of more than 2^28
+// voxels) is released when the build ends, so a one-off large box does not
+// keep its memory; a build that leaves its sites on the device keeps the
+// sites slot, which trim_grid_pool releases once they are copied out.
+constexpr size_t kGridKeepBytes = 256ull << 20;
+
+template <class T>
+T* pool(crab_ctx* ctx, const char* name, size_t count) {
+  return (T*)ctx->dev(name, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+void trim_slots(crab_ctx* ctx, bool keep_sites) {
+  for (auto it = ctx->bufs.begin(); it != ctx->bufs.end();) {
+    if (it->first.compare(0, 5, "grid.") == 0 && it->second.bytes > kGridKeepBytes &&
+        !(keep_sites && it->first == "grid.sites")) {
+      cudaFree(it->second.ptr);
+      it = ctx->bufs.erase(it);
+    } else {
+      ++it;
+    }
   }
-  template <class T>
-  T* alloc(size_t count) {
-    void* p = nullptr;
-    CRAB_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    owned.push_back(p);
-    return (T*)p;
-  }
+}
+
+struct GridPoolTrim {
+  crab_ctx* ctx;
+  bool keep_sites;
+  ~GridPoolTrim() { trim_slots(ctx, keep_sites); }
 };
 
-GridResult compact_sites(crab_ctx* ctx, Scratch& sc, const uint8_t* a, const uint8_t* b, uint64_t count, int kind,
-                         const Box& bx) {
+GridResult compact_sites(crab_ctx* ctx, const uint8_t* a, const uint8_t* b, uint64_t count, int kind,
+                         const Box& bx, bool to_host) {
   cudaStream_t s = ctx->stream;
   const uint64_t chunks = (count + kChunk - 1) / kChunk;
-  uint32_t* d_cnt = sc.alloc<uint32_t>(chunks);
-  uint64_t* d_off = sc.alloc<uint64_t>(chunks + 1);
+  uint32_t* d_cnt = pool<uint32_t>(ctx, "grid.chunk_count", chunks);
+  uint64_t* d_off = pool<uint64_t>(ctx, "grid.chunk_offset", chunks + 1);
   k_count<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, d_cnt);
   CRAB_CUDA_CHECK(cudaGetLastError());
   k_scan_chunks<<<1, 1024, 0, s>>>(d_cnt, chunks, d_off);
@@ -238,18 +288,24 @@ GridResult compact_sites(crab_ctx* ctx, Scratch& sc, const uint8_t* a, const uin
   uint64_t m = 0;
   copy_d2h(ctx, &m, d_off + chunks, sizeof(uint64_t), s);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+  trace_mark("sites counted");
   GridResult r;
-  r.sites.resize(3 * m);
-  r.cells.resize(3 * m);
   r.spacing = bx.spacing;
+  r.m = (int64_t)m;
+  r.build = ctx->grid_builds;
   if (m) {
     require(bx.n[0] < (1ull << 31) && bx.n[1] < (1ull << 31) && bx.n[2] < (1ull << 31), "grid axis too long");
-    double* d_sites = sc.alloc<double>(3 * m);
-    int32_t* d_cells = sc.alloc<int32_t>(3 * m);
+    double* d_sites = pool<double>(ctx, "grid.sites", 3 * m);
+    int32_t* d_cells = pool<int32_t>(ctx, "grid.cells", 3 * m);
     k_emit<<<(unsigned)chunks, kScanThreads, 0, s>>>(a, b, count, kind, bx, d_off, d_sites, d_cells);
     CRAB_CUDA_CHECK(cudaGetLastError());
-    copy_d2h(ctx, r.sites.data(), d_sites, 3 * m * sizeof(double), s);
-    copy_d2h(ctx, r.cells.data(), d_cells, 3 * m * sizeof(int32_t), s);
+    r.d_sites = d_sites;
+    if (to_host) {
+      r.sites.resize(3 * m);
+      r.cells.resize(3 * m);
+      copy_d2h(ctx, r.sites.data(), d_sites, 3 * m * sizeof(double), s);
+      copy_d2h(ctx, r.cells.data(), d_cells, 3 * m * sizeof(int32_t), s);
+    }
     CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   }
   ctx->launches += m ? 4 : 3;
@@ -284,7 +340,7 @@ bool make_box(const double* xyz, int64_t n, double pad, double spacing, Box* b, 
 }  // namespace
 
 GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, double spacing, double clearance,
-                                double padding) {
+                                double padding, bool to_host) {
   GridResult r;
   if (n == 0) {
     r.voxel_volume = adaptive_site_volume(spacing);
@@ -309,11 +365,13 @@ GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, dou
   uint64_t count = 0;
   require(make_box(xyz, n, padding, spacing, &b, &count), "adaptive hydration grid is too large");
   require(count <= (uint64_t)4000000000ull, "adaptive hydration grid exceeds 4e9 voxels");
-  Scratch sc;
+  TraceScope trace("adaptive_grid");
+  ++ctx->grid_builds;
+  GridPoolTrim trim{ctx, !to_host};
   cudaStream_t s = ctx->stream;
-  uint8_t* shell = sc.alloc<uint8_t>(count);
-  uint8_t* mol = sc.alloc<uint8_t>(count);
-  double* d_xyz = sc.alloc<double>(3 * n);
+  uint8_t* shell = pool<uint8_t>(ctx, "grid.mask_a", count);
+  uint8_t* mol = pool<uint8_t>(ctx, "grid.mask_b", count);
+  double* d_xyz = pool<double>(ctx, "grid.xyz", 3 * n);
   CRAB_CUDA_CHECK(cudaMemsetAsync(shell, 0, count, s));
   CRAB_CUDA_CHECK(cudaMemsetAsync(mol, 0, count, s));
   copy_h2d(ctx, d_xyz, xyz, 3 * n * sizeof(double), s);
@@ -323,13 +381,13 @@ GridResult adaptive_grid_device(crab_ctx* ctx, const double* xyz, int64_t n, dou
   k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, nullptr, inner, 0.0, n, b, mol, 1, 0);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 2;
-  r = compact_sites(ctx, sc, shell, mol, count, 0, b);
+  r = compact_sites(ctx, shell, mol, count, 0, b, to_host);
   r.voxel_volume = adaptive_site_volume(spacing);
   return r;
 }
 
 GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* elem, int64_t n, double spacing,
-                                double probe, double thickness) {
+                                double probe, double thickness, bool to_host) {
   GridResult r;
   if (n == 0) {
     r.voxel_volume = (spacing * spacing) * spacing;
@@ -350,12 +408,14 @@ GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* 
   require(make_box(xyz, n, margin, spacing, &b, &count), "solvent grid is too large");
   if (count > 250000000ull)
     throw Error(CRAB_EINVAL, "solvent grid requires " + std::to_string(count) + " voxels; limit is 250000000");
-  Scratch sc;
+  TraceScope trace("exterior_grid");
+  ++ctx->grid_builds;
+  GridPoolTrim trim{ctx, !to_host};
   cudaStream_t s = ctx->stream;
-  uint8_t* state = sc.alloc<uint8_t>(count);
-  double* d_xyz = sc.alloc<double>(3 * n);
-  double* d_rad = sc.alloc<double>(n);
-  int* d_changed = sc.alloc<int>(1);
+  uint8_t* state = pool<uint8_t>(ctx, "grid.mask_a", count);
+  double* d_xyz = pool<double>(ctx, "grid.xyz", 3 * n);
+  double* d_rad = pool<double>(ctx, "grid.radius", n);
+  int* d_changed = pool<int>(ctx, "grid.changed", kRoundsPerSync);
   CRAB_CUDA_CHECK(cudaMemsetAsync(state, 0, count, s));
   copy_h2d(ctx, d_xyz, xyz, 3 * n * sizeof(double), s);
   copy_h2d(ctx, d_rad, radius.data(), n * sizeof(double), s);
@@ -365,28 +425,37 @@ GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* 
   k_seed_boundary<<<std::max<unsigned>(1, (unsigned)std::min<uint64_t>((count + 255) / 256, 65535)), 256, 0, s>>>(state, b);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 2;
-  // sweep until the fixed point; every round is bounded and the total number
-  // of rounds cannot exceed the number of voxels
-  for (uint64_t round = 0; round <= count; ++round) {
-    CRAB_CUDA_CHECK(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
-    for (int axis = 0; axis < 3; ++axis) {
-      const uint64_t lines = axis == 0 ? b.n[1] * b.n[2] : axis == 1 ? b.n[0] * b.n[2] : b.n[0] * b.n[1];
-      k_sweep<<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(state, b, axis, d_changed);
-      CRAB_CUDA_CHECK(cudaGetLastError());
-      ctx->launches += 1;
+  // Sweep rounds until the fixed point, kRoundsPerSync rounds per read of the
+  // flag: round k writes d_changed[k] and returns at once when round k - 1
+  // changed nothing, so the last flag of a batch is 0 exactly when the fill
+  // has converged.  Every productive round labels at least one voxel, so the
+  // number of rounds cannot exceed the number of voxels.
+  for (uint64_t round = 0; round <= count; round += kRoundsPerSync) {
+    CRAB_CUDA_CHECK(cudaMemsetAsync(d_changed, 0, kRoundsPerSync * sizeof(int), s));
+    for (int k = 0; k < kRoundsPerSync; ++k) {
+      const int* prev = k ? d_changed + k - 1 : nullptr;
+      for (int axis = 0; axis < 3; ++axis) {
+        const uint64_t lines = axis == 0 ? b.n[1] * b.n[2] : axis == 1 ? b.n[0] * b.n[2] : b.n[0] * b.n[1];
+        k_sweep<<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(state, b, axis, prev, d_changed + k);
+        CRAB_CUDA_CHECK(cudaGetLastError());
+        ctx->launches += 1;
+      }
     }
     int changed = 0;
-    copy_d2h(ctx, &changed, d_changed, sizeof(int), s);
+    copy_d2h(ctx, &changed, d_changed + kRoundsPerSync - 1, sizeof(int), s);
     CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
     if (!changed) break;
   }
+  trace_mark("flood fill");
   k_rasterize<<<blocks, 256, 0, s>>>(d_xyz, d_rad, 0.0, probe + thickness, n, b, state, 3, 1);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 1;
-  r = compact_sites(ctx, sc, state, state, count, 1, b);
+  r = compact_sites(ctx, state, state, count, 1, b, to_host);
   r.voxel_volume = (spacing * spacing) * spacing;
   return r;
 }
+
+void trim_grid_pool(crab_ctx* ctx) { trim_slots(ctx, false); }
 
 }  // namespace crab
 

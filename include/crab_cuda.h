@@ -234,7 +234,11 @@ int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t 
 
 /* ---- hydration grids ---------------------------------------------------- */
 /* Adaptive coarse shell (solvent.rs:121-223), bit-exact site list in z→y→x
- * order. Two-call size query: pass sites=NULL to read *m. */
+ * order. Two-call size query: pass sites=NULL to read *m.  The query leaves
+ * its sites on the device; a fill call that follows with the same structure
+ * and options copies them out without building the grid again (any other
+ * call builds its own).  A fill with capacity < *m returns CRAB_ECAPACITY
+ * and keeps the query's sites for a retry. */
 int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing, double clearance, double padding,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
 /* Largest box (voxels) crab_hydration_grid_adaptive_noalloc accepts. */
@@ -259,7 +263,8 @@ int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing,
 int crab_hydration_grid_adaptive_noalloc(const double* d_xyz, int64_t n, double spacing, double clearance,
                                          double padding, double* d_sites, int64_t capacity, int64_t* m,
                                          double* voxel_volume, void* stream);
-/* Exterior flood-fill shell (solvent.rs:259-401), bit-exact. */
+/* Exterior flood-fill shell (solvent.rs:259-401), bit-exact; the same
+ * two-call protocol as crab_hydration_grid_adaptive. */
 int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing, double probe, double thickness,
                                  double* sites, int64_t capacity, int64_t* m, double* voxel_volume);
 
