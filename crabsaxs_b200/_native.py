@@ -109,6 +109,11 @@ _SIGS = {
     "crab_combine_solvent_basis": (C.c_int, [D, I64, D, C.c_double, C.c_double, D]),
     "crab_debye_partials": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, D, D]),
     "crab_debye_partials_fp64": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, D, D]),
+    "crab_debye_partials_shard": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, C.c_int, C.c_int, C.c_int,
+                                            D, D]),
+    "crab_debye_solvent_basis_shard": (C.c_int, [P, P, D, I64, C.POINTER(Solvent), C.c_int, C.c_int, C.c_int,
+                                                 C.c_int, D]),
+    "crab_shard_assign": (C.c_int, [C.POINTER(I64), I64, C.c_int32, I32P]),
     "crab_compute_curve": (C.c_int, [P, P, D, I64, C.POINTER(ComputeOpts), D, I32P]),
     "crab_hydration_grid_adaptive": (C.c_int, [P, P, C.c_double, C.c_double, C.c_double, D, I64,
                                                C.POINTER(I64), D]),

@@ -502,16 +502,25 @@ def debye_intensity(structure: Structure, q, implicit_hydrogen: bool = True, eng
 
 
 def debye_solvent_basis(structure: Structure, q, params: SolventParams, implicit_hydrogen: bool = True,
-                        engine: Optional[Engine] = None, fp64: bool = False) -> np.ndarray:
+                        engine: Optional[Engine] = None, fp64: bool = False,
+                        shard: Optional[tuple[int, int]] = None) -> np.ndarray:
     """solvent.rs:504-584: rows vv, ee, hh, ve, vh, eh.  fp64=True runs the pair
-    sums with the FP64 device reference kernel instead of the FP32 recurrence."""
+    sums with the FP64 device reference kernel instead of the FP32 recurrence.
+    shard=(k, n): only part k of n (see crab_debye_solvent_basis_shard); the
+    n parts sum to the whole basis."""
     eng = engine or Engine.default()
     qa = _f64(q)
     out = np.empty((6, len(qa)))
     s = params.to_c()
     prec = N.PREC_FP64 if fp64 else N.PREC_FP32
-    eng.check(N.lib.crab_debye_solvent_basis_ex(eng.handle, structure.handle(eng), _dp(qa), len(qa), C.byref(s),
-                                                1 if implicit_hydrogen else 0, prec, _dp(out)))
+    if shard is None:
+        eng.check(N.lib.crab_debye_solvent_basis_ex(eng.handle, structure.handle(eng), _dp(qa), len(qa), C.byref(s),
+                                                    1 if implicit_hydrogen else 0, prec, _dp(out)))
+    else:
+        k, n = shard
+        eng.check(N.lib.crab_debye_solvent_basis_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
+                                                       C.byref(s), 1 if implicit_hydrogen else 0, prec, int(k),
+                                                       int(n), _dp(out)))
     return out
 
 
@@ -595,8 +604,10 @@ def hydration_grid_exterior(structure: Structure, spacing=1.0, probe=1.4, thickn
     return sites, vol.value
 
 
-def debye_partials(xyz, w, types, n_types: int, q, fp64: bool = False, engine: Optional[Engine] = None):
-    """Per type-pair pair sums P[ab, k] and self sums D[a] (see crab_debye_partials)."""
+def debye_partials(xyz, w, types, n_types: int, q, fp64: bool = False, engine: Optional[Engine] = None,
+                   shard: Optional[tuple[int, int]] = None):
+    """Per type-pair pair sums P[ab, k] and self sums D[a] (see crab_debye_partials).
+    shard=(k, n): only part k of n (crab_debye_partials_shard)."""
     eng = engine or Engine.default()
     x = _f64(xyz).reshape(-1, 3)
     ww = _f64(w)
@@ -605,9 +616,15 @@ def debye_partials(xyz, w, types, n_types: int, q, fp64: bool = False, engine: O
     P = n_types * (n_types + 1) // 2
     out = np.empty((P, len(qa)))
     self_ = np.empty(n_types)
-    fn = N.lib.crab_debye_partials_fp64 if fp64 else N.lib.crab_debye_partials
-    eng.check(fn(eng.handle, _dp(x), _dp(ww), t.ctypes.data_as(N.I32P), x.shape[0], n_types, _dp(qa), len(qa),
-                 _dp(out), _dp(self_)))
+    if shard is None:
+        fn = N.lib.crab_debye_partials_fp64 if fp64 else N.lib.crab_debye_partials
+        eng.check(fn(eng.handle, _dp(x), _dp(ww), t.ctypes.data_as(N.I32P), x.shape[0], n_types, _dp(qa), len(qa),
+                     _dp(out), _dp(self_)))
+    else:
+        k, n = shard
+        eng.check(N.lib.crab_debye_partials_shard(eng.handle, _dp(x), _dp(ww), t.ctypes.data_as(N.I32P), x.shape[0],
+                                                  n_types, _dp(qa), len(qa), N.PREC_FP64 if fp64 else N.PREC_FP32,
+                                                  int(k), int(n), _dp(out), _dp(self_)))
     return out, self_
 
 

@@ -217,7 +217,7 @@ void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const cr
 }
 
 Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,
-                      const GridResult* lattice_sites) {
+                      const GridResult* lattice_sites, int shard, int n_shards) {
   Partials P;
   Layout L;
   {
@@ -230,7 +230,7 @@ Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64
     spec.m = (int64_t)lattice_sites->cells.size() / 3;
     spec.spacing = lattice_sites->spacing;
   }
-  compute_partials(ctx, std::move(L), q, nq, fp64, P, lattice_sites ? &spec : nullptr);
+  compute_partials(ctx, std::move(L), q, nq, fp64, P, lattice_sites ? &spec : nullptr, shard, n_shards);
   return P;
 }
 
@@ -241,7 +241,7 @@ GridResult hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solv
 }
 
 void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
-                 bool implicit, double* out6, bool fp64) {
+                 bool implicit, double* out6, bool fp64, int shard, int n_shards) {
   TraceScope trace("debye_basis");
   GridResult g;
   const bool grid = s.hydration_model != CRAB_HYD_ANALYTIC;
@@ -256,7 +256,7 @@ void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t 
     t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &g.sites : nullptr);
     amplitude_tables(t, q, nq, &s, implicit, g.voxel_volume, V, E, H);
   }
-  Partials P = partials_for(ctx, t, q, nq, fp64, grid ? &g : nullptr);
+  Partials P = partials_for(ctx, t, q, nq, fp64, grid ? &g : nullptr, shard, n_shards);
   quadratic_terms(P, V.data(), V.data(), out6);
   quadratic_terms(P, E.data(), E.data(), out6 + nq);
   quadratic_terms(P, H.data(), H.data(), out6 + 2 * nq);
@@ -452,6 +452,29 @@ int crab_debye_solvent_basis_ex(crab_ctx* ctx, crab_struct* st, const double* q,
   });
 }
 
+int crab_debye_solvent_basis_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq,
+                                   const crab_solvent* solvent, int implicit_hydrogen, int precision, int shard,
+                                   int n_shards, double* out6) {
+  if (!ctx || !st || !solvent || (nq > 0 && (!q || !out6))) return CRAB_EINVAL;
+  if (precision != CRAB_PREC_FP32 && precision != CRAB_PREC_FP64) return CRAB_EINVAL;
+  if (n_shards < 1 || shard < 0 || shard >= n_shards) return CRAB_EINVAL;
+  GUARD(ctx, {
+    validate_q(q, nq);
+    validate_solvent(*solvent);
+    debye_basis(ctx, st, q, nq, *solvent, implicit_hydrogen != 0, out6, precision == CRAB_PREC_FP64, shard,
+                n_shards);
+  });
+}
+
+int crab_shard_assign(const int64_t* cost, int64_t n, int32_t n_shards, int32_t* owner) {
+  if (n < 0 || n_shards < 1 || (n > 0 && (!cost || !owner))) return CRAB_EINVAL;
+  for (int64_t i = 0; i < n; ++i)
+    if (cost[i] < 0) return CRAB_EINVAL;
+  const std::vector<int32_t> o = shard_owners(cost, n, n_shards);
+  std::copy(o.begin(), o.end(), owner);
+  return CRAB_OK;
+}
+
 int crab_combine_solvent_basis(const double* q, int64_t nq, const double* basis6, double c1, double c2, double* out) {
   if (nq < 0 || (nq > 0 && (!q || !basis6 || !out))) return CRAB_EINVAL;
   combine_basis(q, nq, basis6, c1, c2, out);
@@ -459,15 +482,17 @@ int crab_combine_solvent_basis(const double* q, int64_t nq, const double* basis6
 }
 
 static int partials_entry(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
-                          int32_t T, const double* q, int64_t nq, double* out, double* self_out, bool fp64) {
+                          int32_t T, const double* q, int64_t nq, double* out, double* self_out, bool fp64,
+                          int shard = 0, int n_shards = 1) {
   if (!ctx || T <= 0 || n < 0 || nq < 0 || (n > 0 && (!xyz || !w || !type)) || (nq > 0 && (!q || !out)))
     return CRAB_EINVAL;
+  if (n_shards < 1 || shard < 0 || shard >= n_shards) return CRAB_EINVAL;
   GUARD(ctx, {
     validate_q(q, nq);
     for (int64_t i = 0; i < n; ++i) require(type[i] >= 0 && type[i] < T, "atom type out of range");
     Layout L = build_layout(xyz, w, type, n, T, fp64);
     Partials P;
-    compute_partials(ctx, std::move(L), q, nq, fp64, P);
+    compute_partials(ctx, std::move(L), q, nq, fp64, P, nullptr, shard, n_shards);
     std::copy(P.pair.begin(), P.pair.end(), out);
     if (self_out) std::copy(P.self.begin(), P.self.end(), self_out);
   });
@@ -481,6 +506,14 @@ int crab_debye_partials(crab_ctx* ctx, const double* xyz, const double* w, const
 int crab_debye_partials_fp64(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                              int32_t n_types, const double* q, int64_t nq, double* out, double* self_out) {
   return partials_entry(ctx, xyz, w, type, n, n_types, q, nq, out, self_out, true);
+}
+
+int crab_debye_partials_shard(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                              int32_t n_types, const double* q, int64_t nq, int precision, int shard, int n_shards,
+                              double* out, double* self_out) {
+  if (precision != CRAB_PREC_FP32 && precision != CRAB_PREC_FP64) return CRAB_EINVAL;
+  return partials_entry(ctx, xyz, w, type, n, n_types, q, nq, out, self_out, precision == CRAB_PREC_FP64, shard,
+                        n_shards);
 }
 
 struct crab_pair_plan {

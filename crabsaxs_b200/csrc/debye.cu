@@ -638,6 +638,36 @@ std::vector<int2> q_blocks(const std::vector<double>& q, int Qmax) {
   return out;
 }
 
+std::vector<int32_t> shard_owners(const int64_t* cost, int64_t n, int n_shards) {
+  require(n_shards >= 1, "shard count must be positive");
+  std::vector<int64_t> load((size_t)n_shards, 0);
+  std::vector<int32_t> owner((size_t)std::max<int64_t>(n, 0));
+  for (int64_t i = 0; i < n; ++i) {
+    int best = 0;
+    for (int s = 1; s < n_shards; ++s)
+      if (load[s] < load[best]) best = s;
+    owner[i] = best;
+    load[best] += cost[i];
+  }
+  return owner;
+}
+
+// Tile pairs of one work item (i tile, j tiles j0..j1): the diagonal tile
+// counts once.
+inline int64_t work_cost(const int4& w) { return 2 * (int64_t)(w.z - w.y) - (w.y == w.x ? 1 : 0); }
+
+// The items of `work` that shard `shard` owns, in their order.
+std::vector<int4> shard_work(const std::vector<int4>& work, int shard, int n_shards) {
+  if (n_shards <= 1) return work;
+  std::vector<int64_t> cost(work.size());
+  for (size_t i = 0; i < work.size(); ++i) cost[i] = work_cost(work[i]);
+  const std::vector<int32_t> owner = shard_owners(cost.data(), (int64_t)cost.size(), n_shards);
+  std::vector<int4> mine;
+  for (size_t i = 0; i < work.size(); ++i)
+    if (owner[i] == shard) mine.push_back(work[i]);
+  return mine;
+}
+
 // Work list of a batch: every segment (one structure's tiles) is tiled on its
 // own; items of all segments are ordered longest first and carry the output
 // offset of their segment.
@@ -710,7 +740,7 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   P.wide = hmax > 0.8 ? 2 : (hmax > 0.125 ? 1 : 0);
   std::vector<int4> work;
   if (P.segments.empty()) {
-    work = make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile);
+    work = shard_work(make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile), P.shard, P.n_shards);
   } else {
     std::vector<int64_t> out;
     make_work_segments(P, P.n_qblocks, 8, work, out);
@@ -723,9 +753,12 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
 }
 
 std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
-                                         const LatticeSpec* lattice, bool pooled) {
+                                         const LatticeSpec* lattice, bool pooled, int shard, int n_shards) {
+  require(n_shards >= 1 && shard >= 0 && shard < n_shards, "shard index out of range");
   std::unique_ptr<PairPlan> P(new PairPlan());
   P->pooled = pooled;
+  P->shard = shard;
+  P->n_shards = n_shards;
   P->L = std::move(L);
   P->fp64 = fp64;
   P->nq = nq;
@@ -750,7 +783,7 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
     configure_fp32(ctx, *P, v.x, v.y);
   } else {
     P->n_qblocks = (int)((nq + kQD - 1) / kQD);
-    const std::vector<int4> work = make_work(P->L, P->n_qblocks, 8, P->L.n_tiles);
+    const std::vector<int4> work = shard_work(make_work(P->L, P->n_qblocks, 8, P->L.n_tiles), shard, n_shards);
     P->n_work = (int)work.size();
     P->d_atoms64 = upload(ctx, *P, P->owned, "atoms64", (const double4*)P->L.atoms64.data(), (size_t)P->L.n_pad, s);
     P->d_work = upload(ctx, *P, P->owned, "work64", work.data(), work.size(), s);
@@ -760,7 +793,7 @@ std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double
   P->d_out = upload<double>(ctx, *P, P->owned, "out", nullptr, (size_t)P->n_pairs * nq, s);
   P->d_status = upload<int>(ctx, *P, P->owned, "status", nullptr, 2, s);
   P->d_next = P->d_status + 1;
-  if (lattice) lattice_plan_init(ctx, *P, lattice->cells, lattice->m, lattice->spacing);
+  if (lattice && shard == 0) lattice_plan_init(ctx, *P, lattice->cells, lattice->m, lattice->spacing);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   return P;
 }
@@ -883,7 +916,9 @@ void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
         for (int a = 0; a < T; ++a)
           for (int b = a; b < T; ++b)
             out[(size_t)pair_index(a, b, T) * nq + k] =
-                (a == b) ? 0.5 * (P.L.sum_w[a] * P.L.sum_w[a] - P.L.self_w2[a]) : P.L.sum_w[a] * P.L.sum_w[b];
+                P.shard != 0 ? 0.0
+                : (a == b)   ? 0.5 * (P.L.sum_w[a] * P.L.sum_w[a] - P.L.self_w2[a])
+                             : P.L.sum_w[a] * P.L.sum_w[b];
       }
     return;
   }
@@ -894,7 +929,7 @@ void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
       const double w0 = (a == b) ? 0.5 * (P.L.sum_w[a] * P.L.sum_w[a] - P.L.self_w2[a]) : P.L.sum_w[a] * P.L.sum_w[b];
       for (int64_t k = 0; k < nq; ++k) {
         double& v = out[(size_t)ab * nq + k];
-        v = (P.q[k] == 0.0) ? w0 : v / P.q[k];
+        v = (P.q[k] == 0.0) ? (P.shard == 0 ? w0 : 0.0) : v / P.q[k];
       }
     }
   if (P.lattice.active && nq > 0) {
@@ -906,16 +941,17 @@ void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed) {
 }
 
 void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, Partials& out,
-                      const LatticeSpec* lattice) {
+                      const LatticeSpec* lattice, int shard, int n_shards) {
   const bool fp64 = force_fp64;
   if (fp64 && L.atoms64.empty()) throw Error(CRAB_EINVAL, "layout lacks an f64 copy");
   out.T = L.T;
   out.nq = nq;
   out.self = L.self_w2;
+  if (shard != 0) std::fill(out.self.begin(), out.self.end(), 0.0);
   std::unique_ptr<PairPlan> P;
   {
     TraceScope tp("make_pair_plan");
-    P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice, true);  // lives inside this call
+    P = make_pair_plan(ctx, std::move(L), q, nq, fp64, lattice, true, shard, n_shards);  // lives inside this call
   }
   out.pair.assign((size_t)P->n_pairs * nq, 0.0);
   {

@@ -215,6 +215,10 @@ struct PairPlan {
   int* d_next = nullptr;  // work-queue counter (the int after d_status)
   int64_t* d_work_out = nullptr;  // per work item output offset (batches of structures), or null
   int lattice_first_tile = 0;
+  // multi-GPU: this plan sums only the work items of shard `shard` of
+  // `n_shards` (shard_owners); shard 0 alone adds the exact q = 0 sums and
+  // the lattice block, so the shards' outputs add up to the whole
+  int shard = 0, n_shards = 1;
   std::vector<int> segments;  // batch: tile start of every structure plus the end, else empty
   LatticePart lattice;
   ~PairPlan();
@@ -242,14 +246,22 @@ void lattice_plan_init(crab_ctx* ctx, PairPlan& P, const int32_t* cells, int64_t
 void lattice_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s);
 bool q_grid_uniform(const double* q, int64_t nq);
 std::unique_ptr<PairPlan> make_pair_plan(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool fp64,
-                                         const LatticeSpec* lattice = nullptr, bool pooled = false);
+                                         const LatticeSpec* lattice = nullptr, bool pooled = false, int shard = 0,
+                                         int n_shards = 1);
+// Owner shard of every work item for n_shards GPUs: items are taken in the
+// given order (work lists are sorted longest first) and each goes to the
+// shard with the least cost so far, the lowest index among equals, so every
+// rank computes the same owners without communicating.
+std::vector<int32_t> shard_owners(const int64_t* cost, int64_t n, int n_shards);
 // Enqueue the pair kernel on stream s (device time recorded when timed).
 void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed);
 // Copy back and convert raw sums to P_ab(q) (divide by q; exact q = 0).
 void pair_plan_fetch(crab_ctx* ctx, PairPlan& P, double* out, bool timed);
 // One-shot: FP32 recurrence on a uniform grid, FP64 direct otherwise.
+// With n_shards > 1 only shard `shard`'s part (self sums zero except on
+// shard 0): the element-wise sum over all shards is the whole.
 void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bool force_fp64, struct Partials& out,
-                      const LatticeSpec* lattice = nullptr);
+                      const LatticeSpec* lattice = nullptr, int shard = 0, int n_shards = 1);
 
 std::unique_ptr<PairPlan> make_batch_pair_plan(crab_ctx* ctx, std::vector<Layout>&& parts, const double* q,
                                                int64_t nq);

@@ -33,10 +33,12 @@ TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const 
 void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const crab_solvent* solvent, bool implicit,
                       double site_volume, std::vector<double>& V, std::vector<double>& E, std::vector<double>& H);
 Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,
-                      const GridResult* lattice_sites);
+                      const GridResult* lattice_sites, int shard = 0, int n_shards = 1);
 GridResult hydration_sites(crab_ctx* ctx, const crab_struct* st, const crab_solvent& s);
+// With n_shards > 1 only shard `shard`'s part of the six rows (self terms on
+// shard 0 only): the element-wise sum over all shards is the whole basis.
 void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
-                 bool implicit, double* out6, bool fp64);
+                 bool implicit, double* out6, bool fp64, int shard = 0, int n_shards = 1);
 void debye_vacuum(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, bool implicit, double* out,
                   bool fp64);
 void combine_basis(const double* q, int64_t nq, const double* b, double c1, double c2, double* out);

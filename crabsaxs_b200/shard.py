@@ -1,0 +1,78 @@
+"""One structure's Debye sums split over several GPUs.
+
+One process per GPU, each with its own :class:`~crabsaxs_b200.api.Engine`
+and a ``torch.distributed`` process group (NCCL between GPUs, gloo on the
+host).  Every rank builds the same tile layout and work list and keeps the
+work items :func:`shard_assign` gives it, so the split needs no exchange;
+the only collective is one all-reduce (sum) of the result: the six basis
+rows (6 x nq f64, 24 kB at 500 q) or the type-pair partials (T(T+1)/2 x nq
+f64, 60 kB for 5 types at 500 q).  The reference runs on one host and has no
+counterpart; its q loop is split over threads (solvent.rs:528).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from .api import Engine, InvalidInput, SolventParams, Structure, debye_partials, debye_solvent_basis
+
+
+def shard_assign(cost, n_shards: int) -> np.ndarray:
+    """Owner shard of every work item (crab_shard_assign): items in order,
+    each to the shard with the least total cost so far (lowest index among
+    equals).  Host-only."""
+    c = np.ascontiguousarray(np.asarray(cost, dtype=np.int64))
+    owner = np.empty(len(c), dtype=np.int32)
+    rc = N.lib.crab_shard_assign(c.ctypes.data_as(C.POINTER(C.c_int64)), len(c), int(n_shards),
+                                 owner.ctypes.data_as(N.I32P))
+    if rc != N.OK:
+        raise InvalidInput(f"shard_assign: {N.STATUS_NAMES.get(rc, rc)}")
+    return owner
+
+
+def _rank_world(group) -> tuple[int, int]:
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return 0, 1
+    return dist.get_rank(group), dist.get_world_size(group)
+
+
+def reduce_shards(part: np.ndarray, group=None) -> np.ndarray:
+    """Element-wise f64 sum of every rank's ``part`` (same shape on every
+    rank), returned on every rank.  On an NCCL group the sum runs on this
+    rank's current CUDA device; on gloo on the host."""
+    import torch
+    import torch.distributed as dist
+
+    a = np.ascontiguousarray(part, dtype=np.float64)
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return a.copy()
+    t = torch.from_numpy(a.copy())
+    if dist.get_backend(group) == "nccl":
+        t = t.to(torch.device("cuda", torch.cuda.current_device()))
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()
+
+
+def sharded_debye_solvent_basis(structure: Structure, q, params: SolventParams, implicit_hydrogen: bool = True,
+                                group=None, engine: Optional[Engine] = None, fp64: bool = False) -> np.ndarray:
+    """debye_solvent_basis over the ranks of ``group``: this rank's part on
+    its engine's GPU, then the all-reduce.  Every rank returns the whole
+    basis."""
+    rank, world = _rank_world(group)
+    part = debye_solvent_basis(structure, q, params, implicit_hydrogen, engine, fp64, shard=(rank, world))
+    return reduce_shards(part, group)
+
+
+def sharded_debye_partials(xyz, w, types, n_types: int, q, group=None, engine: Optional[Engine] = None,
+                           fp64: bool = False):
+    """debye_partials over the ranks of ``group``: (pair partials, self sums),
+    both whole on every rank."""
+    rank, world = _rank_world(group)
+    pair, self_ = debye_partials(xyz, w, types, n_types, q, fp64, engine, shard=(rank, world))
+    both = reduce_shards(np.concatenate([pair.ravel(), self_]), group)
+    return both[: pair.size].reshape(pair.shape), both[pair.size:]

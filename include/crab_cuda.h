@@ -162,6 +162,25 @@ int crab_debye_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, in
  * (direct f64 sinc on the device: the FP64 reference for error reports). */
 int crab_debye_solvent_basis_ex(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq,
                                 const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6);
+/* Multi-GPU (one process and one context per GPU): shard `shard` of
+ * `n_shards` of crab_debye_solvent_basis_ex.  Each shard sums its share of
+ * the pair work list (the owners of crab_shard_assign over the plan's work
+ * items, the same on every rank, so no exchange is needed to split the
+ * work); the self terms, the exact q = 0 sums and the hydration-site
+ * lattice block are added on shard 0 only.  The element-wise sum of out6
+ * over all shards is crab_debye_solvent_basis_ex's result up to the order of
+ * the f64 additions: the caller all-reduces (sums) out6 across the GPUs,
+ * 6 × nq doubles.  No counterpart in the reference, which runs on one host
+ * (its q loop is split over threads, solvent.rs:528).
+ * n_shards < 1 or shard outside [0, n_shards): CRAB_EINVAL. */
+int crab_debye_solvent_basis_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq,
+                                   const crab_solvent* solvent, int implicit_hydrogen, int precision, int shard,
+                                   int n_shards, double* out6);
+/* Owner shard of each of n work items with the given costs: items in order
+ * (longest first), each to the shard with the least total cost so far, the
+ * lowest index among equals.  Host-only; the sharded entry points apply it
+ * to their work lists (cost = tile pairs of the item). */
+int crab_shard_assign(const int64_t* cost, int64_t n, int32_t n_shards, int32_t* owner);
 /* Recombination I = vv + G²ee + c2²hh − 2G·ve + 2c2·vh − 2G·c2·eh, clamp ≥0
  * (spherical.rs:567-584; G from solvent.rs:448-452). Host-only, f64. */
 int crab_combine_solvent_basis(const double* q, int64_t nq, const double* basis6, double c1, double c2, double* out);
@@ -176,6 +195,13 @@ int crab_debye_partials(crab_ctx* ctx, const double* xyz, const double* w, const
  * recurrence): the on-device FP64 reference used to report errors. */
 int crab_debye_partials_fp64(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                              int32_t n_types, const double* q, int64_t nq, double* out, double* self_out);
+/* Shard `shard` of `n_shards` of crab_debye_partials (CRAB_PREC_FP32) or
+ * crab_debye_partials_fp64 (CRAB_PREC_FP64), split as in
+ * crab_debye_solvent_basis_shard: out and self_out summed over all shards are
+ * the whole (self_out is zero on every shard but 0). */
+int crab_debye_partials_shard(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
+                              int32_t n_types, const double* q, int64_t nq, int precision, int shard, int n_shards,
+                              double* out, double* self_out);
 
 /* Device-resident pair-sum plan: the layout (typed, tiled atoms), work list
  * and q-block parameters are uploaded once; each run launches only the pair

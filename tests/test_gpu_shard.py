@@ -1,0 +1,77 @@
+"""The Debye sums of one structure split into shards (one per GPU in a
+multi-GPU run) add up to the unsplit sums.  Here every shard runs on the one
+GPU in turn, as independent launches.  Every work item is computed exactly
+as in the unsplit run; only the order of the f64 additions across items
+differs, hence 1e-12 of the largest entry."""
+import numpy as np
+import pytest
+
+import crabsaxs_b200 as cs
+from crabsaxs_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def _close(a, b):
+    return np.max(np.abs(a - b)) <= RTOL * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("model", [cs.HydrationModel.Analytic, cs.HydrationModel.AdaptiveGrid])
+@pytest.mark.parametrize("fp64", [False, True])
+def test_basis_shards_sum_to_the_basis(engine, model, fp64):
+    s = synth.protein(31, 2500 if fp64 else 6000, 16.0 if fp64 else 22.0)
+    q = np.linspace(0.0, 0.5, 101)  # q = 0 included: its exact sums come from shard 0 only
+    sp = cs.SolventParams(c1=1.02, c2=0.7, hydration_model=model, hydration_grid_spacing_angstrom=3.0)
+    whole = cs.debye_solvent_basis(s, q, sp, engine=engine, fp64=fp64)
+    for n in (2, 3, 5):
+        parts = [cs.debye_solvent_basis(s, q, sp, engine=engine, fp64=fp64, shard=(k, n)) for k in range(n)]
+        assert _close(sum(parts), whole), n
+        assert all(np.any(p != 0.0) for p in parts)
+
+
+def test_partials_shards_and_self_sums(engine):
+    s = synth.protein(32, 3000, 18.0)
+    w = np.random.default_rng(3).uniform(1.0, 9.0, len(s.xyz))
+    t = s.element.astype(np.int32) % 4
+    q = np.linspace(0.01, 0.45, 300)
+    pair, self_ = cs.debye_partials(s.xyz, w, t, 4, q, engine=engine)
+    for n in (2, 4):
+        got = [cs.debye_partials(s.xyz, w, t, 4, q, engine=engine, shard=(k, n)) for k in range(n)]
+        assert _close(sum(g[0] for g in got), pair)
+        assert np.array_equal(got[0][1], self_) and all(not g[1].any() for g in got[1:])
+
+
+def test_more_shards_than_work_items(engine):
+    """90 atoms: one tile per atom type (at most 4) and one q block, so at
+    most 4 work items; the other shards return zeros and the sum is still the
+    whole."""
+    s = synth.protein(33, 90, 8.0)
+    q = np.linspace(0.001, 0.3, 40)
+    sp = cs.SolventParams()
+    whole = cs.debye_solvent_basis(s, q, sp, engine=engine)
+    parts = [cs.debye_solvent_basis(s, q, sp, engine=engine, shard=(k, 7)) for k in range(7)]
+    assert _close(sum(parts), whole)
+    assert sum(1 for p in parts if not p.any()) >= 3
+
+
+def test_invalid_shard_arguments(engine):
+    s = synth.protein(34, 200, 9.0)
+    q = np.linspace(0.01, 0.3, 10)
+    for shard in ((0, 0), (2, 2), (-1, 3)):
+        with pytest.raises(cs.InvalidInput):
+            cs.debye_solvent_basis(s, q, cs.SolventParams(), engine=engine, shard=shard)
+        with pytest.raises(cs.InvalidInput):
+            cs.debye_partials(s.xyz, np.ones(len(s.xyz)), np.zeros(len(s.xyz), np.int32), 1, q, engine=engine,
+                              shard=shard)
+
+
+def test_sharded_basis_without_a_process_group_is_the_basis(engine):
+    from crabsaxs_b200 import shard as S
+
+    s = synth.protein(35, 1500, 14.0)
+    q = np.linspace(0.001, 0.5, 64)
+    sp = cs.SolventParams(c2=0.3)
+    whole = cs.debye_solvent_basis(s, q, sp, engine=engine)
+    assert _close(S.sharded_debye_solvent_basis(s, q, sp, engine=engine), whole)
