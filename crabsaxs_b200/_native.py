@@ -129,6 +129,11 @@ _SIGS = {
     "crab_chi2_grad": (C.c_int, [P, P, D, D, D, I64, C.POINTER(Solvent), C.c_int, C.c_double, C.c_double, D, D, D]),
     "crab_ensemble_fit": (C.c_int, [P, C.POINTER(P), C.c_int32, D, D, D, I64, C.POINTER(EnsembleOpts),
                                     C.POINTER(FitOpts), C.POINTER(EnsembleResult), I32P, D, D, D, D]),
+    "crab_ensemble_partials": (C.c_int, [P, C.POINTER(P), C.c_int32, D, I64, C.c_int, C.c_int, C.c_int, I32P, D,
+                                         I64]),
+    "crab_ensemble_fit_partials": (C.c_int, [P, C.POINTER(P), C.c_int32, D, D, D, I64, C.POINTER(EnsembleOpts),
+                                             C.POINTER(FitOpts), D, C.c_int32, C.POINTER(EnsembleResult), I32P, D,
+                                             D, D, D]),
     "crab_ensemble_plan_create": (C.c_int, [P, C.POINTER(P), C.c_int32, D, I64, C.POINTER(Solvent), C.c_int, D,
                                             C.c_int32, C.POINTER(P)]),
     "crab_ensemble_plan_autotune": (C.c_int, [P, P, I32P]),

@@ -848,9 +848,39 @@ class EnsembleFitter:
         self.engine = engine or Engine.default()
 
     def fit(self) -> EnsembleResult:
+        return self._fit(None)
+
+    def _handles(self):
+        k = len(self.conformers)
+        return (C.c_void_p * k)(*[c.handle(self.engine) for c in self.conformers])
+
+    def partials(self, shard: tuple[int, int] = (0, 1)) -> tuple[int, np.ndarray]:
+        """This shard's pair sums of the ensemble (crab_ensemble_partials):
+        (type count T, buffer of k blocks, zero for conformers it does not
+        own).  Summing the buffers of all shards gathers every conformer."""
         e = self.engine
         k = len(self.conformers)
-        handles = (C.c_void_p * k)(*[c.handle(e) for c in self.conformers])
+        ex = self.experimental
+        implicit = self.options.fit.to_c().implicit_hydrogen
+        handles = self._handles()
+        t = C.c_int32()
+        e.check(N.lib.crab_ensemble_partials(e.handle, handles, k, _dp(ex.q), len(ex), implicit, int(shard[0]),
+                                             int(shard[1]), C.byref(t), None, 0))
+        T = t.value
+        buf = np.empty(k * (T * (T + 1) // 2 * len(ex) + 2 * T))
+        e.check(N.lib.crab_ensemble_partials(e.handle, handles, k, _dp(ex.q), len(ex), implicit, int(shard[0]),
+                                             int(shard[1]), C.byref(t), _dp(buf), buf.size))
+        return T, buf
+
+    def fit_from_partials(self, n_types: int, partials: np.ndarray) -> EnsembleResult:
+        """fit() with the pair sums of every conformer given (the sum over
+        shards of partials()): crab_ensemble_fit_partials."""
+        return self._fit((int(n_types), np.ascontiguousarray(partials, dtype=np.float64)))
+
+    def _fit(self, given) -> EnsembleResult:
+        e = self.engine
+        k = len(self.conformers)
+        handles = self._handles()
         o = self.options
         eo = N.EnsembleOpts(1 if o.fit_weights else 0, 1 if o.uniform else 0, o.regularization,
                             o.max_conformers or 0, o.bootstrap, o.min_weight, o.seed)
@@ -862,9 +892,19 @@ class EnsembleFitter:
         ex = self.experimental
         intervals = np.empty((k, 3))
         boot = np.empty(max(o.bootstrap, 1))
-        e.check(N.lib.crab_ensemble_fit(e.handle, handles, k, _dp(ex.q), _dp(ex.intensity), _dp(ex.sigma), len(ex),
-                                        C.byref(eo), C.byref(fo), C.byref(res), sel.ctypes.data_as(N.I32P), _dp(w),
-                                        _dp(fitted), _dp(intervals), _dp(boot)))
+        if given is None:
+            e.check(N.lib.crab_ensemble_fit(e.handle, handles, k, _dp(ex.q), _dp(ex.intensity), _dp(ex.sigma),
+                                            len(ex), C.byref(eo), C.byref(fo), C.byref(res),
+                                            sel.ctypes.data_as(N.I32P), _dp(w), _dp(fitted), _dp(intervals),
+                                            _dp(boot)))
+        else:
+            T, buf = given
+            if buf.size != k * (T * (T + 1) // 2 * len(ex) + 2 * T):
+                raise InvalidInput("partials buffer does not match the ensemble")
+            e.check(N.lib.crab_ensemble_fit_partials(e.handle, handles, k, _dp(ex.q), _dp(ex.intensity),
+                                                     _dp(ex.sigma), len(ex), C.byref(eo), C.byref(fo), _dp(buf), T,
+                                                     C.byref(res), sel.ctypes.data_as(N.I32P), _dp(w), _dp(fitted),
+                                                     _dp(intervals), _dp(boot)))
         n = res.n_selected
         return EnsembleResult([self.names[i] for i in sel[:n]], w[:n].copy(),
                               FitParams(res.scale, res.background, res.c1, res.c2), res.chi2, res.reduced_chi2,

@@ -489,6 +489,7 @@ struct EnsemblePlan {
   std::vector<double> self_w2, sum_w;  // [K][T]
   std::vector<double> amp, damp;       // [n_cand][T][nq], [2 n_cand][T][nq]
   std::vector<void*> owned;
+  double* d_partials = nullptr;  // raw pair sums [K][T(T+1)/2][nq]: the pair plan's output, or uploaded
   double *d_q = nullptr, *d_amp = nullptr, *d_damp = nullptr, *d_self = nullptr, *d_sumw = nullptr;
   double *d_curves = nullptr, *d_dcurves = nullptr;
   int* d_sel = nullptr;
@@ -511,9 +512,37 @@ struct EnsemblePlan {
   }
 };
 
+// Scattering classes of the whole ensemble (sorted) and their type indices:
+// every conformer uses the same types.
+static std::map<AtomClass, int> ensemble_class_index(crab_struct* const* sts, int K, bool implicit) {
+  std::map<AtomClass, int> index;
+  for (int c = 0; c < K; ++c) {
+    require(sts[c] && sts[c]->n > 0, "ensemble must contain non-empty conformers");
+    for (int64_t i = 0; i < sts[c]->n; ++i)
+      index[AtomClass{sts[c]->elem[i], implicit ? (int)sts[c]->group[i] : -1}] = 0;
+  }
+  int T = 0;
+  for (auto& kv : index) kv.second = T++;
+  return index;
+}
+
+static std::vector<int32_t> conformer_types(const crab_struct* st, const std::map<AtomClass, int>& index,
+                                            bool implicit) {
+  std::vector<int32_t> type(st->n);
+  for (int64_t i = 0; i < st->n; ++i) type[i] = index.at(AtomClass{st->elem[i], implicit ? (int)st->group[i] : -1});
+  return type;
+}
+
+// Doubles per conformer in a gathered partials buffer: the raw pair sums
+// [T(T+1)/2][nq], then Σw² and Σw per type.
+static size_t partials_block(int T, int64_t nq) { return (size_t)(T * (T + 1) / 2) * nq + 2 * (size_t)T; }
+
+// With `given` (a gathered buffer of K partials blocks) the pair sums are
+// uploaded instead of computed, and no pair plan is built.
 static std::unique_ptr<EnsemblePlan> make_ensemble_plan(crab_ctx* ctx, crab_struct* const* sts, int K, const double* q,
                                                         int64_t nq, const crab_solvent& s, bool implicit,
-                                                        const double* cand, int n_cand) {
+                                                        const double* cand, int n_cand,
+                                                        const double* given = nullptr) {
   require(K > 0 && K <= kMaxK, "ensemble size must be between 1 and 1024");
   require(n_cand > 0, "at least one (c1, c2) candidate");
   require(s.hydration_model == CRAB_HYD_ANALYTIC, "the batched ensemble covers the analytic hydration model");
@@ -530,32 +559,39 @@ static std::unique_ptr<EnsemblePlan> make_ensemble_plan(crab_ctx* ctx, crab_stru
   E->implicit = implicit;
   E->solvent = s;
   // shared scattering types over the whole ensemble
-  std::map<AtomClass, int> index;
-  for (int c = 0; c < K; ++c) {
-    require(sts[c] && sts[c]->n > 0, "ensemble must contain non-empty conformers");
-    for (int64_t i = 0; i < sts[c]->n; ++i)
-      index[AtomClass{sts[c]->elem[i], implicit ? (int)sts[c]->group[i] : -1}] = 0;
-  }
-  int T = 0;
-  for (auto& kv : index) {
-    kv.second = T++;
-    E->classes.push_back(kv.first);
-  }
+  const std::map<AtomClass, int> index = ensemble_class_index(sts, K, implicit);
+  for (const auto& kv : index) E->classes.push_back(kv.first);
+  const int T = (int)index.size();
   E->T = T;
-  std::vector<Layout> parts;
   E->self_w2.assign((size_t)K * T, 0.0);
   E->sum_w.assign((size_t)K * T, 0.0);
-  for (int c = 0; c < K; ++c) {
-    const crab_struct* st = sts[c];
-    std::vector<int32_t> type(st->n);
-    for (int64_t i = 0; i < st->n; ++i) type[i] = index[AtomClass{st->elem[i], implicit ? (int)st->group[i] : -1}];
-    parts.push_back(build_layout(st->xyz.data(), st->occ.data(), type.data(), st->n, T, false));
-    for (int a = 0; a < T; ++a) {
-      E->self_w2[(size_t)c * T + a] = parts.back().self_w2[a];
-      E->sum_w[(size_t)c * T + a] = parts.back().sum_w[a];
+  if (!given) {
+    std::vector<Layout> parts;
+    for (int c = 0; c < K; ++c) {
+      const crab_struct* st = sts[c];
+      const std::vector<int32_t> type = conformer_types(st, index, implicit);
+      parts.push_back(build_layout(st->xyz.data(), st->occ.data(), type.data(), st->n, T, false));
+      for (int a = 0; a < T; ++a) {
+        E->self_w2[(size_t)c * T + a] = parts.back().self_w2[a];
+        E->sum_w[(size_t)c * T + a] = parts.back().sum_w[a];
+      }
     }
+    E->pair = make_batch_pair_plan(ctx, std::move(parts), q, nq);
+    E->d_partials = E->pair->d_out;
+  } else {
+    const size_t P = (size_t)(T * (T + 1) / 2), block = partials_block(T, nq);
+    std::vector<double> raw((size_t)K * P * nq);
+    for (int c = 0; c < K; ++c) {
+      const double* b = given + (size_t)c * block;
+      std::copy(b, b + P * nq, raw.begin() + (size_t)c * P * nq);
+      for (int a = 0; a < T; ++a) {
+        E->self_w2[(size_t)c * T + a] = b[P * nq + a];
+        E->sum_w[(size_t)c * T + a] = b[P * nq + T + a];
+      }
+    }
+    E->d_partials = E->alloc<double>(raw.size());
+    copy_h2d(ctx, E->d_partials, raw.data(), raw.size() * sizeof(double), ctx->stream);
   }
-  E->pair = make_batch_pair_plan(ctx, std::move(parts), q, nq);
   // amplitude tables per candidate and their c1/c2 derivatives
   E->amp.assign((size_t)n_cand * T * nq, 0.0);
   E->damp.assign((size_t)2 * n_cand * T * nq, 0.0);
@@ -595,7 +631,7 @@ static std::unique_ptr<EnsemblePlan> make_ensemble_plan(crab_ctx* ctx, crab_stru
 
 static void ensemble_launch_curves(EnsemblePlan& E, int Ksel) {
   crab_ctx* ctx = E.ctx;
-  k_ens_curves<<<dim3(Ksel, E.n_cand), 128, 0, ctx->stream>>>(E.pair->d_out, E.d_sel, E.d_q, (int)E.nq, E.T, E.d_amp,
+  k_ens_curves<<<dim3(Ksel, E.n_cand), 128, 0, ctx->stream>>>(E.d_partials, E.d_sel, E.d_q, (int)E.nq, E.T, E.d_amp,
                                                              E.d_self, E.d_sumw, Ksel, E.d_curves);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 1;
@@ -639,7 +675,7 @@ static void ensemble_launch_fit(EnsemblePlan& E, int Ksel, const EnsOpts& eo, co
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 1;
   if (ro) {
-    k_ens_dcurves<<<dim3(Ksel, 2 * E.n_cand), 128, 0, sm>>>(E.pair->d_out, E.d_sel, E.d_q, (int)E.nq, E.T, E.d_amp,
+    k_ens_dcurves<<<dim3(Ksel, 2 * E.n_cand), 128, 0, sm>>>(E.d_partials, E.d_sel, E.d_q, (int)E.nq, E.T, E.d_amp,
                                                            E.d_damp, E.d_self, E.d_sumw, Ksel, E.d_curves,
                                                            E.d_dcurves);
     CRAB_CUDA_CHECK(cudaGetLastError());
@@ -665,7 +701,7 @@ static void ensemble_graph_launch(EnsemblePlan& E, const EnsOpts& eo, const RwOp
     const int64_t before = ctx->launches;
     CRAB_CUDA_CHECK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     try {
-      pair_plan_launch(ctx, *E.pair, ctx->stream, false);
+      if (E.pair) pair_plan_launch(ctx, *E.pair, ctx->stream, false);
       ensemble_launch_fit(E, E.K, eo, &ro);
     } catch (...) {
       cudaStreamEndCapture(ctx->stream, &g);
@@ -802,6 +838,139 @@ int crab_ensemble_plan_destroy(crab_ensemble_plan* plan) {
   return CRAB_OK;
 }
 
+}  // extern "C"
+
+// ensemble.rs:302-315: the 5 x 5 (c1, c2) candidate grid.
+static std::vector<double> fit_candidates(const crab_fit_options* fopt) {
+  std::vector<double> cand;
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) {
+      cand.push_back(fopt->c1_lo + (fopt->c1_hi - fopt->c1_lo) * (double)i / 4.0);
+      cand.push_back(fopt->c2_lo + (fopt->c2_hi - fopt->c2_lo) * (double)j / 4.0);
+    }
+  return cand;
+}
+
+static void check_ensemble_inputs(const crab_ensemble_options& eo, const double* y, const double* sigma, int64_t nq) {
+  require(std::isfinite(eo.regularization) && eo.regularization >= 0.0 && std::isfinite(eo.min_weight) &&
+              eo.min_weight >= 0.0 && eo.min_weight <= 1.0 && eo.max_conformers >= 0 && eo.bootstrap >= 0,
+          "ensemble regularization and pruning options are invalid");
+  for (int64_t p = 0; p < nq; ++p)
+    require(std::isfinite(y[p]) && std::isfinite(sigma[p]) && sigma[p] > 0.0, "invalid experimental curve");
+}
+
+// EnsembleFitter::fit (ensemble.rs:127-232) once the pair sums are on the
+// device: fit_core for every pruning round, the optional residual
+// bootstrap, and the outputs.
+static void ensemble_fit_rounds(crab_ctx* ctx, std::unique_ptr<EnsemblePlan>& E, const std::vector<double>& cand,
+                                const double* y, const double* sigma, int64_t nq, const crab_ensemble_options& eo,
+                                const crab_fit_options* fopt, crab_ensemble_result* result, int32_t* selected_out,
+                                double* weights_out, double* fitted_out, double* intervals_out,
+                                double* bootstrap_chi2_out) {
+  ensemble_fit_buffers(*E, y, sigma);
+  const EnsOpts o = ens_opts(fopt, eo.uniform || !eo.fit_weights, eo.regularization);
+  struct Core {
+    std::vector<double> w, fitted;
+    double scale, bg, chi2, c1, c2;
+  };
+  auto fit_core = [&](const std::vector<int>& sel, const double* yy) {
+    copy_h2d(ctx, E->d_sel, sel.data(), sel.size() * sizeof(int), ctx->stream);
+    copy_h2d(ctx, E->d_y, yy, nq * sizeof(double), ctx->stream);
+    ensemble_launch_fit(*E, (int)sel.size(), o, nullptr);
+    std::vector<double> fit(4 * 25);
+    copy_d2h(ctx, fit.data(), E->d_fit, fit.size() * sizeof(double), ctx->stream);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    int best = 0;
+    for (int c = 1; c < 25; ++c)
+      if (fit[4 * c + 2] < fit[4 * best + 2]) best = c;
+    Core core;
+    core.w.resize(sel.size());
+    core.fitted.resize(nq);
+    copy_d2h(ctx, core.w.data(), E->d_weights + (size_t)best * sel.size(), sel.size() * sizeof(double), ctx->stream);
+    copy_d2h(ctx, core.fitted.data(), E->d_fitted + (size_t)best * nq, nq * sizeof(double), ctx->stream);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    core.scale = fit[4 * best];
+    core.bg = fit[4 * best + 1];
+    core.chi2 = fit[4 * best + 2];
+    core.c1 = cand[2 * best];
+    core.c2 = cand[2 * best + 1];
+    return core;
+  };
+  std::vector<int> selected(E->K);
+  std::iota(selected.begin(), selected.end(), 0);
+  Core core = fit_core(selected, y);
+  for (bool changed = true; changed;) {
+    changed = false;
+    std::vector<int> keep;
+    for (size_t i = 0; i < selected.size(); ++i)
+      if (core.w[i] + 1e-12 >= eo.min_weight) keep.push_back(selected[i]);
+    if (keep.empty())
+      keep.push_back(selected[std::max_element(core.w.begin(), core.w.end()) - core.w.begin()]);
+    if (eo.max_conformers > 0 && (int)keep.size() > eo.max_conformers) {
+      std::vector<std::pair<double, int>> ranked;
+      for (size_t i = 0; i < selected.size(); ++i) ranked.push_back({core.w[i], selected[i]});
+      std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+      keep.clear();
+      for (int i = 0; i < eo.max_conformers; ++i) keep.push_back(ranked[i].second);
+    }
+    std::sort(keep.begin(), keep.end());
+    if (keep != selected) {
+      selected = keep;
+      core = fit_core(selected, y);
+      changed = true;
+    }
+  }
+  // weight intervals from a residual bootstrap (ensemble.rs:174-216); the
+  // resampling indices come from a seeded std::mt19937_64 stream (the
+  // reference draws them from ChaCha8, so individual replicates differ)
+  const size_t ns = selected.size();
+  std::vector<std::vector<double>> samples(ns);
+  if (eo.bootstrap > 0) {
+    std::mt19937_64 rng(eo.seed);
+    std::vector<double> resid(nq), synth(nq);
+    for (int64_t p = 0; p < nq; ++p) resid[p] = (y[p] - core.fitted[p]) / sigma[p];
+    for (int b = 0; b < eo.bootstrap; ++b) {
+      for (int64_t p = 0; p < nq; ++p) synth[p] = core.fitted[p] + resid[rng() % (uint64_t)nq] * sigma[p];
+      Core rep = fit_core(selected, synth.data());
+      for (size_t i = 0; i < ns; ++i) samples[i].push_back(rep.w[i]);
+      if (bootstrap_chi2_out) bootstrap_chi2_out[b] = rep.chi2;
+    }
+    copy_h2d(ctx, E->d_y, y, nq * sizeof(double), ctx->stream);
+  }
+  if (intervals_out) {
+    auto quantile = [](const std::vector<double>& v, double prob) {
+      const double pos = std::min(std::max(prob, 0.0), 1.0) * (double)(v.size() - 1);
+      const size_t lo = (size_t)std::floor(pos), hi = (size_t)std::ceil(pos);
+      return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+    };
+    for (size_t i = 0; i < ns; ++i) {
+      if (eo.bootstrap > 0) {
+        std::sort(samples[i].begin(), samples[i].end());
+        intervals_out[3 * i] = quantile(samples[i], 0.5);
+        intervals_out[3 * i + 1] = quantile(samples[i], 0.025);
+        intervals_out[3 * i + 2] = quantile(samples[i], 0.975);
+      } else {
+        intervals_out[3 * i] = intervals_out[3 * i + 1] = intervals_out[3 * i + 2] = core.w[i];
+      }
+    }
+  }
+  const double dof = (double)std::max<int64_t>(nq - 1, 1);
+  result->scale = core.scale;
+  result->background = core.bg;
+  result->c1 = core.c1;
+  result->c2 = core.c2;
+  result->reduced_chi2 = core.chi2;
+  result->chi2 = core.chi2 * dof;
+  result->iterations = 250;
+  result->n_selected = (int)selected.size();
+  if (selected_out)
+    for (size_t i = 0; i < selected.size(); ++i) selected_out[i] = selected[i];
+  if (weights_out) std::copy(core.w.begin(), core.w.end(), weights_out);
+  if (fitted_out) std::copy(core.fitted.begin(), core.fitted.end(), fitted_out);
+}
+
+extern "C" {
+
 // EnsembleFitter::fit (ensemble.rs:127-232): partials once, fit_core on the
 // device for every pruning round, optional residual bootstrap.
 int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, const double* y,
@@ -812,121 +981,86 @@ int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const* structures, int32_t k, 
   return guarded_impl(ctx, [&]() {
     validate_q(q, nq);
     validate_solvent(fopt->solvent);
-    const crab_ensemble_options& eo = *eopt;
-    require(std::isfinite(eo.regularization) && eo.regularization >= 0.0 && std::isfinite(eo.min_weight) &&
-                eo.min_weight >= 0.0 && eo.min_weight <= 1.0 && eo.max_conformers >= 0 && eo.bootstrap >= 0,
-            "ensemble regularization and pruning options are invalid");
-    for (int64_t p = 0; p < nq; ++p)
-      require(std::isfinite(y[p]) && std::isfinite(sigma[p]) && sigma[p] > 0.0, "invalid experimental curve");
-    // ensemble.rs:302-315 candidate grid
-    std::vector<double> cand;
-    for (int i = 0; i < 5; ++i)
-      for (int j = 0; j < 5; ++j) {
-        cand.push_back(fopt->c1_lo + (fopt->c1_hi - fopt->c1_lo) * (double)i / 4.0);
-        cand.push_back(fopt->c2_lo + (fopt->c2_hi - fopt->c2_lo) * (double)j / 4.0);
-      }
+    check_ensemble_inputs(*eopt, y, sigma, nq);
+    const std::vector<double> cand = fit_candidates(fopt);
     auto E = make_ensemble_plan(ctx, structures, k, q, nq, fopt->solvent, fopt->implicit_hydrogen != 0, cand.data(), 25);
     pair_plan_launch(ctx, *E->pair, ctx->stream, false);
-    ensemble_fit_buffers(*E, y, sigma);
-    const EnsOpts o = ens_opts(fopt, eo.uniform || !eo.fit_weights, eo.regularization);
-    struct Core {
-      std::vector<double> w, fitted;
-      double scale, bg, chi2, c1, c2;
-    };
-    auto fit_core = [&](const std::vector<int>& sel, const double* yy) {
-      copy_h2d(ctx, E->d_sel, sel.data(), sel.size() * sizeof(int), ctx->stream);
-      copy_h2d(ctx, E->d_y, yy, nq * sizeof(double), ctx->stream);
-      ensemble_launch_fit(*E, (int)sel.size(), o, nullptr);
-      std::vector<double> fit(4 * 25);
-      copy_d2h(ctx, fit.data(), E->d_fit, fit.size() * sizeof(double), ctx->stream);
-      CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      int best = 0;
-      for (int c = 1; c < 25; ++c)
-        if (fit[4 * c + 2] < fit[4 * best + 2]) best = c;
-      Core core;
-      core.w.resize(sel.size());
-      core.fitted.resize(nq);
-      copy_d2h(ctx, core.w.data(), E->d_weights + (size_t)best * sel.size(), sel.size() * sizeof(double), ctx->stream);
-      copy_d2h(ctx, core.fitted.data(), E->d_fitted + (size_t)best * nq, nq * sizeof(double), ctx->stream);
-      CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
-      core.scale = fit[4 * best];
-      core.bg = fit[4 * best + 1];
-      core.chi2 = fit[4 * best + 2];
-      core.c1 = cand[2 * best];
-      core.c2 = cand[2 * best + 1];
-      return core;
-    };
-    std::vector<int> selected(k);
-    std::iota(selected.begin(), selected.end(), 0);
-    Core core = fit_core(selected, y);
-    for (bool changed = true; changed;) {
-      changed = false;
-      std::vector<int> keep;
-      for (size_t i = 0; i < selected.size(); ++i)
-        if (core.w[i] + 1e-12 >= eo.min_weight) keep.push_back(selected[i]);
-      if (keep.empty())
-        keep.push_back(selected[std::max_element(core.w.begin(), core.w.end()) - core.w.begin()]);
-      if (eo.max_conformers > 0 && (int)keep.size() > eo.max_conformers) {
-        std::vector<std::pair<double, int>> ranked;
-        for (size_t i = 0; i < selected.size(); ++i) ranked.push_back({core.w[i], selected[i]});
-        std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-        keep.clear();
-        for (int i = 0; i < eo.max_conformers; ++i) keep.push_back(ranked[i].second);
-      }
-      std::sort(keep.begin(), keep.end());
-      if (keep != selected) {
-        selected = keep;
-        core = fit_core(selected, y);
-        changed = true;
+    ensemble_fit_rounds(ctx, E, cand, y, sigma, nq, *eopt, fopt, result, selected_out, weights_out, fitted_out,
+                        intervals_out, bootstrap_chi2_out);
+  });
+}
+
+int crab_ensemble_partials(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, int64_t nq,
+                           int implicit_hydrogen, int shard, int n_shards, int32_t* n_types, double* out,
+                           int64_t capacity) {
+  if (!ctx || !structures || k <= 0 || !q || nq <= 0 || !n_types || n_shards < 1 || shard < 0 || shard >= n_shards)
+    return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() {
+    validate_q(q, nq);
+    require(k <= kMaxK, "ensemble size must be between 1 and 1024");
+    const bool implicit = implicit_hydrogen != 0;
+    const std::map<AtomClass, int> index = ensemble_class_index(structures, k, implicit);
+    const int T = (int)index.size();
+    *n_types = T;
+    if (!out) return;
+    const size_t P = (size_t)(T * (T + 1) / 2), block = partials_block(T, nq);
+    if (capacity < 0 || (uint64_t)capacity < block * (size_t)k) throw Error(CRAB_ECAPACITY, "partials buffer too small");
+    std::fill(out, out + block * (size_t)k, 0.0);
+    // conformers longest first by N², then the greedy owners
+    std::vector<int> order(k);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return structures[a]->n > structures[b]->n; });
+    std::vector<int64_t> cost(k);
+    for (int i = 0; i < k; ++i) cost[i] = structures[order[i]]->n * structures[order[i]]->n;
+    const std::vector<int32_t> owner = shard_owners(cost.data(), k, n_shards);
+    std::vector<int> mine;
+    for (int i = 0; i < k; ++i)
+      if (owner[i] == shard) mine.push_back(order[i]);
+    std::sort(mine.begin(), mine.end());
+    if (mine.empty()) return;
+    std::vector<Layout> parts;
+    for (int c : mine) {
+      const crab_struct* st = structures[c];
+      const std::vector<int32_t> type = conformer_types(st, index, implicit);
+      parts.push_back(build_layout(st->xyz.data(), st->occ.data(), type.data(), st->n, T, false));
+      double* b = out + (size_t)c * block;
+      for (int a = 0; a < T; ++a) {
+        b[P * nq + a] = parts.back().self_w2[a];
+        b[P * nq + T + a] = parts.back().sum_w[a];
       }
     }
-    // weight intervals from a residual bootstrap (ensemble.rs:174-216); the
-    // resampling indices come from a seeded std::mt19937_64 stream (the
-    // reference draws them from ChaCha8, so individual replicates differ)
-    const size_t ns = selected.size();
-    std::vector<std::vector<double>> samples(ns);
-    if (eo.bootstrap > 0) {
-      std::mt19937_64 rng(eo.seed);
-      std::vector<double> resid(nq), synth(nq);
-      for (int64_t p = 0; p < nq; ++p) resid[p] = (y[p] - core.fitted[p]) / sigma[p];
-      for (int b = 0; b < eo.bootstrap; ++b) {
-        for (int64_t p = 0; p < nq; ++p) synth[p] = core.fitted[p] + resid[rng() % (uint64_t)nq] * sigma[p];
-        Core rep = fit_core(selected, synth.data());
-        for (size_t i = 0; i < ns; ++i) samples[i].push_back(rep.w[i]);
-        if (bootstrap_chi2_out) bootstrap_chi2_out[b] = rep.chi2;
-      }
-      copy_h2d(ctx, E->d_y, y, nq * sizeof(double), ctx->stream);
-    }
-    if (intervals_out) {
-      auto quantile = [](const std::vector<double>& v, double prob) {
-        const double pos = std::min(std::max(prob, 0.0), 1.0) * (double)(v.size() - 1);
-        const size_t lo = (size_t)std::floor(pos), hi = (size_t)std::ceil(pos);
-        return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
-      };
-      for (size_t i = 0; i < ns; ++i) {
-        if (eo.bootstrap > 0) {
-          std::sort(samples[i].begin(), samples[i].end());
-          intervals_out[3 * i] = quantile(samples[i], 0.5);
-          intervals_out[3 * i + 1] = quantile(samples[i], 0.025);
-          intervals_out[3 * i + 2] = quantile(samples[i], 0.975);
-        } else {
-          intervals_out[3 * i] = intervals_out[3 * i + 1] = intervals_out[3 * i + 2] = core.w[i];
-        }
-      }
-    }
-    const double dof = (double)std::max<int64_t>(nq - 1, 1);
-    result->scale = core.scale;
-    result->background = core.bg;
-    result->c1 = core.c1;
-    result->c2 = core.c2;
-    result->reduced_chi2 = core.chi2;
-    result->chi2 = core.chi2 * dof;
-    result->iterations = 250;
-    result->n_selected = (int)selected.size();
-    if (selected_out)
-      for (size_t i = 0; i < selected.size(); ++i) selected_out[i] = selected[i];
-    if (weights_out) std::copy(core.w.begin(), core.w.end(), weights_out);
-    if (fitted_out) std::copy(core.fitted.begin(), core.fitted.end(), fitted_out);
+    auto plan = make_batch_pair_plan(ctx, std::move(parts), q, nq);
+    pair_plan_launch(ctx, *plan, ctx->stream, false);
+    std::vector<double> raw(mine.size() * P * (size_t)nq);
+    int status = 0;
+    copy_d2h(ctx, raw.data(), plan->d_out, raw.size() * sizeof(double), ctx->stream);
+    copy_d2h(ctx, &status, plan->d_status, sizeof(int), ctx->stream);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    if (status) throw Error(status, "pair kernel: a bounded wait on a j-tile copy ran out");
+    for (size_t i = 0; i < mine.size(); ++i)
+      std::copy(raw.begin() + i * P * nq, raw.begin() + (i + 1) * P * nq, out + (size_t)mine[i] * block);
+  });
+}
+
+int crab_ensemble_fit_partials(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q,
+                               const double* y, const double* sigma, int64_t nq, const crab_ensemble_options* eopt,
+                               const crab_fit_options* fopt, const double* partials, int32_t n_types,
+                               crab_ensemble_result* result, int32_t* selected_out, double* weights_out,
+                               double* fitted_out, double* intervals_out, double* bootstrap_chi2_out) {
+  if (!ctx || !structures || k <= 0 || !q || !y || !sigma || nq <= 0 || !eopt || !fopt || !partials || !result)
+    return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() {
+    validate_q(q, nq);
+    validate_solvent(fopt->solvent);
+    check_ensemble_inputs(*eopt, y, sigma, nq);
+    require((int)ensemble_class_index(structures, k, fopt->implicit_hydrogen != 0).size() == n_types,
+            "partials were computed for another set of atom types");
+    const std::vector<double> cand = fit_candidates(fopt);
+    auto E = make_ensemble_plan(ctx, structures, k, q, nq, fopt->solvent, fopt->implicit_hydrogen != 0, cand.data(), 25,
+                                partials);
+    ensemble_fit_rounds(ctx, E, cand, y, sigma, nq, *eopt, fopt, result, selected_out, weights_out, fitted_out,
+                        intervals_out, bootstrap_chi2_out);
   });
 }
 

@@ -1,13 +1,21 @@
-"""One structure's Debye sums split over several GPUs.
+"""Debye sums split over several GPUs: one structure's pair work, or an
+ensemble's conformers.
 
 One process per GPU, each with its own :class:`~crabsaxs_b200.api.Engine`
 and a ``torch.distributed`` process group (NCCL between GPUs, gloo on the
-host).  Every rank builds the same tile layout and work list and keeps the
-work items :func:`shard_assign` gives it, so the split needs no exchange;
-the only collective is one all-reduce (sum) of the result: the six basis
-rows (6 x nq f64, 24 kB at 500 q) or the type-pair partials (T(T+1)/2 x nq
-f64, 60 kB for 5 types at 500 q).  The reference runs on one host and has no
-counterpart; its q loop is split over threads (solvent.rs:528).
+host).  Every rank derives the same split from the same inputs
+(:func:`shard_assign`: longest first, each item to the least-loaded shard),
+so the split needs no exchange; the only collective is one all-reduce (sum)
+of the result, whose parts are zero where a rank did no work:
+
+- one structure: the six basis rows (6 x nq f64, 24 kB at 500 q) or the
+  type-pair partials (T(T+1)/2 x nq f64, 60 kB for 5 types at 500 q);
+- an ensemble: every conformer's raw pair sums (k blocks of T(T+1)/2 x nq +
+  2T f64, about 9 MB for 256 conformers at 300 q), after which every rank
+  runs the same weight fit.
+
+The reference runs on one host and has no counterpart; its loops over q and
+over conformers are split over threads (solvent.rs:528, ensemble.rs:244).
 """
 from __future__ import annotations
 
@@ -17,7 +25,8 @@ from typing import Optional
 import numpy as np
 
 from . import _native as N
-from .api import Engine, InvalidInput, SolventParams, Structure, debye_partials, debye_solvent_basis
+from .api import (Engine, EnsembleFitter, EnsembleResult, InvalidInput, SolventParams, Structure, debye_partials,
+                  debye_solvent_basis)
 
 
 def shard_assign(cost, n_shards: int) -> np.ndarray:
@@ -76,3 +85,13 @@ def sharded_debye_partials(xyz, w, types, n_types: int, q, group=None, engine: O
     pair, self_ = debye_partials(xyz, w, types, n_types, q, fp64, engine, shard=(rank, world))
     both = reduce_shards(np.concatenate([pair.ravel(), self_]), group)
     return both[: pair.size].reshape(pair.shape), both[pair.size:]
+
+
+def sharded_ensemble_fit(fitter: EnsembleFitter, group=None) -> EnsembleResult:
+    """EnsembleFitter.fit over the ranks of ``group``: each rank's engine sums
+    the pairs of the conformers it owns, the all-reduce gathers them, and
+    every rank runs the same fit (ensemble.rs:127-232) and returns the same
+    result."""
+    rank, world = _rank_world(group)
+    n_types, part = fitter.partials(shard=(rank, world))
+    return fitter.fit_from_partials(n_types, reduce_shards(part, group))

@@ -356,6 +356,30 @@ int crab_ensemble_fit(crab_ctx* ctx, crab_struct* const* structures, int32_t k, 
 /* (intervals: 3 per selected conformer, median/lower/upper of the bootstrap
  * weights (ensemble.rs:174-216); bootstrap_chi2: one per replicate; both may
  * be NULL.) */
+/* Multi-GPU ensemble (one process and context per GPU), in two steps; no
+ * counterpart in the reference, whose conformer loop is split over threads
+ * (ensemble.rs:244).
+ * crab_ensemble_partials: every rank passes all k structures (so all derive
+ * the same atom types) and computes the pair sums of the conformers it owns:
+ * conformers ordered by N² (longest first), owners as crab_shard_assign
+ * gives them for costs N².  *n_types receives the ensemble's type count T;
+ * out == NULL is that size query.  out holds k blocks of
+ * T(T+1)/2 * nq + 2T doubles: the raw pair sums Σ w_i w_j sin(q r)/r per type
+ * pair and q, then Σw² and Σw per type.  Blocks of conformers this rank does
+ * not own are zero, so summing out over all ranks (an all-reduce) gathers
+ * every conformer.  capacity (doubles) below k blocks: CRAB_ECAPACITY.
+ * implicit_hydrogen must be the fit's fopt->implicit_hydrogen. */
+int crab_ensemble_partials(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q, int64_t nq,
+                           int implicit_hydrogen, int shard, int n_shards, int32_t* n_types, double* out,
+                           int64_t capacity);
+/* crab_ensemble_fit with the pair sums taken from the summed partials buffer
+ * (every rank gets the same result); n_types as crab_ensemble_partials
+ * reported it. */
+int crab_ensemble_fit_partials(crab_ctx* ctx, crab_struct* const* structures, int32_t k, const double* q,
+                               const double* y, const double* sigma, int64_t nq, const crab_ensemble_options* eopt,
+                               const crab_fit_options* fopt, const double* partials, int32_t n_types,
+                               crab_ensemble_result* result, int32_t* selected, double* weights, double* fitted,
+                               double* intervals, double* bootstrap_chi2);
 /* Batched curves for k conformers at every (c1,c2) candidate: curves is
  * [n_cand][k][nq]; cand is n_cand (c1,c2) pairs. One persistent launch for
  * all conformers' partials, one recombination launch. */

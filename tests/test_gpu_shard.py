@@ -75,3 +75,67 @@ def test_sharded_basis_without_a_process_group_is_the_basis(engine):
     sp = cs.SolventParams(c2=0.3)
     whole = cs.debye_solvent_basis(s, q, sp, engine=engine)
     assert _close(S.sharded_debye_solvent_basis(s, q, sp, engine=engine), whole)
+
+
+def _ensemble(k, seed):
+    sizes = np.random.default_rng(seed).integers(150, 1500, size=k)
+    return [synth.protein(700 + i, int(n), 6.0 + 0.02 * n) for i, n in enumerate(sizes)]
+
+
+def _fitter(engine, confs, q, curve_index, hidden, **opts):
+    fo = cs.FitOptions(method=cs.ScatteringMethod.Debye)
+    curves = cs.ensemble_curves(confs, q, cs.SolventParams(), cs.solvent_candidates(fo), engine=engine)
+    rng = np.random.default_rng(len(confs))
+    w = rng.dirichlet(np.ones(len(hidden)))
+    clean = (w[:, None] * curves[curve_index][hidden]).sum(axis=0)
+    sigma = 0.01 * clean
+    ex = cs.ExperimentalCurve(q, clean + sigma * rng.normal(size=clean.shape), sigma)
+    names = [f"c{i}" for i in range(len(confs))]
+    return cs.EnsembleFitter(confs, names, ex, cs.EnsembleOptions(fit=fo, **opts), engine=engine)
+
+
+def test_ensemble_partials_shards_gather_every_conformer(engine):
+    """Each conformer's pair sums come from exactly one shard (split by N²,
+    longest first), and the shards' buffers sum to the unsplit buffer."""
+    confs = _ensemble(14, 5)
+    fitter = _fitter(engine, confs, np.linspace(0.005, 0.45, 90), 3, [1, 4])
+    T, whole = fitter.partials()
+    whole = whole.reshape(len(confs), -1)
+    n2 = np.array([c.atom_count ** 2 for c in confs], dtype=float)
+    for n in (2, 3, 5):
+        parts = [fitter.partials(shard=(k, n)) for k in range(n)]
+        assert all(p[0] == T for p in parts)
+        blocks = np.stack([p[1].reshape(len(confs), -1) for p in parts])
+        owned = np.abs(blocks).sum(-1) > 0
+        assert np.all(owned.sum(0) == 1)
+        assert _close(blocks.sum(0), whole)
+        loads = (owned * n2[None, :]).sum(1)
+        assert loads.max() <= n2.sum() / n + n2.max()
+
+
+def test_ensemble_fit_from_gathered_partials_matches_fit(engine):
+    """The fit from the summed shard buffers (what every rank runs after the
+    all-reduce) is EnsembleFitter.fit's: pruning, weights, best candidate and
+    the bootstrap."""
+    confs = _ensemble(10, 21)
+    fitter = _fitter(engine, confs, np.linspace(0.005, 0.45, 80), 6, [2, 5], min_weight=0.02, bootstrap=3)
+    ref = fitter.fit()
+    for n in (1, 3):
+        parts = [fitter.partials(shard=(k, n)) for k in range(n)]
+        got = fitter.fit_from_partials(parts[0][0], sum(p[1] for p in parts))
+        assert got.conformers == ref.conformers
+        assert (got.params.c1, got.params.c2) == (ref.params.c1, ref.params.c2)
+        np.testing.assert_allclose(got.weights, ref.weights, atol=1e-9)
+        assert got.reduced_chi2 == pytest.approx(ref.reduced_chi2, rel=1e-9)
+        np.testing.assert_allclose(got.fitted_curve, ref.fitted_curve, rtol=1e-9)
+        np.testing.assert_allclose(got.bootstrap_reduced_chi2, ref.bootstrap_reduced_chi2, rtol=1e-7)
+
+
+def test_ensemble_fit_from_partials_rejects_a_mismatched_buffer(engine):
+    confs = _ensemble(4, 8)
+    fitter = _fitter(engine, confs, np.linspace(0.01, 0.4, 30), 0, [0, 1])
+    T, buf = fitter.partials()
+    with pytest.raises(cs.InvalidInput):
+        fitter.fit_from_partials(T, buf[:-1])
+    with pytest.raises(cs.InvalidInput):
+        fitter.fit_from_partials(T + 1, np.zeros(len(confs) * ((T + 1) * (T + 2) // 2 * 30 + 2 * (T + 1))))
