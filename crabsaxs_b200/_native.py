@@ -90,6 +90,9 @@ I64 = C.c_int64
 I32P = C.POINTER(C.c_int32)
 I8P = C.POINTER(C.c_int8)
 
+# crab_sum_fn: in-place sum over GPUs of a host buffer of doubles
+SUM_FN = C.CFUNCTYPE(C.c_int, D, I64, P)
+
 _SIGS = {
     "crab_ctx_create": (C.c_int, [C.c_int, C.POINTER(P)]),
     "crab_ctx_destroy": (C.c_int, [P]),
@@ -124,6 +127,10 @@ _SIGS = {
     "crab_multipole_intensity": (C.c_int, [P, P, D, I64, C.c_int, C.c_int, C.c_int, D]),
     "crab_multipole_solvent_basis": (C.c_int, [P, P, D, I64, C.c_int, C.POINTER(Solvent), C.c_int, C.c_int, D]),
     "crab_multipole_last_timing": (C.c_int, [P, D, D, D]),
+    "crab_multipole_intensity_shard": (C.c_int, [P, P, D, I64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, SUM_FN,
+                                                 P, D]),
+    "crab_multipole_solvent_basis_shard": (C.c_int, [P, P, D, I64, C.c_int, C.POINTER(Solvent), C.c_int, C.c_int,
+                                                     C.c_int, C.c_int, SUM_FN, P, D]),
     "crab_fit": (C.c_int, [P, P, D, D, D, I64, C.POINTER(FitOpts), C.c_double, C.c_double,
                            C.POINTER(FitResult), D]),
     "crab_chi2_grad": (C.c_int, [P, P, D, D, D, I64, C.POINTER(Solvent), C.c_int, C.c_double, C.c_double, D, D, D]),

@@ -539,27 +539,70 @@ def solvent_corrected_intensity(structure, q, params: SolventParams, implicit_hy
     return combine_solvent_basis(b, q, params.c1, params.c2)
 
 
+class _MomentSum:
+    """crab_sum_fn around a Python function that sums a float64 array over
+    the ranks in place; an exception inside it ends the library call and is
+    raised again after it returns."""
+
+    def __init__(self, fn):
+        self.error = None
+
+        def call(values, count, user):
+            try:
+                fn(np.ctypeslib.as_array(values, shape=(count,)))
+                return N.OK
+            except BaseException as e:  # noqa: BLE001 - re-raised by check()
+                self.error = e
+                return N.EINVAL
+
+        self.c = N.SUM_FN(call)
+
+    def check(self, eng: "Engine", rc: int):
+        if self.error is not None:
+            raise self.error
+        eng.check(rc)
+
+
 def multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: bool = True,
-                        precision: int = N.PREC_TF32_SPLIT, engine: Optional[Engine] = None) -> np.ndarray:
-    """spherical.rs:266-403."""
+                        precision: int = N.PREC_TF32_SPLIT, engine: Optional[Engine] = None,
+                        shard: Optional[tuple[int, int]] = None, moment_sum=None) -> np.ndarray:
+    """spherical.rs:266-403.  shard=(k, n) with moment_sum(array) (an in-place
+    sum over the ranks): this rank's share of the atoms in the moments, the
+    whole curve returned (crab_multipole_intensity_shard)."""
     eng = engine or Engine.default()
     qa = _f64(q)
     out = np.empty(len(qa))
-    eng.check(N.lib.crab_multipole_intensity(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
-                                             1 if implicit_hydrogen else 0, precision, _dp(out)))
+    if shard is None:
+        eng.check(N.lib.crab_multipole_intensity(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
+                                                 1 if implicit_hydrogen else 0, precision, _dp(out)))
+    else:
+        cb = _MomentSum(moment_sum or (lambda a: None))
+        cb.check(eng, N.lib.crab_multipole_intensity_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
+                                                           l_max, 1 if implicit_hydrogen else 0, precision,
+                                                           int(shard[0]), int(shard[1]), cb.c, None, _dp(out)))
     return out
 
 
 def multipole_solvent_basis(structure: Structure, q, l_max: int, params: SolventParams,
                             implicit_hydrogen: bool = True, precision: int = N.PREC_TF32_SPLIT,
-                            engine: Optional[Engine] = None) -> np.ndarray:
-    """spherical.rs:474-565."""
+                            engine: Optional[Engine] = None, shard: Optional[tuple[int, int]] = None,
+                            moment_sum=None) -> np.ndarray:
+    """spherical.rs:474-565.  shard / moment_sum as in multipole_intensity
+    (crab_multipole_solvent_basis_shard)."""
     eng = engine or Engine.default()
     qa = _f64(q)
     out = np.empty((6, len(qa)))
     s = params.to_c()
-    eng.check(N.lib.crab_multipole_solvent_basis(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
-                                                 C.byref(s), 1 if implicit_hydrogen else 0, precision, _dp(out)))
+    if shard is None:
+        eng.check(N.lib.crab_multipole_solvent_basis(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
+                                                     C.byref(s), 1 if implicit_hydrogen else 0, precision,
+                                                     _dp(out)))
+    else:
+        cb = _MomentSum(moment_sum or (lambda a: None))
+        cb.check(eng, N.lib.crab_multipole_solvent_basis_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
+                                                               l_max, C.byref(s), 1 if implicit_hydrogen else 0,
+                                                               precision, int(shard[0]), int(shard[1]), cb.c, None,
+                                                               _dp(out)))
     return out
 
 

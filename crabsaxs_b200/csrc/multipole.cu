@@ -757,6 +757,13 @@ struct MpInput {
   double rmax_lq;                 // radius for the per-q order (atoms, or atoms and sites)
   std::vector<double> amp;        // K x T x nq amplitude combinations (no occupancy)
   int K = 1;
+  // multi-GPU: this rank takes the atoms [n*shard/n_shards, n*(shard+1)/n_shards)
+  // into its moments, and `sum` replaces them by the sum over all ranks
+  // before the q pass (the radial basis comes from all atoms, so every rank
+  // has the same moment layout)
+  int shard = 0, n_shards = 1;
+  crab_sum_fn sum = nullptr;
+  void* sum_user = nullptr;
 };
 
 // Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
@@ -770,6 +777,10 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const int64_t n = (int64_t)t.w.size();
   std::fill(out, out + (size_t)P * nq, 0.0);
   if (n == 0 || nq == 0) return;
+  require(in.n_shards >= 1 && in.shard >= 0 && in.shard < in.n_shards, "shard index out of range");
+  require(in.n_shards == 1 || in.sum, "a sharded multipole call needs the moment sum callback");
+  // atoms of this rank's moments (all of them unless sharded)
+  const int64_t own0 = n * in.shard / in.n_shards, own1 = n * (in.shard + 1) / in.n_shards;
   // geometry relative to the structure centroid (spherical.rs:165-199)
   std::vector<double> r(n);
   double R = 0.0, qmax = 0.0;
@@ -786,7 +797,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   // group = type * S + segment; points sorted by group, padded per group
   std::vector<int32_t> seg_of(n), group_of(n);
   std::vector<int64_t> count(G, 0);
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = own0; i < own1; ++i) {
     seg_of[i] = std::min(S - 1, (int)(r[i] / R * S));
     group_of[i] = t.type[i] * S + seg_of[i];
     ++count[group_of[i]];
@@ -807,7 +818,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     std::fill(pts + 5 * begin[G], pts + 5 * n_pad, 0.0);
     std::fill(seg + begin[G], seg + n_pad, 0);
   }
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = own0; i < own1; ++i) {
     const int64_t k = fill[group_of[i]]++;
     pts[5 * k] = t.xyz[3 * i] - in.centre[0];
     pts[5 * k + 1] = t.xyz[3 * i + 1] - in.centre[1];
@@ -886,13 +897,16 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     k_mp_prep<double><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                    d_inv, (double*)d_YT, (double*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
-    k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
-                                                                lm_pad, d_work, d_part);
+    if (!work.empty())  // empty only for a rank of a sharded call that owns no atoms
+      k_mp_moments<double><<<(unsigned)work.size(), 256, 0, s>>>((const double*)d_YT, (const double*)d_WT, n_pad,
+                                                                  lm_pad, d_work, d_part);
   } else {
     k_mp_prep<float><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                   d_inv, (float*)d_YT, (float*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
-    if (tc_terms == 0) {
+    if (work.empty()) {
+      // a rank of a sharded call that owns no atoms: k_mp_reduce writes zero moments
+    } else if (tc_terms == 0) {
       k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad,
                                                                  lm_pad, d_work, d_part);
     } else {
@@ -911,6 +925,19 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   k_mp_reduce<<<dim3((unsigned)(G * n_lmt), kReduceSplit), 256, 0, s>>>(d_part, d_gfirst, d_gsplits, n_lmt, lm_pad,
                                                                          d_M);
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
+  if (in.n_shards > 1) {
+    // every rank's moments summed by the caller (an all-reduce over the GPUs)
+    const size_t m_count = (size_t)G * kMaxNodes * lm_pad;
+    auto* h_M = (double*)ctx->host("mp_M", sizeof(double) * m_count);
+    int status = 0;
+    if (tc_terms) copy_d2h(ctx, &status, d_status, sizeof(int), s);
+    copy_d2h(ctx, h_M, d_M, sizeof(double) * m_count, s);
+    CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
+    const int rc = in.sum(h_M, (int64_t)m_count, in.sum_user);
+    if (rc != CRAB_OK) throw Error(rc, "the moment sum callback failed");
+    copy_h2d(ctx, d_M, h_M, sizeof(double) * m_count, s);
+  }
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;
   k_mp_node_bessel<<<(unsigned)((nbess + 127) / 128), 128, 0, s>>>(d_q, d_lq, nq, d_nodes, n_nodes, L, d_Jn);
@@ -950,7 +977,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   CRAB_CUDA_CHECK(cudaEventElapsedTime(&gemm_ms, ev[1], ev[2]));
   ctx->last_mp_ms = total_ms;
   ctx->last_mp_gemm_ms = gemm_ms;
-  ctx->last_mp_gemm_flop = 2.0 * (double)lm_count * nb * (double)n;  // useful rows, nodes and points
+  ctx->last_mp_gemm_flop = 2.0 * (double)lm_count * nb * (double)(own1 - own0);  // useful rows, nodes and points
 }
 
 // (fp64 operands, tensor-core TF32 terms) of a precision mode.
@@ -1038,7 +1065,7 @@ void solvent_setup(crab_ctx* ctx, const crab_struct* st, const double* q, int64_
 }  // namespace
 
 void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
-                              bool implicit, int precision, double* out) {
+                              bool implicit, int precision, double* out, const MpShard& shard) {
   validate_multipole(st, q, nq, l_max);
   const MpPrecision mp = multipole_precision(precision);
   if (st->n == 0) {
@@ -1060,12 +1087,17 @@ void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double
   }
   in.amp = V;
   in.K = 1;
+  in.shard = shard.shard;
+  in.n_shards = shard.n_shards;
+  in.sum = shard.sum;
+  in.sum_user = shard.user;
   multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
 
 void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
-                                  const crab_solvent& s, bool implicit, int precision, double* out6) {
+                                  const crab_solvent& s, bool implicit, int precision, double* out6,
+                                  const MpShard& shard) {
   validate_multipole(st, q, nq, l_max);
   validate_solvent(s);
   const MpPrecision mp = multipole_precision(precision);
@@ -1084,6 +1116,10 @@ void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const do
   in.amp.insert(in.amp.end(), u.V.begin(), u.V.end());
   in.amp.insert(in.amp.end(), u.E.begin(), u.E.end());
   in.amp.insert(in.amp.end(), u.H.begin(), u.H.end());
+  in.shard = shard.shard;
+  in.n_shards = shard.n_shards;
+  in.sum = shard.sum;
+  in.sum_user = shard.user;
   multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out6);
 }
 
@@ -1136,6 +1172,29 @@ int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q
   if (!ctx || !st || !solvent || (nq > 0 && !out6)) return CRAB_EINVAL;
   return guarded_impl(ctx, [&]() {
     multipole_solvent_basis_impl(ctx, st, q, nq, l_max, *solvent, implicit_hydrogen != 0, precision, out6);
+  });
+}
+
+int crab_multipole_intensity_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                   int implicit_hydrogen, int precision, int shard, int n_shards, crab_sum_fn sum,
+                                   void* user, double* out) {
+  if (!ctx || !st || (nq > 0 && !out) || n_shards < 1 || shard < 0 || shard >= n_shards || (n_shards > 1 && !sum))
+    return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() {
+    multipole_intensity_impl(ctx, st, q, nq, l_max, implicit_hydrogen != 0, precision, out,
+                             MpShard{shard, n_shards, sum, user});
+  });
+}
+
+int crab_multipole_solvent_basis_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                       const crab_solvent* solvent, int implicit_hydrogen, int precision, int shard,
+                                       int n_shards, crab_sum_fn sum, void* user, double* out6) {
+  if (!ctx || !st || !solvent || (nq > 0 && !out6) || n_shards < 1 || shard < 0 || shard >= n_shards ||
+      (n_shards > 1 && !sum))
+    return CRAB_EINVAL;
+  return guarded_impl(ctx, [&]() {
+    multipole_solvent_basis_impl(ctx, st, q, nq, l_max, *solvent, implicit_hydrogen != 0, precision, out6,
+                                 MpShard{shard, n_shards, sum, user});
   });
 }
 }

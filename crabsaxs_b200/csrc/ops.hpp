@@ -45,10 +45,19 @@ void combine_basis(const double* q, int64_t nq, const double* b, double c1, doub
 void centre_and_rmax(const crab_struct* st, double* c, double* rmax);
 
 // Multipole engine (multipole.cu).
+// Multi-GPU: with n_shards > 1 this rank's moments cover its share of the
+// atoms and `sum` (called once) replaces them by the sum over all ranks; the
+// output is then the whole result on every rank.
+struct MpShard {
+  int shard = 0, n_shards = 1;
+  crab_sum_fn sum = nullptr;
+  void* user = nullptr;
+};
 void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
-                              bool implicit, int precision, double* out);
+                              bool implicit, int precision, double* out, const MpShard& shard = MpShard());
 void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
-                                  const crab_solvent& s, bool implicit, int precision, double* out6);
+                                  const crab_solvent& s, bool implicit, int precision, double* out6,
+                                  const MpShard& shard = MpShard());
 void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
                                       const crab_solvent& s, bool implicit, int precision, double* out);
 

@@ -12,7 +12,10 @@ of the result, whose parts are zero where a rank did no work:
   type-pair partials (T(T+1)/2 x nq f64, 60 kB for 5 types at 500 q);
 - an ensemble: every conformer's raw pair sums (k blocks of T(T+1)/2 x nq +
   2T f64, about 9 MB for 256 conformers at 300 q), after which every rank
-  runs the same weight fit.
+  runs the same weight fit;
+- the multipole expansion: each rank's moments over its share of the atoms
+  (about 11 MB at 100k atoms and L = 50), after which every rank runs the q
+  pass.
 
 The reference runs on one host and has no counterpart; its loops over q and
 over conformers are split over threads (solvent.rs:528, ensemble.rs:244).
@@ -26,7 +29,7 @@ import numpy as np
 
 from . import _native as N
 from .api import (Engine, EnsembleFitter, EnsembleResult, InvalidInput, SolventParams, Structure, debye_partials,
-                  debye_solvent_basis)
+                  debye_solvent_basis, multipole_intensity, multipole_solvent_basis)
 
 
 def shard_assign(cost, n_shards: int) -> np.ndarray:
@@ -95,3 +98,31 @@ def sharded_ensemble_fit(fitter: EnsembleFitter, group=None) -> EnsembleResult:
     rank, world = _rank_world(group)
     n_types, part = fitter.partials(shard=(rank, world))
     return fitter.fit_from_partials(n_types, reduce_shards(part, group))
+
+
+def _in_place_sum(group):
+    def fn(a: np.ndarray) -> None:
+        a[:] = reduce_shards(a, group)
+
+    return fn
+
+
+def sharded_multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: bool = True,
+                                precision: int = N.PREC_TF32_SPLIT, group=None,
+                                engine: Optional[Engine] = None) -> np.ndarray:
+    """multipole_intensity over the ranks of ``group``: each rank's moments
+    cover its share of the atoms, one all-reduce of the moments (about 11 MB
+    at 100k atoms and L = 50), then every rank runs the q pass."""
+    rank, world = _rank_world(group)
+    return multipole_intensity(structure, q, l_max, implicit_hydrogen, precision, engine, shard=(rank, world),
+                               moment_sum=_in_place_sum(group))
+
+
+def sharded_multipole_solvent_basis(structure: Structure, q, l_max: int, params: SolventParams,
+                                    implicit_hydrogen: bool = True, precision: int = N.PREC_TF32_SPLIT, group=None,
+                                    engine: Optional[Engine] = None) -> np.ndarray:
+    """multipole_solvent_basis over the ranks of ``group`` (as
+    sharded_multipole_intensity)."""
+    rank, world = _rank_world(group)
+    return multipole_solvent_basis(structure, q, l_max, params, implicit_hydrogen, precision, engine,
+                                   shard=(rank, world), moment_sum=_in_place_sum(group))

@@ -314,6 +314,27 @@ int crab_multipole_last_timing(crab_ctx* ctx, double* total_ms, double* moments_
 /* multipole_solvent_basis (spherical.rs:474-565), out6 [6][nq]. */
 int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                                  const crab_solvent* solvent, int implicit_hydrogen, int precision, double* out6);
+/* Sum over GPUs supplied by the caller: replace values[0..count) in place by
+ * their element-wise sum over all ranks (an all-reduce: NCCL, MPI, ...) and
+ * return CRAB_OK; any other return ends the call with that status. */
+typedef int (*crab_sum_fn)(double* values, int64_t count, void* user);
+/* Multi-GPU multipole (one process and context per GPU; no counterpart in
+ * the reference, which splits its q loop over threads, spherical.rs:337-394).
+ * Every rank passes the whole structure; rank `shard` of `n_shards` takes the
+ * atoms (and hydration sites) [n*shard/n_shards, n*(shard+1)/n_shards) of
+ * the typed list into its moments M^t_{lm,b} (the radial basis and centre
+ * come from all atoms, so every rank has the same moment layout).  `sum` is
+ * called once, with this rank's moments in host memory
+ * (types x segments x 64 x (L+1)^2 rounded up to 128, about 11 MB for 100k
+ * atoms at L = 50); after it returns the rank runs the q pass, so every rank
+ * returns the whole curve / basis.  n_shards == 1 needs no `sum` and is the
+ * unsharded call. */
+int crab_multipole_intensity_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                   int implicit_hydrogen, int precision, int shard, int n_shards, crab_sum_fn sum,
+                                   void* user, double* out);
+int crab_multipole_solvent_basis_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
+                                       const crab_solvent* solvent, int implicit_hydrogen, int precision, int shard,
+                                       int n_shards, crab_sum_fn sum, void* user, double* out6);
 
 /* ---- fitting and gradients --------------------------------------------- */
 /* fit_to_experimental_with_options (fit.rs:288-454). fitted (nq) may be NULL. */

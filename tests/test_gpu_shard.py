@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import crabsaxs_b200 as cs
+from crabsaxs_b200 import _native as N
 from crabsaxs_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -139,3 +140,93 @@ def test_ensemble_fit_from_partials_rejects_a_mismatched_buffer(engine):
         fitter.fit_from_partials(T, buf[:-1])
     with pytest.raises(cs.InvalidInput):
         fitter.fit_from_partials(T + 1, np.zeros(len(confs) * ((T + 1) * (T + 2) // 2 * 30 + 2 * (T + 1))))
+
+
+class _Stop(Exception):
+    pass
+
+
+def _moments_of_every_shard(call, n):
+    """Each shard's moments, taken in its sum callback, which then raises:
+    the library call ends with an error and the exception comes back."""
+    got = []
+    for k in range(n):
+        def grab(a):
+            got.append(a.copy())
+            raise _Stop()
+
+        with pytest.raises(_Stop):
+            call(shard=(k, n), moment_sum=grab)
+    return got
+
+
+def _sharded_results(call, n, total):
+    def put(a):
+        a[:] = total
+
+    return [call(shard=(k, n), moment_sum=put) for k in range(n)]
+
+
+@pytest.mark.parametrize("precision,rtol", [(N.PREC_FP64, 1e-12), (N.PREC_TF32_SPLIT, 2e-6)])
+def test_multipole_moments_of_the_shards_sum_to_the_whole(engine, precision, rtol):
+    """Moments are linear in the atoms: the shards' moments summed (the
+    all-reduce) give the unsplit curve on every rank.  FP64 differs only in
+    the order of additions; the TF32 split groups its FP32 accumulations
+    differently, within its own 5e-7 error."""
+    s = synth.protein(36, 5000, 24.0)
+    q = np.linspace(0.001, 0.5, 120)
+
+    def call(**kw):
+        return cs.multipole_intensity(s, q, 30, precision=precision, engine=engine, **kw)
+
+    whole = call()
+    for n in (2, 3):
+        parts = _moments_of_every_shard(call, n)
+        assert len({p.size for p in parts}) == 1 and all(np.any(p != 0.0) for p in parts)
+        for got in _sharded_results(call, n, sum(parts)):
+            assert np.max(np.abs(got - whole)) <= rtol * np.max(whole)
+
+
+def test_multipole_solvent_basis_shards_with_grid_sites(engine):
+    """The hydration sites are part of the typed list the shards divide."""
+    s = synth.protein(37, 3000, 20.0)
+    q = np.linspace(0.001, 0.4, 80)
+    sp = cs.SolventParams(c1=1.01, c2=0.8, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                          hydration_grid_spacing_angstrom=3.0)
+
+    def call(**kw):
+        return cs.multipole_solvent_basis(s, q, 25, sp, precision=N.PREC_FP64, engine=engine, **kw)
+
+    whole = call()
+    parts = _moments_of_every_shard(call, 4)
+    for got in _sharded_results(call, 4, sum(parts)):
+        assert np.max(np.abs(got - whole)) <= 1e-12 * np.max(np.abs(whole))
+
+
+def test_multipole_more_shards_than_atoms(engine):
+    s = cs.Structure(np.array([[0.0, 0.0, 0.0], [3.0, 0.5, -1.0], [-2.0, 2.5, 1.0]]), np.array([1, 2, 3]))
+    q = np.linspace(0.01, 0.5, 30)
+
+    def call(**kw):
+        return cs.multipole_intensity(s, q, 12, precision=N.PREC_FP64, engine=engine, **kw)
+
+    whole = call()
+    parts = _moments_of_every_shard(call, 5)
+    assert sum(1 for p in parts if not p.any()) == 2
+    for got in _sharded_results(call, 5, sum(parts)):
+        assert np.max(np.abs(got - whole)) <= 1e-12 * np.max(whole)
+
+
+def test_multipole_shard_needs_a_sum(engine):
+    """A NULL sum callback (N.SUM_FN()) is refused for two or more shards."""
+    s = synth.protein(38, 300, 9.0)
+    q = np.linspace(0.01, 0.3, 10)
+    out = np.empty(10)
+    rc = N.lib.crab_multipole_intensity_shard(engine.handle, s.handle(engine), q.ctypes.data_as(N.D), 10, 10, 1,
+                                              N.PREC_FP64, 0, 2, N.SUM_FN(), None, out.ctypes.data_as(N.D))
+    assert rc == N.EINVAL
+    # one shard needs no sum: the unsplit call
+    rc = N.lib.crab_multipole_intensity_shard(engine.handle, s.handle(engine), q.ctypes.data_as(N.D), 10, 10, 1,
+                                              N.PREC_FP64, 0, 1, N.SUM_FN(), None, out.ctypes.data_as(N.D))
+    assert rc == N.OK and np.allclose(out, cs.multipole_intensity(s, q, 10, precision=N.PREC_FP64, engine=engine),
+                                      rtol=1e-12)
