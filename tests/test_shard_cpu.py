@@ -88,8 +88,11 @@ def _rank(rank, world, port, out):
         if o == rank:
             part += _pair_sum(xyz, w, q, it, jt)
     total = S.reduce_shards(part)
+    # the multipole moment exchange: an in-place sum of a host buffer
+    moments = np.full(7, rank + 1.0)
+    S._in_place_sum(None)(moments)
     dist.destroy_process_group()
-    out.put((rank, int((owner == rank).sum()), total))
+    out.put((rank, int((owner == rank).sum()), total, moments))
 
 
 @pytest.mark.parametrize("world", [2, 3])
@@ -110,9 +113,10 @@ def test_gloo_ranks_sum_their_shares_to_the_whole(world):
     # every pair i < j exactly once: at q = 0 the sum is ((Σw)² - Σw²)/2
     assert whole[0] == pytest.approx((w.sum() ** 2 - (w * w).sum()) / 2.0, rel=1e-12)
     assert sum(g[1] for g in got) == len(items) and all(g[1] > 0 for g in got)
-    for _, _, total in got:
+    for _, _, total, moments in got:
         assert np.max(np.abs(total - whole)) <= 1e-12 * np.max(np.abs(whole))
         assert np.array_equal(total, got[0][2])  # every rank holds the same sum
+        assert np.all(moments == world * (world + 1) / 2)
 
 
 def test_reduce_without_a_process_group_is_the_identity():
