@@ -190,3 +190,40 @@ def test_grid_size_query_then_fill_with_other_arguments(engine):
     for _ in range(2):
         rc, _, got = _grid_call(engine, "exterior", s1, ext1, big)
         assert rc == N.OK and np.array_equal(got, ref[("exterior", 1)])
+
+
+def _corners(half):
+    return np.array([[x, y, z] for x in (-half, half) for y in (-half, half) for z in (-half, half)], float)
+
+
+def _workspace(engine):
+    import ctypes as C
+
+    from crabsaxs_b200 import _native as N
+
+    b = C.c_int64()
+    assert N.lib.crab_ctx_workspace_bytes(engine.handle, C.byref(b)) == N.OK
+    return b.value
+
+
+def test_exterior_grid_large_box(engine):
+    """Eight atoms at the corners of a 400 Å cube: a 71-million-voxel box at
+    1 Å (the limit is 250 million), bit-exact against the oracle's BFS."""
+    xyz = _corners(200.0) + np.array([0.31, -0.17, 0.05])
+    el = np.full(8, 1, np.int32)
+    got, gv = cs.hydration_grid_exterior(cs.Structure(xyz, el), 1.0, engine=engine)
+    ref, rv = O.exterior_grid(xyz, el, 1.0)
+    assert gv == rv and got.shape == ref.shape and np.array_equal(got, ref)
+
+
+def test_adaptive_grid_large_box_releases_its_masks(engine):
+    """A 321-million-voxel adaptive box (corners of a 660 Å cube, 1 Å):
+    bit-exact, and its two 321 MB voxel masks leave the context's buffer
+    pool when the call returns (grid slots above 256 MB are not kept)."""
+    xyz = _corners(330.0)
+    before = _workspace(engine)
+    got, gv = cs.hydration_grid_adaptive(cs.Structure(xyz, np.full(8, 1)), 1.0, engine=engine)
+    after = _workspace(engine)
+    ref, rv = O.adaptive_grid(xyz, 1.0)
+    assert gv == rv and got.shape == ref.shape and np.array_equal(got, ref)
+    assert after - before < (64 << 20)
