@@ -28,16 +28,21 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
 #include "engine.hpp"
 
+// Atom names, residue names and chain ids have few distinct values: each
+// atom holds an index into the field's table of distinct strings.
 struct crab_parsed {
   std::vector<double> xyz, occ;
   std::vector<int8_t> element, group, hetatm;
   std::vector<int64_t> residue_id;
-  std::vector<std::string> atom_name, residue_name, chain_id;
+  std::vector<uint32_t> text_id[3];           // per atom: atom name, residue name, chain id
+  std::vector<std::string> text_table[3];     // distinct strings of each field
+  const std::string& text(int which, size_t i) const { return text_table[which][text_id[which][i]]; }
 };
 
 namespace crab {
@@ -54,10 +59,13 @@ struct ParseFail {
 
 struct Record {
   bool hetatm = false;
+  int8_t el = -1;  // element code of the element column or the atom name (-1: not yet looked up)
   std::string name, alt, resname, chain, icode, element;
   int64_t resseq = 0;
   double x = 0, y = 0, z = 0, occ = 1.0;
 };
+
+int element_from_symbol(const std::string& s);
 
 std::string trim(const std::string& s) {
   size_t a = 0, b = s.size();
@@ -161,14 +169,32 @@ double column_number(const char* line, size_t n, size_t from, size_t to, const c
   return number(field(line, n, from, to), what, line_no);
 }
 
+// The records of a file and its models: the records stay where the reader
+// stored them (one vector per reader chunk), and each model lists its
+// records in file order by address, so no record is moved or copied.
+struct Models {
+  std::vector<std::vector<Record>> store;
+  std::vector<std::vector<const Record*>> list;
+};
+
 // PDB fixed columns (wwPDB format 3.3): ATOM/HETATM 1-6, name 13-16, altLoc 17,
 // resName 18-20, chainID 22, resSeq 23-26, iCode 27, x 31-38, y 39-46,
 // z 47-54, occupancy 55-60, element 77-78.  Models are MODEL ... ENDMDL.
-std::vector<std::vector<Record>> read_pdb(const char* text, int64_t len) {
-  std::vector<std::vector<Record>> models;
-  int64_t line_no = 0;
-  const char* p = text;
-  const char* end = text + len;
+//
+// The lines of one chunk of the text: its records in order, where MODEL
+// records fall among them, and its line count.
+struct PdbChunk {
+  std::vector<Record> recs;
+  std::vector<size_t> model_starts;  // index in recs of the first record after each MODEL line
+  int64_t lines = 0;
+  bool failed = false;
+};
+
+// Parses the whole lines of [p, end) (line numbers from first_line); a
+// malformed record throws ParseFail naming its line.
+void parse_pdb_lines(const char* p, const char* end, int64_t first_line, PdbChunk& c) {
+  int64_t line_no = first_line - 1;
+  c.recs.reserve((size_t)(end - p) / 81 + 16);  // about 81 bytes a record
   while (p < end) {
     const char* nl = (const char*)memchr(p, '\n', (size_t)(end - p));
     const char* line = p;
@@ -176,23 +202,18 @@ std::vector<std::vector<Record>> read_pdb(const char* text, int64_t len) {
     if (n && line[n - 1] == '\r') --n;
     p = nl ? nl + 1 : end;
     ++line_no;
+    ++c.lines;
     auto starts = [&](const char* tag) {
       const size_t k = std::strlen(tag);
       return n >= k && std::memcmp(line, tag, k) == 0;
     };
-    // a new model reserves for the rest of the text at about 81 bytes a record
-    auto new_model = [&]() {
-      models.emplace_back();
-      models.back().reserve((size_t)(end - p) / 81 + 16);
-    };
     if (starts("MODEL")) {
-      new_model();
+      c.model_starts.push_back(c.recs.size());
       continue;
     }
     const bool het = starts("HETATM");
     const bool atom = !het && starts("ATOM") && (n == 4 || line[4] == ' ');
     if (!atom && !het) continue;
-    if (models.empty()) new_model();  // records outside MODEL/ENDMDL join the current model
     Record r;
     r.hetatm = het;
     r.name = field(line, n, 13, 16);
@@ -209,7 +230,77 @@ std::vector<std::vector<Record>> read_pdb(const char* text, int64_t len) {
     r.occ = blank_occ ? 1.0 : column_number(line, n, 55, 60, "occupancy", line_no);
     r.element = field(line, n, 77, 78);
     if (r.name.empty()) fail(CRAB_EPARSE, "line " + std::to_string(line_no) + ": missing atom name");
-    models.back().push_back(std::move(r));
+    r.el = (int8_t)element_from_symbol(r.element.empty() ? r.name : r.element);
+    c.recs.push_back(std::move(r));
+  }
+}
+
+// Texts above this size are parsed by several threads, one chunk of whole
+// lines each (at least this many bytes a chunk); selections above
+// kParallelFillAtoms atoms fill their output arrays on several threads.
+constexpr int64_t kParallelParseBytes = 1 << 20;
+constexpr int64_t kParseChunkBytes = 1 << 19;
+constexpr size_t kParallelFillAtoms = 1 << 14;
+
+// Every MODEL record starts a model; records outside MODEL/ENDMDL join the
+// current model (a first one if there is none).  Chunks are stitched in
+// order, so the models are those of one pass over the text.  A chunk that
+// failed is parsed again alone from its first line number, which raises the
+// error of its first malformed line: the first in the text, since the
+// chunks before it parsed cleanly.
+Models read_pdb(const char* text, int64_t len) {
+  const int64_t hw = std::max<int64_t>(1, (int64_t)std::thread::hardware_concurrency());
+  const int n_chunks =
+      len < kParallelParseBytes ? 1 : (int)std::min<int64_t>({hw, (int64_t)16, len / kParseChunkBytes});
+  std::vector<const char*> cut(n_chunks + 1);
+  cut[0] = text;
+  cut[n_chunks] = text + len;
+  for (int k = 1; k < n_chunks; ++k) {
+    const char* at = std::max(cut[k - 1], text + len * k / n_chunks);
+    const char* nl = (const char*)memchr(at, '\n', (size_t)(text + len - at));
+    cut[k] = nl ? nl + 1 : text + len;
+  }
+  std::vector<PdbChunk> chunks(n_chunks);
+  auto run = [&](int k) {
+    try {
+      parse_pdb_lines(cut[k], cut[k + 1], 1, chunks[k]);
+    } catch (...) {
+      chunks[k].failed = true;
+    }
+  };
+  if (n_chunks == 1) {
+    parse_pdb_lines(text, text + len, 1, chunks[0]);
+  } else {
+    std::vector<std::thread> pool;
+    for (int k = 1; k < n_chunks; ++k) pool.emplace_back(run, k);
+    run(0);
+    for (auto& t : pool) t.join();
+  }
+  Models models;
+  int64_t first_line = 1;
+  for (int k = 0; k < n_chunks; ++k) {
+    PdbChunk& c = chunks[k];
+    if (c.failed) {
+      PdbChunk again;
+      parse_pdb_lines(cut[k], cut[k + 1], first_line, again);  // throws the error
+      c = std::move(again);
+    }
+    first_line += c.lines;
+    const size_t n_seg = c.model_starts.size();
+    auto append = [&](size_t from, size_t to) {
+      std::vector<const Record*>& m = models.list.back();
+      for (size_t i = from; i < to; ++i) m.push_back(&c.recs[i]);
+    };
+    const size_t head_end = n_seg ? c.model_starts[0] : c.recs.size();
+    if (head_end > 0) {
+      if (models.list.empty()) models.list.emplace_back();
+      append(0, head_end);
+    }
+    for (size_t s = 0; s < n_seg; ++s) {
+      models.list.emplace_back();
+      append(c.model_starts[s], s + 1 < n_seg ? c.model_starts[s + 1] : c.recs.size());
+    }
+    models.store.push_back(std::move(c.recs));  // moving the vector keeps the records' addresses
   }
   return models;
 }
@@ -239,7 +330,7 @@ std::vector<std::string> cif_tokens(const std::string& line) {
   return t;
 }
 
-std::vector<std::vector<Record>> read_cif(const char* text, int64_t len) {
+std::vector<std::vector<Record>> read_cif_records(const char* text, int64_t len) {
   std::istringstream in(std::string(text, (size_t)len));
   std::string line;
   std::vector<std::string> cols;
@@ -374,10 +465,7 @@ std::string residue_key(const Record& r) {
 
 // Blank-altloc atoms of a residue that also has named altlocs go into every
 // named conformer with occupancy / (named + 1), in the named conformers' order.
-std::vector<Record> expand_conformers(const std::vector<Record>& in) {
-  bool any_alt = false;
-  for (const Record& r : in) any_alt = any_alt || !r.alt.empty();
-  if (!any_alt) return in;
+std::vector<Record> expand_conformers(const std::vector<const Record*>& in) {
   struct Res {
     std::vector<size_t> atoms;
     std::vector<std::string> alts;
@@ -385,7 +473,7 @@ std::vector<Record> expand_conformers(const std::vector<Record>& in) {
   std::vector<Res> res;
   std::unordered_map<std::string, size_t> index;
   for (size_t i = 0; i < in.size(); ++i) {
-    const std::string key = residue_key(in[i]);
+    const std::string key = residue_key(*in[i]);
     auto it = index.find(key);
     if (it == index.end()) {
       it = index.emplace(key, res.size()).first;
@@ -393,14 +481,14 @@ std::vector<Record> expand_conformers(const std::vector<Record>& in) {
     }
     Res& r = res[it->second];
     r.atoms.push_back(i);
-    if (!in[i].alt.empty() && std::find(r.alts.begin(), r.alts.end(), in[i].alt) == r.alts.end())
-      r.alts.push_back(in[i].alt);
+    if (!in[i]->alt.empty() && std::find(r.alts.begin(), r.alts.end(), in[i]->alt) == r.alts.end())
+      r.alts.push_back(in[i]->alt);
   }
   std::vector<Record> out;
   out.reserve(in.size());
   for (const Res& r : res) {
     for (size_t i : r.atoms) {
-      const Record& a = in[i];
+      const Record& a = *in[i];
       if (!a.alt.empty() || r.alts.empty()) {
         out.push_back(a);
         continue;
@@ -444,12 +532,17 @@ struct Ranks {
   }
 };
 
-crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_options& o) {
+crab_parsed* select_atoms(const std::vector<const Record*>& model_in, const crab_parse_options& o) {
   std::vector<Record> expanded;
+  std::vector<const Record*> expanded_list;
   bool any_alt = false;
-  for (const Record& r : model_in) any_alt = any_alt || !r.alt.empty();
-  if (any_alt) expanded = expand_conformers(model_in);
-  const std::vector<Record>& model = any_alt ? expanded : model_in;
+  for (const Record* r : model_in) any_alt = any_alt || !r->alt.empty();
+  if (any_alt) {
+    expanded = expand_conformers(model_in);
+    expanded_list.reserve(expanded.size());
+    for (const Record& r : expanded) expanded_list.push_back(&r);
+  }
+  const std::vector<const Record*>& model = any_alt ? expanded_list : model_in;
   std::vector<std::string> chains;
   for (int32_t k = 0; k < o.n_chains; ++k) chains.emplace_back(o.chains[k] ? o.chains[k] : "");
   static const std::string kUnk("UNK");
@@ -463,7 +556,7 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
   kept.reserve(model.size());
   Ranks chain_r, icode_r, name_r, res_r;
   for (uint32_t i = 0; i < (uint32_t)model.size(); ++i) {
-    const Record& r = model[i];
+    const Record& r = *model[i];
     const std::string& resname = r.resname.empty() ? kUnk : r.resname;
     if (o.n_chains > 0 && std::find(chains.begin(), chains.end(), r.chain) == chains.end()) continue;
     if (r.hetatm) {
@@ -471,7 +564,7 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
       if (kind == kWater && !o.include_waters) continue;
       if (!o.include_hetatm && !(o.include_glycans && kind == kGlycan)) continue;
     }
-    const int el = element_from_symbol(r.element.empty() ? r.name : r.element);
+    const int el = r.el >= 0 ? r.el : element_from_symbol(r.element.empty() ? r.name : r.element);
     if (el == CRAB_EL_OTHER && !o.allow_unknown_elements) fail(CRAB_EELEMENT, "unsupported element: " + r.name);
     kept.push_back({i, chain_r.add(r.chain), icode_r.add(r.icode), name_r.add(r.name), res_r.add(resname), el});
   }
@@ -489,7 +582,7 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
   std::vector<Key> keys(kept.size());
   for (uint32_t k = 0; k < (uint32_t)kept.size(); ++k) {
     const Kept& e = kept[k];
-    const uint64_t seq = (uint64_t)((int64_t)model[e.rec].resseq + ((int64_t)1 << 40));
+    const uint64_t seq = (uint64_t)((int64_t)model[e.rec]->resseq + ((int64_t)1 << 40));
     keys[k] = {((uint64_t)chain_r.rank[e.chain] << 42) | (seq & (((uint64_t)1 << 42) - 1)),
                ((uint64_t)name_r.rank[e.name] << 32) | icode_r.rank[e.icode], k};
   }
@@ -527,7 +620,7 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
   };
   std::vector<Out> atoms;
   atoms.reserve(groups.size());
-  auto occ_of = [&](size_t s) { return std::max(model[kept[keys[s].k].rec].occ, 0.0); };
+  auto occ_of = [&](size_t s) { return std::max(model[kept[keys[s].k].rec]->occ, 0.0); };
   for (const Group& g : groups) {
     if (o.altloc_policy == CRAB_ALTLOC_ALL) {
       for (size_t s = g.begin; s < g.end; ++s) atoms.push_back({keys[s].k, occ_of(s)});
@@ -535,10 +628,10 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
     }
     const size_t count = g.end - g.begin;
     const bool has_alt = count > 1;
-    const Record& r0 = model[kept[keys[g.begin].k].rec];
+    const Record& r0 = *model[kept[keys[g.begin].k].rec];
     bool same_pos = has_alt;
     for (size_t s = g.begin + 1; s < g.end && same_pos; ++s) {
-      const Record& r = model[kept[keys[s].k].rec];
+      const Record& r = *model[kept[keys[s].k].rec];
       same_pos = r.x == r0.x && r.y == r0.y && r.z == r0.z;
     }
     size_t pick = g.begin;
@@ -559,28 +652,45 @@ crab_parsed* select_atoms(const std::vector<Record>& model_in, const crab_parse_
   p->group.resize(n);
   p->hetatm.resize(n);
   p->residue_id.resize(n);
-  p->atom_name.resize(n);
-  p->residue_name.resize(n);
-  p->chain_id.resize(n);
-  std::unordered_map<uint64_t, int8_t> group_cache;  // (residue name, atom name) -> united-atom group
-  for (size_t i = 0; i < n; ++i) {
-    const Kept& e = kept[atoms[i].k];
-    const Record& r = model[e.rec];
-    p->xyz[3 * i] = r.x;
-    p->xyz[3 * i + 1] = r.y;
-    p->xyz[3 * i + 2] = r.z;
-    p->occ[i] = atoms[i].occ;
-    p->element[i] = (int8_t)e.element;
-    p->residue_name[i] = *res_r.str[e.resname];
-    const uint64_t gk = ((uint64_t)e.resname << 32) | e.name;
-    auto it = group_cache.find(gk);
-    if (it == group_cache.end())
-      it = group_cache.emplace(gk, (int8_t)united_atom_group(p->residue_name[i].c_str(), r.name.c_str())).first;
-    p->group[i] = it->second;
-    p->hetatm[i] = r.hetatm ? 1 : 0;
-    p->residue_id[i] = r.resseq;
-    p->atom_name[i] = r.name;
-    p->chain_id[i] = r.chain;
+  const Ranks* fields[3] = {&name_r, &res_r, &chain_r};
+  for (int f = 0; f < 3; ++f) {
+    p->text_id[f].resize(n);
+    for (const std::string* str : fields[f]->str) p->text_table[f].push_back(*str);
+  }
+  // every atom's fields are independent: large structures fill them in
+  // ranges on several threads, each with its own group cache
+  auto fill = [&](size_t a, size_t b) {
+    std::unordered_map<uint64_t, int8_t> group_cache;  // (residue name, atom name) -> united-atom group
+    for (size_t i = a; i < b; ++i) {
+      const Kept& e = kept[atoms[i].k];
+      const Record& r = *model[e.rec];
+      p->xyz[3 * i] = r.x;
+      p->xyz[3 * i + 1] = r.y;
+      p->xyz[3 * i + 2] = r.z;
+      p->occ[i] = atoms[i].occ;
+      p->element[i] = (int8_t)e.element;
+      p->text_id[0][i] = e.name;
+      p->text_id[1][i] = e.resname;
+      p->text_id[2][i] = e.chain;
+      const uint64_t gk = ((uint64_t)e.resname << 32) | e.name;
+      auto it = group_cache.find(gk);
+      if (it == group_cache.end())
+        it = group_cache.emplace(gk, (int8_t)united_atom_group(res_r.str[e.resname]->c_str(), r.name.c_str())).first;
+      p->group[i] = it->second;
+      p->hetatm[i] = r.hetatm ? 1 : 0;
+      p->residue_id[i] = r.resseq;
+    }
+  };
+  const size_t n_fill = n < kParallelFillAtoms ? 1
+                                               : std::min<size_t>({(size_t)std::max(1u, std::thread::hardware_concurrency()),
+                                                                   16, n / (kParallelFillAtoms / 2)});
+  if (n_fill <= 1) {
+    fill(0, n);
+  } else {
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < n_fill; ++k) pool.emplace_back(fill, n * k / n_fill, n * (k + 1) / n_fill);
+    fill(0, n / n_fill);
+    for (auto& t : pool) t.join();
   }
   return p;
 }
@@ -593,9 +703,16 @@ bool looks_like_cif(const char* text, int64_t len) {
   return head.find("_atom_site.") != std::string::npos;
 }
 
-std::vector<std::vector<Record>> read_models(const char* text, int64_t len, int format) {
+Models read_models(const char* text, int64_t len, int format) {
   const bool cif = format == CRAB_FORMAT_MMCIF || (format == CRAB_FORMAT_AUTO && looks_like_cif(text, len));
-  return cif ? read_cif(text, len) : read_pdb(text, len);
+  if (!cif) return read_pdb(text, len);
+  Models m;
+  m.store = read_cif_records(text, len);
+  for (const auto& v : m.store) {
+    m.list.emplace_back();
+    for (const Record& r : v) m.list.back().push_back(&r);
+  }
+  return m;
 }
 
 template <class F>
@@ -654,10 +771,10 @@ int crab_parse_structure(const char* text, int64_t len, int32_t format, const cr
     if (len < 0) fail(CRAB_EINVAL, "negative text length");
     if (format < CRAB_FORMAT_AUTO || format > CRAB_FORMAT_MMCIF) fail(CRAB_EINVAL, "unknown format");
     validate(options);
-    auto models = read_models(text, len, format);
-    if ((size_t)options->model_index >= models.size())
+    const Models models = read_models(text, len, format);
+    if ((size_t)options->model_index >= models.list.size())
       fail(CRAB_EPARSE, "model " + std::to_string(options->model_index) + " is not present");
-    *out = select_atoms(models[(size_t)options->model_index], *options);
+    *out = select_atoms(models.list[(size_t)options->model_index], *options);
   });
 }
 
@@ -665,7 +782,7 @@ int crab_parse_model_count(const char* text, int64_t len, int32_t format, int32_
   if (!n_models) return CRAB_EINVAL;
   return parse_guard([&]() {
     if ((!text && len > 0) || len < 0) fail(CRAB_EINVAL, "invalid text");
-    *n_models = (int32_t)read_models(text, len, format).size();
+    *n_models = (int32_t)read_models(text, len, format).list.size();
   });
 }
 
@@ -701,25 +818,27 @@ int crab_parsed_arrays(const crab_parsed* p, double* xyz, double* occupancy, int
 }
 
 const char* crab_parsed_atom_name(const crab_parsed* p, int64_t i) {
-  return (p && i >= 0 && (size_t)i < p->atom_name.size()) ? p->atom_name[(size_t)i].c_str() : nullptr;
+  return (p && i >= 0 && (size_t)i < p->occ.size()) ? p->text(0, (size_t)i).c_str() : nullptr;
 }
 const char* crab_parsed_residue_name(const crab_parsed* p, int64_t i) {
-  return (p && i >= 0 && (size_t)i < p->residue_name.size()) ? p->residue_name[(size_t)i].c_str() : nullptr;
+  return (p && i >= 0 && (size_t)i < p->occ.size()) ? p->text(1, (size_t)i).c_str() : nullptr;
 }
 const char* crab_parsed_chain_id(const crab_parsed* p, int64_t i) {
-  return (p && i >= 0 && (size_t)i < p->chain_id.size()) ? p->chain_id[(size_t)i].c_str() : nullptr;
+  return (p && i >= 0 && (size_t)i < p->occ.size()) ? p->text(2, (size_t)i).c_str() : nullptr;
 }
 
 int crab_parsed_strings(const crab_parsed* p, int32_t which, char* buf, int64_t cap, int64_t* len) {
   if (!p || !len || which < 0 || which > 2 || cap < 0 || (cap > 0 && !buf)) return CRAB_EINVAL;
-  const auto& v = which == 0 ? p->atom_name : (which == 1 ? p->residue_name : p->chain_id);
+  const std::vector<uint32_t>& ids = p->text_id[which];
+  const std::vector<std::string>& table = p->text_table[which];
   int64_t need = 0;
-  for (const auto& x : v) need += (int64_t)x.size() + 1;
+  for (uint32_t id : ids) need += (int64_t)table[id].size() + 1;
   *len = need;
   if (!buf) return CRAB_OK;
   if (cap < need) return CRAB_ECAPACITY;
   char* o = buf;
-  for (const auto& x : v) {
+  for (uint32_t id : ids) {
+    const std::string& x = table[id];
     std::memcpy(o, x.data(), x.size());
     o += x.size();
     *o++ = '\n';

@@ -321,3 +321,78 @@ def test_calc_of_the_example_structure_with_adaptive_hydration(engine):  # tests
     a = O.Atoms(s.xyz, s.element, s.group, s.occupancy)
     ref = O.multipole_solvent_intensity(a, q, l_max, c1=1.0, c2=0.02, model=2, spacing=4.0)
     assert np.max(np.abs(got.intensity - ref) / np.abs(ref)) <= 1e-5
+
+
+# ---------------------------------------------------------------- large files
+# Texts above 1 MB are read by several threads, one chunk of whole lines each,
+# and stitched in order; these cases cross many chunk boundaries.
+def _big_models(seed, n_models):
+    rng = np.random.default_rng(seed)
+    return _records(rng, n_models)
+
+
+def _big_text(models, head=None, crlf=False):
+    text = _pdb_text(models)
+    if head is not None:  # records before the first MODEL line
+        text = _pdb_text([head]).replace("END\n", "") + text
+    return text.replace("\n", "\r\n") if crlf else text
+
+
+@pytest.mark.parametrize("crlf", [False, True])
+def test_large_multi_model_pdb_matches_the_restatement(crlf):
+    models = _big_models(41, 330)
+    text = _big_text(models, crlf=crlf)
+    assert len(text) > (1 << 20)
+    n = ctypes_model_count(text)
+    assert n == 330
+    for k in (0, 1, 164, 329):
+        opt = cs.ParseOptions(model_index=k, include_hetatm=True, allow_unknown_elements=True)
+        oopt = OS.Options(model_index=k, include_hetatm=True, allow_unknown_elements=True)
+        ref = _oracle_tuples(OS.parse(text.replace("\r\n", "\n"), oopt))
+        assert _as_tuples(cs.Structure.from_text(text, opt)) == ref, k
+
+
+def test_large_pdb_with_records_before_the_first_model():
+    models = _big_models(42, 300)
+    head = _big_models(43, 1)[0]
+    text = _big_text(models, head=head)
+    assert len(text) > (1 << 20) and ctypes_model_count(text) == 301
+    for k in (0, 1, 300):
+        opt = cs.ParseOptions(model_index=k, include_hetatm=True, allow_unknown_elements=True)
+        oopt = OS.Options(model_index=k, include_hetatm=True, allow_unknown_elements=True)
+        assert _as_tuples(cs.Structure.from_text(text, opt)) == _oracle_tuples(OS.parse(text, oopt)), k
+
+
+def test_large_single_model_pdb():
+    """One model of about 28,000 records (no MODEL lines) over every chunk."""
+    rng = np.random.default_rng(44)
+    recs = [r for m in _records(rng, 560) for r in m]
+    text = _pdb_text([recs])
+    assert len(text) > (2 << 20) and ctypes_model_count(text) == 1
+    opt = cs.ParseOptions(include_hetatm=True, allow_unknown_elements=True, altloc_policy=cs.AltlocPolicy.All)
+    oopt = OS.Options(include_hetatm=True, allow_unknown_elements=True, altloc="all")
+    assert _as_tuples(cs.Structure.from_text(text, opt)) == _oracle_tuples(OS.parse(text, oopt))
+
+
+@pytest.mark.parametrize("where", [0.02, 0.5, 0.97])
+def test_large_pdb_reports_the_first_malformed_line(where):
+    lines = _big_text(_big_models(45, 330)).split("\n")
+    atom_lines = [i for i, l in enumerate(lines) if l.startswith(("ATOM", "HETATM"))]
+    bad = atom_lines[int(where * len(atom_lines))]
+    later = atom_lines[-3]
+    for i in (bad, later):  # two malformed records: the first one is reported
+        lines[i] = lines[i][:30] + "  12x.45" + lines[i][38:]
+    text = "\n".join(lines)
+    with pytest.raises(cs.StructureParse, match=rf"^line {bad + 1}: invalid x coordinate"):
+        cs.Structure.from_text(text, cs.ParseOptions(include_hetatm=True, allow_unknown_elements=True))
+
+
+def ctypes_model_count(text):
+    import ctypes as C
+
+    from crabsaxs_b200 import _native as N
+
+    data = text.encode()
+    m = C.c_int32()
+    assert N.lib.crab_parse_model_count(data, len(data), N.FORMAT_PDB, C.byref(m)) == N.OK
+    return m.value
