@@ -160,11 +160,36 @@ def united_atom_group(residue_name: str, atom_name: str) -> int:
     return int(N.lib.crab_united_atom_group(residue_name.encode(), atom_name.encode()))
 
 
+def _text_field(which: int, name: str):
+    """Per-atom strings of a parsed structure (atom names, residue names,
+    chain ids): kept as the library's newline-joined bytes and split into a
+    list on first use."""
+
+    def get(self):
+        v = self.__dict__.get(name)
+        if v is None:
+            raw = self.__dict__.get("_text_raw")
+            if raw is None:
+                raise AttributeError(name)
+            v = raw[which].decode().split("\n")[: self.atom_count]
+            self.__dict__[name] = v
+        return v
+
+    def put(self, value):
+        self.__dict__[name] = value
+
+    return property(get, put)
+
+
 class Structure:
     """Atoms as arrays (xyz f64 [n,3], element, occupancy, united-atom group).
 
     The device copy is created lazily per engine and cached.
     """
+
+    atom_name = _text_field(0, "atom_name")
+    residue_name = _text_field(1, "residue_name")
+    chain_id = _text_field(2, "chain_id")
 
     def __init__(self, xyz, element, occupancy=None, group=None):
         self.xyz = _f64(xyz).reshape(-1, 3)
@@ -231,7 +256,7 @@ class Structure:
             s = cls(xyz, el, occ, grp)
             s.is_hetatm = het.astype(bool)
             s.residue_id = rid
-            s.atom_name, s.residue_name, s.chain_id = (_parsed_strings(p, k, n) for k in range(3))
+            s._text_raw = [_parsed_bytes(p, k) for k in range(3)]
             return s
         finally:
             N.lib.crab_parsed_destroy(p)
@@ -321,12 +346,12 @@ class ParseOptions:
         return o
 
 
-def _parsed_strings(p: C.c_void_p, which: int, n: int) -> list:
+def _parsed_bytes(p: C.c_void_p, which: int) -> bytes:
     size = C.c_int64()
     N.lib.crab_parsed_strings(p, which, None, 0, C.byref(size))
     buf = C.create_string_buffer(max(size.value, 1))
     N.lib.crab_parsed_strings(p, which, buf, size.value, C.byref(size))
-    return buf.raw[:size.value].decode().split("\n")[:n]
+    return buf.raw[:size.value]
 
 
 def _parse_check(status: int) -> None:
