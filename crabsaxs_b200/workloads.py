@@ -4,6 +4,7 @@
     python -m crabsaxs_b200.workloads multipole-config3 [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
     python -m crabsaxs_b200.workloads gradient-config4 [--repeats N]
     python -m crabsaxs_b200.workloads pr-config3 [--bins B] [--repeats N]
+    python -m crabsaxs_b200.workloads grid-config2 [--repeats N]
 
 debye-config2: the 20,000-atom synthetic protein plus its adaptive 3 Å
 hydration sites, 500 q on [0.001, 0.5], one lattice pair plan (atoms by the
@@ -14,6 +15,8 @@ multipole-config3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.
 gradient-config4: 5,000 atoms (R 28 Å), 100 q, chi^2 and its full gradient.
 pr-config3: coordinate features (Rg, Dmax, P(r) with 160 bins) of the
 100,000-atom structure of multipole-config3.
+grid-config2: the exterior 1 Å hydration grid (1.28 million voxels) and the
+adaptive 3 Å grid of the debye-config2 structure, one public call each.
 Each prints one line with its device or wall times.
 """
 from __future__ import annotations
@@ -96,9 +99,26 @@ def pr_config3(engine: cs.Engine, bins: int, repeats: int) -> str:
             f"device_ms={np.round(dev, 3).tolist()} histogram_ms={np.round(hist, 3).tolist()}")
 
 
+def grid_config2(engine: cs.Engine, repeats: int) -> str:
+    w = synth.CONFIG2
+    s = synth.protein(w.seed, w.n_atoms, w.radius)
+    ext, ada = [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        sites_e, _ = cs.hydration_grid_exterior(s, engine=engine)
+        t1 = time.perf_counter()
+        sites_a, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
+        t2 = time.perf_counter()
+        ext.append((t1 - t0) * 1e3)
+        ada.append((t2 - t1) * 1e3)
+    return (f"grid-config2 exterior_sites={len(sites_e)} adaptive_sites={len(sites_a)} "
+            f"exterior_wall_ms={np.round(ext, 3).tolist()} adaptive_wall_ms={np.round(ada, 3).tolist()}")
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
-    ap.add_argument("workload", choices=["debye-config2", "multipole-config3", "gradient-config4", "pr-config3"])
+    ap.add_argument("workload",
+                    choices=["debye-config2", "multipole-config3", "gradient-config4", "pr-config3", "grid-config2"])
     ap.add_argument("--bins", type=int, default=160)
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
@@ -111,6 +131,8 @@ def main(argv=None) -> None:
         print(multipole_config3(engine, a.precision, a.repeats))
     elif a.workload == "pr-config3":
         print(pr_config3(engine, a.bins, a.repeats))
+    elif a.workload == "grid-config2":
+        print(grid_config2(engine, a.repeats))
     else:
         print(gradient_config4(engine, a.repeats))
 
