@@ -293,7 +293,7 @@ void centre_and_rmax(const crab_struct* st, double* c, double* rmax) {
   *rmax = 0.0;
   for (int64_t i = 0; i < st->n; ++i) {
     const double dx = st->xyz[3 * i] - c[0], dy = st->xyz[3 * i + 1] - c[1], dz = st->xyz[3 * i + 2] - c[2];
-    *rmax = std::fmax(*rmax, std::sqrt(((0.0 + dx * dx) + dy * dy) + dz * dz));
+    *rmax = max_num(*rmax, std::sqrt(((0.0 + dx * dx) + dy * dy) + dz * dz));
   }
 }
 
@@ -630,6 +630,7 @@ int crab_compute_curve(crab_ctx* ctx, crab_struct* st, const double* q, int64_t 
                        double* out, int32_t* method_used) {
   if (!ctx || !st || !opt || (nq > 0 && (!q || !out))) return CRAB_EINVAL;
   GUARD(ctx, {
+    TraceScope trace("compute_curve");
     validate_q(q, nq);
     if (opt->has_solvent) validate_solvent(opt->solvent);
     if (opt->l_max != 0 && (opt->l_max < 8 || opt->l_max > 64))

@@ -41,6 +41,13 @@ inline void require(bool ok, const char* msg) {
   if (!ok) throw Error(CRAB_EINVAL, msg);
 }
 
+// std::fmin / std::fmax of operands that are not NaN (the second operand when
+// the two compare equal, as minsd / maxsd give it), written as comparisons
+// the compiler keeps inline; for the O(N) passes over validated, finite
+// coordinates, where the library calls cost five times as much.
+inline double min_num(double a, double b) { return a < b ? a : b; }
+inline double max_num(double a, double b) { return a > b ? a : b; }
+
 // Host-phase tracing: with CRAB_TRACE=1 in the environment every TraceScope
 // prints "[crab] <name> <ms>" to stderr when it closes (wall time of the
 // phase, including the stream synchronisations inside it).

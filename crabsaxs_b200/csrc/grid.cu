@@ -317,8 +317,8 @@ bool make_box(const double* xyz, int64_t n, double pad, double spacing, Box* b, 
   double mn[3] = {xyz[0], xyz[1], xyz[2]}, mx[3] = {xyz[0], xyz[1], xyz[2]};
   for (int64_t i = 1; i < n; ++i)
     for (int d = 0; d < 3; ++d) {
-      mn[d] = std::fmin(mn[d], xyz[3 * i + d]);
-      mx[d] = std::fmax(mx[d], xyz[3 * i + d]);
+      mn[d] = min_num(mn[d], xyz[3 * i + d]);
+      mx[d] = max_num(mx[d], xyz[3 * i + d]);
     }
   for (int d = 0; d < 3; ++d) {
     b->mn[d] = mn[d] - pad;
@@ -400,7 +400,7 @@ GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* 
   std::vector<double> radius(n);
   for (int64_t i = 0; i < n; ++i) {
     radius[i] = vdw_radius(elem[i]);
-    vmax = std::fmax(vmax, radius[i]);
+    vmax = max_num(vmax, radius[i]);
   }
   const double margin = vmax + probe + thickness + spacing;
   Box b;

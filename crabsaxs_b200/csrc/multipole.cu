@@ -1043,10 +1043,14 @@ struct MpSolventSetup {
 
 void solvent_setup(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, const crab_solvent& s,
                    bool implicit, MpSolventSetup& u) {
+  TraceScope trace("mp_solvent_setup");
   const bool grid = s.hydration_model != CRAB_HYD_ANALYTIC;
   if (grid) u.g = hydration_sites(ctx, st, s);
+  trace_mark("hydration sites");
   u.t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &u.g.sites : nullptr);
+  trace_mark("type_atoms");
   multipole_tables(u.t, q, nq, &s, implicit, u.g.voxel_volume, u.V, u.E, u.H);
+  trace_mark("tables");
   double rmax;
   centre_and_rmax(st, u.centre, &rmax);
   u.rmax_lq = rmax;
