@@ -194,6 +194,67 @@ __device__ __forceinline__ int pr_exact_bin(const double4& pi, const double4& pj
 constexpr float kPrMagic = 12582912.0f;  // 1.5 * 2^23: x + kPrMagic holds floor(x) in its low bits
 constexpr int kPrMagicBits = 0x4B400000;
 
+// Packed f32x2 arithmetic (two pairs per instruction, each lane rounded as
+// the scalar operation).
+__device__ __forceinline__ unsigned long long pr_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void pr_unpack(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long pr_sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long pr_mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long pr_fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned long long pr_add2_rd(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
+// Two pairs (i, j) and (i, j+1) from the packed j tile: their bin coordinates
+// x, x + kPrMagic rounded down (whose bits are kPrMagicBits + floor(x)), and
+// whether each is within delta of a bin edge.
+struct PrTwo {
+  float xa, xb, ta, tb;
+  bool edge_a, edge_b;
+};
+__device__ __forceinline__ PrTwo pr_two(unsigned long long fx2, unsigned long long fy2, unsigned long long fz2,
+                                        const float4& xy, const float2& zz, unsigned long long magic2,
+                                        unsigned long long half2, float near_edge) {
+  const unsigned long long dx = pr_sub2(fx2, pr_pack(xy.x, xy.y));
+  const unsigned long long dy = pr_sub2(fy2, pr_pack(xy.z, xy.w));
+  const unsigned long long dz = pr_sub2(fz2, pr_pack(zz.x, zz.y));
+  const unsigned long long d2 = pr_fma2(dx, dx, pr_fma2(dy, dy, pr_mul2(dz, dz)));
+  float d2a, d2b;
+  pr_unpack(d2, d2a, d2b);
+  PrTwo r;
+  r.xa = pr_sqrt_approx(d2a);
+  r.xb = pr_sqrt_approx(d2b);
+  const unsigned long long x2 = pr_pack(r.xa, r.xb);
+  const unsigned long long t2 = pr_add2_rd(x2, magic2);
+  const unsigned long long c2 = pr_sub2(pr_sub2(x2, pr_sub2(t2, magic2)), half2);  // frac - 0.5
+  float ca, cb;
+  pr_unpack(t2, r.ta, r.tb);
+  pr_unpack(c2, ca, cb);
+  r.edge_a = fabsf(ca) > near_edge;
+  r.edge_b = fabsf(cb) > near_edge;
+  return r;
+}
+
 template <int kMode>
 struct PrAcc {
   unsigned* c;  // kPrCounts
@@ -216,6 +277,9 @@ __global__ void __launch_bounds__(kPrThreads, 8)
   extern __shared__ double pr_dyn[];
   __shared__ double4 sj[kPrThreads];
   __shared__ float4 sj32[kPrThreads];
+  // the j tile in bins as pairs of atoms: {x_j, x_j+1, y_j, y_j+1} and {z_j, z_j+1}
+  __shared__ float4 sjp[kPrThreads / 2];
+  __shared__ float2 sjz[kPrThreads / 2];
   if (par->degenerate) return;
   const float inv_step = par->inv_step;
   // a pair is near an edge when its fractional bin coordinate is within delta
@@ -254,8 +318,9 @@ __global__ void __launch_bounds__(kPrThreads, 8)
     for (int k = threadIdx.x; k < bins; k += kPrThreads) {
       unsigned long long sum = 0ull;
       for (int c = 0; c < copies; ++c) {
-        sum += Hc[(size_t)c * bins + k];
-        Hc[(size_t)c * bins + k] = 0u;
+        unsigned* h = Hc + (size_t)c * bins;
+        sum += h[k];
+        h[k] = 0u;
       }
       if (sum) atomicAdd(&counts[(size_t)cur_pair * bins + k], sum);
     }
@@ -279,7 +344,14 @@ __global__ void __launch_bounds__(kPrThreads, 8)
         const int64_t g = (int64_t)b * kPrThreads + threadIdx.x;
         const float4 f = pos32[g];
         sj[threadIdx.x] = pos[g];
-        sj32[threadIdx.x] = make_float4(f.x * inv_step, f.y * inv_step, f.z * inv_step, 0.0f);
+        const float4 fs = make_float4(f.x * inv_step, f.y * inv_step, f.z * inv_step, 0.0f);
+        sj32[threadIdx.x] = fs;
+        float* xy = reinterpret_cast<float*>(&sjp[threadIdx.x >> 1]);
+        float* z = reinterpret_cast<float*>(&sjz[threadIdx.x >> 1]);
+        const int h = threadIdx.x & 1;
+        xy[h] = fs.x;
+        xy[2 + h] = fs.y;
+        z[h] = fs.z;
       }
       __syncthreads();
       cur_b = b;
@@ -291,26 +363,28 @@ __global__ void __launch_bounds__(kPrThreads, 8)
       double wi = 0.0;
       if constexpr (kMode != kPrCounts) wi = pos[gi].w;
       if (a != b && tb.y == kPrThreads) {
-        // full off-diagonal tile: 32 pairs per chunk without branches; pairs
-        // near an edge are marked and placed exactly after the chunk
+        // full off-diagonal tile: 32 pairs per chunk without branches, two
+        // pairs per packed instruction; pairs near an edge are marked and
+        // placed exactly after the chunk
+        const unsigned long long fx2 = pr_pack(fi.x, fi.x), fy2 = pr_pack(fi.y, fi.y), fz2 = pr_pack(fi.z, fi.z);
+        const unsigned long long magic2 = pr_pack(kPrMagic, kPrMagic), half2 = pr_pack(0.5f, 0.5f);
 #pragma unroll 1
         for (int jc = 0; jc < kPrThreads; jc += 32) {
           unsigned marked = 0u;
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj) {
-            const float x = pr_bin_coord(fi, sj32[jc + jj]);
-            const float t = __fadd_rd(x, kPrMagic);
-            const float frac = x - (t - kPrMagic);
-            const bool edge = fabsf(frac - 0.5f) > near_edge;
-            marked |= (edge ? 1u : 0u) << jj;
+          for (int jj = 0; jj < 32; jj += 2) {
+            const PrTwo r = pr_two(fx2, fy2, fz2, sjp[(jc + jj) >> 1], sjz[(jc + jj) >> 1], magic2, half2, near_edge);
+            marked |= ((r.edge_a ? 1u : 0u) | (r.edge_b ? 2u : 0u)) << jj;
             if constexpr (kMode == kPrCounts) {
               // t's bits are kPrMagicBits + floor(x): the counter's shared address
               // comes from one shift and add on the offset base
-              const unsigned addr = cbase + ((unsigned)min(__float_as_int(t), top) << 2);
-              if (!edge) asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr) : "memory");
+              const unsigned addr_a = cbase + ((unsigned)min(__float_as_int(r.ta), top) << 2);
+              const unsigned addr_b = cbase + ((unsigned)min(__float_as_int(r.tb), top) << 2);
+              if (!r.edge_a) asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr_a) : "memory");
+              if (!r.edge_b) asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr_b) : "memory");
             } else {
-              const int e = min(__float_as_int(t), top) - kPrMagicBits;
-              if (!edge) acc.add(e, wi * sj[jc + jj].w);
+              if (!r.edge_a) acc.add(min(__float_as_int(r.ta), top) - kPrMagicBits, wi * sj[jc + jj].w);
+              if (!r.edge_b) acc.add(min(__float_as_int(r.tb), top) - kPrMagicBits, wi * sj[jc + jj + 1].w);
             }
           }
           while (marked) {
