@@ -471,9 +471,13 @@ std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_fr
       for (int b = 0; b < n_qblocks; ++b) items.push_back({cost, make_int4(it, j0, j1, b)});
     }
   }
-  std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  // stable sort by cost, longest first: costs are 1 .. 2 * run, so one
+  // counting pass places every item
+  std::vector<size_t> start((size_t)2 * run + 2, 0);
+  for (const auto& it : items) ++start[(size_t)(2 * run - it.first) + 1];
+  for (size_t c = 1; c < start.size(); ++c) start[c] += start[c - 1];
   std::vector<int4> work(items.size());
-  for (size_t i = 0; i < items.size(); ++i) work[i] = items[i].second;
+  for (const auto& it : items) work[start[(size_t)(2 * run - it.first)]++] = it.second;
   return work;
 }
 
@@ -511,7 +515,8 @@ T* upload(crab_ctx* ctx, PairPlan& P, std::vector<void*>& list, const char* name
 
 }  // namespace
 
-Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64) {
+Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64,
+                    bool spatial) {
   Layout L;
   L.T = T;
   L.n = n;
@@ -533,9 +538,10 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
     rmax = std::max(rmax, std::sqrt(r2));
   }
   L.extent = 2.0 * rmax;
-  // order: type, then the 30-bit Morton code of the centred position, ties by
-  // input index (a counting sort by type, then a stable LSD radix sort of the
-  // packed (Morton code, index) words within each type, three 10-bit digits)
+  // order: type, then (spatial) the 30-bit Morton code of the centred
+  // position, ties by input index (a counting sort by type, then a stable LSD
+  // radix sort of the packed (Morton code, index) words within each type,
+  // three 10-bit digits); without `spatial`, type then input index
   require(n < ((int64_t)1 << 32), "at most 2^32 - 1 atoms per pair problem");
   static const std::vector<uint32_t> spread = [] {
     std::vector<uint32_t> t(1024);
@@ -553,15 +559,16 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
     std::vector<int64_t> pos(tstart.begin(), tstart.end() - 1);
     for (int64_t i = 0; i < n; ++i) {
       uint32_t m = 0;
-      for (int d = 0; d < 3; ++d) {
-        const double cell = (xyz[3 * i + d] - c[d] - lo[d]) * scale[d];
-        const int ci = cell <= 0.0 ? 0 : (cell >= 1023.0 ? 1023 : (int)cell);
-        m |= spread[ci] << d;
-      }
+      if (spatial)
+        for (int d = 0; d < 3; ++d) {
+          const double cell = (xyz[3 * i + d] - c[d] - lo[d]) * scale[d];
+          const int ci = cell <= 0.0 ? 0 : (cell >= 1023.0 ? 1023 : (int)cell);
+          m |= spread[ci] << d;
+        }
       word[pos[type[i]]++] = ((uint64_t)m << 32) | (uint64_t)i;
     }
   }
-  for (int t = 0; t < T; ++t) {
+  for (int t = 0; t < T && spatial; ++t) {
     const int64_t a = tstart[t], b = tstart[t + 1];
     for (int shift = 32; shift < 62; shift += 10) {
       int64_t digit[1025] = {0};
@@ -685,12 +692,16 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
         for (int b = 0; b < n_qblocks; ++b) items.push_back({cost, {make_int4(it, j0, j1, b), base}});
       }
   }
-  std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  // stable sort by cost, longest first (costs 1 .. 2 * run): one counting pass
+  std::vector<size_t> start((size_t)2 * run + 2, 0);
+  for (const auto& it : items) ++start[(size_t)(2 * run - it.first) + 1];
+  for (size_t c = 1; c < start.size(); ++c) start[c] += start[c - 1];
   work.resize(items.size());
   out.resize(items.size());
-  for (size_t i = 0; i < items.size(); ++i) {
-    work[i] = items[i].second.first;
-    out[i] = items[i].second.second;
+  for (const auto& it : items) {
+    const size_t k = start[(size_t)(2 * run - it.first)]++;
+    work[k] = it.second.first;
+    out[k] = it.second.second;
   }
 }
 

@@ -178,7 +178,12 @@ struct Layout {
   double extent = 0.0;             // max pair distance bound
 };
 
-Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64);
+// spatial: order the atoms of each type along a Morton curve, so that tiles
+// are spatially compact (the P(r) distance bounds need it); otherwise they
+// keep their input order within each type (the Debye sums compute every pair
+// of a tile pair, so the order only changes the order of additions).
+Layout build_layout(const double* xyz, const double* w, const int32_t* type, int64_t n, int T, bool with_f64,
+                    bool spatial = false);
 
 // Self + pair partials of a layout at every q (P = T(T+1)/2 rows).
 struct Partials {

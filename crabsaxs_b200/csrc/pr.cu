@@ -529,7 +529,7 @@ double pair_distance_histogram(crab_ctx* ctx, const double* xyz, const double* w
   Layout L;
   {
     TraceScope t2("pr.layout");
-    L = build_layout(xyz, w, type.data(), n, mode == kPrCounts ? T : 1, false);
+    L = build_layout(xyz, w, type.data(), n, mode == kPrCounts ? T : 1, false, true);
   }
   const int n_tiles = L.n_tiles;
   const int64_t n_pad = L.n_pad;
