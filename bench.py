@@ -45,6 +45,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "pair·q/s (Debye); batched χ²+∇ curves/s vs plain GPU; both at ≤1e-5 rel err"
+WORKLOAD = "debye pair sums per type pair, 20k-atom structure + adaptive 3 Å hydration sites, 500 q on [0.001, 0.5]"
 UNIT = "pair·q/s"
 N_ATOMS, RADIUS, SEED = 20000, 45.0, 2
 Q = np.linspace(0.001, 0.5, 500)
@@ -217,7 +218,10 @@ def run_reference(args, rank, world):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import synth
 
+    import oracle as O
+
     s = synth.protein(SEED, N_ATOMS, RADIUS)
+    n_sites = len(O.adaptive_grid(s.xyz, 3.0)[0])  # the workload's sites (the timed sample is half the atoms)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_baseline_run(s, threads, 0.5)
@@ -233,8 +237,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "debye pair sums, 20k-atom structure + adaptive 3 Å hydration sites, 500 q",
-                   "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_q": len(Q)},
+        "config": {"workload": WORKLOAD, "n_atoms": N_ATOMS, "n_sites": int(n_sites), "n_q": len(Q)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -741,8 +744,7 @@ def run_ours(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "debye pair sums per type pair, 20k-atom structure + adaptive 3 Å hydration "
-                                   "sites, 500 q on [0.001, 0.5]",
+            "config": {"workload": WORKLOAD,
                        "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_types": T, "n_q": len(Q),
                        "kernel_variant": _variant_name(chosen.value), "autotune_ms": tuning,
                        "parallelism": f"independent structure per GPU x{world}",
