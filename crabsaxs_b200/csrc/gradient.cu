@@ -15,7 +15,10 @@
 // one thread per atom i, j tiles in shared memory, sin and cos of q r
 // advanced together along each uniform q block by the Reinsch recurrence in
 // one packed f32x2 register pair, the q sums accumulated per block in FP32
-// and per atom in FP64.
+// and per atom in FP64.  A pair's term for atom j is the negative of its
+// term for atom i (g_ab = g_ba), so only tile pairs it <= jt run: a diagonal
+// tile computes its ordered pairs for its own atoms, an off-diagonal one also
+// sums each j's terms over the block (a warp shuffle, then shared memory).
 
 #include <cuda_runtime.h>
 
@@ -33,15 +36,29 @@ using namespace dev;
 
 constexpr int kGT = 128;
 
+// Tile pair (it, jt), it <= jt, of block w = jt (jt + 1) / 2 + it.
+__device__ __forceinline__ void grad_tri_decode(int w, int& it, int& jt) {
+  int b = (int)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);
+  while (b > 0 && b * (b + 1) / 2 > w) --b;
+  while ((b + 1) * (b + 2) / 2 <= w) ++b;
+  jt = b;
+  it = w - b * (b + 1) / 2;
+}
+
 __global__ void __launch_bounds__(kGT, 4)
     k_chi2_grad(const float4* __restrict__ atoms, const int* __restrict__ tile_type, int T,
                 const float2* __restrict__ coef, int nq, const float4* __restrict__ qpar,
                 const int2* __restrict__ qrange, int n_qb, int wide, double* __restrict__ grad) {
   extern __shared__ float2 s_coef[];  // nq (alpha, beta) of this tile pair's type pair
   __shared__ float4 sj[kGT];
-  const int it = blockIdx.y, jt = blockIdx.x, tid = threadIdx.x;
+  __shared__ double s_gj[kGT][3];     // the j tile's terms (off-diagonal tile pairs)
+  int it, jt;
+  grad_tri_decode((int)blockIdx.x, it, jt);
+  const int tid = threadIdx.x, lane = tid & 31;
+  const bool diag = it == jt;
   const float4 ai = atoms[(size_t)it * kGT + tid];
   sj[tid] = atoms[(size_t)jt * kGT + tid];
+  s_gj[tid][0] = s_gj[tid][1] = s_gj[tid][2] = 0.0;
   const int ta = tile_type[it], tb = tile_type[jt];
   const int a = min(ta, tb), b = max(ta, tb);
   const int ab = a * T - a * (a - 1) / 2 + (b - a);
@@ -93,11 +110,32 @@ __global__ void __launch_bounds__(kGT, 4)
     gx += gr * dx;
     gy += gr * dy;
     gz += gr * dz;
+    if (!diag) {  // uniform over the block: every thread is at the same j
+      double jx = -gr * dx, jy = -gr * dy, jz = -gr * dz;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        jx += __shfl_xor_sync(0xffffffffu, jx, o);
+        jy += __shfl_xor_sync(0xffffffffu, jy, o);
+        jz += __shfl_xor_sync(0xffffffffu, jz, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&s_gj[j][0], jx);
+        atomicAdd(&s_gj[j][1], jy);
+        atomicAdd(&s_gj[j][2], jz);
+      }
+    }
   }
   double* out = grad + 3 * ((size_t)it * kGT + tid);
   atomicAdd(out, gx);
   atomicAdd(out + 1, gy);
   atomicAdd(out + 2, gz);
+  if (!diag) {
+    __syncthreads();
+    double* outj = grad + 3 * ((size_t)jt * kGT + tid);
+    atomicAdd(outj, s_gj[tid][0]);
+    atomicAdd(outj + 1, s_gj[tid][1]);
+    atomicAdd(outj + 2, s_gj[tid][2]);
+  }
 }
 
 }  // namespace
@@ -198,7 +236,9 @@ void chi2_grad_impl(crab_ctx* ctx, const crab_struct* st, const double* q, const
   require(smem <= 200 * 1024, "too many q values for the gradient kernel");
   if (smem > 48 * 1024)
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_chi2_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_chi2_grad<<<dim3(L.n_tiles, L.n_tiles), kGT, smem, sm>>>(d_atoms, d_tt, T, d_coef, (int)nq, d_qp, d_qr,
+  const int64_t n_blocks = (int64_t)L.n_tiles * (L.n_tiles + 1) / 2;  // tile pairs it <= jt
+  require(n_blocks < ((int64_t)1 << 31), "too many atoms for the gradient kernel");
+  k_chi2_grad<<<(unsigned)n_blocks, kGT, smem, sm>>>(d_atoms, d_tt, T, d_coef, (int)nq, d_qp, d_qr,
                                                             (int)qr.size(), wide, d_grad);
   CRAB_CUDA_CHECK(cudaGetLastError());
   ctx->launches += 1;
