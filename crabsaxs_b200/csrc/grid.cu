@@ -245,6 +245,91 @@ __global__ void k_sweep(uint8_t* __restrict__ s, Box b, int axis, const int* __r
   if (any) atomicOr(changed, 1);
 }
 
+// Lines of at most kWarpLine voxels are swept by one warp each: lane l holds
+// voxels 4l .. 4l+3 (past the end of the line: molecular, never written).
+// The forward pass carries the label through a voxel by one of three maps of
+// the carry (exterior: set, molecular: clear, unknown: unchanged), and maps of
+// this kind compose as "the later constant wins"; an inclusive shuffle scan of
+// the lanes' composed maps gives every lane its incoming carry, and the lane
+// then steps through its four voxels as the sequential pass does.  The
+// backward pass does the same from the right on the updated voxels, so the
+// line ends as k_sweep's forward and backward passes leave it.
+constexpr int kWarpLine = 128;
+
+// Carry map of four voxels in the given order: (constant?, value).
+__device__ __forceinline__ void carry_map(const uint8_t (&v)[4], bool forward, int& is_const, int& value) {
+  is_const = 0;
+  value = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint8_t x = v[forward ? e : 3 - e];
+    if (x == 2) { is_const = 1; value = 1; }
+    else if (x != 0) { is_const = 1; value = 0; }
+  }
+}
+
+__global__ void k_sweep_warp(uint8_t* __restrict__ s, Box b, int axis, const int* __restrict__ prev_changed,
+                             int* __restrict__ changed) {
+  if (prev_changed && *prev_changed == 0) return;
+  const uint64_t nx = b.n[0], ny = b.n[1], nz = b.n[2];
+  uint64_t lines, len, stride;
+  if (axis == 0) { lines = ny * nz; len = nx; stride = 1; }
+  else if (axis == 1) { lines = nx * nz; len = ny; stride = nx; }
+  else { lines = nx * ny; len = nz; stride = nx * ny; }
+  const uint64_t l = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // one line per warp
+  if (l >= lines) return;  // the whole warp
+  const int lane = threadIdx.x & 31;
+  uint64_t start;
+  if (axis == 0) start = l * nx;
+  else if (axis == 1) start = (l / nx) * nx * ny + (l % nx);
+  else start = l;
+  uint8_t* line = s + start;
+  uint8_t v[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint64_t k = (uint64_t)(4 * lane + e);
+    v[e] = k < len ? line[k * stride] : (uint8_t)1;
+  }
+  unsigned wrote = 0u;  // bit e: voxel e became exterior
+  // forward: lanes in increasing order
+  int c, val;
+  carry_map(v, true, c, val);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int pc = __shfl_up_sync(0xffffffffu, c, o), pv = __shfl_up_sync(0xffffffffu, val, o);
+    if (lane >= o && !c) { c = pc; val = pv; }
+  }
+  int carry = __shfl_up_sync(0xffffffffu, val, 1);
+  if (lane == 0) carry = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    if (v[e] == 2) carry = 1;
+    else if (v[e] == 0) {
+      if (carry) { v[e] = 2; wrote |= 1u << e; }
+    } else carry = 0;
+  }
+  // backward: lanes in decreasing order, on the updated voxels
+  carry_map(v, false, c, val);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int pc = __shfl_down_sync(0xffffffffu, c, o), pv = __shfl_down_sync(0xffffffffu, val, o);
+    if (lane + o < 32 && !c) { c = pc; val = pv; }
+  }
+  carry = __shfl_down_sync(0xffffffffu, val, 1);
+  if (lane == 31) carry = 0;
+#pragma unroll
+  for (int e = 3; e >= 0; --e) {
+    if (v[e] == 2) carry = 1;
+    else if (v[e] == 0) {
+      if (carry) { v[e] = 2; wrote |= 1u << e; }
+    } else carry = 0;
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (wrote & (1u << e)) line[(uint64_t)(4 * lane + e) * stride] = 2;
+  if (__any_sync(0xffffffffu, wrote != 0u) && lane == 0) atomicOr(changed, 1);
+}
+
 // Grid buffers live in the context's pool ("grid." slots), so repeated calls
 // allocate nothing.  A slot above kGridKeepBytes (a box of more than 2^28
 // voxels) is released when the build ends, so a one-off large box does not
@@ -436,7 +521,10 @@ GridResult exterior_grid_device(crab_ctx* ctx, const double* xyz, const int8_t* 
       const int* prev = k ? d_changed + k - 1 : nullptr;
       for (int axis = 0; axis < 3; ++axis) {
         const uint64_t lines = axis == 0 ? b.n[1] * b.n[2] : axis == 1 ? b.n[0] * b.n[2] : b.n[0] * b.n[1];
-        k_sweep<<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(state, b, axis, prev, d_changed + k);
+        if (b.n[axis] <= (uint64_t)kWarpLine)  // one warp per line
+          k_sweep_warp<<<(unsigned)((lines + 3) / 4), 128, 0, s>>>(state, b, axis, prev, d_changed + k);
+        else  // one thread per line
+          k_sweep<<<(unsigned)((lines + 127) / 128), 128, 0, s>>>(state, b, axis, prev, d_changed + k);
         CRAB_CUDA_CHECK(cudaGetLastError());
         ctx->launches += 1;
       }
