@@ -43,7 +43,7 @@ namespace {
 using namespace dev;
 
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
-constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 100, 126, 128, 150};  // compiled q-block lengths
+constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 100, 126, 128, 150, 168};  // compiled q-block lengths
 // jb values at or above kPackedQ select the q-packed kernel with
 // (jb - kPackedQ) % kDenser chains; + kDenser asks for 3 CTAs per SM.
 constexpr int kPackedQ = 8;
@@ -708,8 +708,10 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
 // Untuned choice of (Q, jb): the block length by a cost model (launched steps
 // of 3 FP32 ops each plus a per-pair seed of about 60 ops per block), and the
 // q-packed kernel where it is compiled for that length (one chain and three
-// CTAs per SM at Q = 100 and 128, two chains below: the fastest on the
-// 20k-atom config-2 workload).
+// CTAs per SM at Q = 100, 126 and 128; one chain and two CTAs at Q = 150 and
+// 168, whose fewer seeds per pair outweigh the lower occupancy: 3 x 168 for
+// 500 q and 2 x 150 for 300 q are 1.3 % and 3 % faster than 4 x 126 and
+// 3 x 100; two chains below Q = 100).
 int2 default_variant(const std::vector<double>& q) {
   int bestQ = 64;
   long best_cost = -1;
@@ -721,7 +723,8 @@ int2 default_variant(const std::vector<double>& q) {
     }
   }
   if (bestQ == 128 || bestQ == 126 || bestQ == 100) return make_int2(bestQ, 1 + kPackedQ + kDenser);
-  if (bestQ == 150) return make_int2(150, 1 + kPackedQ);  // 75 packed accumulators: two CTAs per SM
+  // 75 or 84 packed accumulators: two CTAs per SM
+  if (bestQ == 150 || bestQ == 168) return make_int2(bestQ, 1 + kPackedQ);
   const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
@@ -898,6 +901,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH_PQ(100, 1, 3, 1 + kPackedQ + kDenser)
     CRAB_LAUNCH_PQ(126, 1, 3, 1 + kPackedQ + kDenser)
     CRAB_LAUNCH_PQ(150, 1, 2, 1 + kPackedQ)
+    CRAB_LAUNCH_PQ(168, 1, 2, 1 + kPackedQ)
 #undef CRAB_LAUNCH_PQ
     if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
   }
@@ -1038,7 +1042,7 @@ static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2
                                      {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
                                      {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
-                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}};
+                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ}};
 
 bool pair_variant_known(int variant) {
   const int Q = variant / 16, jb = variant % 16;
@@ -1062,7 +1066,7 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out
   static const int kVariants[][2] = {{64, 2},  {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
                                      {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
-                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}};
+                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;

@@ -307,7 +307,7 @@ def test_lattice_plan_matches_fp64_config2(engine):
 # Every kernel variant the plan can dispatch (Q*16 + jb; jb >= 8: q-packed, jb >= 12: 3 CTAs/SM).
 ALL_VARIANTS = [8 * 16 + 2, 16 * 16 + 2, 32 * 16 + 2, 48 * 16 + 2, 64 * 16 + 2, 96 * 16 + 2, 128 * 16 + 2,
                 64 * 16 + 4, 96 * 16 + 4, 64 * 16 + 10, 96 * 16 + 10, 128 * 16 + 9, 128 * 16 + 10, 128 * 16 + 13,
-                100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9]
+                100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9, 168 * 16 + 9]
 
 
 @pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "wide"])
