@@ -207,7 +207,7 @@ void chi2_grad_impl(crab_ctx* ctx, const crab_struct* st, const double* q, const
       }
   Layout L = build_layout(t.xyz.data(), t.w.data(), t.type.data(), (int64_t)t.w.size(), T, false);
   std::vector<double> qv(q, q + nq);
-  const std::vector<int2> qr = q_blocks(qv, 64);
+  const std::vector<int2> qr = q_blocks(qv, 128);
   std::vector<float4> qp(qr.size());
   double max_half = 0.0;
   for (size_t bk = 0; bk < qr.size(); ++bk) {
