@@ -186,7 +186,7 @@ def typed_arrays(s, sites):
 
 def traffic_per_launch():
     """DRAM bytes per pair-kernel launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "debye_pair_fp32_config2.txt"
+    p = ROOT / "profiles" / "debye_pair_fp32_20k_500q.txt"
     if not p.exists():
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
@@ -246,7 +246,7 @@ def run_reference(args, rank, world):
 
 
 def ensemble_section(eng, rank, with_cpu=False):
-    """Config 5: 256 conformers (log-uniform 2k-40k atoms), 300 q, the 25 (c1, c2)
+    """Ensemble of 256 conformers (log-uniform 2k-40k atoms), 300 q, the 25 (c1, c2)
     candidates of ensemble.rs:302-315.  Batched: one CUDA graph per scoring pass
     (pair sums of all conformers, 25x256 curves, per-candidate simplex weights,
     gradients, KL reweighting).  Plain: one compute_curve per conformer per
@@ -256,7 +256,7 @@ def ensemble_section(eng, rank, with_cpu=False):
     from crabsaxs_b200 import synth
 
     confs = synth.ensemble(256, 5 + 7919 * rank)
-    q = synth.CONFIG5_Q
+    q = synth.ENSEMBLE_Q
     fo = cs.FitOptions(method=cs.ScatteringMethod.Debye)
     cand = cs.solvent_candidates(fo)
     rng = np.random.default_rng(55)
@@ -316,18 +316,18 @@ def ensemble_section(eng, rank, with_cpu=False):
 
 
 def multipole_section(eng, rank, fp32_peak, with_cpu=False):
-    """Config 3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.  The
+    """100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.  The
     default path runs the moment GEMM on tcgen05 tensor cores (TF32 hi+lo, 3
     products per K step); the FP32 SIMT GEMM is timed beside it.  Reports the
     call's wall and device time, each GEMM against its peak, the error against
     the FP64 device multipole (all q; precision) and against FP64 Debye (every
-    50th q; truncation of the expansion at L), and config 2's solvent curve by
+    50th q; truncation of the expansion at L), and the 20,000-atom solvent curve by
     multipole (L = 30) for comparison with Debye."""
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG3
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
     L = 50
     tot, gm, fl = C.c_double(), C.c_double(), C.c_double()
@@ -363,14 +363,14 @@ def multipole_section(eng, rank, fp32_peak, with_cpu=False):
     except (OSError, ValueError):
         pass
     tf32_peak = 0.5 * float(peaks.get("bf16_tflops", 1590.0))  # dense TF32 runs at half the BF16 rate
-    # config 2 curve with the adaptive 3 Å grid by multipole, L = 30
-    s2 = synth.protein(synth.CONFIG2.seed, synth.CONFIG2.n_atoms, synth.CONFIG2.radius)
+    # the 20,000-atom curve with the adaptive 3 Å grid by multipole, L = 30
+    s2 = synth.protein(synth.DEBYE_20K_SOLVATED.seed, synth.DEBYE_20K_SOLVATED.n_atoms, synth.DEBYE_20K_SOLVATED.radius)
     sp = cs.SolventParams(hydration_model=cs.HydrationModel.AdaptiveGrid, hydration_grid_spacing_angstrom=3.0)
     opt = cs.ComputeOptions(method=cs.ScatteringMethod.Multipole, solvent=sp, multipole_l_max=30)
-    cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
+    cs.compute_curve(s2, synth.DEBYE_20K_SOLVATED.q, opt, engine=eng)
     t0 = time.perf_counter()
     for _ in range(3):
-        cs.compute_curve(s2, synth.CONFIG2.q, opt, engine=eng)
+        cs.compute_curve(s2, synth.DEBYE_20K_SOLVATED.q, opt, engine=eng)
     c2_ms = (time.perf_counter() - t0) * 1e3 / 3
     cpu = None
     if with_cpu and rank == 0:
@@ -404,12 +404,12 @@ def multipole_section(eng, rank, fp32_peak, with_cpu=False):
             "fp32_simt_max_rel_err_vs_fp64_multipole": float(rel32.max()),
             "max_rel_err_vs_fp64_debye_every_50th_q": float(trunc.max()),
             "rms_rel_err_vs_fp64_debye_every_50th_q": float(np.sqrt(np.mean(trunc**2))),
-            "config2_multipole_l30_curve_ms": c2_ms}
+            "solvated_20k_multipole_l30_curve_ms": c2_ms}
 
 
 def grid_and_gradient_section(eng, rank):
-    """Hydration grid of config 2 (adaptive, 3 Å spacing; bit-exact against the
-    oracle in the tests) and chi^2 with its full adjoint gradient on config 4
+    """Hydration grid of the 20,000-atom structure (adaptive, 3 Å spacing; bit-exact against the
+    oracle in the tests) and chi^2 with its full adjoint gradient on 5,000 atoms
     (5,000 atoms, 100 q): wall time per public call, median of 5 after a warm-up."""
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import synth
@@ -423,28 +423,28 @@ def grid_and_gradient_section(eng, rank):
             ts.append((time.perf_counter() - t0) * 1e3)
         return float(np.median(ts))
 
-    s2 = synth.protein(synth.CONFIG2.seed + 1000 * rank, synth.CONFIG2.n_atoms, synth.CONFIG2.radius)
+    s2 = synth.protein(synth.DEBYE_20K_SOLVATED.seed + 1000 * rank, synth.DEBYE_20K_SOLVATED.n_atoms, synth.DEBYE_20K_SOLVATED.radius)
     sites, _ = cs.hydration_grid_adaptive(s2, 3.0, engine=eng)
     grid_ms = med(lambda: cs.hydration_grid_adaptive(s2, 3.0, engine=eng))
     ext = cs.hydration_grid_exterior(s2, engine=eng)[0]
     ext_ms = med(lambda: cs.hydration_grid_exterior(s2, engine=eng))
-    w = synth.CONFIG4
+    w = synth.GRADIENT_5K
     s4 = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
     y = cs.compute_curve(s4, w.q, cs.ComputeOptions(method=cs.ScatteringMethod.Debye,
                                                     solvent=cs.SolventParams())).intensity
     sigma = 0.01 * y
     grad_ms = med(lambda: cs.chi2_grad(s4, w.q, 1.01 * y, sigma, cs.SolventParams(), 1.0, 0.0, engine=eng))
     pairq = s4.atom_count * (s4.atom_count - 1) / 2.0 * len(w.q)
-    return {"adaptive_grid_config2": {"ms": grid_ms, "sites": int(len(sites)), "atoms": s2.atom_count},
-            "exterior_grid_config2": {"ms": ext_ms, "sites": int(len(ext))},
-            "chi2_grad_config4": {"ms": grad_ms, "atoms": s4.atom_count, "n_q": len(w.q),
+    return {"adaptive_grid_20k": {"ms": grid_ms, "sites": int(len(sites)), "atoms": s2.atom_count},
+            "exterior_grid_20k": {"ms": ext_ms, "sites": int(len(ext))},
+            "chi2_grad_5k": {"ms": grad_ms, "atoms": s4.atom_count, "n_q": len(w.q),
                                   "pair_q_per_s": 2.0 * pairq / (grad_ms * 1e-3),
                                   "note": "ordered pairs (i, j) and (j, i): 2 * N(N-1)/2 * nq per call"}}
 
 
 def pr_section(eng, rank, with_cpu):
     """Coordinate features (metrics.rs:236-270): Rg, Dmax and the 160-bin P(r)
-    of config 3's 100,000-atom structure (5e9 pairs).  Wall time of the public
+    of the 100,000-atom structure (5e9 pairs).  Wall time of the public
     call and device time of its kernels, median of 5 after a warm-up; the CPU
     baseline is the oracle (the reference's 64-row-chunk loop, OpenMP on every
     host core) on a seeded 20,000-atom subset."""
@@ -452,7 +452,7 @@ def pr_section(eng, rank, with_cpu):
     import oracle as O
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG3
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius)
     cs.coordinate_features(s, engine=eng)
     walls, dev, hist = [], [], []
@@ -492,7 +492,7 @@ def _pdb_text(s):
 
 
 def ingest_section(rank, with_cpu):
-    """Structure ingest (structure.rs:209-327): the config-3 structure as
+    """Structure ingest (structure.rs:209-327): the 100,000-atom structure as
     100,000 PDB ATOM records parsed by crab_parse_structure with the default
     options, median of 5; the CPU baseline is the Python restatement of the
     reference's reader and policies on the first 10,000 records."""
@@ -502,7 +502,7 @@ def ingest_section(rank, with_cpu):
     from crabsaxs_b200 import _native as N
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG3
+    w = synth.ATOMS_100K
     text = _pdb_text(synth.protein(w.seed + 1000 * rank, w.n_atoms, w.radius))
     o = cs.ParseOptions().to_c()
     ts, n = [], 0

@@ -40,16 +40,16 @@ class Workload:
     seed: int
 
 
-# Config 1: 1,000 atoms, R 20 Å, q 0.005..0.5 step 0.005.
-CONFIG1 = Workload("debye-1k", 1000, 20.0, np.arange(1, 101) * 0.005, 1)
-# Config 2: 20,000 atoms, R 45 Å, plus adaptive 3 Å hydration sites; 500 q on [0.001, 0.5].
-CONFIG2 = Workload("debye-20k-solvated", 20000, 45.0, q_grid(0.001, 0.5, 500), 2)
-# Config 3: 100,000 atoms, R 80 Å, 1000 q on [0.001, 0.6], l_max 50.
-CONFIG3 = Workload("multipole-100k", 100000, 80.0, q_grid(0.001, 0.6, 1000), 3)
-# Config 4: 5,000 atoms, R 28 Å, q 0.005..0.5 step 0.005.
-CONFIG4 = Workload("gradient-5k", 5000, 28.0, np.arange(1, 101) * 0.005, 4)
-# Config 5: 256 conformers, N log-uniform in [2000, 40000]; 300 q on [0.005, 0.45].
-CONFIG5_Q = q_grid(0.005, 0.45, 300)
+# 1,000 atoms, R 20 Å, q 0.005..0.5 step 0.005.
+DEBYE_1K = Workload("debye-1k", 1000, 20.0, np.arange(1, 101) * 0.005, 1)
+# 20,000 atoms, R 45 Å, plus adaptive 3 Å hydration sites; 500 q on [0.001, 0.5].
+DEBYE_20K_SOLVATED = Workload("debye-20k-solvated", 20000, 45.0, q_grid(0.001, 0.5, 500), 2)
+# 100,000 atoms, R 80 Å, 1000 q on [0.001, 0.6], l_max 50.
+ATOMS_100K = Workload("multipole-100k", 100000, 80.0, q_grid(0.001, 0.6, 1000), 3)
+# 5,000 atoms, R 28 Å, q 0.005..0.5 step 0.005.
+GRADIENT_5K = Workload("gradient-5k", 5000, 28.0, np.arange(1, 101) * 0.005, 4)
+# Ensemble: 256 conformers, N log-uniform in [2000, 40000]; 300 q on [0.005, 0.45].
+ENSEMBLE_Q = q_grid(0.005, 0.45, 300)
 
 
 def ensemble_sizes(k: int = 256, seed: int = 5, lo: int = 2000, hi: int = 40000) -> np.ndarray:
@@ -65,6 +65,6 @@ def ensemble(k: int = 256, seed: int = 5, lo: int = 2000, hi: int = 40000) -> li
 
 
 def solvent_draw(seed: int = 2) -> tuple[float, float]:
-    """c1 ~ U[0.95, 1.05], c2 ~ U[0, 2] from the seed (config 2)."""
+    """c1 ~ U[0.95, 1.05], c2 ~ U[0, 2] from the seed (the 20,000-atom solvated workload)."""
     rng = np.random.default_rng(seed)
     return float(rng.uniform(0.95, 1.05)), float(rng.uniform(0.0, 2.0))

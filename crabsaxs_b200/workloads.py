@@ -1,22 +1,22 @@
 """Named benchmark workloads, run a fixed number of times (for profilers).
 
-    python -m crabsaxs_b200.workloads debye-config2 [--variant V] [--repeats N]
-    python -m crabsaxs_b200.workloads multipole-config3 [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
-    python -m crabsaxs_b200.workloads gradient-config4 [--repeats N]
-    python -m crabsaxs_b200.workloads pr-config3 [--bins B] [--repeats N]
-    python -m crabsaxs_b200.workloads grid-config2 [--repeats N]
+    python -m crabsaxs_b200.workloads debye-20k [--variant V] [--repeats N]
+    python -m crabsaxs_b200.workloads multipole-100k [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
+    python -m crabsaxs_b200.workloads gradient-5k [--repeats N]
+    python -m crabsaxs_b200.workloads pr-100k [--bins B] [--repeats N]
+    python -m crabsaxs_b200.workloads grid-20k [--repeats N]
 
-debye-config2: the 20,000-atom synthetic protein plus its adaptive 3 Å
+debye-20k: the 20,000-atom synthetic protein plus its adaptive 3 Å
 hydration sites, 500 q on [0.001, 0.5], one lattice pair plan (atoms by the
 FP32 recurrence kernel, site-site pairs by the exact lattice histogram),
 `repeats` launches of the chosen kernel variant (Q*16 + jb; default: the
 plan's untuned choice).
-multipole-config3: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.
-gradient-config4: 5,000 atoms (R 28 Å), 100 q, chi^2 and its full gradient.
-pr-config3: coordinate features (Rg, Dmax, P(r) with 160 bins) of the
-100,000-atom structure of multipole-config3.
-grid-config2: the exterior 1 Å hydration grid (1.28 million voxels) and the
-adaptive 3 Å grid of the debye-config2 structure, one public call each.
+multipole-100k: 100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50.
+gradient-5k: 5,000 atoms (R 28 Å), 100 q, chi^2 and its full gradient.
+pr-100k: coordinate features (Rg, Dmax, P(r) with 160 bins) of the
+100,000-atom structure of multipole-100k.
+grid-20k: the exterior 1 Å hydration grid (1.28 million voxels) and the
+adaptive 3 Å grid of the debye-20k structure, one public call each.
 Each prints one line with its device or wall times.
 """
 from __future__ import annotations
@@ -32,8 +32,8 @@ from . import api as cs
 from . import synth
 
 
-def debye_config2(engine: cs.Engine, variant: int | None, repeats: int) -> str:
-    w = synth.CONFIG2
+def debye_20k(engine: cs.Engine, variant: int | None, repeats: int) -> str:
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     sites, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
     el = s.element.astype(np.int64)
@@ -56,11 +56,11 @@ def debye_config2(engine: cs.Engine, variant: int | None, repeats: int) -> str:
         engine.check(N.lib.crab_pair_plan_run(engine.handle, plan, repeats, 0, ms.ctypes.data_as(N.D)))
     finally:
         N.lib.crab_pair_plan_destroy(plan)
-    return f"debye-config2 variant={variant} step_ms={np.round(ms, 3).tolist()}"
+    return f"debye-20k variant={variant} step_ms={np.round(ms, 3).tolist()}"
 
 
-def multipole_config3(engine: cs.Engine, precision: str, repeats: int) -> str:
-    w = synth.CONFIG3
+def multipole_100k(engine: cs.Engine, precision: str, repeats: int) -> str:
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     prec = {"fp64": N.PREC_FP64, "fp32": N.PREC_FP32, "tf32": N.PREC_TF32, "tf32x2": N.PREC_TF32_SPLIT}[precision]
     wall = []
@@ -68,11 +68,11 @@ def multipole_config3(engine: cs.Engine, precision: str, repeats: int) -> str:
         t0 = time.perf_counter()
         cs.multipole_intensity(s, w.q, 50, precision=prec, engine=engine)
         wall.append((time.perf_counter() - t0) * 1e3)
-    return f"multipole-config3 precision={precision} wall_ms={np.round(wall, 3).tolist()}"
+    return f"multipole-100k precision={precision} wall_ms={np.round(wall, 3).tolist()}"
 
 
-def gradient_config4(engine: cs.Engine, repeats: int) -> str:
-    w = synth.CONFIG4
+def gradient_5k(engine: cs.Engine, repeats: int) -> str:
+    w = synth.GRADIENT_5K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     y = np.ones(len(w.q))
     sigma = np.full(len(w.q), 0.01)
@@ -81,11 +81,11 @@ def gradient_config4(engine: cs.Engine, repeats: int) -> str:
         t0 = time.perf_counter()
         cs.chi2_grad(s, w.q, y, sigma, cs.SolventParams(), 1.0, 0.0, engine=engine)
         wall.append((time.perf_counter() - t0) * 1e3)
-    return f"gradient-config4 wall_ms={np.round(wall, 3).tolist()}"
+    return f"gradient-5k wall_ms={np.round(wall, 3).tolist()}"
 
 
-def pr_config3(engine: cs.Engine, bins: int, repeats: int) -> str:
-    w = synth.CONFIG3
+def pr_100k(engine: cs.Engine, bins: int, repeats: int) -> str:
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     wall, dev, hist = [], [], []
     for _ in range(repeats):
@@ -95,12 +95,12 @@ def pr_config3(engine: cs.Engine, bins: int, repeats: int) -> str:
         total_ms, hist_ms, pairs, mode = cs.pr_last_timing(engine)
         dev.append(total_ms)
         hist.append(hist_ms)
-    return (f"pr-config3 bins={bins} mode={mode} pairs={pairs:.6g} wall_ms={np.round(wall, 3).tolist()} "
+    return (f"pr-100k bins={bins} mode={mode} pairs={pairs:.6g} wall_ms={np.round(wall, 3).tolist()} "
             f"device_ms={np.round(dev, 3).tolist()} histogram_ms={np.round(hist, 3).tolist()}")
 
 
-def grid_config2(engine: cs.Engine, repeats: int) -> str:
-    w = synth.CONFIG2
+def grid_20k(engine: cs.Engine, repeats: int) -> str:
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     ext, ada = [], []
     for _ in range(repeats):
@@ -111,30 +111,30 @@ def grid_config2(engine: cs.Engine, repeats: int) -> str:
         t2 = time.perf_counter()
         ext.append((t1 - t0) * 1e3)
         ada.append((t2 - t1) * 1e3)
-    return (f"grid-config2 exterior_sites={len(sites_e)} adaptive_sites={len(sites_a)} "
+    return (f"grid-20k exterior_sites={len(sites_e)} adaptive_sites={len(sites_a)} "
             f"exterior_wall_ms={np.round(ext, 3).tolist()} adaptive_wall_ms={np.round(ada, 3).tolist()}")
 
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
     ap.add_argument("workload",
-                    choices=["debye-config2", "multipole-config3", "gradient-config4", "pr-config3", "grid-config2"])
+                    choices=["debye-20k", "multipole-100k", "gradient-5k", "pr-100k", "grid-20k"])
     ap.add_argument("--bins", type=int, default=160)
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
     ap.add_argument("--repeats", type=int, default=2)
     a = ap.parse_args(argv)
     engine = cs.Engine.default(0)
-    if a.workload == "debye-config2":
-        print(debye_config2(engine, a.variant, a.repeats))
-    elif a.workload == "multipole-config3":
-        print(multipole_config3(engine, a.precision, a.repeats))
-    elif a.workload == "pr-config3":
-        print(pr_config3(engine, a.bins, a.repeats))
-    elif a.workload == "grid-config2":
-        print(grid_config2(engine, a.repeats))
+    if a.workload == "debye-20k":
+        print(debye_20k(engine, a.variant, a.repeats))
+    elif a.workload == "multipole-100k":
+        print(multipole_100k(engine, a.precision, a.repeats))
+    elif a.workload == "pr-100k":
+        print(pr_100k(engine, a.bins, a.repeats))
+    elif a.workload == "grid-20k":
+        print(grid_20k(engine, a.repeats))
     else:
-        print(gradient_config4(engine, a.repeats))
+        print(gradient_5k(engine, a.repeats))
 
 
 if __name__ == "__main__":

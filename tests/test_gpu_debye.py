@@ -88,10 +88,10 @@ def test_vacuum_intensity_matches_oracle_helix(engine, implicit):  # scattering.
     assert np.max(np.abs(got - ref) / ref) <= INTENSITY_RTOL
 
 
-def test_vacuum_intensity_config1(engine):
+def test_vacuum_intensity_1k(engine):
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG1
+    w = synth.DEBYE_1K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     got = cs.debye_intensity(s, w.q, engine=engine)
     ref = O.debye_intensity(_oracle_atoms(s), w.q)
@@ -136,10 +136,10 @@ def test_solvent_basis_two_atoms_nonuniform_q(engine):  # solvent.rs:650-665
 
 
 @pytest.mark.parametrize("c1,c2", [(1.0, 0.0), (0.97, 1.3), (1.05, 2.0)])
-def test_solvent_config1_matches_oracle(engine, c1, c2):
+def test_solvent_1k_matches_oracle(engine, c1, c2):
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG1
+    w = synth.DEBYE_1K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     sp = cs.SolventParams(c1=c1, c2=c2)
     got = cs.solvent_corrected_intensity(s, w.q, sp, engine=engine)
@@ -164,12 +164,12 @@ def test_adaptive_grid_solvent_basis_matches_oracle(engine, spacing):
         assert np.max(np.abs(gb[k] - rb[k]) / rb[k]) <= INTENSITY_RTOL
 
 
-def test_config2_fp32_matches_fp64_and_oracle(engine):
-    """Full config 2 (20k atoms + 3 Å adaptive sites, 500 q): FP32 vs the FP64 device kernel
+def test_20k_solvated_fp32_matches_fp64_and_oracle(engine):
+    """The full solvated workload (20k atoms + 3 Å adaptive sites, 500 q): FP32 vs the FP64 device kernel
     at every q, and vs the CPU oracle at four q values."""
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG2
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     c1, c2 = synth.solvent_draw(w.seed)
     sp = cs.SolventParams(c1=c1, c2=c2, hydration_model=cs.HydrationModel.AdaptiveGrid,
@@ -267,7 +267,7 @@ def test_pair_kernel_launches_are_counted(engine):
     assert launches >= 1 and ms > 0 and pq == pytest.approx(300 * 299 / 2 * 40)
 
 
-def test_lattice_plan_matches_fp64_config2(engine):
+def test_lattice_plan_matches_fp64_20k(engine):
     """The site–site block from the lattice histogram equals the FP64 pair sum
     over the same sites; every other block stays within the FP32 bound."""
     import ctypes as C
@@ -275,7 +275,7 @@ def test_lattice_plan_matches_fp64_config2(engine):
     from crabsaxs_b200 import _native as N
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG2
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     sites, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
     el = s.element.astype(np.int64)

@@ -94,10 +94,10 @@ def _debye_experiment(s, q, c1, c2, scale, bg, seed):
     return clean + sigma * np.random.default_rng(seed).normal(size=len(q)), sigma
 
 
-def test_lbfgs_and_nelder_mead_agree_on_config4(engine):
+def test_lbfgs_and_nelder_mead_agree_on_5k_atoms(engine):
     """5,000 atoms (R 28 Å), 100 q, Debye method: the analytic-gradient L-BFGS fit
     and the derivative-free Nelder-Mead fit land on the same optimum."""
-    w = synth.CONFIG4
+    w = synth.GRADIENT_5K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     y, sigma = _debye_experiment(s, w.q, 1.015, 0.9, 3.7, 50.0, 11)
     ex = cs.ExperimentalCurve(w.q, y, sigma)

@@ -42,7 +42,7 @@ def _sinc(x):
 
 
 def _experiment(s, q, seed):
-    """Config 4: Debye of a copy perturbed by N(0, 0.5 Å), scale 3.7, background 1e-3·I(0),
+    """5,000 atoms: Debye of a copy perturbed by N(0, 0.5 Å), scale 3.7, background 1e-3·I(0),
     σ(q) = 0.01·I(q) + 1e-4·I(0), Gaussian noise of that σ."""
     rng = np.random.default_rng(seed)
     pert = cs.Structure(s.xyz + rng.normal(scale=0.5, size=s.xyz.shape), s.element)
@@ -69,13 +69,13 @@ def test_gradient_matches_oracle_analytic(engine):
         assert np.max(np.abs(gp - rgp) / np.maximum(np.abs(rgp), 1e-12 * np.abs(rgp).max())) <= 1e-4
 
 
-def test_gradient_config4_central_differences(engine):
+def test_gradient_5k_central_differences(engine):
     """5,000 atoms (R 28 Å), 100 q: 64 seeded coordinates against FP64 central differences
     (h = 1e-4 Å) computed with incremental O(N·Nq) pair deltas, and the four scalars against
     FP64 central differences of the oracle's χ²."""
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG4
+    w = synth.GRADIENT_5K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     q = w.q
     y, sigma = _experiment(s, q, 4)

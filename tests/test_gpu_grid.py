@@ -32,10 +32,10 @@ def test_adaptive_grid_bit_exact(engine, spacing):
         assert np.array_equal(got, ref), name
 
 
-def test_adaptive_grid_config2_bit_exact(engine):
+def test_adaptive_grid_20k_bit_exact(engine):
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG2
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     got, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
     ref, _ = O.adaptive_grid(s.xyz, 3.0)
@@ -120,11 +120,11 @@ def test_exterior_grid_many_sweep_rounds(engine):
     assert not chamber(0.0).any() and chamber(10.0).any()
 
 
-def test_exterior_grid_config2_bit_exact(engine):
+def test_exterior_grid_20k_bit_exact(engine):
     """20,000 atoms at 1 Å: a 1.3-million-voxel box filled in about 11 rounds."""
     from crabsaxs_b200 import synth
 
-    w = synth.CONFIG2
+    w = synth.DEBYE_20K_SOLVATED
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     got, gv = cs.hydration_grid_exterior(s, engine=engine)
     ref, rv = O.exterior_grid(s.xyz, s.element.astype(np.int32))

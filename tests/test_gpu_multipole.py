@@ -130,10 +130,10 @@ def test_wide_q_range_uses_several_radial_segments(engine):
     assert _rel(got32, ref) <= FP32_RTOL
 
 
-def test_config3_subset_matches_oracle_and_fp64(engine):
+def test_100k_subset_matches_oracle_and_fp64(engine):
     """100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50: FP32 against the
     FP64 device path on every q, and against the oracle on every 50th q."""
-    w = synth.CONFIG3
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     got32 = cs.multipole_intensity(s, w.q, 50, engine=engine)
     got64 = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_FP64, engine=engine)
@@ -184,11 +184,11 @@ def test_tensor_core_moments_match_oracle(engine, prec, tol):
     assert _rel(got2, ref2) <= tol
 
 
-def test_tensor_core_split_matches_fp64_on_config3(engine):
+def test_tensor_core_split_matches_fp64_on_100k_atoms(engine):
     """100,000 atoms, 1000 q, L = 50: the two-term TF32 GEMM against the FP64
     device path (2e-6), and the solvent basis on a grid (1e-6 of each term's
     largest magnitude; the combined curve within the FP32 contract)."""
-    w = synth.CONFIG3
+    w = synth.ATOMS_100K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
     got = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_TF32_SPLIT, engine=engine)
     ref = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_FP64, engine=engine)

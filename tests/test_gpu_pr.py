@@ -170,11 +170,11 @@ def test_large_structure_matches_oracle(engine):
     assert dmax == rd and np.max(np.abs(hist - rh)) <= SUM_RTOL * np.max(rh)
 
 
-def test_config3_size_properties(engine):
+def test_100k_atoms_size_properties(engine):
     """100,000 atoms (R 80 Å): unit weights count every pair exactly once
     (sum n(n-1)/2, exact in f64), weighted sums total ((Σw)² - Σw²)/2, and
     dmax is at least the largest distance between extreme atoms."""
-    w_ = synth.CONFIG3
+    w_ = synth.ATOMS_100K
     s = synth.protein(w_.seed, w_.n_atoms, w_.radius)
     n = len(s.xyz)
     _, h1 = cs.pair_distance_histogram(s.xyz, np.ones(n), 160, engine=engine)
