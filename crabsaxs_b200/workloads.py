@@ -115,7 +115,7 @@ def grid_20k(engine: cs.Engine, repeats: int) -> str:
             f"exterior_wall_ms={np.round(ext, 3).tolist()} adaptive_wall_ms={np.round(ada, 3).tolist()}")
 
 
-def main(argv=None) -> None:
+def parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser(prog="python -m crabsaxs_b200.workloads", description=__doc__.splitlines()[0])
     ap.add_argument("workload",
                     choices=["debye-20k", "multipole-100k", "gradient-5k", "pr-100k", "grid-20k"])
@@ -123,7 +123,11 @@ def main(argv=None) -> None:
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
     ap.add_argument("--repeats", type=int, default=2)
-    a = ap.parse_args(argv)
+    return ap
+
+
+def main(argv=None) -> None:
+    a = parser().parse_args(argv)
     engine = cs.Engine.default(0)
     if a.workload == "debye-20k":
         print(debye_20k(engine, a.variant, a.repeats))
