@@ -212,15 +212,25 @@ def cpu_baseline_run(s, threads: int, fraction: float = 1.0):
     return (m * (m - 1) / 2.0) * len(sub) / dt, len(sub), dt, m
 
 
+class _OracleStructure:
+    """The workload structure as plain arrays (the fields cpu_baseline_run reads)."""
+
+    def __init__(self, xyz, element):
+        self.xyz = xyz
+        self.element = element
+        self.group = np.full(len(element), -1, dtype=np.int8)
+        self.occupancy = np.ones(len(element))
+        self.atom_count = len(element)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    import crabsaxs_b200 as cs
-    from crabsaxs_b200 import synth
-
     import oracle as O
 
-    s = synth.protein(SEED, N_ATOMS, RADIUS)
+    # the same seeded structure as the GPU arm's, made by the oracle library
+    # (this arm loads no product code)
+    s = _OracleStructure(*O.synth_protein(SEED, N_ATOMS, RADIUS))
     n_sites = len(O.adaptive_grid(s.xyz, 3.0)[0])  # the workload's sites (the timed sample is half the atoms)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):

@@ -100,6 +100,8 @@ _SIGS = {
     "crab_ctx_stats": (C.c_int, [P, C.POINTER(I64), D, D]),
     "crab_ctx_reset_stats": (C.c_int, [P]),
     "crab_ctx_workspace_bytes": (C.c_int, [P, C.POINTER(I64)]),
+    "crab_ctx_set_wait_budget": (C.c_int, [P, I64]),
+    "crab_ctx_fail_allocations": (C.c_int, [P, I64]),
     "crab_united_atom_group": (C.c_int, [C.c_char_p, C.c_char_p]),
     "crab_form_factor": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
     "crab_excluded_volume_for_atom": (C.c_double, [C.c_int, C.c_int, C.c_int]),

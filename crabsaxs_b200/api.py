@@ -111,6 +111,17 @@ class Engine:
     def reset_stats(self) -> None:
         N.lib.crab_ctx_reset_stats(self.handle)
 
+    def set_wait_budget(self, iterations: int | None) -> None:
+        """Iteration budget of the kernels' bounded device-side waits (None:
+        the defaults; 0: the first wait gives up and the call raises Other
+        with status CRAB_ETIMEOUT).  For tests of the error paths."""
+        self.check(N.lib.crab_ctx_set_wait_budget(self.handle, -1 if iterations is None else int(iterations)))
+
+    def fail_allocations(self, after: int | None) -> None:
+        """Let `after` more device or pinned host allocations of this context
+        succeed and fail the rest with CRAB_ENOMEM (None: off).  For tests."""
+        self.check(N.lib.crab_ctx_fail_allocations(self.handle, -1 if after is None else int(after)))
+
     def close(self) -> None:
         if self.handle:
             N.lib.crab_ctx_destroy(self.handle)

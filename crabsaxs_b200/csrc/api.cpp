@@ -49,9 +49,16 @@ void crab::trace_mark(const char* name) {
                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g_trace_top->t0).count());
 }
 
+void crab_ctx::alloc_check() {
+  if (fail_alloc_after < 0) return;
+  if (fail_alloc_after == 0) throw crab::Error(CRAB_ENOMEM, "allocation failed (injected by crab_ctx_fail_allocations)");
+  --fail_alloc_after;
+}
+
 void* crab_ctx::dev(const std::string& name, size_t bytes) {
   crab::DevBuf& b = bufs[name];
   if (b.bytes < bytes || !b.ptr) {
+    alloc_check();
     if (b.ptr) cudaFree(b.ptr);
     b.ptr = nullptr;
     b.bytes = 0;
@@ -65,6 +72,7 @@ void* crab_ctx::dev(const std::string& name, size_t bytes) {
 void* crab_ctx::host(const std::string& name, size_t bytes) {
   crab::HostBuf& b = hbufs[name];
   if (b.bytes < bytes || !b.ptr) {
+    alloc_check();
     if (b.ptr) cudaFreeHost(b.ptr);
     b.ptr = nullptr;
     b.bytes = 0;
@@ -593,6 +601,16 @@ int crab_ctx_set_pair_variant(crab_ctx* ctx, int32_t variant) {
     require(variant == 0 || pair_variant_known(variant), "unknown kernel variant " + std::to_string(variant));
     ctx->pair_variant = variant;
   });
+}
+
+int crab_ctx_set_wait_budget(crab_ctx* ctx, int64_t iterations) {
+  if (!ctx) return CRAB_EINVAL;
+  GUARD(ctx, { ctx->wait_budget = iterations < 0 ? -1 : (int)std::min<int64_t>(iterations, 1 << 30); });
+}
+
+int crab_ctx_fail_allocations(crab_ctx* ctx, int64_t after) {
+  if (!ctx) return CRAB_EINVAL;
+  GUARD(ctx, { ctx->fail_alloc_after = after < 0 ? -1 : after; });
 }
 
 int crab_pair_plan_select(crab_ctx* ctx, crab_pair_plan* plan, int32_t variant) {

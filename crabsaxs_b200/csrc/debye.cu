@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     k_pair_fp32(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                 int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T, int wide,
                 double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
-                const int64_t* __restrict__ work_out) {
+                const int64_t* __restrict__ work_out, int budget) {
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
   __syncthreads();
   unsigned phase_bits = 0u;  // bit b: parity of the next completion of bar[b]
   bool ok = true;
+  if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(next_work, 1);
@@ -210,12 +211,24 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
         mbar_expect_tx(&bar[buf ^ 1], kTile * sizeof(float4));
         bulk_g2s(&sj[buf ^ 1][0], atoms + (size_t)(jt + 1) * kTile, kTile * sizeof(float4), &bar[buf ^ 1]);
       }
-      if (!mbar_wait(&bar[buf], (phase_bits >> buf) & 1u)) {
+      const unsigned ph = (phase_bits >> buf) & 1u;
+      if (!mbar_wait(&bar[buf], ph, budget)) {
         if (tid == 0) atomicExch(status, CRAB_ETIMEOUT);
         ok = false;
       }
       phase_bits ^= 1u << buf;
-      if (!__syncthreads_and(ok)) { ok = false; break; }
+      if (!__syncthreads_and(ok)) {
+        // leave only after this CTA's copies in flight have landed: the
+        // current tile's and the prefetched one's (their shared memory may
+        // belong to the next CTA on this SM once this one exits)
+        if (tid == 0) {
+          mbar_wait(&bar[buf], ph, kDrainBudget);
+          if (jt + 1 < jt1) mbar_wait(&bar[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u, kDrainBudget);
+        }
+        __syncthreads();
+        ok = false;
+        break;
+      }
       const bool diag = (jt == it);
       // JB j atoms per iteration, their recurrences advanced in pairs in
       // packed f32x2 registers (JB/2 independent chains per instruction stream)
@@ -296,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                    int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
                    int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
-                   const int64_t* __restrict__ work_out) {
+                   const int64_t* __restrict__ work_out, int budget) {
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
@@ -311,6 +324,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
   __syncthreads();
   unsigned phase_bits = 0u;
   bool ok = true;
+  if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(next_work, 1);
@@ -345,12 +359,24 @@ __global__ void __launch_bounds__(kThreads, OCC)
         mbar_expect_tx(&bar[buf ^ 1], kTile * sizeof(float4));
         bulk_g2s(&sj[buf ^ 1][0], atoms + (size_t)(jt + 1) * kTile, kTile * sizeof(float4), &bar[buf ^ 1]);
       }
-      if (!mbar_wait(&bar[buf], (phase_bits >> buf) & 1u)) {
+      const unsigned ph = (phase_bits >> buf) & 1u;
+      if (!mbar_wait(&bar[buf], ph, budget)) {
         if (tid == 0) atomicExch(status, CRAB_ETIMEOUT);
         ok = false;
       }
       phase_bits ^= 1u << buf;
-      if (!__syncthreads_and(ok)) { ok = false; break; }
+      if (!__syncthreads_and(ok)) {
+        // leave only after this CTA's copies in flight have landed: the
+        // current tile's and the prefetched one's (their shared memory may
+        // belong to the next CTA on this SM once this one exits)
+        if (tid == 0) {
+          mbar_wait(&bar[buf], ph, kDrainBudget);
+          if (jt + 1 < jt1) mbar_wait(&bar[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u, kDrainBudget);
+        }
+        __syncthreads();
+        ok = false;
+        break;
+      }
       const bool diag = (jt == it);
 #pragma unroll 1
       for (int j = 0; j < kTile; j += JB) {
@@ -484,24 +510,24 @@ std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_fr
 template <int Q, int JB>
 void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
                  const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
-                 int* next_work, const int64_t* work_out) {
+                 int* next_work, const int64_t* work_out, int budget) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q, JB>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
-                                                     status, next_work, work_out);
+                                                     status, next_work, work_out, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
 template <int Q, int JB, int OCC>
 void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                     int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
-                    int* status, int* next_work, const int64_t* work_out) {
+                    int* status, int* next_work, const int64_t* work_out, int budget) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32_pq<Q, JB, OCC><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
-                                                        status, next_work, work_out);
+                                                        status, next_work, work_out, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -873,7 +899,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH(QQ, JJ)                                                                                    \
   if (P.Q == QQ && P.jb == JJ) {                                                                                 \
     launch_fp32<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
-                        T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);                                  \
+                        T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget);               \
     launched = true;                                                                                             \
   }
     bool launched = false;
@@ -890,7 +916,8 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH_PQ(QQ, JJ, OO, CODE)                                                                        \
   if (P.Q == QQ && P.jb == CODE) {                                                                               \
     launch_fp32_pq<QQ, JJ, OO>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,          \
-                               P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out);           \
+                               P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,            \
+                               ctx->wait_budget);                                                                 \
     launched = true;                                                                                             \
   }
     CRAB_LAUNCH_PQ(64, 2, 4, 2 + kPackedQ)

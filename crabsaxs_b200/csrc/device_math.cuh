@@ -25,11 +25,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                "l"(src), "r"(bytes), "r"(b)
                : "memory");
 }
+// Iteration budgets of the bounded waits.  The kernels take the budget of
+// their context (crab_ctx_set_wait_budget; these defaults otherwise); a CTA
+// that gives up drains its own copies in flight with kDrainBudget, which no
+// context option shortens.
+constexpr int kWaitBudget = 1 << 22;   // suspending try_wait (pair kernels)
+constexpr int kSpinBudget = 1 << 26;   // non-suspending test_wait (tensor-core pipeline)
+constexpr int kDrainBudget = 1 << 24;
+
 // Bounded wait on an mbarrier phase. Returns false when the iteration budget
-// runs out (the caller records an error and stops using the buffer).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+// runs out (the caller records an error and stops using the buffer); a
+// budget of 0 gives up at once.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase, int budget = kWaitBudget) {
   unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < budget; ++it) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -97,9 +106,9 @@ __device__ __forceinline__ void unpack2(unsigned long long v, float& x, float& y
 
 // Bounded spin on an mbarrier phase with the non-suspending test_wait (for
 // waits expected to be short, where a suspended try_wait would oversleep).
-__device__ __forceinline__ bool mbar_spin(uint64_t* bar, unsigned phase) {
+__device__ __forceinline__ bool mbar_spin(uint64_t* bar, unsigned phase, int budget = kSpinBudget) {
   unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-  for (int it = 0; it < (1 << 26); ++it) {
+  for (int it = 0; it < budget; ++it) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

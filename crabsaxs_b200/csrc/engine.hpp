@@ -100,6 +100,16 @@ struct crab_ctx {
   // GEMM alone, and the GEMM's algorithmic FLOP count
   double last_mp_ms = 0.0, last_mp_gemm_ms = 0.0, last_mp_gemm_flop = 0.0;
   int pair_variant = 0;  // kernel variant of plans built by one-shot calls (0: automatic)
+  // Failure injection on the host (crab_ctx_set_wait_budget,
+  // crab_ctx_fail_allocations): the iteration budget of the kernels'
+  // bounded waits (-1: their defaults), and the number of device or pinned
+  // host allocations that still succeed before the next one fails with
+  // CRAB_ENOMEM (-1: never).
+  int wait_budget = -1;
+  int64_t fail_alloc_after = -1;
+  // Called before every allocation the context makes: throws CRAB_ENOMEM
+  // once the injected failure is due.
+  void alloc_check();
   // device times of the last pair-distance histogram: all its kernels, the
   // histogram kernel alone, and the pairs it binned
   double last_pr_ms = 0.0, last_pr_hist_ms = 0.0, last_pr_pairs = 0.0;
@@ -242,6 +252,7 @@ struct PairPlan {
 inline void* plan_alloc(crab_ctx* ctx, PairPlan& P, std::vector<void*>& list, const char* name, size_t bytes) {
   bytes = bytes ? bytes : 1;
   if (P.pooled) return ctx->dev(std::string("pair.") + name, bytes);
+  ctx->alloc_check();
   void* p = nullptr;
   CRAB_CUDA_CHECK(cudaMalloc(&p, bytes));
   list.push_back(p);

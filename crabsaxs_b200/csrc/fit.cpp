@@ -360,90 +360,7 @@ void mix_curves(const std::vector<const double*>& curves, const double* w, int64
   }
 }
 
-// ensemble.rs:383-434
-void solve_linear_fixed(const double* th, const Data& d, int scale_mode, double scale_value, int bg_mode,
-                        double bg_value, double* so, double* bo, double* co) {
-  double scale;
-  if (scale_mode == CRAB_SCALE_FIT) {
-    double num = 0, den = 0;
-    for (int64_t i = 0; i < d.n; ++i) {
-      num += th[i] * d.y[i] / (d.sigma[i] * d.sigma[i]);
-      den += th[i] * th[i] / (d.sigma[i] * d.sigma[i]);
-    }
-    scale = den > 0.0 ? num / den : 0.0;
-  } else scale = scale_value;
-  scale = std::fmax(scale, 0.0);
-  double bg;
-  if (bg_mode == CRAB_BG_FIT) {
-    double num = 0, den = 0;
-    for (int64_t i = 0; i < d.n; ++i) {
-      num += (d.y[i] - scale * th[i]) / (d.sigma[i] * d.sigma[i]);
-      den += 1.0 / (d.sigma[i] * d.sigma[i]);
-    }
-    bg = den > 0.0 ? num / den : 0.0;
-  } else if (bg_mode == CRAB_BG_FIXED_ZERO) bg = 0.0;
-  else bg = bg_value;
-  double chi = 0.0;
-  for (int64_t i = 0; i < d.n; ++i) {
-    const double r = (scale * th[i] + bg - d.y[i]) / d.sigma[i];
-    chi += r * r;
-  }
-  *so = scale;
-  *bo = bg;
-  *co = chi / (double)std::max<int64_t>(d.n - 1, 1);
-}
-
 }  // namespace
-
-// ensemble.rs:449-465
-void project_simplex(const double* v, int64_t n, double* out) {
-  std::vector<double> sorted(v, v + n);
-  std::sort(sorted.begin(), sorted.end(), [](double a, double b) { return a > b; });
-  double cumulative = 0.0;
-  int64_t rho = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    cumulative += sorted[i];
-    if (sorted[i] + (1.0 - cumulative) / (double)(i + 1) > 0.0) rho = i + 1;
-  }
-  double top = 0.0;
-  for (int64_t i = 0; i < rho; ++i) top += sorted[i];
-  const double theta = (top - 1.0) / (double)std::max<int64_t>(rho, 1);
-  for (int64_t i = 0; i < n; ++i) out[i] = std::fmax(v[i] - theta, 0.0);
-}
-
-// ensemble.rs:317-381 — projected gradient on the simplex for one candidate.
-void optimize_weights(const std::vector<const double*>& curves, const Data& d, const crab_fit_options& o, bool uniform,
-                      double regularization, double* w, double* so, double* bo, double* chi2, double* fitted) {
-  const int64_t K = (int64_t)curves.size(), nq = d.n;
-  std::vector<double> mix(nq), res(nq), grad(K), step(K), prop(K);
-  for (int64_t k = 0; k < K; ++k) w[k] = 1.0 / (double)K;
-  if (!uniform) {
-    for (int it = 0; it < 250; ++it) {
-      mix_curves(curves, w, nq, mix.data());
-      double s, b, c;
-      solve_linear_fixed(mix.data(), d, o.scale_mode, o.scale_value, o.bg_mode, o.bg_value, &s, &b, &c);
-      for (int64_t i = 0; i < nq; ++i) res[i] = (s * mix[i] + b - d.y[i]) / d.sigma[i];
-      for (int64_t k = 0; k < K; ++k) {
-        double acc = 0.0;
-        for (int64_t i = 0; i < nq; ++i) acc += res[i] * s * curves[k][i] / d.sigma[i];
-        grad[k] = 2.0 * acc + 2.0 * regularization * (w[k] - 1.0 / (double)K);
-      }
-      double nrm = 0.0;
-      for (int64_t k = 0; k < K; ++k) nrm += grad[k] * grad[k];
-      nrm = std::fmax(std::sqrt(nrm), 1.0);
-      for (int64_t k = 0; k < K; ++k) step[k] = w[k] - 0.05 * grad[k] / nrm;
-      project_simplex(step.data(), K, prop.data());
-      double delta = 0.0;
-      for (int64_t k = 0; k < K; ++k) delta += std::fabs(prop[k] - w[k]);
-      std::copy(prop.begin(), prop.end(), w);
-      if (delta < 1e-8) break;
-    }
-  }
-  mix_curves(curves, w, nq, mix.data());
-  solve_linear_fixed(mix.data(), d, o.scale_mode, o.scale_value, o.bg_mode, o.bg_value, so, bo, chi2);
-  if (fitted)
-    for (int64_t i = 0; i < nq; ++i) fitted[i] = *so * mix[i] + *bo;
-}
 
 }  // namespace crab
 

@@ -571,7 +571,7 @@ struct NoAllocHeader {
   Box box;
   uint64_t count;
   double inner, outer;
-  int status;  // 0 ok, 1 grid larger than the static scratch
+  int status;  // 0 ok, 1 grid larger than the static scratch, 2 a coordinate not finite
 };
 static_assert(sizeof(NoAllocHeader) <= 256, "header must fit its 256-byte slot");
 
@@ -591,8 +591,17 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 __global__ void k_noalloc_prologue(const double* __restrict__ xyz, int64_t n, double spacing, double clearance,
                                    double padding, NoAllocHeader* hdr) {
   double c[3] = {0.0, 0.0, 0.0};
+  bool finite = true;  // the allocating entry point rejects the same input (crab_structure_create)
   for (int64_t i = 0; i < n; ++i)
-    for (int d = 0; d < 3; ++d) c[d] = __dadd_rn(c[d], xyz[3 * i + d]);
+    for (int d = 0; d < 3; ++d) {
+      finite = finite && isfinite(xyz[3 * i + d]);
+      c[d] = __dadd_rn(c[d], xyz[3 * i + d]);
+    }
+  if (!finite) {
+    hdr->status = 2;
+    hdr->count = 0ull;
+    return;
+  }
   for (int d = 0; d < 3; ++d) c[d] = __ddiv_rn(c[d], (double)n);
   double acc = 0.0;
   for (int64_t i = 0; i < n; ++i) {
@@ -660,6 +669,9 @@ __global__ void k_noalloc_emit(const uint8_t* __restrict__ shell, const uint8_t*
 
 // Device address of the scratch array, looked up once per device (the name
 // g_noalloc_scratch is only a host-side handle; kernels need this address).
+// The cached address belongs to the device's current CUDA context: after a
+// cudaDeviceReset of that device it is stale, so a process that resets a
+// device must not call the entry point on it again.
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_dev[256] = {};
 
@@ -702,7 +714,7 @@ extern "C" int crab_hydration_grid_adaptive_noalloc(const double* d_xyz, int64_t
   NoAllocHeader h;
   if (cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CRAB_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return CRAB_ECUDA;
-  if (h.status) return CRAB_EINVAL;  // grid larger than CRAB_NOALLOC_MAX_VOXELS
+  if (h.status) return CRAB_EINVAL;  // a coordinate not finite, or a grid larger than CRAB_NOALLOC_MAX_VOXELS
   uint8_t* shell = base + kShellOff;
   uint8_t* mol = base + kMolOff;
   uint32_t* cnt = (uint32_t*)(base + kCntOff);

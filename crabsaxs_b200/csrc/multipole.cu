@@ -382,8 +382,10 @@ __device__ __forceinline__ void tc_chunk(int c, int t, int& row, int& c4) {
 template <int S>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_mp_moments_tc(const float* __restrict__ YT, const float* __restrict__ WT, int64_t n_pad, int lm_pad,
-                    const MpWork* __restrict__ work, double* __restrict__ part, int* __restrict__ status) {
+                    const MpWork* __restrict__ work, double* __restrict__ part, int* __restrict__ status,
+                    int budget) {
   static_assert(S == 1 || S == 2, "one or two TF32 terms");
+  if (budget < 0) budget = dev::kSpinBudget;  // the context's default
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);  // S A terms, then S B terms
   unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int d = s % kTcSlots;
       cp_async_wait<kTcRing - 1>();  // this thread's chunks of stage s have landed
       const float4* mine = reinterpret_cast<const float4*>(ring + ((s % kTcRing) * kTcProducers + t) * kTcChunks * 16);
-      if (s >= kTcSlots && (failed() || !dev::mbar_spin(&empty[d], (unsigned)((s / kTcSlots - 1) & 1)))) {
+      if (s >= kTcSlots && (failed() || !dev::mbar_spin(&empty[d], (unsigned)((s / kTcSlots - 1) & 1), budget))) {
         ok = false;
         break;
       }
@@ -479,8 +481,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
       for (int s = 0; s < nk; ++s) {
         const int d = s % kTcSlots, a = s % kTcAccs;
-        if (failed() || !dev::mbar_spin(&full[d], (unsigned)((s / kTcSlots) & 1)) ||
-            (s >= kTcAccs && !dev::mbar_spin(&accfree[a], (unsigned)((s / kTcAccs - 1) & 1)))) {
+        if (failed() || !dev::mbar_spin(&full[d], (unsigned)((s / kTcSlots) & 1), budget) ||
+            (s >= kTcAccs && !dev::mbar_spin(&accfree[a], (unsigned)((s / kTcAccs - 1) & 1), budget))) {
           ok = false;
           break;
         }
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     for (int i = 0; i < 32; ++i) acc[i] = 0.0;
     for (int s = 0; s < nk; ++s) {
       const int a = s % kTcAccs;
-      if (failed() || !dev::mbar_spin(&accfull[a], (unsigned)((s / kTcAccs) & 1))) {
+      if (failed() || !dev::mbar_spin(&accfull[a], (unsigned)((s / kTcAccs) & 1), budget)) {
         ok = false;
         break;
       }
@@ -915,7 +917,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_tc<SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                          (int)tc_smem_bytes<SS>()));                                              \
     k_mp_moments_tc<SS><<<(unsigned)work.size(), kTcThreads, tc_smem_bytes<SS>(), s>>>(                           \
-        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_part, d_status);                            \
+        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_part, d_status, ctx->wait_budget);          \
   }
       CRAB_TC(1)
       CRAB_TC(2)

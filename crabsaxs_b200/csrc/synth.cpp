@@ -9,13 +9,17 @@
 // Elements are drawn C 63 %, N 17 %, O 19 %, S 1 %.  The generator uses
 // splitmix64-seeded xoshiro256** and Box–Muller normals so the same seed gives
 // the same structure on every platform.
+//
+// This file depends on nothing but the C ABI header, so the oracle library
+// compiles the same source under another symbol name: a measurement of the
+// reference's CPU path can build its input without loading this library.
 
 #include <cmath>
 #include <cstdint>
 #include <unordered_map>
 #include <vector>
 
-#include "engine.hpp"
+#include "crab_cuda.h"
 
 namespace {
 

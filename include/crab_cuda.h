@@ -129,6 +129,19 @@ int crab_ctx_stats(crab_ctx* ctx, int64_t* kernel_launches, double* last_pair_ke
 int crab_ctx_reset_stats(crab_ctx* ctx);
 /* Device-resident workspace size in bytes (for sizing studies). */
 int crab_ctx_workspace_bytes(crab_ctx* ctx, int64_t* bytes);
+/* Failure injection for tests of the error paths (no counterpart in the
+ * reference; its error cases are SaxsError values, src/error.rs:4-25).
+ * crab_ctx_set_wait_budget: iteration budget of every bounded device-side
+ * wait (mbarrier waits on bulk copies and tensor-core stages) in kernels
+ * this context launches; 0 makes the first wait give up, a negative value
+ * restores the defaults.  A kernel whose wait runs out drains its own copies
+ * and tensor-core work in flight (with a budget this option does not
+ * shorten), and the call returns CRAB_ETIMEOUT; the context stays usable.
+ * crab_ctx_fail_allocations: the next `after` device or pinned host
+ * allocations of this context succeed, the one after fails with CRAB_ENOMEM
+ * (and every later one until the option is reset); negative: off. */
+int crab_ctx_set_wait_budget(crab_ctx* ctx, int64_t iterations);
+int crab_ctx_fail_allocations(crab_ctx* ctx, int64_t after);
 
 /* ---- atom typing (host) ------------------------------------------------- */
 /* formfactor.rs:357-417 united_atom_group: residue + atom name -> group code,
@@ -280,12 +293,15 @@ int crab_hydration_grid_adaptive(crab_ctx* ctx, crab_struct* st, double spacing,
  * the library until the process exits); a larger box returns CRAB_EINVAL.
  * The function calls no cudaMalloc, cudaFree or allocating library routine.
  * Its first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share
+ * device); make that first call before any stream capture.  The address is
+ * kept for the life of the process: after a cudaDeviceReset of a device, do
+ * not call this function on that device again.  All calls share
  * the array, so calls whose work overlaps on the GPU race: serialise them.
  * *m receives the site count; capacity 0 is a size query (returns CRAB_OK);
  * with a smaller non-zero capacity the sites beyond it are not written and
- * the call returns CRAB_ECAPACITY.  The call
- * synchronises `stream` before returning. */
+ * the call returns CRAB_ECAPACITY.  A coordinate that is not finite returns
+ * CRAB_EINVAL, as crab_structure_create does.  The call synchronises
+ * `stream` before returning. */
 int crab_hydration_grid_adaptive_noalloc(const double* d_xyz, int64_t n, double spacing, double clearance,
                                          double padding, double* d_sites, int64_t capacity, int64_t* m,
                                          double* voxel_volume, void* stream);

@@ -63,6 +63,7 @@ _SIGS = {
     "orc_pair_distance_histogram": (C.c_double, [I64, D, D, I64, D]),
     "orc_normalize_distribution": (C.c_int, [I64, D, D, D, D]),
     "orc_coordinate_features": (C.c_int, [I64, D, I32, I32, D, I64, D, D, D, D, C.POINTER(I64), D, D]),
+    "orc_synth_protein": (C.c_int, [C.c_uint64, I64, C.c_double, D, C.POINTER(C.c_int8)]),
 }
 for _n, (_r, _a) in _SIGS.items():
     _f = getattr(lib, _n)
@@ -291,3 +292,14 @@ def coordinate_features(a: Atoms, bins=160):
         raise ValueError("coordinate features require a non-empty structure")
     k = used.value
     return dict(rg=rg.value, dmax=dmax.value, r=r[:k].copy(), p=p[:k].copy(), pr_rg=prg.value, pr_dmax=pdm.value)
+
+
+def synth_protein(seed, n_atoms, radius):
+    """The seeded synthetic structure of crabsaxs_b200.synth.protein (same
+    generator source, compiled into this library): (xyz [n,3], element int8)."""
+    xyz = np.empty((int(n_atoms), 3))
+    el = np.empty(int(n_atoms), dtype=np.int8)
+    if lib.orc_synth_protein(C.c_uint64(seed), int(n_atoms), float(radius), _d(xyz),
+                             el.ctypes.data_as(C.POINTER(C.c_int8))) != 0:
+        raise ValueError("invalid synthetic structure request")
+    return xyz, el

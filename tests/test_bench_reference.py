@@ -1,6 +1,7 @@
 """bench.py --impl reference (the reference's CPU algorithm, the oracle's f64
 restatement, on the host cores) prints one JSON line with the keys the bench
-contract asks for, on the same workload as the GPU arm."""
+contract asks for, on the same workload as the GPU arm, without loading the
+product library."""
 import json
 import subprocess
 import sys
@@ -9,10 +10,24 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parents[1]
 
 
+RUN_AND_LIST_LIBRARIES = """
+import runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "3"]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit as e:
+    if e.code:
+        raise
+maps = open("/proc/self/maps").read()
+print("PRODUCT_LIBRARY_LOADED=" + str("libcrabsaxs_b200" in maps or "crabsaxs_b200" in sys.modules))
+"""
+
+
 def test_reference_arm_prints_its_line():
-    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    out = subprocess.run([sys.executable, "-c", RUN_AND_LIST_LIBRARIES], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
+    assert "PRODUCT_LIBRARY_LOADED=False" in out.stdout  # the reference arm runs no product code
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])

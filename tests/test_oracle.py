@@ -359,3 +359,14 @@ def test_coordinate_pr_bins_on_exact_edges():
 def test_coordinate_pr_bins_floor_at_sixteen():  # metrics.rs:268: options.bins.max(16)
     f = O.coordinate_features(_two_carbons_4a(), bins=3)
     assert len(f["p"]) == 16
+
+
+def test_oracle_synthetic_generator_equals_the_library_one():
+    """The reference arm of bench.py builds its input with the oracle's copy of
+    the generator: it must be the same structure bit for bit."""
+    from crabsaxs_b200 import synth
+
+    for seed, n, radius in [(2, 20000, 45.0), (7, 1000, 20.0), (11, 3, 5.0)]:
+        xyz, el = O.synth_protein(seed, n, radius)
+        s = synth.protein(seed, n, radius)
+        assert np.array_equal(xyz, s.xyz) and np.array_equal(el, s.element)

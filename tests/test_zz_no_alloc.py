@@ -55,3 +55,7 @@ def test_noalloc_grid_reports_capacity_and_limits(engine):
     far = np.array([[0.0, 0.0, 0.0], [2000.0, 2000.0, 2000.0]])
     st, _, _, _ = _noalloc(far, 3.0, 0)
     assert st == N.EINVAL
+    bad = s.xyz.copy()
+    bad[123, 2] = np.nan
+    st, m, _, _ = _noalloc(bad, 4.0, 0)
+    assert st == N.EINVAL and m == 0
