@@ -372,7 +372,23 @@ def multipole_section(eng, rank, fp32_peak, with_cpu=False):
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except (OSError, ValueError):
         pass
-    tf32_peak = 0.5 * float(peaks.get("bf16_tflops", 1590.0))  # dense TF32 runs at half the BF16 rate
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    peak_source = "of measured (MEASURED_PEAKS.json bf16_tflops)" if "bf16_tflops" in peaks else \
+        "of fallback (1.59 PFLOP/s bf16, an earlier measurement on this pool)"
+    tf32_peak = 0.5 * bf16_peak  # dense TF32 runs at half the BF16 rate
+    # BF16 operands (Y_lm generated inside the GEMM kernel): hi+lo for every l,
+    # and one term; tensor FLOP = products per K step x useful FLOP
+    bf = {}
+    for name, prec, products in [("bf16_split", N.PREC_BF16_SPLIT, 3), ("bf16", N.PREC_BF16, 1),
+                                 ("tf32_split_fused", N.PREC_TF32_SPLIT_FUSED, 3)]:
+        out, wall, dev, gemm, _ = timed(prec)
+        r = np.abs(out - f64) / np.abs(f64)
+        pk = tf32_peak if name.startswith("tf32") else bf16_peak
+        bf[name] = {"wall_ms": wall, "device_ms": dev, "gemm_ms": gemm,
+                    "tensor_tflops": products * flop / (gemm * 1e-3) / 1e12, "peak_tflops": pk,
+                    "frac": products * flop / (gemm * 1e-3) / 1e12 / pk,
+                    "max_rel_err_vs_fp64_multipole": float(r.max()),
+                    "rms_rel_err_vs_fp64_multipole": float(np.sqrt(np.mean(r ** 2)))}
     # the 20,000-atom curve with the adaptive 3 Å grid by multipole, L = 30
     s2 = synth.protein(synth.DEBYE_20K_SOLVATED.seed, synth.DEBYE_20K_SOLVATED.n_atoms, synth.DEBYE_20K_SOLVATED.radius)
     sp = cs.SolventParams(hydration_model=cs.HydrationModel.AdaptiveGrid, hydration_grid_spacing_angstrom=3.0)
@@ -401,7 +417,7 @@ def multipole_section(eng, rank, fp32_peak, with_cpu=False):
             "moments_gemm_tensor": {
                 "ms": tc_gemm, "useful_flop": flop, "tensor_flop": 3.0 * flop,
                 "achieved_tflops": 3.0 * flop / (tc_gemm * 1e-3) / 1e12, "peak_tflops": tf32_peak,
-                "peak_source": "0.5 x bf16_tflops of MEASURED_PEAKS.json (dense TF32 = half the BF16 rate)",
+                "peak_source": "0.5 x bf16 peak (dense TF32 = half the BF16 rate), " + peak_source,
                 "frac": 3.0 * flop / (tc_gemm * 1e-3) / 1e12 / tf32_peak,
                 "note": "3 TF32 products per K step (h h', h m', m h'); includes the split reduction"},
             "moments_gemm_fp32_simt": {"ms": f32_gemm, "achieved_tflops": flop / (f32_gemm * 1e-3) / 1e12,
@@ -414,7 +430,11 @@ def multipole_section(eng, rank, fp32_peak, with_cpu=False):
             "fp32_simt_max_rel_err_vs_fp64_multipole": float(rel32.max()),
             "max_rel_err_vs_fp64_debye_every_50th_q": float(trunc.max()),
             "rms_rel_err_vs_fp64_debye_every_50th_q": float(np.sqrt(np.mean(trunc**2))),
-            "solvated_20k_multipole_l30_curve_ms": c2_ms}
+            "solvated_20k_multipole_l30_curve_ms": c2_ms,
+            "other_tensor_modes": bf,
+            "other_tensor_modes_note": "gemm_ms includes the split reduction; BF16 modes and tf32_split_fused "
+                                       "generate Y_lm inside the GEMM kernel (the default TF32 modes stage it "
+                                       "through device memory: k_mp_prep, outside gemm_ms); bf16 peak " + peak_source}
 
 
 def grid_and_gradient_section(eng, rank):

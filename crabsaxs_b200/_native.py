@@ -25,6 +25,7 @@ OCC_REPORTED, OCC_SELECTED_FULL = 0, 1
 HYD_ANALYTIC, HYD_GRID, HYD_ADAPTIVE = 0, 1, 2
 METHOD_AUTO, METHOD_DEBYE, METHOD_MULTIPOLE = 0, 1, 2
 PREC_FP64, PREC_TF32, PREC_BF16, PREC_BF16_SPLIT, PREC_TF32_SPLIT, PREC_FP32 = 0, 1, 2, 3, 4, 5
+PREC_TF32_FUSED, PREC_TF32_SPLIT_FUSED = 6, 7
 SCALE_FIT, SCALE_FIXED = 0, 1
 BG_FIT, BG_FIXED_ZERO, BG_FIXED = 0, 1, 2
 

@@ -552,14 +552,556 @@ constexpr size_t tc_smem_bytes() {
          kTcRingBytes + sizeof(uint64_t) * kTcBars + 16;
 }
 
-// M[g][b][t*128 + r] = sum over the point splits of group g of the partial
-// tiles of lm tile t; one block per (group, lm tile), in a fixed order.
+// ---- fused moment GEMM: Y_lm generated by the producer warps ----
+//
+// The staged path above writes Y_lm of every point to device memory
+// (k_mp_prep: 1 GB at 100,000 atoms and L = 50) and the GEMM reads it back.
+// Here the producer warps run the harmonic recurrence themselves and write
+// the operand terms straight into the swizzled shared tiles, so Y_lm never
+// reaches device memory.
+//
+// Rows are taken in m-major order, the order in which the recurrence of
+// spherical.rs:54-93 produces them: m = 0 with l = 0..L, then for every
+// m >= 1 and l = m..L the cos row and the sin row.  A point's walk through
+// the rows is then one pass of the recurrence, and its state (P_m^m,
+// P_{l-1}^m, P_l^m, cos m phi, sin m phi) carries from one 128-row lm tile
+// to the next.  A CTA owns a chunk of stages of one group and runs every lm
+// tile over it, tile-major; the walk state of its points waits in a device
+// array between tiles (40 bytes per point, L2-resident).  The values are the
+// ones k_mp_prep writes, bit for bit: the same f64 operations in the same
+// order, then the same rounding to the operand type.  k_mp_reduce maps rows
+// back to the l^2 + l + m order of the moments.
+//
+// Element types; both give 128-byte stage rows, so the swizzled layout, the
+// descriptors and the four K steps of 32 bytes per stage are those of the
+// staged kernel:
+//   E = 0, TF32: 32-point stages, K = 8 per MMA (kind::tf32)
+//   E = 1, BF16: 64-point stages, K = 16 per MMA (kind::f16, BF16 A and B)
+// S = 2 splits both operands into hi + lo terms (3 products per K step).
+// W = w L_b(r) is the same for every lm tile: k_mp_prep_fused writes it once,
+// already split and swizzled, one 8 KB block per (stage, term), and the
+// producer warp of a stage fetches its blocks with a 1D bulk copy.
+//
+// Roles: producer warps 0..P-1 (warp p takes the stages c = p mod P of
+// every tile into its own slot p, so a stage's walk state and a slot are
+// handled by one warp only), the MMA
+// issuer (warp P, lane 0) and 8 drain warps, which read each stage's FP32
+// accumulator from TMEM into f64 registers (one stage per accumulator, as in
+// the staged kernel) and store the f64 tile of the chunk at the end of each
+// lm tile.  Every wait is bounded, and the role waits suspend the warp
+// (try_wait) rather than spin, so waiting warps leave the issue slots to the
+// producers; a CTA that gives up drains its bulk copies and MMAs before it
+// frees TMEM and exits.
+constexpr int kFuDrainers = 256;
+template <int S>
+struct FuCfg {
+  static constexpr int P = S == 1 ? 6 : 4;  // producer warps, one slot each
+  static constexpr int Slots = P;
+  static constexpr int SlotBytes = S * (kTcABytes + kTcBBytes);
+  static constexpr int Threads = (P + 1) * 32 + kFuDrainers;
+  static constexpr int Bars = 3 * Slots + 2 * kTcAccs + 1;
+  // slots, then per producer warp the normalisations of one tile's rows
+  // (kGemmM doubles), the 1/k table (kMaxL + 2 doubles), the barriers
+  static constexpr size_t NormOff = (size_t)Slots * SlotBytes;
+  static constexpr size_t InvOff = NormOff + (size_t)P * kGemmM * sizeof(double);
+  static constexpr size_t BarOff = InvOff + (kMaxL + 2) * sizeof(double);
+  static constexpr size_t Smem = 1024 + BarOff + sizeof(uint64_t) * Bars + 16;
+};
+static_assert(FuCfg<1>::Smem <= 232448 && FuCfg<2>::Smem <= 232448, "shared memory of the fused GEMM");
+
+template <int E>
+__host__ __device__ constexpr int fu_stage_points() { return E == 0 ? 32 : 64; }
+
+// BF16, FP32 accumulate, K-major A and B, N = 64, M = 128
+constexpr uint32_t kBfIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+__device__ __forceinline__ void tc_mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(kBfIdesc), "r"(accumulate)
+      : "memory");
+}
+// Two FP32 values rounded to BF16 (nearest even) in one word: lo = a, hi = b.
+__device__ __forceinline__ uint32_t bf16x2_rn(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
+}
+__device__ __forceinline__ uint16_t bf16_rn(float a) {
+  uint16_t r;
+  asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ float bf16_lo_f32(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi_f32(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+// Byte offset of element (row, k) in a K-major 128-byte-swizzled tile whose
+// rows hold 128 bytes of K (32 TF32 or 64 BF16 values).
+template <int E>
+__host__ __device__ __forceinline__ uint32_t fu_swz(int row, int k) {
+  const int chunk = E == 0 ? (k >> 2) : (k >> 3);
+  const int within = E == 0 ? (k & 3) * 4 : (k & 7) * 2;
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4) + within);
+}
+
+// The recurrence of spherical.rs:54-93 in the order of k_mp_prep.  Per point
+// the walk keeps P_m^m (pmm), P_{l-1}^m, P_l^m (prev, cur) and cos, sin (m phi);
+// the walk position (m, l, and whether the next row is the sin row of (l, m))
+// is the same for every point.  The f64 operations and their order are
+// k_mp_prep's, so the values are its values bit for bit.
+struct FuWalk {
+  double pmm, prev, cur, cm, sm;
+};
+// P_{m+1}^m = (x (2m+1)) P_m^m
+__device__ __forceinline__ void fu_first_l(int m, const double4& k4, FuWalk& w) {
+  const double nxt = __dmul_rn(__dmul_rn(k4.x, (double)(2 * m + 1)), w.pmm);
+  w.prev = w.cur;
+  w.cur = nxt;
+}
+// P_l^m = ((2l-1) x P_{l-1}^m - (l+m-1) P_{l-2}^m) / (l-m), with a = 2l-1,
+// b = l+m-1 and iv = 1/(l-m) given
+__device__ __forceinline__ void fu_next_l(double a, double b, double iv, const double4& k4, FuWalk& w) {
+  const double num = __dadd_rn(__dmul_rn(__dmul_rn(a, k4.x), w.cur), -__dmul_rn(b, w.prev));
+  w.prev = w.cur;
+  w.cur = __dmul_rn(num, iv);
+}
+// next m: P_m^m = P_{m-1}^{m-1} (-(2m-1) sin theta), (cos, sin)(m phi) rotated
+__device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
+  w.pmm = __dmul_rn(w.pmm, __dmul_rn(-(double)(2 * m - 1), k4.y));
+  const double next_cos = __dadd_rn(__dmul_rn(w.cm, k4.z), -__dmul_rn(w.sm, k4.w));
+  w.sm = __dadd_rn(__dmul_rn(w.sm, k4.z), __dmul_rn(w.cm, k4.w));
+  w.cm = next_cos;
+  w.cur = w.pmm;
+  w.prev = 0.0;
+}
+
+// One row of the A tile: the S operand terms of this lane's PPT values at
+// row r of the slot (shared address sa_s).
+// The slot (sa) and the tables the generator reads (srow, inv) are passed as
+// __restrict__ pointers: the compiler may then move the table loads of the
+// next rows above this row's stores, and the rows' dependency chains overlap.
+template <int E, int S, int PPT>
+__device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, int lane, const double (&v)[PPT]) {
+  const uint32_t off = fu_swz<E>(r, PPT * lane);
+  if (E == 0) {
+    const float f = (float)v[0];
+    const float h = tf32_rna(f);
+    *reinterpret_cast<float*>(sa + off) = h;
+    if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - h);
+  } else {
+    const float fa = (float)v[0], fb = (float)v[PPT - 1];
+    const uint32_t h = bf16x2_rn(fa, fb);
+    *reinterpret_cast<uint32_t*>(sa + off) = h;
+    if (S == 2) *reinterpret_cast<uint32_t*>(sa + kTcABytes + off) = bf16x2_rn(fa - bf16_lo_f32(h), fb - bf16_hi_f32(h));
+  }
+}
+
+// The rows of (l, m): one row for m = 0 (norm P_l^0), else the cos and the
+// sin row (sqrt(2) norm P_l^m times cos / sin (m phi)); sn is the row's
+// normalisation.
+template <int E, int S, int PPT>
+__device__ __forceinline__ void fu_emit_entry(unsigned char* __restrict__ sa, int r, int lane, int m, double sn,
+                                              const FuWalk (&w)[PPT]) {
+  double v[PPT];
+  if (m == 0) {
+#pragma unroll
+    for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(sn, w[jj].cur);
+    fu_emit<E, S, PPT>(sa, r, lane, v);
+  } else {
+    double c[PPT];
+#pragma unroll
+    for (int jj = 0; jj < PPT; ++jj) {
+      const double vv = __dmul_rn(sn, w[jj].cur);
+      c[jj] = __dmul_rn(vv, w[jj].cm);
+      v[jj] = __dmul_rn(vv, w[jj].sm);
+    }
+    fu_emit<E, S, PPT>(sa, r, lane, c);
+    fu_emit<E, S, PPT>(sa, r + 1, lane, v);
+  }
+}
+
+// The 128 rows of one lm tile for this lane's points, from the walk position
+// ts = (m, l, sin row next) at the tile's first row (srow: the rows'
+// normalisations, in shared memory; inv[k] = 1/k); the walk state w moves
+// on to the first row of the next tile.  Rows are produced run by run (one
+// run = the l = m..L of one m); inside a run the steps are the same, so the
+// loop over them has no branches and consecutive rows overlap.
+template <int E, int S, int PPT>
+__device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int lane, int4 ts, int L,
+                                            const double4 (&k4)[PPT], FuWalk (&w)[PPT],
+                                            const double* __restrict__ srow, const double* __restrict__ inv) {
+  int m = ts.x, l = ts.y, half = ts.z, r = 0;
+  auto next_m = [&]() {
+    ++m;
+    if (m <= L) {
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) fu_next_m(m, k4[jj], w[jj]);
+    }
+    l = m;
+  };
+  auto step_from = [&]() {  // after the rows of (l, m): on to (l+1, m) or to the next m
+    if (l == L) {
+      next_m();
+    } else {
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) {
+        if (l == m) fu_first_l(m, k4[jj], w[jj]);
+        else fu_next_l((double)(2 * l + 1), (double)(l + m), inv[l + 1 - m], k4[jj], w[jj]);
+      }
+      ++l;
+    }
+  };
+  while (r < kGemmM) {
+    if (m > L) {  // padding rows past the last harmonic
+      const double z[PPT] = {};
+      for (; r < kGemmM; ++r) fu_emit<E, S, PPT>(sa, r, lane, z);
+      break;
+    }
+    const double sn = srow[r];
+    if (half) {  // the sin row of (l, m) opens the tile
+      double v[PPT];
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].sm);
+      fu_emit<E, S, PPT>(sa, r++, lane, v);
+      half = 0;
+      step_from();
+      continue;
+    }
+    const int per = m > 0 ? 2 : 1;
+    if (r + per > kGemmM) {  // one row left: the cos row of (l, m); its sin row opens the next tile
+      double v[PPT];
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].cm);
+      fu_emit<E, S, PPT>(sa, r++, lane, v);
+      break;
+    }
+    const int n = min(L - l + 1, (kGemmM - r) / per);  // entries of this run in this tile (>= 1)
+    fu_emit_entry<E, S, PPT>(sa, r, lane, m, sn, w);
+    r += per;
+    step_from();
+    if (m > L || l == m) continue;  // the run ended with its first entry
+    // entries 2..n: every one but a run-closing (L, m) steps with the same form
+    const int rest = n - 1, steady = min(rest, L - l);
+    double a = (double)(2 * l + 1), b = (double)(l + m);  // coefficients of the step from l to l+1
+#pragma unroll 4
+    for (int k = 0; k < steady; ++k) {
+      fu_emit_entry<E, S, PPT>(sa, r, lane, m, srow[r], w);
+      r += per;
+      const double iv = inv[l + 1 - m];
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) fu_next_l(a, b, iv, k4[jj], w[jj]);
+      a += 2.0;
+      b += 1.0;
+      ++l;
+    }
+    if (rest > steady) {  // (L, m) closes the run inside this tile
+      fu_emit_entry<E, S, PPT>(sa, r, lane, m, srow[r], w);
+      r += per;
+      next_m();
+    }
+  }
+}
+
+// Walk state arrays (structure of arrays over the padded points).
+struct FuState {
+  double* pmm;
+  double* prev;
+  double* cur;
+  double* cm;
+  double* sm;
+};
+__device__ __forceinline__ void fu_load(const FuState& st, int64_t i, FuWalk& w) {
+  w.pmm = st.pmm[i];
+  w.prev = st.prev[i];
+  w.cur = st.cur[i];
+  w.cm = st.cm[i];
+  w.sm = st.sm[i];
+}
+__device__ __forceinline__ void fu_store(const FuState& st, int64_t i, const FuWalk& w) {
+  st.pmm[i] = w.pmm;
+  st.prev[i] = w.prev;
+  st.cur[i] = w.cur;
+  st.cm[i] = w.cm;
+  st.sm[i] = w.sm;
+}
+
+// Per point: the recurrence constants (cos theta, sin theta, cos phi, sin phi;
+// spherical.rs:165-199, as k_mp_prep) and the weighted Lagrange basis
+// w L_b(r), rounded to the operand type, split into S terms and written into
+// the swizzled B blocks of its stage.
+template <int E, int S>
+__global__ void k_mp_prep_fused(const double* __restrict__ pts, const int32_t* __restrict__ seg, int64_t n_pad, int nb,
+                                const double* __restrict__ nodes, const double* __restrict__ bary,
+                                double4* __restrict__ cst, unsigned char* __restrict__ Bimg) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pad) return;
+  const double px = pts[5 * i], py = pts[5 * i + 1], pz = pts[5 * i + 2], w = pts[5 * i + 3], r = pts[5 * i + 4];
+  double x, phi;
+  if (r < 1e-12) {
+    x = 1.0;
+    phi = 0.0;
+  } else {
+    x = fmin(fmax(__ddiv_rn(pz, r), -1.0), 1.0);
+    phi = atan2(py, px);
+  }
+  const double sin_theta = sqrt(fmax(__dadd_rn(1.0, -__dmul_rn(x, x)), 0.0));
+  double sin_phi, cos_phi;
+  sincos(phi, &sin_phi, &cos_phi);
+  cst[i] = make_double4(x, sin_theta, cos_phi, sin_phi);
+  constexpr int KS = fu_stage_points<E>();
+  const int64_t stage = i / KS;
+  const int k = (int)(i % KS);
+  unsigned char* blk = Bimg + (size_t)stage * S * kTcBBytes;
+  const double* nd = nodes + (int64_t)seg[i] * nb;
+  int hit = -1;
+  double den = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    const double d = r - nd[b];
+    if (d == 0.0) hit = b;
+    else den += bary[b] / d;
+  }
+  for (int b = 0; b < kMaxNodes; ++b) {
+    double v = 0.0;
+    if (b < nb) {
+      if (hit >= 0) v = (b == hit) ? w : 0.0;
+      else v = w * ((bary[b] / (r - nd[b])) / den);
+    }
+    const float f = (float)v;
+    const uint32_t off = fu_swz<E>(b, k);
+    if (E == 0) {
+      const float h = tf32_rna(f);
+      *reinterpret_cast<float*>(blk + off) = h;
+      if (S == 2) *reinterpret_cast<float*>(blk + kTcBBytes + off) = tf32_rna(f - h);
+    } else {
+      const uint16_t h = bf16_rn(f);
+      *reinterpret_cast<uint16_t*>(blk + off) = h;
+      if (S == 2) *reinterpret_cast<uint16_t*>(blk + kTcBBytes + off) = bf16_rn(f - __uint_as_float((uint32_t)h << 16));
+    }
+  }
+}
+
+// Work item of the fused GEMM: (group, first stage, stage count, unused).
+template <int E, int S>
+__global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
+    k_mp_moments_fused(const double4* __restrict__ cst, const unsigned char* __restrict__ Bimg,
+                       const int4* __restrict__ work, const int4* __restrict__ tstart, int n_lmt, int L,
+                       const double* __restrict__ snorm_rows, const double* __restrict__ inv, FuState state,
+                       double* __restrict__ part, int* __restrict__ status, int budget) {
+  using Cfg = FuCfg<S>;
+  constexpr int P = Cfg::P, Slots = Cfg::Slots, KS = fu_stage_points<E>();
+  static_assert(Slots == P, "one slot per producer warp");
+  extern __shared__ __align__(1024) unsigned char fu_smem[];
+  if (budget < 0) budget = dev::kWaitBudget;  // the context's default
+  unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)fu_smem + 1023) & ~(uintptr_t)1023);
+  double* s_inv = reinterpret_cast<double*>(smem + Cfg::InvOff);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::BarOff);
+  uint64_t* full = bars;                 // [Slots], the 32 lanes of the producing warp
+  uint64_t* bfull = bars + Slots;        // [Slots], the W blocks' bulk copy (one arrival + bytes)
+  uint64_t* empty = bars + 2 * Slots;    // [Slots], MMA commit
+  uint64_t* accfull = bars + 3 * Slots;  // [kTcAccs], MMA commit
+  uint64_t* accfree = accfull + kTcAccs; // [kTcAccs], one arrival per drainer
+  uint64_t* done = accfree + kTcAccs;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + Cfg::Bars);
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int4 wk = work[blockIdx.x];
+  const int nc = wk.z, n_units = n_lmt * nc;
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int d = 0; d < Slots; ++d) {
+      dev::mbar_init(&full[d], 32);
+      dev::mbar_init(&bfull[d], 1);
+      dev::mbar_init(&empty[d], 1);
+    }
+    for (int a = 0; a < kTcAccs; ++a) {
+      dev::mbar_init(&accfull[a], 1);
+      dev::mbar_init(&accfree[a], kFuDrainers);
+    }
+    dev::mbar_init(done, 1);
+    dev::fence_mbar_init();
+    s_fail = 0;
+  }
+  for (int k = tid; k < L + 2; k += blockDim.x) s_inv[k] = inv[k];
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+  auto failed = [&]() { return *((volatile int*)&s_fail) != 0; };
+
+  if (warp < P) {
+    // ---------------- producers
+    // this warp's stages: c = warp + k P of every tile, item j = t * n_mine + k,
+    // which is also the use index of its slot
+    constexpr int PPT = E == 0 ? 1 : 2;  // points per lane
+    const int n_mine = nc > warp ? (nc - warp + P - 1) / P : 0, total = n_mine * n_lmt;
+    unsigned char* sa = smem + (size_t)warp * Cfg::SlotBytes;
+    unsigned char* sb = sa + S * kTcABytes;
+    double* srow = reinterpret_cast<double*>(smem + Cfg::NormOff) + (size_t)warp * kGemmM;
+    double nrm[kGemmM / 32];  // this lane's share of the next tile's row normalisations
+    if (total > 0)
+#pragma unroll
+      for (int i = 0; i < kGemmM / 32; ++i) nrm[i] = snorm_rows[lane + 32 * i];
+    bool issued = false;  // lane 0: a W copy into this warp's slot was issued (parity of the last: issued_ph)
+    unsigned issued_ph = 0u;
+    // walk state and constants of the current item (the first item starts the walk)
+    double4 k4[PPT];
+    FuWalk wv[PPT];
+    if (total > 0)
+#pragma unroll
+      for (int jj = 0; jj < PPT; ++jj) {
+        k4[jj] = cst[(int64_t)(wk.y + warp) * KS + PPT * lane + jj];
+        wv[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0};
+      }
+    for (int j = 0; j < total; ++j) {
+      const int t = j / n_mine, c = warp + (j % n_mine) * P;
+      if (j > 0 && (failed() || !dev::mbar_wait(&empty[warp], (unsigned)((j - 1) & 1), budget))) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
+        dev::mbar_expect_tx(&bfull[warp], S * kTcBBytes);
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+          dev::bulk_g2s(sb + p * kTcBBytes, Bimg + ((size_t)(wk.y + c) * S + p) * kTcBBytes, kTcBBytes,
+                        &bfull[warp]);
+        issued = true;
+        issued_ph = (unsigned)(j & 1);
+      }
+      if (j % n_mine == 0) {  // first stage of a tile: its row normalisations into shared memory
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kGemmM / 32; ++i) srow[lane + 32 * i] = nrm[i];
+        __syncwarp();
+        if (t + 1 < n_lmt)  // and the next tile's into registers
+#pragma unroll
+          for (int i = 0; i < kGemmM / 32; ++i) nrm[i] = snorm_rows[(size_t)(t + 1) * kGemmM + lane + 32 * i];
+      }
+      const int64_t p0 = (int64_t)(wk.y + c) * KS + PPT * lane;
+      // prefetch the next item's constants and walk state (a stage of this
+      // warp whose state was stored an item or more ago); with one stage per
+      // tile the state simply stays in registers
+      const bool has_next = j + 1 < total, same = n_mine == 1;
+      double4 k4n[PPT];
+      FuWalk wn[PPT];
+      if (has_next && !same) {
+        const int tn = (j + 1) / n_mine, cn = warp + ((j + 1) % n_mine) * P;
+        const int64_t pn = (int64_t)(wk.y + cn) * KS + PPT * lane;
+#pragma unroll
+        for (int jj = 0; jj < PPT; ++jj) {
+          k4n[jj] = cst[pn + jj];
+          if (tn == 0) wn[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0};
+          else fu_load(state, pn + jj, wn[jj]);
+        }
+      }
+      fu_generate<E, S, PPT>(sa, lane, tstart[t], L, k4, wv, srow, s_inv);
+      if (has_next && !same && t + 1 < n_lmt)
+#pragma unroll
+        for (int jj = 0; jj < PPT; ++jj) fu_store(state, p0 + jj, wv[jj]);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&full[warp]);
+      if (has_next && !same)
+#pragma unroll
+        for (int jj = 0; jj < PPT; ++jj) {
+          k4[jj] = k4n[jj];
+          wv[jj] = wn[jj];
+        }
+    }
+    if (lane == 0 && issued && !ok)  // no bulk copy may land after the CTA exits
+      dev::mbar_wait(&bfull[warp], issued_ph, dev::kDrainBudget);
+  } else if (warp == P) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
+      constexpr int np = S == 1 ? 1 : 3;  // (A term, B term): hh', hm', mh'
+      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+      for (int u = 0; u < n_units; ++u) {
+        const int t = u / nc, c = u % nc, d = c % P, a = u % kTcAccs;
+        const unsigned ph = (unsigned)((t * ((nc - d + P - 1) / P) + c / P) & 1);
+        if (failed() || !dev::mbar_wait(&full[d], ph, budget) || !dev::mbar_wait(&bfull[d], ph, budget) ||
+            (u >= kTcAccs && !dev::mbar_wait(&accfree[a], (unsigned)((u / kTcAccs - 1) & 1), budget))) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_base + (uint32_t)d * Cfg::SlotBytes, b0 = a0 + S * kTcABytes;
+        const uint32_t acc_cols = tmem + (uint32_t)(a * 64);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+          for (int p = 0; p < np; ++p) {
+            const uint64_t da = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32);
+            const uint64_t db = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32);
+            if (E == 0) tc_mma(acc_cols, da, db, (kk || p) ? 1u : 0u);
+            else tc_mma_bf16(acc_cols, da, db, (kk || p) ? 1u : 0u);
+          }
+        tc_commit(&empty[d]);
+        tc_commit(&accfull[a]);
+      }
+    }
+  } else {
+    // ---------------- drainers
+    const int quarter = warp & 3, hf = (warp - P - 1) >> 2;
+    double acc[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+    for (int t = 0; t < n_lmt && ok; ++t)
+      for (int c = 0; c < nc; ++c) {
+        const int u = t * nc + c, a = u % kTcAccs;
+        if (failed() || !dev::mbar_wait(&accfull[a], (unsigned)((u / kTcAccs) & 1), budget)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int c16 = 0; c16 < 2; ++c16) {
+          float v[16];
+          tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + hf * 32 + c16 * 16), v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&accfree[a]);
+        if (c == nc - 1) {
+          double* tile = part + ((int64_t)blockIdx.x * n_lmt + t) * kTileElems + quarter * 32 + lane;
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            tile[(hf * 32 + i) * kGemmM] = acc[i];
+            acc[i] = 0.0;
+          }
+        }
+      }
+  }
+  if (!ok) atomicExch(&s_fail, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (s_fail) {
+    // bounded wait for every MMA this CTA issued before freeing TMEM
+    if (tid == P * 32) {
+      tc_commit(done);
+      atomicExch(status, CRAB_ETIMEOUT);
+    }
+    dev::mbar_spin(done, 0);
+  }
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+}
+
+// M[g][b][perm(t*128 + r)] = sum over the point splits of group g of the
+// partial tiles of lm tile t, in a fixed order (perm: the l^2 + l + m
+// position of a GEMM row; NULL for rows already in that order).
 // One CTA per (group, lm tile, 1/kReduceSplit of the tile's elements).
 constexpr int kReduceSplit = 8;
 static_assert(kTileElems % kReduceSplit == 0, "reduce split");
 __global__ void __launch_bounds__(256) k_mp_reduce(const double* __restrict__ part, const int32_t* __restrict__ gfirst,
                                                    const int32_t* __restrict__ gsplits, int n_lmt, int lm_pad,
-                                                   double* __restrict__ M) {
+                                                   const int32_t* __restrict__ perm, double* __restrict__ M) {
   const int g = blockIdx.x / n_lmt, t = blockIdx.x % n_lmt;
   const int first = gfirst[g], n = gsplits[g];
   constexpr int kPer = kTileElems / kReduceSplit;
@@ -568,7 +1110,8 @@ __global__ void __launch_bounds__(256) k_mp_reduce(const double* __restrict__ pa
     double v = 0.0;
 #pragma unroll 4
     for (int k = 0; k < n; ++k) v += part[(int64_t)(first + k * n_lmt + t) * kTileElems + e];
-    M[((int64_t)g * kMaxNodes + e / kGemmM) * lm_pad + t * kGemmM + e % kGemmM] = v;
+    const int row = t * kGemmM + e % kGemmM;
+    M[((int64_t)g * kMaxNodes + e / kGemmM) * lm_pad + (perm ? perm[row] : row)] = v;
   }
 }
 
@@ -768,11 +1311,67 @@ struct MpInput {
   void* sum_user = nullptr;
 };
 
+// Chunk size (stages) of the fused GEMM's work items: items of one group
+// cover whole stages of it; one CTA per SM, so the time goes as the rounds
+// of items times the stages per item, plus the partial tiles every item
+// writes and k_mp_reduce reads (n_lmt x 64 KB f64, counted here as 0.073 of
+// a TF32 hi+lo stage per tile).
+int fused_chunk_stages(const std::vector<int64_t>& group_stages, int sm_count, double stage_cost) {
+  int64_t most = 1;
+  for (int64_t v : group_stages) most = std::max(most, v);
+  int best = 1;
+  double best_cost = 1e300;
+  for (int cs = 1; cs <= most; ++cs) {
+    int64_t items = 0;
+    for (int64_t v : group_stages) items += (v + cs - 1) / cs;
+    const double rounds = (double)((items + sm_count - 1) / std::max(sm_count, 1));
+    const double cost = rounds * cs * stage_cost + 0.073 * (double)items;
+    if (cost < best_cost * (1.0 - 1e-12)) {
+      best_cost = cost;
+      best = cs;
+    }
+  }
+  return best;
+}
+
+// Rows of the fused GEMM in the m-major order of the recurrence: the walk
+// position (m, l, sin row next) at the start of every 128-row tile, and
+// perm[row] = the l^2 + l + m position of the row (rows past the last
+// harmonic keep their own index).
+void fused_row_walk(int L, int lm_pad, std::vector<int4>& tstart, std::vector<int32_t>& perm) {
+  tstart.assign((size_t)lm_pad / kGemmM, make_int4(0, 0, 0, 0));
+  perm.assign((size_t)lm_pad, 0);
+  int m = 0, l = 0, half = 0;
+  for (int row = 0; row < lm_pad; ++row) {
+    if (row % kGemmM == 0) tstart[row / kGemmM] = make_int4(m, l, half, 0);
+    if (m > L) {
+      perm[row] = row;
+      continue;
+    }
+    perm[row] = l * l + l + (half ? -m : m);
+    if (m > 0 && half == 0) {
+      half = 1;
+      continue;
+    }
+    half = 0;
+    if (l < L) {
+      ++l;
+    } else {
+      ++m;
+      l = m;
+    }
+  }
+}
+
+// GEMM kernel of a precision mode: gemm = 0 SIMT (FP32, or FP64 with fp64),
+// 1 the staged tensor-core kernel (Y_lm through device memory), 2 the fused
+// tensor-core kernel with TF32 operands, 3 the fused kernel with BF16
+// operands; tc_terms = operand terms (1, or 2 for hi + lo).
+enum { kGemmSimt = 0, kGemmStaged = 1, kGemmFusedTf32 = 2, kGemmFusedBf16 = 3 };
+
 // Sums 4 pi sum A^c A^d for the requested combinations; out is [K(K+1)/2][nq].
-// tc_terms: 0 = SIMT GEMM (FP32 or FP64 operands), 1..2 = tensor-core GEMM
-// with that many TF32 terms per operand (FP32 operands).
 void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq, int L, bool fp64, int tc_terms,
-                   double* out) {
+                   int gemm, double* out) {
   TraceScope trace("multipole_run");
   const TypedAtoms& t = *in.t;
   const int T = t.T, K = in.K, P = K * (K + 1) / 2;
@@ -805,8 +1404,10 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     ++count[group_of[i]];
   }
   std::vector<int64_t> begin(G + 1, 0);
-  for (int g = 0; g < G; ++g) begin[g + 1] = begin[g] + (count[g] + kPointAlign - 1) / kPointAlign * kPointAlign;
-  const int64_t n_pad = std::max<int64_t>(begin[G], kPointAlign);
+  // groups padded to whole GEMM stages (64 points for BF16 operands)
+  const int align = gemm == kGemmFusedBf16 ? 2 * kPointAlign : kPointAlign;
+  for (int g = 0; g < G; ++g) begin[g + 1] = begin[g] + (count[g] + align - 1) / align * align;
+  const int64_t n_pad = std::max<int64_t>(begin[G], align);
   // points are built in the context's pinned staging buffers (reused across
   // calls, uploaded asynchronously); padding slots are zeroed explicitly
   auto* pts = (double*)ctx->host("mp_pts", sizeof(double) * 5 * (size_t)n_pad);
@@ -832,20 +1433,54 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const int lm_pad = (lm_count + kGemmM - 1) / kGemmM * kGemmM;
   std::vector<int32_t> lq(nq);
   for (int64_t k = 0; k < nq; ++k) lq[k] = adaptive_l(q[k], in.rmax_lq, L);
-  // work items: group, then point split, then lm tile (k_mp_reduce relies on this order)
   const int n_lmt = lm_pad / kGemmM;
-  std::vector<MpWork> work;
+  const bool fused = gemm == kGemmFusedTf32 || gemm == kGemmFusedBf16;
   std::vector<int32_t> gfirst(G), gsplits(G);
-  for (int g = 0; g < G; ++g) {
-    gfirst[g] = (int32_t)work.size();
-    gsplits[g] = 0;
-    for (int64_t k0 = begin[g]; k0 < begin[g + 1]; k0 += kSplitK, ++gsplits[g])
-      for (int lm0 = 0; lm0 < lm_pad; lm0 += kGemmM)
-        work.push_back(MpWork{g, lm0, k0, std::min(begin[g + 1], k0 + kSplitK)});
+  // staged and SIMT GEMMs: items (group, point split, lm tile), lm tile fastest
+  // (k_mp_reduce relies on this order)
+  std::vector<MpWork> work;
+  // fused GEMM: items (group, first stage, stage count), each over every lm
+  // tile; partial tiles item-major, lm tile fastest (the same order for
+  // k_mp_reduce with gfirst in units of items x tiles)
+  std::vector<int4> fwork, tstart;
+  std::vector<int32_t> perm;
+  std::vector<double> snorm;
+  const int KS = gemm == kGemmFusedBf16 ? 64 : 32;
+  if (!fused) {
+    for (int g = 0; g < G; ++g) {
+      gfirst[g] = (int32_t)work.size();
+      gsplits[g] = 0;
+      for (int64_t k0 = begin[g]; k0 < begin[g + 1]; k0 += kSplitK, ++gsplits[g])
+        for (int lm0 = 0; lm0 < lm_pad; lm0 += kGemmM)
+          work.push_back(MpWork{g, lm0, k0, std::min(begin[g + 1], k0 + kSplitK)});
+    }
+  } else {
+    std::vector<int64_t> gst(G);
+    for (int g = 0; g < G; ++g) gst[g] = (begin[g + 1] - begin[g]) / KS;
+    const double stage_cost = (tc_terms == 2 ? 1.0 : 0.5) * (KS / 32.0);
+    const int cs = fused_chunk_stages(gst, ctx->sm_count, stage_cost);
+    for (int g = 0; g < G; ++g) {
+      gfirst[g] = (int32_t)(fwork.size() * n_lmt);
+      gsplits[g] = 0;
+      for (int64_t s0 = begin[g] / KS; s0 < begin[g + 1] / KS; s0 += cs, ++gsplits[g])
+        fwork.push_back(make_int4(g, (int)s0, (int)std::min<int64_t>(cs, begin[g + 1] / KS - s0), 0));
+    }
   }
   const std::vector<double> norms = harmonic_norms(L);
   std::vector<double> inv(L + 2, 0.0);
   for (int k = 1; k <= L + 1; ++k) inv[k] = 1.0 / (double)k;
+  if (fused) {  // the walk's tile starts, and per row the norm as k_mp_prep applies it
+    fused_row_walk(L, lm_pad, tstart, perm);
+    snorm.assign((size_t)lm_pad, 0.0);  // row order; zero past the last harmonic
+    const double sqrt2 = std::sqrt(2.0);
+    for (int row = 0; row < lm_pad; ++row) {
+      if (perm[row] >= lm_count) continue;
+      const int l = (int)std::sqrt((double)perm[row]), m = std::abs(perm[row] - l * l - l);
+      const int pos = l * l + l + m;
+      snorm[row] = m == 0 ? norms[pos] : sqrt2 * norms[pos];
+    }
+  }
+  const size_t n_items = fused ? fwork.size() * (size_t)n_lmt : work.size();
 
   trace_mark("mp_host_prep");
   TraceScope tdev("multipole_device");
@@ -857,11 +1492,11 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_inv = (double*)ctx->dev("mp_inv", sizeof(double) * inv.size());
   double* d_nodes = (double*)ctx->dev("mp_nodes", sizeof(double) * B.nodes.size());
   double* d_bary = (double*)ctx->dev("mp_bary", sizeof(double) * B.bary.size());
-  void* d_YT = ctx->dev("mp_Y", esz * (size_t)lm_pad * n_pad);
-  void* d_WT = ctx->dev("mp_W", esz * (size_t)kMaxNodes * n_pad);
-  MpWork* d_work = (MpWork*)ctx->dev("mp_work", sizeof(MpWork) * work.size());
+  void* d_YT = fused ? nullptr : ctx->dev("mp_Y", esz * (size_t)lm_pad * n_pad);
+  void* d_WT = fused ? nullptr : ctx->dev("mp_W", esz * (size_t)kMaxNodes * n_pad);
+  MpWork* d_work = fused ? nullptr : (MpWork*)ctx->dev("mp_work", sizeof(MpWork) * std::max<size_t>(work.size(), 1));
   double* d_M = (double*)ctx->dev("mp_M", sizeof(double) * (size_t)G * kMaxNodes * lm_pad);
-  double* d_part = (double*)ctx->dev("mp_part", sizeof(double) * (size_t)kTileElems * work.size());
+  double* d_part = (double*)ctx->dev("mp_part", sizeof(double) * (size_t)kTileElems * std::max<size_t>(n_items, 1));
   int32_t* d_gfirst = (int32_t*)ctx->dev("mp_gfirst", sizeof(int32_t) * G);
   int32_t* d_gsplits = (int32_t*)ctx->dev("mp_gsplits", sizeof(int32_t) * G);
   double* d_q = (double*)ctx->dev("mp_q", sizeof(double) * nq);
@@ -870,13 +1505,35 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   double* d_amp = (double*)ctx->dev("mp_amp", sizeof(double) * in.amp.size());
   double* d_out = (double*)ctx->dev("mp_out", sizeof(double) * (size_t)P * nq);
   int* d_status = (int*)ctx->dev("mp_status", sizeof(int));
+  // fused GEMM: recurrence constants, W blocks, walk state, row tables
+  double4* d_cst = nullptr;
+  unsigned char* d_Bimg = nullptr;
+  FuState fst{};
+  int4* d_fwork = nullptr;
+  int32_t* d_perm = nullptr;
+  int4* d_tstart = nullptr;
+  double* d_snorm = nullptr;
+  if (fused) {
+    d_cst = (double4*)ctx->dev("mp_cst", sizeof(double4) * (size_t)n_pad);
+    d_Bimg = (unsigned char*)ctx->dev("mp_Bimg", (size_t)(n_pad / KS) * tc_terms * kTcBBytes);
+    double* st = (double*)ctx->dev("mp_walk", sizeof(double) * 5 * (size_t)n_pad);
+    fst = FuState{st, st + n_pad, st + 2 * n_pad, st + 3 * n_pad, st + 4 * n_pad};
+    d_fwork = (int4*)ctx->dev("mp_fwork", sizeof(int4) * std::max<size_t>(fwork.size(), 1));
+    d_perm = (int32_t*)ctx->dev("mp_perm", sizeof(int32_t) * perm.size());
+    d_tstart = (int4*)ctx->dev("mp_tstart", sizeof(int4) * tstart.size());
+    d_snorm = (double*)ctx->dev("mp_snorm", sizeof(double) * snorm.size());
+    copy_h2d(ctx, d_fwork, fwork.data(), sizeof(int4) * fwork.size(), s);
+    copy_h2d(ctx, d_perm, perm.data(), sizeof(int32_t) * perm.size(), s);
+    copy_h2d(ctx, d_tstart, tstart.data(), sizeof(int4) * tstart.size(), s);
+    copy_h2d(ctx, d_snorm, snorm.data(), sizeof(double) * snorm.size(), s);
+  }
   copy_h2d(ctx, d_pts, pts, sizeof(double) * 5 * (size_t)n_pad, s);
   copy_h2d(ctx, d_seg, seg, sizeof(int32_t) * n_pad, s);
   copy_h2d(ctx, d_norms, norms.data(), sizeof(double) * norms.size(), s);
   copy_h2d(ctx, d_inv, inv.data(), sizeof(double) * inv.size(), s);
   copy_h2d(ctx, d_nodes, B.nodes.data(), sizeof(double) * B.nodes.size(), s);
   copy_h2d(ctx, d_bary, B.bary.data(), sizeof(double) * B.bary.size(), s);
-  copy_h2d(ctx, d_work, work.data(), sizeof(MpWork) * work.size(), s);
+  if (!fused) copy_h2d(ctx, d_work, work.data(), sizeof(MpWork) * work.size(), s);
   copy_h2d(ctx, d_q, q, sizeof(double) * nq, s);
   copy_h2d(ctx, d_lq, lq.data(), sizeof(int32_t) * nq, s);
   copy_h2d(ctx, d_amp, in.amp.data(), sizeof(double) * in.amp.size(), s);
@@ -895,7 +1552,24 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   for (int i = 0; i < 4; ++i) CRAB_CUDA_CHECK(cudaEventCreate(&ev[i]));
   CRAB_CUDA_CHECK(cudaEventRecord(ev[0], s));
   const unsigned prep_blocks = (unsigned)((n_pad + 127) / 128);
-  if (fp64) {
+  if (fused) {
+#define CRAB_FUSED(EE, SS)                                                                                        \
+  if (KS == fu_stage_points<EE>() && tc_terms == SS) {                                                            \
+    k_mp_prep_fused<EE, SS><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, nb, d_nodes, d_bary, d_cst, d_Bimg);   \
+    CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));                                                                    \
+    if (!fwork.empty()) {                                                                                          \
+      CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_fused<EE, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                           (int)FuCfg<SS>::Smem));                                                 \
+      k_mp_moments_fused<EE, SS><<<(unsigned)fwork.size(), FuCfg<SS>::Threads, FuCfg<SS>::Smem, s>>>(              \
+          d_cst, d_Bimg, d_fwork, d_tstart, n_lmt, L, d_snorm, d_inv, fst, d_part, d_status, ctx->wait_budget);   \
+    }                                                                                                              \
+  }
+    CRAB_FUSED(0, 1)
+    CRAB_FUSED(0, 2)
+    CRAB_FUSED(1, 1)
+    CRAB_FUSED(1, 2)
+#undef CRAB_FUSED
+  } else if (fp64) {
     k_mp_prep<double><<<prep_blocks, 128, 0, s>>>(d_pts, d_seg, n_pad, L, lm_pad, nb, d_norms, d_nodes, d_bary,
                                                    d_inv, (double*)d_YT, (double*)d_WT);
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));
@@ -925,14 +1599,14 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     }
   }
   k_mp_reduce<<<dim3((unsigned)(G * n_lmt), kReduceSplit), 256, 0, s>>>(d_part, d_gfirst, d_gsplits, n_lmt, lm_pad,
-                                                                         d_M);
+                                                                         fused ? d_perm : nullptr, d_M);
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   if (in.n_shards > 1) {
     // every rank's moments summed by the caller (an all-reduce over the GPUs)
     const size_t m_count = (size_t)G * kMaxNodes * lm_pad;
     auto* h_M = (double*)ctx->host("mp_M", sizeof(double) * m_count);
     int status = 0;
-    if (tc_terms) copy_d2h(ctx, &status, d_status, sizeof(int), s);
+    if (gemm != kGemmSimt) copy_d2h(ctx, &status, d_status, sizeof(int), s);
     copy_d2h(ctx, h_M, d_M, sizeof(double) * m_count, s);
     CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
     if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
@@ -971,7 +1645,7 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   ctx->launches += 5;
   copy_d2h(ctx, out, d_out, sizeof(double) * (size_t)P * nq, s);
   int status = 0;
-  if (tc_terms) copy_d2h(ctx, &status, d_status, sizeof(int), s);
+  if (gemm != kGemmSimt) copy_d2h(ctx, &status, d_status, sizeof(int), s);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
   if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
   float total_ms = 0.0f, gemm_ms = 0.0f;
@@ -986,15 +1660,20 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
 struct MpPrecision {
   bool fp64;
   int tc_terms;
+  int gemm;
 };
 MpPrecision multipole_precision(int precision) {
   switch (precision) {
-    case CRAB_PREC_FP64: return {true, 0};
-    case CRAB_PREC_FP32: return {false, 0};
-    case CRAB_PREC_TF32: return {false, 1};
-    case CRAB_PREC_TF32_SPLIT: return {false, 2};
+    case CRAB_PREC_FP64: return {true, 0, kGemmSimt};
+    case CRAB_PREC_FP32: return {false, 0, kGemmSimt};
+    case CRAB_PREC_TF32: return {false, 1, kGemmStaged};
+    case CRAB_PREC_TF32_SPLIT: return {false, 2, kGemmStaged};
+    case CRAB_PREC_BF16: return {false, 1, kGemmFusedBf16};
+    case CRAB_PREC_BF16_SPLIT: return {false, 2, kGemmFusedBf16};
+    case CRAB_PREC_TF32_FUSED: return {false, 1, kGemmFusedTf32};
+    case CRAB_PREC_TF32_SPLIT_FUSED: return {false, 2, kGemmFusedTf32};
     default:
-      throw Error(CRAB_EINVAL, "multipole precision must be FP64, FP32, TF32 or TF32_SPLIT");
+      throw Error(CRAB_EINVAL, "unknown multipole precision");
   }
 }
 
@@ -1097,7 +1776,7 @@ void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double
   in.n_shards = shard.n_shards;
   in.sum = shard.sum;
   in.sum_user = shard.user;
-  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, mp.gemm, out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
 
@@ -1126,7 +1805,7 @@ void multipole_solvent_basis_impl(crab_ctx* ctx, const crab_struct* st, const do
   in.n_shards = shard.n_shards;
   in.sum = shard.sum;
   in.sum_user = shard.user;
-  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out6);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, mp.gemm, out6);
 }
 
 void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t nq, int l_max,
@@ -1152,7 +1831,7 @@ void multipole_solvent_intensity_impl(crab_ctx* ctx, const crab_struct* st, cons
       const size_t o = (size_t)a * nq + k;
       in.amp[o] = u.V[o] - excluded_volume_scale(q[k], s.c1) * u.E[o] + s.c2 * u.H[o];
     }
-  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, out);
+  multipole_run(ctx, in, q, nq, l_max, mp.fp64, mp.tc_terms, mp.gemm, out);
   for (int64_t k = 0; k < nq; ++k) out[k] = std::fmax(out[k], 0.0);
 }
 

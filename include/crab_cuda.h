@@ -67,7 +67,7 @@ enum { CRAB_HYD_ANALYTIC = 0, CRAB_HYD_GRID = 1, CRAB_HYD_ADAPTIVE = 2 };
 enum { CRAB_METHOD_AUTO = 0, CRAB_METHOD_DEBYE = 1, CRAB_METHOD_MULTIPOLE = 2 };
 /* Multipole GEMM precision. */
 enum { CRAB_PREC_FP64 = 0, CRAB_PREC_TF32 = 1, CRAB_PREC_BF16 = 2, CRAB_PREC_BF16_SPLIT = 3, CRAB_PREC_TF32_SPLIT = 4,
-       CRAB_PREC_FP32 = 5 };
+       CRAB_PREC_FP32 = 5, CRAB_PREC_TF32_FUSED = 6, CRAB_PREC_TF32_SPLIT_FUSED = 7 };
 /* fit.rs:30-47 modes. */
 enum { CRAB_SCALE_FIT = 0, CRAB_SCALE_FIXED = 1 };
 enum { CRAB_BG_FIT = 0, CRAB_BG_FIXED_ZERO = 1, CRAB_BG_FIXED = 2 };
@@ -319,7 +319,14 @@ int crab_hydration_grid_exterior(crab_ctx* ctx, crab_struct* st, double spacing,
  *   CRAB_PREC_TF32_SPLIT  tcgen05 tensor cores, TF32 hi+lo terms (about 5e-7;
  *                         the compute_curve default)
  *   CRAB_PREC_TF32        tcgen05, single TF32 term (about 1e-3)
- * BF16 modes return CRAB_EINVAL. */
+ *   CRAB_PREC_BF16_SPLIT  tcgen05, BF16 hi+lo terms for every l (1e-5 to 6e-5)
+ *   CRAB_PREC_BF16        tcgen05, single BF16 term (about 6e-3)
+ *   CRAB_PREC_TF32_SPLIT_FUSED, CRAB_PREC_TF32_FUSED  the TF32 products with
+ *                         Y_lm generated inside the GEMM kernel (the same
+ *                         values bit for bit, no (L+1)^2 x N buffer in device
+ *                         memory, slower at 100,000 atoms)
+ * The TF32 modes write Y_lm to device memory and stream it into the GEMM;
+ * the BF16 modes generate it inside the GEMM kernel. */
 int crab_multipole_intensity(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                              int implicit_hydrogen, int precision, double* out);
 /* Device time of the last multipole call on this context: all its kernels

@@ -53,7 +53,8 @@ def test_solvent_basis_wait_runs_out_then_recovers(engine, fresh):
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("precision", [N.PREC_TF32_SPLIT, N.PREC_TF32])
+@pytest.mark.parametrize("precision", [N.PREC_TF32_SPLIT, N.PREC_TF32, N.PREC_TF32_SPLIT_FUSED, N.PREC_BF16_SPLIT,
+                                       N.PREC_BF16])
 def test_tensor_core_gemm_wait_runs_out_then_recovers(engine, fresh, precision):
     s = synth.protein(303, 3000, 22.0)
     q = np.linspace(0.001, 0.5, 120)

@@ -160,13 +160,21 @@ def test_empty_structure_and_invalid_arguments(engine):
     with pytest.raises(cs.InvalidInput):
         cs.multipole_intensity(s, q, 65, engine=engine)
     with pytest.raises(cs.InvalidInput):
-        cs.multipole_intensity(s, q, 16, precision=N.PREC_BF16, engine=engine)
+        cs.multipole_intensity(s, q, 16, precision=99, engine=engine)
     with pytest.raises(cs.InvalidInput):
         cs.multipole_intensity(s, np.array([0.1, -0.2]), 16, engine=engine)
 
 
-# Tensor-core moment GEMM (tcgen05): TF32 operands as one term or split in two.
-TC_MODES = [(N.PREC_TF32_SPLIT, FP32_RTOL), (N.PREC_TF32, 5e-3)]
+# Tensor-core moment GEMM (tcgen05): TF32 or BF16 operands as one term or
+# split in two (hi + lo).  Tolerances per q against f64: TF32 hi+lo is within
+# the FP32 contract; the others are set by their operand rounding (measured
+# at 100,000 atoms, L = 50: TF32 8e-4, BF16 hi+lo 1.3e-5, BF16 5.9e-3; BF16
+# hi+lo reaches 5.5e-5 on 700 atoms at L = 0 and q up to 0.9, where the
+# monopole sum cancels).
+BF16_SPLIT_RTOL = 1e-4
+BF16_RTOL = 2e-2
+TC_MODES = [(N.PREC_TF32_SPLIT, FP32_RTOL), (N.PREC_TF32, 5e-3), (N.PREC_TF32_SPLIT_FUSED, FP32_RTOL),
+            (N.PREC_TF32_FUSED, 5e-3), (N.PREC_BF16_SPLIT, BF16_SPLIT_RTOL), (N.PREC_BF16, BF16_RTOL)]
 
 
 @pytest.mark.parametrize("prec,tol", TC_MODES)
@@ -204,3 +212,51 @@ def test_tensor_core_split_matches_fp64_on_100k_atoms(engine):
     i64 = cs.combine_solvent_basis(b64, q, p.c1, p.c2)
     itc = cs.combine_solvent_basis(btc, q, p.c1, p.c2)
     assert _rel(itc, i64) <= FP32_RTOL
+
+
+@pytest.mark.parametrize("prec", [N.PREC_TF32_SPLIT, N.PREC_TF32])
+def test_fused_tf32_equals_staged_tf32(engine, prec):
+    """The fused kernel generates Y_lm with k_mp_prep's f64 operations in the
+    same order and rounds them the same way, and its 32-point stages hold the
+    same points: the curves agree to f64 round-off of the stage sums."""
+    s = synth.protein(37, 3000, 20.0)
+    q = np.linspace(0.001, 0.5, 150)
+    fused = {N.PREC_TF32_SPLIT: N.PREC_TF32_SPLIT_FUSED, N.PREC_TF32: N.PREC_TF32_FUSED}[prec]
+    a = cs.multipole_intensity(s, q, 30, precision=prec, engine=engine)
+    b = cs.multipole_intensity(s, q, 30, precision=fused, engine=engine)
+    assert _rel(b, a) <= 1e-12
+
+
+@pytest.mark.parametrize("l_max", [0, 1, 7, 8, 20, 64])
+def test_fused_modes_at_tile_boundaries(engine, l_max):
+    """L = 0..64: tiles that start inside a run of m, on the sin row of an
+    (l, m), or in the padding past the last harmonic (a wrong walk gives
+    errors of order one; q on the workloads' range)."""
+    s = synth.protein(38, 700, 12.0)
+    q = np.linspace(0.01, 0.6, 50)
+    ref = O.multipole_intensity(_oracle_atoms(s), q, l_max)
+    for prec, tol in [(N.PREC_TF32_SPLIT_FUSED, FP32_RTOL), (N.PREC_BF16_SPLIT, BF16_SPLIT_RTOL),
+                      (N.PREC_BF16, BF16_RTOL)]:
+        got = cs.multipole_intensity(s, q, l_max, precision=prec, engine=engine)
+        assert _rel(got, ref) <= tol, (prec, l_max)
+
+
+def test_bf16_modes_match_fp64_on_100k_atoms(engine):
+    """100,000 atoms (R 80 Å), 1000 q on [0.001, 0.6], L = 50: max and RMS
+    relative error per q of the BF16 hi+lo and BF16 GEMMs against the FP64
+    device multipole, and the solvent basis of a grid-hydrated structure."""
+    w = synth.ATOMS_100K
+    s = synth.protein(w.seed, w.n_atoms, w.radius)
+    ref = cs.multipole_intensity(s, w.q, 50, precision=N.PREC_FP64, engine=engine)
+    for prec, tol, rms_tol in [(N.PREC_BF16_SPLIT, BF16_SPLIT_RTOL, 1e-5), (N.PREC_BF16, BF16_RTOL, 5e-3)]:
+        got = cs.multipole_intensity(s, w.q, 50, precision=prec, engine=engine)
+        rel = np.abs(got - ref) / ref
+        assert rel.max() <= tol and np.sqrt(np.mean(rel**2)) <= rms_tol, (prec, rel.max())
+    s2 = synth.protein(36, 2000, 16.0)
+    q = np.linspace(0.01, 0.5, 80)
+    p = cs.SolventParams(c1=1.01, c2=0.9, hydration_model=cs.HydrationModel.AdaptiveGrid,
+                         hydration_grid_spacing_angstrom=3.0)
+    b64 = cs.multipole_solvent_basis(s2, q, 28, p, precision=N.PREC_FP64, engine=engine)
+    bbf = cs.multipole_solvent_basis(s2, q, 28, p, precision=N.PREC_BF16_SPLIT, engine=engine)
+    for k in range(6):
+        assert np.max(np.abs(bbf[k] - b64[k])) / np.max(np.abs(b64[k])) <= BF16_SPLIT_RTOL, k
