@@ -55,8 +55,13 @@ FLUSH_BYTES = 256 << 20
 
 def _variant_name(v: int) -> str:
     """Autotuner variant code Q*16 + jb; jb >= 8 is the q-packed kernel with (jb-8) % 4 chains,
-    jb >= 12 its build for three CTAs per SM."""
+    jb >= 12 its build for three CTAs per SM; jb 5, 6, 7, 3 the q-packed kernel with the weight
+    folded into the recurrence (1 chain / 2 CTAs, 2 / 2, 1 / 3, 1 / 4)."""
     q, jb = int(v) // 16, int(v) % 16
+    folded = {5: (1, 2), 6: (2, 2), 7: (1, 3), 3: (1, 4)}
+    if jb in folded:
+        chains, ctas = folded[jb]
+        return f"Q{q}xJ{chains}pq-fold-{ctas}cta"
     if jb < 8:
         return f"Q{q}xJ{jb}"
     return f"Q{q}xJ{(jb - 8) % 4}pq" + ("-3cta" if jb >= 12 else "")

@@ -43,11 +43,14 @@ namespace {
 using namespace dev;
 
 constexpr int kThreads = 128;  // one i atom per thread; equals kTile
-constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 100, 126, 128, 150, 168};  // compiled q-block lengths
+constexpr int kQBlocks[] = {8, 16, 32, 48, 64, 96, 100, 126, 128, 150, 168};  // q-block lengths of the untuned choice
 // jb values at or above kPackedQ select the q-packed kernel with
 // (jb - kPackedQ) % kDenser chains; + kDenser asks for 3 CTAs per SM.
 constexpr int kPackedQ = 8;
 constexpr int kDenser = 4;
+// q-packed with the weight folded into the recurrence state (pair_setup_pq_folded):
+// one chain at two CTAs per SM, two chains at two, one chain at three, one at four
+constexpr int kFolded1 = 5, kFolded2 = 6, kFolded1x3 = 7, kFolded1x4 = 3;
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
 template <int Q>
@@ -148,6 +151,19 @@ __device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj
   nl2 = pack2(nl, nl);
   s2 = pack2(S, sB);
   d2 = pack2(dA, dB);
+}
+
+// The same with the weight folded into the recurrence state: s' = u s and
+// d' = u d follow the same linear recurrence, so the accumulate step becomes
+// acc += s' (a packed add with two register sources instead of a packed FMA
+// with three, and u needs no register during the steps).
+__device__ __forceinline__ void pair_setup_pq_folded(const float4& ai, const float4& aj, float wj, const float4& qp,
+                                                     int wide, unsigned long long& nl2, unsigned long long& s2,
+                                                     unsigned long long& d2) {
+  unsigned long long u2;
+  pair_setup_pq(ai, aj, wj, qp, wide, u2, nl2, s2, d2);
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(u2));
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(d2) : "l"(u2));
 }
 
 // Work item: (i tile, first j tile, end j tile, q block); items are taken
@@ -304,7 +320,7 @@ __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2],
   __syncthreads();
 }
 
-template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2))>
+template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)), bool FOLD = false>
 __global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                    int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
@@ -385,13 +401,15 @@ __global__ void __launch_bounds__(kThreads, OCC)
         for (int c = 0; c < JB; ++c) {
           const float4 aj = sj[buf][j + c];
           const float wj = (diag && j + c <= tid) ? 0.0f : aj.w;
-          pair_setup_pq(ai, aj, wj, qp, wide >= 1, u2[c], nl2[c], s2[c], d2[c]);
+          if (FOLD) pair_setup_pq_folded(ai, aj, wj, qp, wide >= 1, nl2[c], s2[c], d2[c]);
+          else pair_setup_pq(ai, aj, wj, qp, wide >= 1, u2[c], nl2[c], s2[c], d2[c]);
         }
 #pragma unroll
         for (int m = 0; m < Q / 2; ++m) {
 #pragma unroll
           for (int c = 0; c < JB; ++c) {
-            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2[m]) : "l"(u2[c]), "l"(s2[c]));
+            if (FOLD) asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc2[m]) : "l"(s2[c]));
+            else asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2[m]) : "l"(u2[c]), "l"(s2[c]));
             asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2[c]) : "l"(nl2[c]), "l"(s2[c]));
             asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2[c]) : "l"(d2[c]));
           }
@@ -519,14 +537,15 @@ void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const i
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
-template <int Q, int JB, int OCC>
+template <int Q, int JB, int OCC, bool FOLD = false>
 void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                     int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
                     int* status, int* next_work, const int64_t* work_out, int budget) {
   int per_sm = 0;
-  CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC>, kThreads, 0));
+  CRAB_CUDA_CHECK(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC, FOLD>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
-  k_pair_fp32_pq<Q, JB, OCC><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
+  k_pair_fp32_pq<Q, JB, OCC, FOLD><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
                                                         status, next_work, work_out, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
@@ -781,7 +800,11 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   P.wide = hmax > 0.8 ? 2 : (hmax > 0.125 ? 1 : 0);
   std::vector<int4> work;
   if (P.segments.empty()) {
-    work = shard_work(make_work(P.L, P.n_qblocks, 8, P.lattice_first_tile), P.shard, P.n_shards);
+    // runs of up to 8 j tiles per item, shorter when that leaves fewer items
+    // than about four per resident CTA (small structures)
+    const int64_t tile_pairs = (int64_t)P.L.n_tiles * (P.L.n_tiles + 1) / 2 * P.n_qblocks;
+    const int run = (int)std::max<int64_t>(1, std::min<int64_t>(8, tile_pairs / (4 * 3 * (int64_t)ctx->sm_count)));
+    work = shard_work(make_work(P.L, P.n_qblocks, run, P.lattice_first_tile), P.shard, P.n_shards);
   } else {
     std::vector<int64_t> out;
     make_work_segments(P, P.n_qblocks, 8, work, out);
@@ -930,6 +953,22 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH_PQ(150, 1, 2, 1 + kPackedQ)
     CRAB_LAUNCH_PQ(168, 1, 2, 1 + kPackedQ)
 #undef CRAB_LAUNCH_PQ
+#define CRAB_LAUNCH_PQF(QQ, JJ, OO, CODE)                                                                       \
+  if (P.Q == QQ && P.jb == CODE) {                                                                               \
+    launch_fp32_pq<QQ, JJ, OO, true>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,    \
+                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,      \
+                                     ctx->wait_budget);                                                           \
+    launched = true;                                                                                             \
+  }
+    CRAB_LAUNCH_PQF(168, 1, 2, kFolded1)
+    CRAB_LAUNCH_PQF(150, 1, 2, kFolded1)
+    CRAB_LAUNCH_PQF(168, 2, 2, kFolded2)
+    CRAB_LAUNCH_PQF(150, 2, 2, kFolded2)
+    CRAB_LAUNCH_PQF(128, 2, 2, kFolded2)
+    CRAB_LAUNCH_PQF(126, 1, 3, kFolded1x3)
+    CRAB_LAUNCH_PQF(100, 1, 3, kFolded1x3)
+    CRAB_LAUNCH_PQF(84, 1, 4, kFolded1x4)
+#undef CRAB_LAUNCH_PQF
     if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
   }
   ctx->launches += 1;
@@ -1069,7 +1108,9 @@ static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2
                                      {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
                                      {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
-                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ}};
+                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
+                                     {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}};
 
 bool pair_variant_known(int variant) {
   const int Q = variant / 16, jb = variant % 16;
@@ -1093,7 +1134,9 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out
   static const int kVariants[][2] = {{64, 2},  {96, 2},  {128, 2}, {64, 4}, {96, 4}, {64, 2 + kPackedQ},
                                      {96, 2 + kPackedQ}, {128, 1 + kPackedQ}, {128, 2 + kPackedQ},
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
-                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ}};
+                                     {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
+                                     {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;

@@ -11,14 +11,20 @@
 //   ∂χ²/∂x_i = Σ_{j≠i} occ_i occ_j g_ab(r_ij) (x_i - x_j)/r_ij,
 //   g_ab(r) = (1/r) Σ_k α_ab,k cos(q_k r) - (1/r²) Σ_k β_ab,k sin(q_k r),
 //   α_ab,k = 2 w_k Â_a Â_b,  β_ab,k = α_ab,k / q_k.
-// The kernel recomputes every pair term per tile (nothing O(N²) is stored):
-// one thread per atom i, j tiles in shared memory, sin and cos of q r
-// advanced together along each uniform q block by the Reinsch recurrence in
-// one packed f32x2 register pair, the q sums accumulated per block in FP32
-// and per atom in FP64.  A pair's term for atom j is the negative of its
-// term for atom i (g_ab = g_ba), so only tile pairs it <= jt run: a diagonal
-// tile computes its ordered pairs for its own atoms, an off-diagonal one also
-// sums each j's terms over the block (a warp shuffle, then shared memory).
+// Since A_i depends only on the atom's type, the pair term depends only on
+// the type pair and the distance:
+//   ∂χ²/∂x_i = Σ_j occ_i occ_j h_ab(r_ij) (x_i - x_j),
+//   h_ab(r) = g_ab(r) / r = Σ_k α_ab,k q_k² F(q_k r),  F(x) = (cos x - sin x / x) / x²,
+// and F is smooth and even (F(0) = -1/3), so h_ab is a band-limited function
+// of r (bandwidth q_max).  k_grad_table evaluates it in f64 on a uniform grid
+// r_n = n δr, δr = 0.02 / q_max, up to the structure's largest pair distance;
+// the pair kernel interpolates it with the 4-point Lagrange cubic (error below
+// 4e-9 of max |h|, from (q_max δr)^4 × 0.0234), from one float4 of the four
+// taps per grid cell.  Nothing O(N²) is stored: the table is O(T² × q_max × D).
+// k_grad_pairs: one thread per atom i, j tiles staged in shared memory, every
+// ordered pair (no cross-lane reductions); per (i tile, chunk of j tiles) an
+// FP32 sum per j tile added into f64, and k_grad_reduce adds the chunks in a
+// fixed order (deterministic).
 
 #include <cuda_runtime.h>
 
@@ -36,106 +42,111 @@ using namespace dev;
 
 constexpr int kGT = 128;
 
-// Tile pair (it, jt), it <= jt, of block w = jt (jt + 1) / 2 + it.
-__device__ __forceinline__ void grad_tri_decode(int w, int& it, int& jt) {
-  int b = (int)((sqrt(8.0 * (double)w + 1.0) - 1.0) * 0.5);
-  while (b > 0 && b * (b + 1) / 2 > w) --b;
-  while ((b + 1) * (b + 2) / 2 <= w) ++b;
-  jt = b;
-  it = w - b * (b + 1) / 2;
+// F(x) = (cos x - sin x / x) / x² in f64: its series sum_{n>=1} (-1)^n 2n x^{2n-2} / (2n+1)!
+// below 0.5 (ten terms: the next is below 1e-17 of F), the closed form above.
+__device__ __forceinline__ double grad_F(double x) {
+  if (x < 0.5) {
+    const double x2 = x * x;
+    double term = -1.0 / 3.0, sum = 0.0;  // n = 1
+    for (int n = 1; n <= 10; ++n) {
+      sum += term;
+      // term_{n+1} / term_n = -x² (2n+2) / (2n) / ((2n+2)(2n+3)) = -x² / (2n (2n+3))
+      term *= -x2 / ((double)(2 * n) * (double)(2 * n + 3));
+    }
+    return sum;
+  }
+  double sx, cx;
+  sincos(x, &sx, &cx);
+  return (cx - sx / x) / (x * x);
 }
 
-__global__ void __launch_bounds__(kGT, 4)
-    k_chi2_grad(const float4* __restrict__ atoms, const int* __restrict__ tile_type, int T,
-                const float2* __restrict__ coef, int nq, const float4* __restrict__ qpar,
-                const int2* __restrict__ qrange, int n_qb, int wide, double* __restrict__ grad) {
-  extern __shared__ float2 s_coef[];  // nq (alpha, beta) of this tile pair's type pair
-  __shared__ float4 sj[kGT];
-  __shared__ double s_gj[kGT][3];     // the j tile's terms (off-diagonal tile pairs)
-  int it, jt;
-  grad_tri_decode((int)blockIdx.x, it, jt);
-  const int tid = threadIdx.x, lane = tid & 31;
-  const bool diag = it == jt;
-  const float4 ai = atoms[(size_t)it * kGT + tid];
-  sj[tid] = atoms[(size_t)jt * kGT + tid];
-  s_gj[tid][0] = s_gj[tid][1] = s_gj[tid][2] = 0.0;
-  const int ta = tile_type[it], tb = tile_type[jt];
-  const int a = min(ta, tb), b = max(ta, tb);
-  const int ab = a * T - a * (a - 1) / 2 + (b - a);
-  for (int k = tid; k < nq; k += kGT) s_coef[k] = coef[(size_t)ab * nq + k];
-  __syncthreads();
-  double gx = 0.0, gy = 0.0, gz = 0.0;
-  for (int j = 0; j < kGT; ++j) {
-    const float4 aj = sj[j];
-    const float wij = (jt == it && j == tid) ? 0.0f : ai.w * aj.w;
-    const float dx = ai.x - aj.x, dy = ai.y - aj.y, dz = ai.z - aj.z;
-    const float x = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-8f);
-    const float y0 = rsqrtf(x);
-    const float sq = x * y0;
-    const float hy = 0.5f * y0;
-    const float r = fmaf(fmaf(-sq, sq, x), hy, sq);
-    const float rinv = fmaf(fmaf(-sq, y0, 1.0f), hy, y0);
-    double Csum = 0.0, Ssum = 0.0;
-    for (int blk = 0; blk < n_qb; ++blk) {
-      const float4 qp = qpar[blk];
-      const int2 qr = qrange[blk];
-      const float phi = fmaf(qp.x, r, qp.y * r);
-      const float h = fmaf(qp.z, r, qp.w * r);
-      float s0, c0, sh, ch;
-      sincos_seed(phi, &s0, &c0);
-      if (wide) sincos_seed(h, &sh, &ch);
-      else sincos_small(h, &sh, &ch);
-      const float half_l = 2.0f * sh * sh;     // λ/2 = 1 - cos θ
-      const float sin_t = 2.0f * sh * ch;      // sin θ
-      const float ds = fmaf(s0, half_l, c0 * sin_t);   // sin φ - sin(φ-θ)
-      const float dc = fmaf(c0, half_l, -s0 * sin_t);  // cos φ - cos(φ-θ)
-      unsigned long long cs2 = pack2(c0, s0), d2 = pack2(dc, ds);
-      const unsigned long long nl2 = pack2(-2.0f * half_l, -2.0f * half_l);
-      unsigned long long acc2 = pack2(0.0f, 0.0f);
-      const unsigned long long* cf = reinterpret_cast<const unsigned long long*>(s_coef) + qr.x;
-#pragma unroll 4
-      for (int k = 0; k < qr.y; ++k) {
-        const unsigned long long ab2 = cf[k];
-        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2) : "l"(ab2), "l"(cs2));
-        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2) : "l"(nl2), "l"(cs2));
-        asm("add.rn.f32x2 %0, %0, %1;" : "+l"(cs2) : "l"(d2));
-      }
-      float C, S;
-      unpack2(acc2, C, S);
-      Csum += (double)C;
-      Ssum += (double)S;
-    }
-    const double g = (double)wij * ((double)rinv * (Csum - Ssum * (double)rinv));
-    const double gr = g * (double)rinv;
-    gx += gr * dx;
-    gy += gr * dy;
-    gz += gr * dz;
-    if (!diag) {  // uniform over the block: every thread is at the same j
-      double jx = -gr * dx, jy = -gr * dy, jz = -gr * dz;
+// h_ab(r_n) for n = 0 .. n_r + 2 (r_n = n dr) of every type pair: out[ab][n].
+// One warp per grid point, the lanes over q, then a warp reduction (fixed order).
+__global__ void k_grad_h(const double* __restrict__ alpha, const double* __restrict__ q, int nq, int n_pairs,
+                         int n_r, double dr, double* __restrict__ out) {
+  const int64_t idx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t per = (int64_t)n_r + 3;
+  if (idx >= per * n_pairs) return;  // uniform over the warp
+  const int ab = (int)(idx / per), n = (int)(idx % per);
+  const double r = n * dr;
+  const double* al = alpha + (size_t)ab * nq;
+  double h = 0.0;
+  for (int k = lane; k < nq; k += 32) h += al[k] * q[k] * q[k] * grad_F(q[k] * r);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        jx += __shfl_xor_sync(0xffffffffu, jx, o);
-        jy += __shfl_xor_sync(0xffffffffu, jy, o);
-        jz += __shfl_xor_sync(0xffffffffu, jz, o);
-      }
-      if (lane == 0) {
-        atomicAdd(&s_gj[j][0], jx);
-        atomicAdd(&s_gj[j][1], jy);
-        atomicAdd(&s_gj[j][2], jz);
-      }
-    }
-  }
-  double* out = grad + 3 * ((size_t)it * kGT + tid);
-  atomicAdd(out, gx);
-  atomicAdd(out + 1, gy);
-  atomicAdd(out + 2, gz);
-  if (!diag) {
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+  if (lane == 0) out[idx] = h;
+}
+
+// The four taps of cell n, h(r_{n-1}) .. h(r_{n+2}) (h is even: h(r_{-1}) = h(r_1)).
+__global__ void k_grad_taps(const double* __restrict__ h, int n_pairs, int n_r, float4* __restrict__ taps) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)(n_r + 1) * n_pairs) return;
+  const int ab = (int)(idx / (n_r + 1)), n = (int)(idx % (n_r + 1));
+  const double* row = h + (size_t)ab * (n_r + 3);
+  taps[idx] = make_float4((float)row[n == 0 ? 1 : n - 1], (float)row[n], (float)row[n + 1], (float)row[n + 2]);
+}
+
+// Partial coordinate gradient of the atoms of tile it over the j tiles of
+// chunk c: part[c][it*128 + tid][3].
+__global__ void __launch_bounds__(kGT)
+    k_grad_pairs(const float4* __restrict__ atoms, const int* __restrict__ tile_type, int T, int n_tiles,
+                 int chunk, const float4* __restrict__ taps, int n_r, float inv_dr, double* __restrict__ part) {
+  __shared__ float4 sj[kGT];
+  const int it = blockIdx.x, c = blockIdx.y, tid = threadIdx.x;
+  const float4 ai = atoms[(size_t)it * kGT + tid];
+  const int ta = tile_type[it];
+  const float rmax_cell = (float)n_r - 0.001f;  // last cell index the taps cover, minus a margin
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  const int jt0 = c * chunk, jt1 = min(n_tiles, jt0 + chunk);
+  for (int jt = jt0; jt < jt1; ++jt) {
     __syncthreads();
-    double* outj = grad + 3 * ((size_t)jt * kGT + tid);
-    atomicAdd(outj, s_gj[tid][0]);
-    atomicAdd(outj + 1, s_gj[tid][1]);
-    atomicAdd(outj + 2, s_gj[tid][2]);
+    sj[tid] = atoms[(size_t)jt * kGT + tid];
+    __syncthreads();
+    const int tb = tile_type[jt];
+    const int a = min(ta, tb), b = max(ta, tb);
+    const float4* tp = taps + (size_t)(a * T - a * (a - 1) / 2 + (b - a)) * (n_r + 1);
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+#pragma unroll 4
+    for (int j = 0; j < kGT; ++j) {
+      const float4 aj = sj[j];
+      const float dx = ai.x - aj.x, dy = ai.y - aj.y, dz = ai.z - aj.z;
+      const float x = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-12f);
+      const float y0 = rsqrtf(x);
+      const float sq = x * y0;
+      const float r = fmaf(fmaf(-sq, sq, x), 0.5f * y0, sq);  // Newton-refined sqrt
+      const float t = fminf(r * inv_dr, rmax_cell);
+      const float fl = floorf(t);
+      const float u = t - fl;
+      const float4 v = __ldg(tp + (int)fl);
+      // Lagrange cubic on nodes -1, 0, 1, 2 at u in [0, 1)
+      const float um1 = u - 1.0f, um2 = u - 2.0f, up1 = u + 1.0f;
+      const float w0 = -u * um1 * um2 * (1.0f / 6.0f), w1 = up1 * um1 * um2 * 0.5f;
+      const float w2 = -up1 * u * um2 * 0.5f, w3 = up1 * u * um1 * (1.0f / 6.0f);
+      const float hv = fmaf(w0, v.x, fmaf(w1, v.y, fmaf(w2, v.z, w3 * v.w)));
+      const float coefj = hv * (ai.w * aj.w);  // a pair of one atom with itself has dx = 0
+      fx = fmaf(coefj, dx, fx);
+      fy = fmaf(coefj, dy, fy);
+      fz = fmaf(coefj, dz, fz);
+    }
+    gx += (double)fx;
+    gy += (double)fy;
+    gz += (double)fz;
   }
+  double* out = part + ((size_t)c * n_tiles * kGT + (size_t)it * kGT + tid) * 3;
+  out[0] = gx;
+  out[1] = gy;
+  out[2] = gz;
+}
+
+// grad[slot] = the sum over the chunks, in chunk order.
+__global__ void k_grad_reduce(const double* __restrict__ part, int64_t n_slots, int n_chunks,
+                              double* __restrict__ grad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_slots * 3) return;
+  double s = 0.0;
+  for (int c = 0; c < n_chunks; ++c) s += part[(size_t)c * n_slots * 3 + i];
+  grad[i] = s;
 }
 
 }  // namespace
@@ -192,56 +203,52 @@ void chi2_grad_impl(crab_ctx* ctx, const crab_struct* st, const double* q, const
   if (!grad_xyz) return;
   std::fill(grad_xyz, grad_xyz + 3 * st->n, 0.0);
   if (t.w.empty()) return;
-  // per type pair and q: (alpha, beta)
+  // per type pair and q: alpha = 2 w_k A_a A_b (zero at q = 0, where the term has no r dependence)
   const int NP = T * (T + 1) / 2;
-  std::vector<float2> coef((size_t)NP * nq);
+  std::vector<double> alpha((size_t)NP * nq, 0.0);
+  double qmax = 0.0;
+  for (int64_t k = 0; k < nq; ++k) qmax = std::max(qmax, q[k]);
   for (int a = 0; a < T; ++a)
     for (int bb = a; bb < T; ++bb)
       for (int64_t k = 0; k < nq; ++k) {
+        if (!(q[k] > 0.0)) continue;
         const double G = excluded_volume_scale(q[k], s.c1);
         const double Aa = V[(size_t)a * nq + k] - G * E[(size_t)a * nq + k] + s.c2 * H[(size_t)a * nq + k];
         const double Ab = V[(size_t)bb * nq + k] - G * E[(size_t)bb * nq + k] + s.c2 * H[(size_t)bb * nq + k];
-        const double alpha = 2.0 * w[k] * Aa * Ab;
-        const double beta = q[k] > 0.0 ? alpha / q[k] : 0.0;
-        coef[(size_t)pair_index(a, bb, T) * nq + k] = make_float2((float)(q[k] > 0.0 ? alpha : 0.0), (float)beta);
+        alpha[(size_t)pair_index(a, bb, T) * nq + k] = 2.0 * w[k] * Aa * Ab;
       }
   Layout L = build_layout(t.xyz.data(), t.w.data(), t.type.data(), (int64_t)t.w.size(), T, false);
-  std::vector<double> qv(q, q + nq);
-  const std::vector<int2> qr = q_blocks(qv, 128);
-  std::vector<float4> qp(qr.size());
-  double max_half = 0.0;
-  for (size_t bk = 0; bk < qr.size(); ++bk) {
-    const int64_t st0 = qr[bk].x, cnt = qr[bk].y;
-    const double q0 = q[st0];
-    const double half = cnt > 1 ? 0.5 * (q[st0 + cnt - 1] - q[st0]) / (double)(cnt - 1) : 0.0;
-    const float q0h = (float)q0, hh = (float)half;
-    qp[bk] = make_float4(q0h, (float)(q0 - (double)q0h), hh, (float)(half - (double)hh));
-    max_half = std::max(max_half, std::fabs(half));
-  }
-  const int wide = (max_half * (L.extent + 1.0) > 0.8) ? 1 : 0;
+  // radial grid: dr = 0.02 / q_max up to the largest pair distance (bounded by the layout's extent)
+  const double dr = qmax > 0.0 ? 0.02 / qmax : 1.0;
+  const double reach = L.extent * 1.001 + 4.0 * dr;
+  require(reach / dr < 4.0e7, "radial table of the gradient too long");
+  const int n_r = std::max(2, (int)std::ceil(reach / dr));
   cudaStream_t sm = ctx->stream;
   float4* d_atoms = (float4*)ctx->dev("grad.atoms", (size_t)L.n_pad * sizeof(float4));
   int* d_tt = (int*)ctx->dev("grad.tt", L.tile_type.size() * sizeof(int));
-  float2* d_coef = (float2*)ctx->dev("grad.coef", coef.size() * sizeof(float2));
-  float4* d_qp = (float4*)ctx->dev("grad.qpar", qp.size() * sizeof(float4));
-  int2* d_qr = (int2*)ctx->dev("grad.qrange", qr.size() * sizeof(int2));
-  double* d_grad = (double*)ctx->dev("grad.out", (size_t)L.n_pad * 3 * sizeof(double));
+  double* d_alpha = (double*)ctx->dev("grad.alpha", alpha.size() * sizeof(double));
+  double* d_q = (double*)ctx->dev("grad.q", (size_t)nq * sizeof(double));
+  double* d_h = (double*)ctx->dev("grad.h", (size_t)NP * (n_r + 3) * sizeof(double));
+  float4* d_taps = (float4*)ctx->dev("grad.taps", (size_t)NP * (n_r + 1) * sizeof(float4));
   copy_h2d(ctx, d_atoms, L.atoms.data(), (size_t)L.n_pad * sizeof(float4), sm);
   copy_h2d(ctx, d_tt, L.tile_type.data(), L.tile_type.size() * sizeof(int), sm);
-  copy_h2d(ctx, d_coef, coef.data(), coef.size() * sizeof(float2), sm);
-  copy_h2d(ctx, d_qp, qp.data(), qp.size() * sizeof(float4), sm);
-  copy_h2d(ctx, d_qr, qr.data(), qr.size() * sizeof(int2), sm);
-  CRAB_CUDA_CHECK(cudaMemsetAsync(d_grad, 0, (size_t)L.n_pad * 3 * sizeof(double), sm));
-  const size_t smem = (size_t)nq * sizeof(float2);
-  require(smem <= 200 * 1024, "too many q values for the gradient kernel");
-  if (smem > 48 * 1024)
-    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_chi2_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t n_blocks = (int64_t)L.n_tiles * (L.n_tiles + 1) / 2;  // tile pairs it <= jt
-  require(n_blocks < ((int64_t)1 << 31), "too many atoms for the gradient kernel");
-  k_chi2_grad<<<(unsigned)n_blocks, kGT, smem, sm>>>(d_atoms, d_tt, T, d_coef, (int)nq, d_qp, d_qr,
-                                                            (int)qr.size(), wide, d_grad);
+  copy_h2d(ctx, d_alpha, alpha.data(), alpha.size() * sizeof(double), sm);
+  copy_h2d(ctx, d_q, q, (size_t)nq * sizeof(double), sm);
+  const int64_t nh = (int64_t)NP * (n_r + 3), ntp = (int64_t)NP * (n_r + 1);
+  k_grad_h<<<(unsigned)((nh * 32 + 255) / 256), 256, 0, sm>>>(d_alpha, d_q, (int)nq, NP, n_r, dr, d_h);
+  k_grad_taps<<<(unsigned)((ntp + 127) / 128), 128, 0, sm>>>(d_h, NP, n_r, d_taps);
+  // (i tile, chunk of j tiles) blocks: about four per SM
+  const int n_tiles = L.n_tiles;
+  const int want = std::max(1, (4 * ctx->sm_count + n_tiles - 1) / std::max(n_tiles, 1));
+  const int chunk = std::max(1, (n_tiles + want - 1) / want);
+  const int n_chunks = (n_tiles + chunk - 1) / chunk;
+  double* d_part = (double*)ctx->dev("grad.part", (size_t)n_chunks * L.n_pad * 3 * sizeof(double));
+  double* d_grad = (double*)ctx->dev("grad.out", (size_t)L.n_pad * 3 * sizeof(double));
+  k_grad_pairs<<<dim3((unsigned)n_tiles, (unsigned)n_chunks), kGT, 0, sm>>>(d_atoms, d_tt, T, n_tiles, chunk, d_taps,
+                                                                             n_r, (float)(1.0 / dr), d_part);
+  k_grad_reduce<<<(unsigned)((L.n_pad * 3 + 255) / 256), 256, 0, sm>>>(d_part, L.n_pad, n_chunks, d_grad);
   CRAB_CUDA_CHECK(cudaGetLastError());
-  ctx->launches += 1;
+  ctx->launches += 4;
   std::vector<double> g((size_t)L.n_pad * 3);
   copy_d2h(ctx, g.data(), d_grad, g.size() * sizeof(double), sm);
   CRAB_CUDA_CHECK(cudaStreamSynchronize(sm));

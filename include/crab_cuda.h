@@ -238,7 +238,9 @@ int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int
  * = q values one thread advances per pair between exact re-seeds, and JB = j
  * atoms per thread iteration; JB >= 8 selects the q-packed kernel, whose f32x2
  * registers hold two consecutive q points, with (JB-8) % 4 independent chains,
- * built for three CTAs per SM when JB >= 12) and
+ * built for three CTAs per SM when JB >= 12; JB = 5, 6, 7, 3: the q-packed
+ * kernel with the pair weight folded into the recurrence state, with 1, 2,
+ * 1, 1 chains at 2, 2, 3, 4 CTAs per SM) and
  * keep the fastest.  *chosen = Q*16 + JB;
  * the first `capacity` variants and their times (ms) are written to
  * variants/ms (may be NULL), their count to *n_variants. */

@@ -304,10 +304,13 @@ def test_lattice_plan_matches_fp64_20k(engine):
     assert err.max() <= PARTIAL_ATOL
 
 
-# Every kernel variant the plan can dispatch (Q*16 + jb; jb >= 8: q-packed, jb >= 12: 3 CTAs/SM).
+# Every kernel variant the plan can dispatch (Q*16 + jb; jb >= 8: q-packed, jb >= 12: 3 CTAs/SM;
+# jb 5, 6, 7, 3: q-packed with the weight folded into the recurrence, 1 or 2 chains, 2 to 4 CTAs/SM).
 ALL_VARIANTS = [8 * 16 + 2, 16 * 16 + 2, 32 * 16 + 2, 48 * 16 + 2, 64 * 16 + 2, 96 * 16 + 2, 128 * 16 + 2,
                 64 * 16 + 4, 96 * 16 + 4, 64 * 16 + 10, 96 * 16 + 10, 128 * 16 + 9, 128 * 16 + 10, 128 * 16 + 13,
-                100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9, 168 * 16 + 9]
+                100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9, 168 * 16 + 9,
+                168 * 16 + 5, 150 * 16 + 5, 168 * 16 + 6, 150 * 16 + 6, 128 * 16 + 6, 126 * 16 + 7, 100 * 16 + 7,
+                84 * 16 + 3]
 
 
 @pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "wide"])
