@@ -20,9 +20,11 @@ second, pairs = M(M-1)/2 over the M atoms + sites.
   algorithm) on all host threads, on a q subset of the same workload.
 
 ``--impl reference`` times that CPU restatement alone (the reference crate is
-Rust and cannot be built here) with the same metric.  Under torchrun each rank
-runs its own structure on its own GPU (independent objects, weak scaling, no
-data-path collective); time is the max over ranks.
+Rust and cannot be built here) with the same metric.  Under torchrun the one
+structure is split over the GPUs (strong scaling): every rank takes the work
+items crab_shard_assign gives it (crab_pair_plan_create_lattice_shard), and
+each step ends with one NCCL all-reduce of the 60 KB of partials (in ``e2e``:
+of the six-term basis); time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -170,7 +172,8 @@ class ClockSampler:
 
 
 def workload(rank: int):
-    """Structure of this rank plus its adaptive 3 Å hydration sites, as typed pair-sum arrays."""
+    """The seeded 20,000-atom structure (rank 0's; the other seeds make the per-rank
+    structures of the auxiliary sections)."""
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import synth
 
@@ -650,44 +653,76 @@ def run_ours(args, rank, world, local):
     peak = C.c_double()
     eng.check(lib.crab_measure_fp32_peak(eng.handle, 150.0, C.byref(peak)))
 
-    s = workload(rank)
+    # one structure; with N > 1 ranks it is split over the GPUs (every rank
+    # builds the same structure and takes the work items crab_shard_assign
+    # gives it; one NCCL all-reduce of the partials per step completes the sums)
+    s = workload(0)
     sites, vol = cs.hydration_grid_adaptive(s, 3.0, engine=eng)
     xyz, w, t, T = typed_arrays(s, sites)
     m = len(w)
     # the sites lie on a 3 Å lattice: integer voxel offsets for the exact site–site histogram
     cells = np.ascontiguousarray(np.rint((sites - sites.min(axis=0)) / 3.0).astype(np.int32))
     plan = C.c_void_p()
-    eng.check(lib.crab_pair_plan_create_lattice(eng.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
-                                                t.ctypes.data_as(N.I32P), m, T, Q.ctypes.data_as(N.D), len(Q),
-                                                cells.ctypes.data_as(N.I32P), len(sites), 3.0, C.byref(plan)))
+    eng.check(lib.crab_pair_plan_create_lattice_shard(eng.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
+                                                      t.ctypes.data_as(N.I32P), m, T, Q.ctypes.data_as(N.D),
+                                                      len(Q), cells.ctypes.data_as(N.I32P), len(sites), 3.0, rank,
+                                                      world, C.byref(plan)))
     chosen = C.c_int32()
-    tv = np.zeros(16, dtype=np.int32)
-    tms = np.zeros(16)
+    tv = np.zeros(32, dtype=np.int32)
+    tms = np.zeros(32)
     ntv = C.c_int32()
     eng.check(lib.crab_pair_plan_autotune(eng.handle, plan, C.byref(chosen), tv.ctypes.data_as(N.I32P),
-                                          tms.ctypes.data_as(N.D), 16, C.byref(ntv)))
+                                          tms.ctypes.data_as(N.D), 32, C.byref(ntv)))
     tuning = {_variant_name(v): round(float(t), 3) for v, t in zip(tv[:ntv.value], tms[:ntv.value])}
     pairq = lib.crab_pair_plan_pairq(plan)
     ns = len(sites)
     kernel_pairq = pairq - ns * (ns - 1) / 2.0 * len(Q)  # the lattice path sums the site–site pairs
 
-    # warm-up, then K timed steps (each a flushed, event-bracketed kernel)
+    # warm-up, then K timed steps (each a flushed, event-bracketed kernel;
+    # with N > 1 each step also all-reduces this rank's partials over NCCL,
+    # timed with CUDA events on torch's stream)
     eng.check(lib.crab_pair_plan_run(eng.handle, plan, args.warmup, FLUSH_BYTES, None))
     step_ms = np.zeros(args.steps)
+    reduce_ms = np.zeros(args.steps)
+    n_part = T * (T + 1) // 2 * len(Q)
+    part_host = np.zeros(n_part)
+    if world > 1:
+        import torch
+
+        part_dev = torch.zeros(n_part, dtype=torch.float64, device=f"cuda:{local}")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(args.warmup):
+            dist.dist.all_reduce(part_dev)
+        torch.cuda.synchronize()
     eng.reset_stats()
+    one = np.zeros(1)
     with ClockSampler(local) as clocks:
         dist.barrier()
         t0 = time.perf_counter()
-        eng.check(lib.crab_pair_plan_run(eng.handle, plan, args.steps, FLUSH_BYTES, step_ms.ctypes.data_as(N.D)))
+        if world == 1:
+            eng.check(lib.crab_pair_plan_run(eng.handle, plan, args.steps, FLUSH_BYTES, step_ms.ctypes.data_as(N.D)))
+        else:
+            for k in range(args.steps):
+                eng.check(lib.crab_pair_plan_run(eng.handle, plan, 1, FLUSH_BYTES, one.ctypes.data_as(N.D)))
+                step_ms[k] = one[0]
+                eng.check(lib.crab_pair_plan_read(eng.handle, plan, part_host.ctypes.data_as(N.D), None))
+                part_dev.copy_(torch.from_numpy(part_host))
+                ev0.record()
+                dist.dist.all_reduce(part_dev)
+                ev1.record()
+                ev1.synchronize()
+                reduce_ms[k] = ev0.elapsed_time(ev1)
         wall = time.perf_counter() - t0
         dist.barrier()
     launches, _, _ = eng.stats()
-    device_s = float(step_ms.sum()) / 1e3
+    device_s = float(step_ms.sum() + reduce_ms.sum()) / 1e3
     max_s = dist.max(device_s)
-    total_units = dist.sum(pairq * args.steps)
+    total_units = pairq * args.steps  # the one structure's pair·q, however many GPUs share it
     value = total_units / max_s
     ms_per_step = 1e3 * max_s / args.steps
-    achieved = 4.0 * kernel_pairq / (float(step_ms.mean()) * 1e-3) / 1e12
+    # roofline of this rank's kernel: its share of the kernel-evaluated pair·q (the
+    # shards' items are near equal in cost) over its kernel time
+    achieved = 4.0 * kernel_pairq / world / (float(step_ms.mean()) * 1e-3) / 1e12
 
     # accuracy of this curve against the FP64 device reference (outside the timed region)
     import crabsaxs_b200.synth as synth
@@ -713,16 +748,26 @@ def run_ours(args, rank, world, local):
     _, he = pinned(s.element)
     _, hg = pinned(s.group)
     _, hq = pinned(Q)
-    _, hout = pinned(np.zeros((6, len(Q))))
+    tout, hout = pinned(np.zeros((6, len(Q))))
     solv = sp.to_c()
+
+    basis_dev = torch.zeros((6, len(Q)), dtype=torch.float64, device=f"cuda:{local}") if world > 1 else None
 
     def e2e_step():
         st = C.c_void_p()
         eng.check(lib.crab_structure_create(eng.handle, hx.ctypes.data_as(N.D), ho.ctypes.data_as(N.D),
                                             he.ctypes.data_as(N.I8P), hg.ctypes.data_as(N.I8P), len(ho),
                                             C.byref(st)))
-        eng.check(lib.crab_debye_solvent_basis(eng.handle, st, hq.ctypes.data_as(N.D), len(hq), C.byref(solv), 1,
-                                               hout.ctypes.data_as(N.D)))
+        if world == 1:
+            eng.check(lib.crab_debye_solvent_basis(eng.handle, st, hq.ctypes.data_as(N.D), len(hq), C.byref(solv),
+                                                   1, hout.ctypes.data_as(N.D)))
+        else:  # this rank's share of the basis, then the sum over the GPUs, read back
+            eng.check(lib.crab_debye_solvent_basis_shard(eng.handle, st, hq.ctypes.data_as(N.D), len(hq),
+                                                         C.byref(solv), 1, N.PREC_FP32, rank, world,
+                                                         hout.ctypes.data_as(N.D)))
+            basis_dev.copy_(tout, non_blocking=True)
+            dist.dist.all_reduce(basis_dev)
+            tout.copy_(basis_dev)
         lib.crab_structure_destroy(st)
 
     for _ in range(args.warmup):
@@ -748,8 +793,9 @@ def run_ours(args, rank, world, local):
         run_launches, _, _ = eng.stats()
         h2d, d2h = C.c_int64(), C.c_int64()
         lib.crab_ctx_transfer_stats(eng.handle, C.byref(h2d), C.byref(d2h))
+        exch = 6 * len(Q) * 8 * args.steps if world > 1 else 0  # the basis to and from the all-reduce
         e2e_runs.append({"seconds": dist.max(run_s), "steps_ms": steps_ms, "launches": int(run_launches),
-                         "h2d": int(h2d.value), "d2h": int(d2h.value)})
+                         "h2d": int(h2d.value) + exch, "d2h": int(d2h.value) + exch})
     best = min(e2e_runs, key=lambda r: r["seconds"])
     e2e_s, e2e_steps, e2e_launches = best["seconds"], best["steps_ms"], best["launches"]
     e2e_value = total_units / e2e_s
@@ -777,12 +823,16 @@ def run_ours(args, rank, world, local):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD,
                        "n_atoms": N_ATOMS, "n_sites": int(len(sites)), "n_types": T, "n_q": len(Q),
                        "kernel_variant": _variant_name(chosen.value), "autotune_ms": tuning,
-                       "parallelism": f"independent structure per GPU x{world}",
+                       "parallelism": "one GPU" if world == 1 else
+                       f"one structure split over {world} GPUs (work items by crab_shard_assign, "
+                       f"NCCL all-reduce of the partials each step)",
+                       "allreduce_ms_per_step": float(np.mean(reduce_ms)) if world > 1 else 0.0,
                        "l2": "flushed before every step (256 MiB memset, outside the step events)"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value, "traffic": traffic_per_launch(),

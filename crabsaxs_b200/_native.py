@@ -174,6 +174,8 @@ _SIGS = {
     "crab_pair_plan_create": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, C.POINTER(P)]),
     "crab_pair_plan_create_lattice": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, I32P, I64, C.c_double,
                                                 C.POINTER(P)]),
+    "crab_pair_plan_create_lattice_shard": (C.c_int, [P, D, D, I32P, I64, C.c_int32, D, I64, I32P, I64, C.c_double,
+                                                      C.c_int32, C.c_int32, C.POINTER(P)]),
     "crab_pair_plan_run": (C.c_int, [P, P, C.c_int32, I64, D]),
     "crab_pair_plan_autotune": (C.c_int, [P, P, I32P, I32P, D, C.c_int32, I32P]),
     "crab_pair_plan_select": (C.c_int, [P, P, C.c_int32]),

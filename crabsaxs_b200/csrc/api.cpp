@@ -546,8 +546,15 @@ int crab_pair_plan_create(crab_ctx* ctx, const double* xyz, const double* w, con
 int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                                   int32_t T, const double* q, int64_t nq, const int32_t* cells, int64_t m,
                                   double spacing, crab_pair_plan** out) {
+  return crab_pair_plan_create_lattice_shard(ctx, xyz, w, type, n, T, q, nq, cells, m, spacing, 0, 1, out);
+}
+
+int crab_pair_plan_create_lattice_shard(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type,
+                                        int64_t n, int32_t T, const double* q, int64_t nq, const int32_t* cells,
+                                        int64_t m, double spacing, int32_t shard, int32_t n_shards,
+                                        crab_pair_plan** out) {
   if (!ctx || !out || T <= 0 || n < 0 || nq < 0 || (n > 0 && (!xyz || !w || !type)) || (nq > 0 && !q) ||
-      m < 0 || (m > 0 && !cells) || !(spacing > 0.0))
+      m < 0 || (m > 0 && !cells) || !(spacing > 0.0) || n_shards < 1 || shard < 0 || shard >= n_shards)
     return CRAB_EINVAL;
   *out = nullptr;
   GUARD(ctx, {
@@ -563,7 +570,8 @@ int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double
     require(last == m, "cells must list every atom of the last type");
     Layout L = build_layout(xyz, w, type, n, T, false);
     LatticeSpec spec{cells, m, spacing};
-    crab_pair_plan* p = new crab_pair_plan{ctx, make_pair_plan(ctx, std::move(L), q, nq, false, &spec)};
+    crab_pair_plan* p =
+        new crab_pair_plan{ctx, make_pair_plan(ctx, std::move(L), q, nq, false, &spec, false, shard, n_shards)};
     *out = p;
   });
 }
@@ -577,7 +585,10 @@ int crab_pair_plan_read(crab_ctx* ctx, crab_pair_plan* plan, double* out, double
   if (!ctx || !plan || !out) return CRAB_EINVAL;
   GUARD(ctx, {
     pair_plan_fetch(ctx, *plan->plan, out, false);
-    if (self_out) std::copy(plan->plan->L.self_w2.begin(), plan->plan->L.self_w2.end(), self_out);
+    if (self_out) {  // the self sums belong to shard 0 (the shards' results add up to the whole)
+      std::copy(plan->plan->L.self_w2.begin(), plan->plan->L.self_w2.end(), self_out);
+      if (plan->plan->shard != 0) std::fill(self_out, self_out + plan->plan->L.T, 0.0);
+    }
   });
 }
 

@@ -229,6 +229,14 @@ int crab_pair_plan_create(crab_ctx* ctx, const double* xyz, const double* w, con
 int crab_pair_plan_create_lattice(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                                   int32_t n_types, const double* q, int64_t nq, const int32_t* cells, int64_t m,
                                   double spacing, crab_pair_plan** out);
+/* The plan of shard `shard` of `n_shards` of the same problem (one per GPU):
+ * the work items crab_shard_assign gives this shard, the self sums, q = 0
+ * and the lattice block on shard 0 only, so the element-wise sum of the
+ * shards' crab_pair_plan_read results (an all-reduce) is the whole. */
+int crab_pair_plan_create_lattice_shard(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type,
+                                        int64_t n, int32_t n_types, const double* q, int64_t nq,
+                                        const int32_t* cells, int64_t m, double spacing, int32_t shard,
+                                        int32_t n_shards, crab_pair_plan** out);
 /* Launch the pair kernel `repeats` times.  Before each launch, when
  * flush_bytes > 0, a buffer of that size is overwritten on the same stream
  * (evicting L2); each launch is bracketed by CUDA events and its device time

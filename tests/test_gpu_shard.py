@@ -44,6 +44,48 @@ def test_partials_shards_and_self_sums(engine):
         assert np.array_equal(got[0][1], self_) and all(not g[1].any() for g in got[1:])
 
 
+def test_lattice_plan_shards_sum_to_the_plan(engine):
+    """The sharded pair plan of the bench's multi-GPU split: the shards'
+    partials (read back after one run each) add up to the unsplit plan's."""
+    import ctypes as C
+
+    s = synth.protein(39, 3000, 18.0)
+    sites, _ = cs.hydration_grid_adaptive(s, 3.0, engine=engine)
+    el = np.unique(s.element)
+    xyz = np.ascontiguousarray(np.concatenate([s.xyz, sites]))
+    w = np.ascontiguousarray(np.concatenate([s.occupancy, np.ones(len(sites))]))
+    t = np.ascontiguousarray(np.concatenate([np.searchsorted(el, s.element), np.full(len(sites), len(el))]).astype(np.int32))
+    T = len(el) + 1
+    cells = np.ascontiguousarray(np.rint((sites - sites.min(axis=0)) / 3.0).astype(np.int32))
+    q = np.ascontiguousarray(np.linspace(0.0, 0.5, 120))
+
+    def run(shard, n):
+        plan = C.c_void_p()
+        engine.check(N.lib.crab_pair_plan_create_lattice_shard(
+            engine.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D), t.ctypes.data_as(N.I32P), len(w), T,
+            q.ctypes.data_as(N.D), len(q), cells.ctypes.data_as(N.I32P), len(sites), 3.0, shard, n, C.byref(plan)))
+        try:
+            engine.check(N.lib.crab_pair_plan_run(engine.handle, plan, 1, 0, None))
+            out = np.empty((T * (T + 1) // 2, len(q)))
+            self_ = np.empty(T)
+            engine.check(N.lib.crab_pair_plan_read(engine.handle, plan, out.ctypes.data_as(N.D),
+                                                   self_.ctypes.data_as(N.D)))
+            return out, self_
+        finally:
+            N.lib.crab_pair_plan_destroy(plan)
+
+    whole, whole_self = run(0, 1)
+    for n in (2, 3, 8):
+        parts = [run(k, n) for k in range(n)]
+        assert _close(sum(p[0] for p in parts), whole), n
+        assert np.array_equal(parts[0][1], whole_self) and all(not p[1].any() for p in parts[1:])
+    bad = C.c_void_p()
+    assert N.lib.crab_pair_plan_create_lattice_shard(engine.handle, xyz.ctypes.data_as(N.D), w.ctypes.data_as(N.D),
+                                                     t.ctypes.data_as(N.I32P), len(w), T, q.ctypes.data_as(N.D),
+                                                     len(q), cells.ctypes.data_as(N.I32P), len(sites), 3.0, 2, 2,
+                                                     C.byref(bad)) == N.EINVAL
+
+
 def test_more_shards_than_work_items(engine):
     """90 atoms: one tile per atom type (at most 4) and one q block, so at
     most 10 tile-pair work items; the other shards return zeros and the sum is
