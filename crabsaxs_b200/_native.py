@@ -103,6 +103,7 @@ _SIGS = {
     "crab_ctx_workspace_bytes": (C.c_int, [P, C.POINTER(I64)]),
     "crab_ctx_set_wait_budget": (C.c_int, [P, I64]),
     "crab_ctx_fail_allocations": (C.c_int, [P, I64]),
+    "crab_ctx_set_device_sums": (C.c_int, [P, C.c_int32]),
     "crab_united_atom_group": (C.c_int, [C.c_char_p, C.c_char_p]),
     "crab_form_factor": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
     "crab_excluded_volume_for_atom": (C.c_double, [C.c_int, C.c_int, C.c_int]),

@@ -578,14 +578,18 @@ def solvent_corrected_intensity(structure, q, params: SolventParams, implicit_hy
 class _MomentSum:
     """crab_sum_fn around a Python function that sums a float64 array over
     the ranks in place; an exception inside it ends the library call and is
-    raised again after it returns."""
+    raised again after it returns.  With device=True the function receives
+    (device pointer as an int, count) instead of a host array."""
 
-    def __init__(self, fn):
+    def __init__(self, fn, device: bool = False):
         self.error = None
 
         def call(values, count, user):
             try:
-                fn(np.ctypeslib.as_array(values, shape=(count,)))
+                if device:
+                    fn(C.cast(values, C.c_void_p).value, int(count))
+                else:
+                    fn(np.ctypeslib.as_array(values, shape=(count,)))
                 return N.OK
             except BaseException as e:  # noqa: BLE001 - re-raised by check()
                 self.error = e
@@ -599,12 +603,30 @@ class _MomentSum:
         eng.check(rc)
 
 
+class _DeviceSums:
+    """crab_ctx_set_device_sums on for the duration of one call."""
+
+    def __init__(self, eng: "Engine", on: bool):
+        self.eng, self.on = eng, on
+
+    def __enter__(self):
+        if self.on:
+            self.eng.check(N.lib.crab_ctx_set_device_sums(self.eng.handle, 1))
+
+    def __exit__(self, *exc):
+        if self.on:
+            N.lib.crab_ctx_set_device_sums(self.eng.handle, 0)
+
+
 def multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: bool = True,
                         precision: int = N.PREC_TF32_SPLIT, engine: Optional[Engine] = None,
-                        shard: Optional[tuple[int, int]] = None, moment_sum=None) -> np.ndarray:
+                        shard: Optional[tuple[int, int]] = None, moment_sum=None,
+                        device_sums: bool = False) -> np.ndarray:
     """spherical.rs:266-403.  shard=(k, n) with moment_sum(array) (an in-place
     sum over the ranks): this rank's share of the atoms in the moments, the
-    whole curve returned (crab_multipole_intensity_shard)."""
+    whole curve returned (crab_multipole_intensity_shard).  device_sums=True:
+    moment_sum(device pointer, count) sums the moments in device memory
+    (crab_ctx_set_device_sums)."""
     eng = engine or Engine.default()
     qa = _f64(q)
     out = np.empty(len(qa))
@@ -612,19 +634,21 @@ def multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: 
         eng.check(N.lib.crab_multipole_intensity(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
                                                  1 if implicit_hydrogen else 0, precision, _dp(out)))
     else:
-        cb = _MomentSum(moment_sum or (lambda a: None))
-        cb.check(eng, N.lib.crab_multipole_intensity_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
-                                                           l_max, 1 if implicit_hydrogen else 0, precision,
-                                                           int(shard[0]), int(shard[1]), cb.c, None, _dp(out)))
+        cb = _MomentSum(moment_sum or (lambda *a: None), device=device_sums)
+        with _DeviceSums(eng, device_sums):
+            rc = N.lib.crab_multipole_intensity_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa), l_max,
+                                                      1 if implicit_hydrogen else 0, precision, int(shard[0]),
+                                                      int(shard[1]), cb.c, None, _dp(out))
+        cb.check(eng, rc)
     return out
 
 
 def multipole_solvent_basis(structure: Structure, q, l_max: int, params: SolventParams,
                             implicit_hydrogen: bool = True, precision: int = N.PREC_TF32_SPLIT,
                             engine: Optional[Engine] = None, shard: Optional[tuple[int, int]] = None,
-                            moment_sum=None) -> np.ndarray:
-    """spherical.rs:474-565.  shard / moment_sum as in multipole_intensity
-    (crab_multipole_solvent_basis_shard)."""
+                            moment_sum=None, device_sums: bool = False) -> np.ndarray:
+    """spherical.rs:474-565.  shard / moment_sum / device_sums as in
+    multipole_intensity (crab_multipole_solvent_basis_shard)."""
     eng = engine or Engine.default()
     qa = _f64(q)
     out = np.empty((6, len(qa)))
@@ -634,11 +658,13 @@ def multipole_solvent_basis(structure: Structure, q, l_max: int, params: Solvent
                                                      C.byref(s), 1 if implicit_hydrogen else 0, precision,
                                                      _dp(out)))
     else:
-        cb = _MomentSum(moment_sum or (lambda a: None))
-        cb.check(eng, N.lib.crab_multipole_solvent_basis_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
-                                                               l_max, C.byref(s), 1 if implicit_hydrogen else 0,
-                                                               precision, int(shard[0]), int(shard[1]), cb.c, None,
-                                                               _dp(out)))
+        cb = _MomentSum(moment_sum or (lambda *a: None), device=device_sums)
+        with _DeviceSums(eng, device_sums):
+            rc = N.lib.crab_multipole_solvent_basis_shard(eng.handle, structure.handle(eng), _dp(qa), len(qa),
+                                                          l_max, C.byref(s), 1 if implicit_hydrogen else 0,
+                                                          precision, int(shard[0]), int(shard[1]), cb.c, None,
+                                                          _dp(out))
+        cb.check(eng, rc)
     return out
 
 

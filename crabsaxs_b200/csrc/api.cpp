@@ -619,6 +619,11 @@ int crab_ctx_set_wait_budget(crab_ctx* ctx, int64_t iterations) {
   GUARD(ctx, { ctx->wait_budget = iterations < 0 ? -1 : (int)std::min<int64_t>(iterations, 1 << 30); });
 }
 
+int crab_ctx_set_device_sums(crab_ctx* ctx, int32_t on) {
+  if (!ctx) return CRAB_EINVAL;
+  GUARD(ctx, { ctx->device_sums = on != 0; });
+}
+
 int crab_ctx_fail_allocations(crab_ctx* ctx, int64_t after) {
   if (!ctx) return CRAB_EINVAL;
   GUARD(ctx, { ctx->fail_alloc_after = after < 0 ? -1 : after; });

@@ -107,6 +107,9 @@ struct crab_ctx {
   // CRAB_ENOMEM (-1: never).
   int wait_budget = -1;
   int64_t fail_alloc_after = -1;
+  // crab_ctx_set_device_sums: sharded multipole calls hand the sum callback
+  // the moments in device memory instead of a host copy
+  bool device_sums = false;
   // Called before every allocation the context makes: throws CRAB_ENOMEM
   // once the injected failure is due.
   void alloc_check();

@@ -1602,17 +1602,26 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
                                                                          fused ? d_perm : nullptr, d_M);
   CRAB_CUDA_CHECK(cudaEventRecord(ev[2], s));
   if (in.n_shards > 1) {
-    // every rank's moments summed by the caller (an all-reduce over the GPUs)
+    // every rank's moments summed by the caller (an all-reduce over the GPUs),
+    // in device memory (the context's buffer, stream synchronised first) or
+    // in a host copy
     const size_t m_count = (size_t)G * kMaxNodes * lm_pad;
-    auto* h_M = (double*)ctx->host("mp_M", sizeof(double) * m_count);
     int status = 0;
     if (gemm != kGemmSimt) copy_d2h(ctx, &status, d_status, sizeof(int), s);
-    copy_d2h(ctx, h_M, d_M, sizeof(double) * m_count, s);
-    CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
-    if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
-    const int rc = in.sum(h_M, (int64_t)m_count, in.sum_user);
-    if (rc != CRAB_OK) throw Error(rc, "the moment sum callback failed");
-    copy_h2d(ctx, d_M, h_M, sizeof(double) * m_count, s);
+    if (ctx->device_sums) {
+      CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
+      const int rc = in.sum(d_M, (int64_t)m_count, in.sum_user);
+      if (rc != CRAB_OK) throw Error(rc, "the moment sum callback failed");
+    } else {
+      auto* h_M = (double*)ctx->host("mp_M", sizeof(double) * m_count);
+      copy_d2h(ctx, h_M, d_M, sizeof(double) * m_count, s);
+      CRAB_CUDA_CHECK(cudaStreamSynchronize(s));
+      if (status != 0) throw Error(status, "multipole tensor-core GEMM: an mbarrier wait ran out");
+      const int rc = in.sum(h_M, (int64_t)m_count, in.sum_user);
+      if (rc != CRAB_OK) throw Error(rc, "the moment sum callback failed");
+      copy_h2d(ctx, d_M, h_M, sizeof(double) * m_count, s);
+    }
   }
   const int n_nodes = S * nb;
   const int64_t nbess = nq * n_nodes;

@@ -14,8 +14,8 @@ of the result, whose parts are zero where a rank did no work:
   2T f64, about 9 MB for 256 conformers at 300 q), after which every rank
   runs the same weight fit;
 - the multipole expansion: each rank's moments over its share of the atoms
-  (about 11 MB at 100k atoms and L = 50), after which every rank runs the q
-  pass.
+  (about 11 MB at 100k atoms and L = 50), summed in place in device memory
+  on an NCCL group, after which every rank runs the q pass.
 
 The reference runs on one host and has no counterpart; its loops over q and
 over conformers are split over threads (solvent.rs:528, ensemble.rs:244).
@@ -107,6 +107,80 @@ def _in_place_sum(group):
     return fn
 
 
+# DLPack description of a device buffer, so that torch can wrap the
+# library's moment buffer without a copy (torch.utils.dlpack.from_dlpack).
+class _DLDevice(C.Structure):
+    _fields_ = [("device_type", C.c_int), ("device_id", C.c_int)]
+
+
+class _DLDataType(C.Structure):
+    _fields_ = [("code", C.c_uint8), ("bits", C.c_uint8), ("lanes", C.c_uint16)]
+
+
+class _DLTensor(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("device", _DLDevice), ("ndim", C.c_int), ("dtype", _DLDataType),
+                ("shape", C.POINTER(C.c_int64)), ("strides", C.POINTER(C.c_int64)), ("byte_offset", C.c_uint64)]
+
+
+class _DLManagedTensor(C.Structure):
+    pass
+
+
+_DL_DELETER = C.CFUNCTYPE(None, C.POINTER(_DLManagedTensor))
+_DLManagedTensor._fields_ = [("dl_tensor", _DLTensor), ("manager_ctx", C.c_void_p), ("deleter", _DL_DELETER)]
+_DL_KEEP: dict[int, tuple] = {}
+
+
+@_DL_DELETER
+def _dl_delete(ptr):
+    _DL_KEEP.pop(C.addressof(ptr.contents), None)
+
+
+def device_array(ptr: int, count: int, device: int):
+    """A torch float64 tensor over `count` doubles of CUDA device memory at
+    `ptr` (no copy).  It views memory the library owns: use it only inside the
+    callback that received the pointer."""
+    import torch
+    from torch.utils.dlpack import from_dlpack
+
+    shape = (C.c_int64 * 1)(int(count))
+    m = _DLManagedTensor()
+    m.dl_tensor = _DLTensor(C.c_void_p(ptr), _DLDevice(2, int(device)), 1, _DLDataType(2, 64, 1), shape, None, 0)
+    m.manager_ctx = None
+    m.deleter = _dl_delete
+    _DL_KEEP[C.addressof(m)] = (m, shape)
+    pycapsule_new = C.pythonapi.PyCapsule_New
+    pycapsule_new.restype = C.py_object
+    pycapsule_new.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+    t = from_dlpack(pycapsule_new(C.addressof(m), b"dltensor", None))
+    assert t.device.type == "cuda" and t.dtype == torch.float64
+    return t
+
+
+def _device_sum(group, device: int):
+    """In-place all-reduce of the moments in device memory (NCCL)."""
+    def fn(ptr: int, count: int) -> None:
+        import torch
+        import torch.distributed as dist
+
+        t = device_array(ptr, count, device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        torch.cuda.current_stream(device).synchronize()  # the sum is complete before the library goes on
+
+    return fn
+
+
+def _moment_sum(group, engine: Optional[Engine]):
+    """(callback, device mode): device memory and an NCCL all-reduce in place
+    on an NCCL group, a host copy otherwise."""
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized() and dist.get_backend(group) == "nccl":
+        eng = engine or Engine.default()
+        return _device_sum(group, eng.device), True
+    return _in_place_sum(group), False
+
+
 def sharded_multipole_intensity(structure: Structure, q, l_max: int, implicit_hydrogen: bool = True,
                                 precision: int = N.PREC_TF32_SPLIT, group=None,
                                 engine: Optional[Engine] = None) -> np.ndarray:
@@ -114,8 +188,11 @@ def sharded_multipole_intensity(structure: Structure, q, l_max: int, implicit_hy
     cover its share of the atoms, one all-reduce of the moments (about 11 MB
     at 100k atoms and L = 50), then every rank runs the q pass."""
     rank, world = _rank_world(group)
+    if world == 1:
+        return multipole_intensity(structure, q, l_max, implicit_hydrogen, precision, engine)
+    fn, on_device = _moment_sum(group, engine)
     return multipole_intensity(structure, q, l_max, implicit_hydrogen, precision, engine, shard=(rank, world),
-                               moment_sum=_in_place_sum(group))
+                               moment_sum=fn, device_sums=on_device)
 
 
 def sharded_multipole_solvent_basis(structure: Structure, q, l_max: int, params: SolventParams,
@@ -124,5 +201,8 @@ def sharded_multipole_solvent_basis(structure: Structure, q, l_max: int, params:
     """multipole_solvent_basis over the ranks of ``group`` (as
     sharded_multipole_intensity)."""
     rank, world = _rank_world(group)
+    if world == 1:
+        return multipole_solvent_basis(structure, q, l_max, params, implicit_hydrogen, precision, engine)
+    fn, on_device = _moment_sum(group, engine)
     return multipole_solvent_basis(structure, q, l_max, params, implicit_hydrogen, precision, engine,
-                                   shard=(rank, world), moment_sum=_in_place_sum(group))
+                                   shard=(rank, world), moment_sum=fn, device_sums=on_device)

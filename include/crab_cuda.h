@@ -351,6 +351,13 @@ int crab_multipole_solvent_basis(crab_ctx* ctx, crab_struct* st, const double* q
  * their element-wise sum over all ranks (an all-reduce: NCCL, MPI, ...) and
  * return CRAB_OK; any other return ends the call with that status. */
 typedef int (*crab_sum_fn)(double* values, int64_t count, void* user);
+/* No counterpart in the reference.  on != 0: the sharded multipole calls of
+ * this context pass `sum` a pointer to the moments in DEVICE memory (the
+ * context's own buffer on its device, the context's stream synchronised
+ * before the call); the callback sums them in place over the ranks (an NCCL
+ * all-reduce, say) and returns once the sum is complete, with no copy
+ * through the host.  on == 0 (the default): a host copy. */
+int crab_ctx_set_device_sums(crab_ctx* ctx, int32_t on);
 /* Multi-GPU multipole (one process and context per GPU; no counterpart in
  * the reference, which splits its q loop over threads, spherical.rs:337-394).
  * Every rank passes the whole structure; rank `shard` of `n_shards` takes the
@@ -359,9 +366,9 @@ typedef int (*crab_sum_fn)(double* values, int64_t count, void* user);
  * come from all atoms, so every rank has the same moment layout).  `sum` is
  * called once, with this rank's moments in host memory
  * (types x segments x 64 x (L+1)^2 rounded up to 128, about 11 MB for 100k
- * atoms at L = 50); after it returns the rank runs the q pass, so every rank
- * returns the whole curve / basis.  n_shards == 1 needs no `sum` and is the
- * unsharded call. */
+ * atoms at L = 50), or in device memory after crab_ctx_set_device_sums;
+ * after it returns the rank runs the q pass, so every rank returns the whole
+ * curve / basis.  n_shards == 1 needs no `sum` and is the unsharded call. */
 int crab_multipole_intensity_shard(crab_ctx* ctx, crab_struct* st, const double* q, int64_t nq, int l_max,
                                    int implicit_hydrogen, int precision, int shard, int n_shards, crab_sum_fn sum,
                                    void* user, double* out);

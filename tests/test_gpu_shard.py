@@ -229,6 +229,47 @@ def test_multipole_moments_of_the_shards_sum_to_the_whole(engine, precision, rto
             assert np.max(np.abs(got - whole)) <= rtol * np.max(whole)
 
 
+@pytest.mark.parametrize("precision", [N.PREC_FP64, N.PREC_BF16_SPLIT])
+def test_multipole_moments_summed_in_device_memory(engine, precision):
+    """crab_ctx_set_device_sums: the callback gets the moments in device
+    memory (wrapped for torch without a copy by shard.device_array), sums
+    them in place, and the curves are those of the host-memory path."""
+    import torch
+
+    from crabsaxs_b200 import shard as S
+
+    s = synth.protein(38, 4000, 22.0)
+    q = np.linspace(0.001, 0.5, 100)
+
+    def call(**kw):
+        return cs.multipole_intensity(s, q, 30, precision=precision, engine=engine, **kw)
+
+    host_parts = _moments_of_every_shard(call, 2)
+    dev_parts = []
+    for k in range(2):
+        def grab(ptr, count):
+            dev_parts.append(S.device_array(ptr, count, engine.device).cpu().numpy())
+            raise _Stop()
+
+        with pytest.raises(_Stop):
+            call(shard=(k, 2), moment_sum=grab, device_sums=True)
+    for h, d in zip(host_parts, dev_parts):
+        assert np.array_equal(h, d)
+    total = torch.from_numpy(sum(host_parts)).to(f"cuda:{engine.device}")
+
+    def put(ptr, count):
+        S.device_array(ptr, count, engine.device).copy_(total)
+        torch.cuda.synchronize(engine.device)
+
+    host = _sharded_results(call, 2, sum(host_parts))
+    for k in range(2):
+        got = call(shard=(k, 2), moment_sum=put, device_sums=True)
+        assert np.array_equal(got, host[k])
+    # the option is per call: the next sharded call without it gets host memory again
+    again = _sharded_results(call, 2, sum(host_parts))
+    assert np.array_equal(again[0], host[0])
+
+
 def test_multipole_solvent_basis_shards_with_grid_sites(engine):
     """The hydration sites are part of the typed list the shards divide."""
     s = synth.protein(37, 3000, 20.0)
