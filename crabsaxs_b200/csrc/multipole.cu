@@ -388,7 +388,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (budget < 0) budget = dev::kSpinBudget;  // the context's default
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);  // S A terms, then S B terms
-  unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
+  // 1024-byte alignment as an offset into the shared array, so that pointers
+  // derived from it keep the shared state space (shared loads and stores,
+  // not generic ones)
+  unsigned char* smem = tc_smem + ((1024u - ((uint32_t)__cvta_generic_to_shared(tc_smem) & 1023u)) & 1023u);
   unsigned char* ring = smem + kTcSlots * slot_bytes + kTcBBytes;  // after a B-sized gap
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kTcRingBytes);
   uint64_t* full = bars;                      // [kTcSlots], one arrival per producer
@@ -892,7 +895,9 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
   static_assert(Slots == P, "one slot per producer warp");
   extern __shared__ __align__(1024) unsigned char fu_smem[];
   if (budget < 0) budget = dev::kWaitBudget;  // the context's default
-  unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)fu_smem + 1023) & ~(uintptr_t)1023);
+  // 1024-byte alignment as an offset into the shared array (pointers derived
+  // from it keep the shared state space)
+  unsigned char* smem = fu_smem + ((1024u - ((uint32_t)__cvta_generic_to_shared(fu_smem) & 1023u)) & 1023u);
   double* s_inv = reinterpret_cast<double*>(smem + Cfg::InvOff);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::BarOff);
   uint64_t* full = bars;                 // [Slots], the 32 lanes of the producing warp

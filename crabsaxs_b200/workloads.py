@@ -1,7 +1,8 @@
 """Named benchmark workloads, run a fixed number of times (for profilers).
 
     python -m crabsaxs_b200.workloads debye-20k [--variant V] [--repeats N]
-    python -m crabsaxs_b200.workloads multipole-100k [--precision fp32|fp64|tf32|tf32x2] [--repeats N]
+    python -m crabsaxs_b200.workloads multipole-100k [--precision fp32|fp64|tf32|tf32x2|tf32x2-fused|bf16|bf16x2]
+                                      [--repeats N]
     python -m crabsaxs_b200.workloads gradient-5k [--repeats N]
     python -m crabsaxs_b200.workloads pr-100k [--bins B] [--repeats N]
     python -m crabsaxs_b200.workloads grid-20k [--repeats N]
@@ -62,7 +63,8 @@ def debye_20k(engine: cs.Engine, variant: int | None, repeats: int) -> str:
 def multipole_100k(engine: cs.Engine, precision: str, repeats: int) -> str:
     w = synth.ATOMS_100K
     s = synth.protein(w.seed, w.n_atoms, w.radius)
-    prec = {"fp64": N.PREC_FP64, "fp32": N.PREC_FP32, "tf32": N.PREC_TF32, "tf32x2": N.PREC_TF32_SPLIT}[precision]
+    prec = {"fp64": N.PREC_FP64, "fp32": N.PREC_FP32, "tf32": N.PREC_TF32, "tf32x2": N.PREC_TF32_SPLIT,
+            "tf32x2-fused": N.PREC_TF32_SPLIT_FUSED, "bf16": N.PREC_BF16, "bf16x2": N.PREC_BF16_SPLIT}[precision]
     wall = []
     for _ in range(repeats):
         t0 = time.perf_counter()
@@ -121,7 +123,8 @@ def parser() -> argparse.ArgumentParser:
                     choices=["debye-20k", "multipole-100k", "gradient-5k", "pr-100k", "grid-20k"])
     ap.add_argument("--bins", type=int, default=160)
     ap.add_argument("--variant", type=int, default=None)
-    ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2"], default="tf32x2")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "tf32", "tf32x2", "tf32x2-fused", "bf16", "bf16x2"],
+                    default="tf32x2")
     ap.add_argument("--repeats", type=int, default=2)
     return ap
 
