@@ -1039,8 +1039,8 @@ void compute_partials(crab_ctx* ctx, Layout&& L, const double* q, int64_t nq, bo
   out.pair.assign((size_t)P->n_pairs * nq, 0.0);
   {
     TraceScope tr("pair_launch+fetch");
-    pair_plan_launch(ctx, *P, ctx->stream, !fp64);
-    pair_plan_fetch(ctx, *P, out.pair.data(), !fp64);
+    pair_plan_launch(ctx, *P, ctx->stream, true);
+    pair_plan_fetch(ctx, *P, out.pair.data(), true);
   }
   TraceScope td("pair_plan_free");
   P.reset();
