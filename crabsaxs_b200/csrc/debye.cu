@@ -51,6 +51,12 @@ constexpr int kDenser = 4;
 // q-packed with the weight folded into the recurrence state (pair_setup_pq_folded):
 // one chain at two CTAs per SM, two chains at two, one chain at three, one at four
 constexpr int kFolded1 = 5, kFolded2 = 6, kFolded1x3 = 7, kFolded1x4 = 3;
+// set-up and recurrences in separate warpgroups (k_pair_split), one or two
+// chains per recurrence thread
+constexpr int kSplit1 = 14, kSplit2 = 15;
+// the split with one recurrence warpgroup for each of three q blocks per item
+// (k_pair_split3)
+constexpr int kSplit3 = 12;
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
 template <int Q>
@@ -116,20 +122,23 @@ __device__ __forceinline__ void pair_setup(const float4& ai, const float4& aj, f
 // angle is at most 0.25 rad (wide == 0), else from the reduced seed.  Then:
 //   lane A: s = S,                   d = S - sin(q0 r - 2Δr) = 2 s1 cos(q0 r - Δr)
 //   lane B: s = sin(q0 r + Δr),      d = sin(q0 r + Δr) - sin(q0 r - Δr) = 2 s1 C.
-__device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj, float wj, const float4& qp, int wide,
-                                              unsigned long long& u2, unsigned long long& nl2,
-                                              unsigned long long& s2, unsigned long long& d2) {
+// The per-pair part: r and u = w_i w_j / r.
+__device__ __forceinline__ void pair_geom(const float4& ai, const float4& aj, float wj, float& r, float& u) {
   const float dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
   const float x = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-8f);
   const float y0 = rsqrtf(x);
   const float sq = x * y0;
   const float hy = 0.5f * y0;
-  const float r = fmaf(fmaf(-sq, sq, x), hy, sq);
+  r = fmaf(fmaf(-sq, sq, x), hy, sq);
   const float rinv = fmaf(fmaf(-sq, y0, 1.0f), hy, y0);
-  const float u = ai.w * wj * rinv;
+  u = ai.w * wj * rinv;
+}
+// The per-block part: seeds and step of the block qp at distance r.
+__device__ __forceinline__ void pair_seed_pq(float r, const float4& qp, int wide, float& nl, float& S, float& sB,
+                                             float& dA, float& dB) {
   const float phi = fmaf(qp.x, r, qp.y * r);
   const float g = 2.0f * fmaf(qp.z, r, qp.w * r);  // Δr
-  float S, C, s1, c1;
+  float C, s1, c1;
   sincos_seed(phi, &S, &C);
   if (wide) {
     sincos_seed(g, &s1, &c1);
@@ -143,10 +152,17 @@ __device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj
     pc = fmaf(g2, pc, -0.5f);
     c1 = fmaf(g2, pc, 1.0f);
   }
-  const float sB = fmaf(S, c1, C * s1);
-  const float dA = 2.0f * s1 * fmaf(C, c1, S * s1);
-  const float dB = 2.0f * s1 * C;
-  const float nl = -4.0f * s1 * s1;
+  sB = fmaf(S, c1, C * s1);
+  dA = 2.0f * s1 * fmaf(C, c1, S * s1);
+  dB = 2.0f * s1 * C;
+  nl = -4.0f * s1 * s1;
+}
+__device__ __forceinline__ void pair_setup_pq(const float4& ai, const float4& aj, float wj, const float4& qp, int wide,
+                                              unsigned long long& u2, unsigned long long& nl2,
+                                              unsigned long long& s2, unsigned long long& d2) {
+  float r, u, nl, S, sB, dA, dB;
+  pair_geom(ai, aj, wj, r, u);
+  pair_seed_pq(r, qp, wide, nl, S, sB, dA, dB);
   u2 = pack2(u, u);
   nl2 = pack2(nl, nl);
   s2 = pack2(S, sB);
@@ -425,6 +441,431 @@ __global__ void __launch_bounds__(kThreads, OCC)
   }
 }
 
+// ---- set-up / recurrence split ---------------------------------------------
+// One warpgroup (threads 0-127, one i atom each) computes the folded
+// recurrence state (s', d', λ') of every pair of a chunk of kSpJ j atoms into
+// a ring of shared-memory stages; two warpgroups (threads 128-383) run only
+// the recurrences, each thread one i atom and every other j of the chunk.  The
+// set-up work is that of k_pair_fp32_pq, but it leaves the recurrence warps'
+// instruction streams: with two recurrence warps and one set-up warp per
+// scheduler the FP32 pipe stays fed while a set-up chain waits on its latency.
+// Each chunk carries a header {item, j tile, chunk, sequence number}.  The
+// recurrence warps take every decision (new item, type change, end) from it,
+// per warp, so no barrier spans recurrence warps and a wait that runs out
+// (status CRAB_ETIMEOUT) cannot leave another warp waiting: a thread whose wait
+// gave up stops waiting, a recurrence warp leaves at the first header whose
+// sequence number is not the one it expects, and the set-up warps finish the
+// work list.  Nothing is copied asynchronously, so nothing is in flight when a
+// CTA leaves.
+constexpr int kSpJ = 16;               // j atoms per chunk
+constexpr int kSpStages = 4;           // chunks in the ring
+constexpr int kSpThreads = 3 * kTile;  // set-up warpgroup + two recurrence warpgroups
+struct SpSmem {
+  static constexpr int kSd = 0;                                    // ulonglong2 [stage][jj][i]: (s', d')
+  static constexpr int kNl = kSd + kSpStages * kSpJ * kTile * 16;  // u64 [stage][jj][i]: λ'
+  static constexpr int kSj = kNl + kSpStages * kSpJ * kTile * 8;   // float4 [2][kTile]: j tiles
+  static constexpr int kHdr = kSj + 2 * kTile * 16;                // int4 [stage]
+  static constexpr int kBar = kHdr + kSpStages * 16;               // u64 full[stage], empty[stage]
+  static constexpr int kItem = kBar + 2 * kSpStages * 8;           // int: the set-up warps' next item
+  static constexpr int kBytes = kItem + 16;
+};
+static_assert(kTile % kSpJ == 0 && kSpJ % 4 == 0, "chunks tile the j tile; two warpgroups take alternate j");
+
+__device__ __forceinline__ void sp_arrive(uint64_t* bar) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+// Barrier 1 among the 128 set-up threads only.
+__device__ __forceinline__ void sp_setup_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTile) : "memory"); }
+
+// A bounded wait that gives up once per thread: after the first wait that
+// runs out the thread records CRAB_ETIMEOUT and waits no more.
+__device__ __forceinline__ void sp_wait(uint64_t* bar, unsigned parity, int budget, bool& ok, int* status) {
+  if (!ok) return;
+  if (!mbar_wait(bar, parity, budget)) {
+    ok = false;
+    atomicExch(status, CRAB_ETIMEOUT);
+  }
+}
+
+// Warp sum of N = Q/2 packed accumulators by recursive halving: at offset o a
+// lane keeps the half of its values that its lane bit o selects and adds the
+// partner's copy of that half, so after five steps lane L holds the sums of
+// packed values [L·P/32, (L+1)·P/32) (P = N rounded up to a multiple of 32):
+// 31·P/32 packed shuffles and adds instead of 5·N.  Every lane then adds its
+// own q points into the f64 partials.  Resets the accumulators.
+template <int Q>
+__device__ __forceinline__ void flush_split(unsigned long long (&acc2)[Q / 2], int ab, int qstart, int qcount,
+                                            int nq, double* __restrict__ partials) {
+  constexpr int N = Q / 2;
+  constexpr int P = (N + 31) / 32 * 32;
+  const int lane = threadIdx.x & 31;
+  unsigned long long v[P / 2];
+  {
+    const bool upper = (lane & 16) != 0;
+#pragma unroll
+    for (int m = 0; m < P / 2; ++m) {
+      const unsigned long long lo = m < N ? acc2[m] : 0ull;
+      const unsigned long long hi = m + P / 2 < N ? acc2[m + P / 2] : 0ull;
+      const unsigned long long got = __shfl_xor_sync(0xffffffffu, upper ? lo : hi, 16);
+      asm("add.rn.f32x2 %0, %1, %2;" : "=l"(v[m]) : "l"(upper ? hi : lo), "l"(got));
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < N; ++m) acc2[m] = 0ull;
+#pragma unroll
+  for (int st = 1; st < 5; ++st) {
+    const int o = 16 >> st;
+    const int half = P >> (st + 1);
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int m = 0; m < half; ++m) {
+      const unsigned long long got = __shfl_xor_sync(0xffffffffu, upper ? v[m] : v[m + half], o);
+      asm("add.rn.f32x2 %0, %1, %2;" : "=l"(v[m]) : "l"(upper ? v[m + half] : v[m]), "l"(got));
+    }
+  }
+  constexpr int per = P / 32;
+#pragma unroll
+  for (int m = 0; m < per; ++m) {
+    const int k = 2 * (lane * per + m);
+    float a, b;
+    unpack2(v[m], a, b);
+    if (k < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k], (double)a);
+    if (k + 1 < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k + 1], (double)b);
+  }
+}
+
+template <int Q, int JB>
+__global__ void __launch_bounds__(kSpThreads, 1)
+    k_pair_split(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
+                 int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
+                 int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
+                 const int64_t* __restrict__ work_out, int budget) {
+  static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
+  static_assert(kSpJ % (2 * JB) == 0, "each warpgroup takes JB of its j atoms per step");
+  extern __shared__ __align__(16) unsigned char sp_smem[];
+  ulonglong2* sd = (ulonglong2*)(sp_smem + SpSmem::kSd);
+  unsigned long long* nlb = (unsigned long long*)(sp_smem + SpSmem::kNl);
+  float4* sj = (float4*)(sp_smem + SpSmem::kSj);
+  int4* hdr = (int4*)(sp_smem + SpSmem::kHdr);
+  uint64_t* full = (uint64_t*)(sp_smem + SpSmem::kBar);
+  uint64_t* empty = full + kSpStages;
+  int* s_item = (int*)(sp_smem + SpSmem::kItem);
+  const int tid = threadIdx.x;
+  if (tid < kSpStages) {
+    mbar_init(&full[tid], kTile);
+    mbar_init(&empty[tid], 2 * kTile);
+    hdr[tid] = make_int4(-1, -1, -1, -1);
+  }
+  if (tid == 0) fence_mbar_init();
+  __syncthreads();
+  if (budget < 0) budget = kWaitBudget;  // the context's default
+  bool ok = true;
+
+  if (tid < kTile) {
+    // ---- set-up warpgroup: thread i = tid ----
+    int n = 0, buf = 0;
+    for (;;) {
+      if (tid == 0) *s_item = atomicAdd(next_work, 1);
+      sp_setup_sync();
+      const int w = *s_item;  // thread 0 writes it again only after the tile barrier below
+      if (w >= n_work) {
+        const int stage = n % kSpStages;
+        sp_wait(&empty[stage], ((n / kSpStages) & 1) ^ 1, budget, ok, status);
+        if (tid == 0) hdr[stage] = make_int4(-1, 0, 0, n);
+        sp_arrive(&full[stage]);
+        break;
+      }
+      const int4 wk = work[w];
+      const int it = wk.x, jt0 = wk.y, jt1 = wk.z;
+      const float4 ai = atoms[(size_t)it * kTile + tid];
+      const float4 qp = qpar[wk.w];
+      float4 v = atoms[(size_t)jt0 * kTile + tid];
+      for (int jt = jt0; jt < jt1; ++jt) {
+        sj[buf * kTile + tid] = v;
+        sp_setup_sync();  // the tile is in place; every reader of this buffer's previous tile is past it
+        if (jt + 1 < jt1) v = atoms[(size_t)(jt + 1) * kTile + tid];
+        const bool diag = (jt == it);
+        const float4* tj = sj + buf * kTile;
+#pragma unroll 1
+        for (int c = 0; c < kTile / kSpJ; ++c, ++n) {
+          const int stage = n % kSpStages;
+          sp_wait(&empty[stage], ((n / kSpStages) & 1) ^ 1, budget, ok, status);
+          ulonglong2* sdo = sd + (size_t)stage * kSpJ * kTile + tid;
+          unsigned long long* nlo = nlb + (size_t)stage * kSpJ * kTile + tid;
+#pragma unroll 4
+          for (int jj = 0; jj < kSpJ; ++jj) {
+            const int j = c * kSpJ + jj;
+            const float4 aj = tj[j];
+            const float wj = (diag && j <= tid) ? 0.0f : aj.w;
+            unsigned long long nl2, s2, d2;
+            pair_setup_pq_folded(ai, aj, wj, qp, wide >= 1, nl2, s2, d2);
+            sdo[jj * kTile] = make_ulonglong2(s2, d2);
+            nlo[jj * kTile] = nl2;
+          }
+          if (tid == 0) hdr[stage] = make_int4(w, jt, c, n);
+          sp_arrive(&full[stage]);
+        }
+        buf ^= 1;
+      }
+    }
+    return;
+  }
+
+  // ---- recurrence warpgroups: thread i = (tid - 128) % 128, j parity g ----
+  const int r = tid - kTile, g = r / kTile, i = r % kTile;
+  unsigned long long acc2[Q / 2];
+#pragma unroll
+  for (int m = 0; m < Q / 2; ++m) acc2[m] = 0ull;
+  int cur_w = -1, ti = 0, cur = 0, jlo = 0, jhi = 0;
+  int2 qr = make_int2(0, 0);
+  double* __restrict__ out = partials;
+  for (int n = 0;; ++n) {
+    const int stage = n % kSpStages;
+    sp_wait(&full[stage], (n / kSpStages) & 1, budget, ok, status);
+    int4 h = hdr[stage];
+    h.x = __shfl_sync(0xffffffffu, h.x, 0);
+    h.y = __shfl_sync(0xffffffffu, h.y, 0);
+    h.z = __shfl_sync(0xffffffffu, h.z, 0);
+    h.w = __shfl_sync(0xffffffffu, h.w, 0);
+    if (h.w != n || h.x < 0 || h.x >= n_work) break;  // the end, or a ring that a failed wait left behind
+    if (h.x != cur_w) {
+      if (cur_w >= 0) {
+        const int a = min(ti, cur), b = max(ti, cur);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+      }
+      const int4 wk = work[h.x];
+      cur_w = h.x;
+      ti = tile_type[wk.x];
+      cur = tile_type[wk.y];
+      jlo = wk.y;
+      jhi = wk.z;
+      qr = qrange[wk.w];
+      out = partials + (work_out ? work_out[h.x] : 0);
+    }
+    if (h.y < jlo || h.y >= jhi) break;
+    if (h.z == 0) {
+      const int tj = tile_type[h.y];
+      if (tj != cur) {
+        const int a = min(ti, cur), b = max(ti, cur);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        cur = tj;
+      }
+    }
+    const ulonglong2* sdi = sd + (size_t)stage * kSpJ * kTile + i;
+    const unsigned long long* nli = nlb + (size_t)stage * kSpJ * kTile + i;
+#pragma unroll 1
+    for (int jj = g; jj < kSpJ; jj += 2 * JB) {
+      unsigned long long s2[JB], d2[JB], nl2[JB];
+#pragma unroll
+      for (int c = 0; c < JB; ++c) {
+        const ulonglong2 x = sdi[(jj + 2 * c) * kTile];
+        s2[c] = x.x;
+        d2[c] = x.y;
+        nl2[c] = nli[(jj + 2 * c) * kTile];
+      }
+#pragma unroll
+      for (int m = 0; m < Q / 2; ++m) {
+#pragma unroll
+        for (int c = 0; c < JB; ++c) {
+          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc2[m]) : "l"(s2[c]));
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2[c]) : "l"(nl2[c]), "l"(s2[c]));
+          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2[c]) : "l"(d2[c]));
+        }
+      }
+    }
+    sp_arrive(&empty[stage]);
+  }
+  if (cur_w >= 0) {
+    const int a = min(ti, cur), b = max(ti, cur);
+    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+  }
+}
+
+// ---- set-up / recurrence split over three q blocks ------------------------
+// The same ring as k_pair_split, with one recurrence warpgroup per q block:
+// a work item covers kS3Blocks consecutive q blocks, the set-up warpgroup
+// computes each pair's distance and weight once and its seed for every block,
+// and recurrence warpgroup b runs block b of the item over every j of the
+// chunk.  512 threads leave 128 registers per thread, so 12 recurrence warps
+// per SM run blocks of up to about 100 q (three per scheduler where
+// k_pair_split has two).  A warpgroup whose block lies past the end of the q
+// grid consumes the chunks without computing.
+constexpr int kS3Blocks = 3;
+constexpr int kS3J = 8;        // j atoms per chunk
+constexpr int kS3Stages = 3;
+constexpr int kS3Threads = (1 + kS3Blocks) * kTile;
+struct S3Smem {
+  static constexpr int kSd = 0;  // ulonglong2 [stage][block][jj][i]: (s', d')
+  static constexpr int kNl = kSd + kS3Stages * kS3Blocks * kS3J * kTile * 16;  // float [stage][block][jj][i]: λ'
+  static constexpr int kSj = kNl + kS3Stages * kS3Blocks * kS3J * kTile * 4;  // float4 [2][kTile]
+  static constexpr int kHdr = kSj + 2 * kTile * 16;                           // int4 [stage]
+  static constexpr int kBar = kHdr + kS3Stages * 16;                          // u64 full[stage], empty[stage]
+  static constexpr int kItem = kBar + 2 * kS3Stages * 8;
+  static constexpr int kBytes = kItem + 16;
+};
+static_assert(kTile % kS3J == 0, "chunks tile the j tile");
+
+template <int Q>
+__global__ void __launch_bounds__(kS3Threads, 1)
+    k_pair_split3(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
+                  int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int n_qblocks,
+                  int nq, int T, int wide, double* __restrict__ partials, int* __restrict__ status,
+                  int* __restrict__ next_work, const int64_t* __restrict__ work_out, int budget) {
+  static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
+  extern __shared__ __align__(16) unsigned char s3_smem[];
+  ulonglong2* sd = (ulonglong2*)(s3_smem + S3Smem::kSd);
+  float* nlb = (float*)(s3_smem + S3Smem::kNl);
+  float4* sj = (float4*)(s3_smem + S3Smem::kSj);
+  int4* hdr = (int4*)(s3_smem + S3Smem::kHdr);
+  uint64_t* full = (uint64_t*)(s3_smem + S3Smem::kBar);
+  uint64_t* empty = full + kS3Stages;
+  int* s_item = (int*)(s3_smem + S3Smem::kItem);
+  constexpr int kStage = kS3Blocks * kS3J * kTile;  // states per stage
+  const int tid = threadIdx.x;
+  if (tid < kS3Stages) {
+    mbar_init(&full[tid], kTile);
+    mbar_init(&empty[tid], kS3Blocks * kTile);
+    hdr[tid] = make_int4(-1, -1, -1, -1);
+  }
+  if (tid == 0) fence_mbar_init();
+  __syncthreads();
+  if (budget < 0) budget = kWaitBudget;
+  bool ok = true;
+
+  if (tid < kTile) {
+    // ---- set-up warpgroup: thread i = tid ----
+    int n = 0, buf = 0;
+    for (;;) {
+      if (tid == 0) *s_item = atomicAdd(next_work, 1);
+      sp_setup_sync();
+      const int w = *s_item;
+      if (w >= n_work) {
+        const int stage = n % kS3Stages;
+        sp_wait(&empty[stage], ((n / kS3Stages) & 1) ^ 1, budget, ok, status);
+        if (tid == 0) hdr[stage] = make_int4(-1, 0, 0, n);
+        sp_arrive(&full[stage]);
+        break;
+      }
+      const int4 wk = work[w];
+      const int it = wk.x, jt0 = wk.y, jt1 = wk.z;
+      const int b0 = wk.w * kS3Blocks;
+      const int nb = min(kS3Blocks, n_qblocks - b0);
+      const float4 ai = atoms[(size_t)it * kTile + tid];
+      float4 qp[kS3Blocks];
+#pragma unroll
+      for (int b = 0; b < kS3Blocks; ++b) qp[b] = qpar[b0 + min(b, nb - 1)];
+      float4 v = atoms[(size_t)jt0 * kTile + tid];
+      for (int jt = jt0; jt < jt1; ++jt) {
+        sj[buf * kTile + tid] = v;
+        sp_setup_sync();
+        if (jt + 1 < jt1) v = atoms[(size_t)(jt + 1) * kTile + tid];
+        const bool diag = (jt == it);
+        const float4* tj = sj + buf * kTile;
+#pragma unroll 1
+        for (int c = 0; c < kTile / kS3J; ++c, ++n) {
+          const int stage = n % kS3Stages;
+          sp_wait(&empty[stage], ((n / kS3Stages) & 1) ^ 1, budget, ok, status);
+          ulonglong2* sdo = sd + (size_t)stage * kStage + tid;
+          float* nlo = nlb + (size_t)stage * kStage + tid;
+#pragma unroll 2
+          for (int jj = 0; jj < kS3J; ++jj) {
+            const int j = c * kS3J + jj;
+            const float4 aj = tj[j];
+            const float wj = (diag && j <= tid) ? 0.0f : aj.w;
+            float r, u;
+            pair_geom(ai, aj, wj, r, u);
+            const unsigned long long u2 = pack2(u, u);
+#pragma unroll
+            for (int b = 0; b < kS3Blocks; ++b) {
+              float nl, S, sB, dA, dB;
+              pair_seed_pq(r, qp[b], wide, nl, S, sB, dA, dB);
+              unsigned long long s2 = pack2(S, sB), d2 = pack2(dA, dB);
+              asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(u2));
+              asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(d2) : "l"(u2));
+              sdo[(b * kS3J + jj) * kTile] = make_ulonglong2(s2, d2);
+              nlo[(b * kS3J + jj) * kTile] = nl;
+            }
+          }
+          if (tid == 0) hdr[stage] = make_int4(w, jt, c, n);
+          sp_arrive(&full[stage]);
+        }
+        buf ^= 1;
+      }
+    }
+    return;
+  }
+
+  // ---- recurrence warpgroups: thread i = (tid - 128) % 128, q block b of the item ----
+  const int r = tid - kTile, blk = r / kTile, i = r % kTile;
+  unsigned long long acc2[Q / 2];
+#pragma unroll
+  for (int m = 0; m < Q / 2; ++m) acc2[m] = 0ull;
+  int cur_w = -1, ti = 0, cur = 0, jlo = 0, jhi = 0;
+  bool live = false;  // this warpgroup's block of the current item exists
+  int2 qr = make_int2(0, 0);
+  double* __restrict__ out = partials;
+  for (int n = 0;; ++n) {
+    const int stage = n % kS3Stages;
+    sp_wait(&full[stage], (n / kS3Stages) & 1, budget, ok, status);
+    int4 h = hdr[stage];
+    h.x = __shfl_sync(0xffffffffu, h.x, 0);
+    h.y = __shfl_sync(0xffffffffu, h.y, 0);
+    h.z = __shfl_sync(0xffffffffu, h.z, 0);
+    h.w = __shfl_sync(0xffffffffu, h.w, 0);
+    if (h.w != n || h.x < 0 || h.x >= n_work) break;
+    if (h.x != cur_w) {
+      if (live) {
+        const int a = min(ti, cur), b = max(ti, cur);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+      }
+      const int4 wk = work[h.x];
+      cur_w = h.x;
+      const int qb = wk.w * kS3Blocks + blk;
+      live = qb < n_qblocks;
+      ti = tile_type[wk.x];
+      cur = tile_type[wk.y];
+      jlo = wk.y;
+      jhi = wk.z;
+      qr = live ? qrange[qb] : make_int2(0, 0);
+      out = partials + (work_out ? work_out[h.x] : 0);
+    }
+    if (h.y < jlo || h.y >= jhi) break;
+    if (h.z == 0) {
+      const int tj = tile_type[h.y];
+      if (tj != cur) {
+        if (live) {
+          const int a = min(ti, cur), b = max(ti, cur);
+          flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        }
+        cur = tj;
+      }
+    }
+    if (live) {
+      const ulonglong2* sdi = sd + (size_t)stage * kStage + (size_t)blk * kS3J * kTile + i;
+      const float* nli = nlb + (size_t)stage * kStage + (size_t)blk * kS3J * kTile + i;
+#pragma unroll 1
+      for (int jj = 0; jj < kS3J; ++jj) {
+        const ulonglong2 x = sdi[jj * kTile];
+        unsigned long long s2 = x.x, d2 = x.y;
+        const float nl = nli[jj * kTile];
+        const unsigned long long nl2 = pack2(nl, nl);
+#pragma unroll
+        for (int m = 0; m < Q / 2; ++m) {
+          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc2[m]) : "l"(s2));
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d2) : "l"(nl2), "l"(s2));
+          asm("add.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(d2));
+        }
+      }
+    }
+    sp_arrive(&empty[stage]);
+  }
+  if (live) {
+    const int a = min(ti, cur), b = max(ti, cur);
+    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+  }
+}
+
 // FP64 reference: direct sinc per pair and q, QD q values per work item.
 constexpr int kQD = 8;
 __global__ void __launch_bounds__(kThreads)
@@ -547,6 +988,40 @@ void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, cons
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32_pq<Q, JB, OCC, FOLD><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
                                                         status, next_work, work_out, budget);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int Q, int JB>
+void launch_split(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
+                  const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
+                  int* next_work, const int64_t* work_out, int budget) {
+  static bool attr = false;  // one CTA per SM: the ring takes most of the shared memory
+  if (!attr) {
+    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pair_split<Q, JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SpSmem::kBytes));
+    attr = true;
+  }
+  const int grid = std::max(1, std::min(n_work, sm_count));
+  k_pair_split<Q, JB><<<grid, kSpThreads, SpSmem::kBytes, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T,
+                                                                    wide, partials, status, next_work, work_out,
+                                                                    budget);
+  CRAB_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int Q>
+void launch_split3(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
+                   int n_work, const float4* qpar, const int2* qrange, int n_qblocks, int nq, int T, int wide,
+                   double* partials, int* status, int* next_work, const int64_t* work_out, int budget) {
+  static bool attr = false;
+  if (!attr) {
+    CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pair_split3<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         S3Smem::kBytes));
+    attr = true;
+  }
+  const int grid = std::max(1, std::min(n_work, sm_count));
+  k_pair_split3<Q><<<grid, kS3Threads, S3Smem::kBytes, stream>>>(atoms, tt, work, n_work, qpar, qrange, n_qblocks,
+                                                                 nq, T, wide, partials, status, next_work, work_out,
+                                                                 budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -798,16 +1273,18 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   // whose step is 2h (1); otherwise both use short polynomials (0)
   const double hmax = max_half * (P.L.extent + 1.0);
   P.wide = hmax > 0.8 ? 2 : (hmax > 0.125 ? 1 : 0);
+  // work items name a q block, or for k_pair_split3 a group of kS3Blocks
+  const int item_blocks = jb == kSplit3 ? (P.n_qblocks + kS3Blocks - 1) / kS3Blocks : P.n_qblocks;
   std::vector<int4> work;
   if (P.segments.empty()) {
     // runs of up to 8 j tiles per item, shorter when that leaves fewer items
     // than about four per resident CTA (small structures)
-    const int64_t tile_pairs = (int64_t)P.L.n_tiles * (P.L.n_tiles + 1) / 2 * P.n_qblocks;
+    const int64_t tile_pairs = (int64_t)P.L.n_tiles * (P.L.n_tiles + 1) / 2 * item_blocks;
     const int run = (int)std::max<int64_t>(1, std::min<int64_t>(8, tile_pairs / (4 * 3 * (int64_t)ctx->sm_count)));
-    work = shard_work(make_work(P.L, P.n_qblocks, run, P.lattice_first_tile), P.shard, P.n_shards);
+    work = shard_work(make_work(P.L, item_blocks, run, P.lattice_first_tile), P.shard, P.n_shards);
   } else {
     std::vector<int64_t> out;
-    make_work_segments(P, P.n_qblocks, 8, work, out);
+    make_work_segments(P, item_blocks, 8, work, out);
     P.d_work_out = upload(ctx, P, P.qcfg, "work_out", out.data(), out.size(), ctx->stream);
   }
   P.n_work = (int)work.size();
@@ -969,6 +1446,26 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH_PQF(100, 1, 3, kFolded1x3)
     CRAB_LAUNCH_PQF(84, 1, 4, kFolded1x4)
 #undef CRAB_LAUNCH_PQF
+#define CRAB_LAUNCH_SPLIT(QQ, JJ, CODE)                                                                          \
+  if (P.Q == QQ && P.jb == CODE) {                                                                               \
+    launch_split<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
+                         T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget);              \
+    launched = true;                                                                                             \
+  }
+    CRAB_LAUNCH_SPLIT(126, 1, kSplit1)
+    CRAB_LAUNCH_SPLIT(126, 2, kSplit2)
+    CRAB_LAUNCH_SPLIT(100, 1, kSplit1)
+    CRAB_LAUNCH_SPLIT(100, 2, kSplit2)
+#undef CRAB_LAUNCH_SPLIT
+#define CRAB_LAUNCH_SPLIT3(QQ)                                                                                    \
+  if (P.Q == QQ && P.jb == kSplit3) {                                                                            \
+    launch_split3<QQ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange,       \
+                      P.n_qblocks, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget); \
+    launched = true;                                                                                             \
+  }
+    CRAB_LAUNCH_SPLIT3(84)
+    CRAB_LAUNCH_SPLIT3(100)
+#undef CRAB_LAUNCH_SPLIT3
     if (!launched) throw Error(CRAB_EINVAL, "unsupported q block");
   }
   ctx->launches += 1;
@@ -1110,7 +1607,9 @@ static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
                                      {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
                                      {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
-                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}};
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4},
+                                     {126, kSplit1}, {126, kSplit2}, {100, kSplit1}, {100, kSplit2},
+                                     {84, kSplit3}, {100, kSplit3}};
 
 bool pair_variant_known(int variant) {
   const int Q = variant / 16, jb = variant % 16;
@@ -1136,7 +1635,9 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
                                      {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
                                      {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
-                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}};
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4},
+                                     {126, kSplit1}, {126, kSplit2}, {100, kSplit1}, {100, kSplit2},
+                                     {84, kSplit3}, {100, kSplit3}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;
   float best_ms = -1.0f;
   cudaEvent_t a, b;

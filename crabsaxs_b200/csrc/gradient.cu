@@ -16,7 +16,7 @@
 //   ∂χ²/∂x_i = Σ_j occ_i occ_j h_ab(r_ij) (x_i - x_j),
 //   h_ab(r) = g_ab(r) / r = Σ_k α_ab,k q_k² F(q_k r),  F(x) = (cos x - sin x / x) / x²,
 // and F is smooth and even (F(0) = -1/3), so h_ab is a band-limited function
-// of r (bandwidth q_max).  k_grad_table evaluates it in f64 on a uniform grid
+// of r (bandwidth q_max).  k_grad_h evaluates it in f64 on a uniform grid
 // r_n = n δr, δr = 0.02 / q_max, up to the structure's largest pair distance;
 // the pair kernel interpolates it with the 4-point Lagrange cubic (error below
 // 4e-9 of max |h|, from (q_max δr)^4 × 0.0234), from one float4 of the four

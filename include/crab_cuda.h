@@ -248,8 +248,11 @@ int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int
  * registers hold two consecutive q points, with (JB-8) % 4 independent chains,
  * built for three CTAs per SM when JB >= 12; JB = 5, 6, 7, 3: the q-packed
  * kernel with the pair weight folded into the recurrence state, with 1, 2,
- * 1, 1 chains at 2, 2, 3, 4 CTAs per SM) and
- * keep the fastest.  *chosen = Q*16 + JB;
+ * 1, 1 chains at 2, 2, 3, 4 CTAs per SM; JB = 14, 15: the folded recurrence
+ * with the per-pair set-up in a warpgroup of its own that feeds two
+ * recurrence warpgroups through shared memory, 1 or 2 chains per thread, one
+ * CTA per SM; JB = 12: the same split with one recurrence warpgroup for each
+ * of three q blocks per work item) and keep the fastest.  *chosen = Q*16 + JB;
  * the first `capacity` variants and their times (ms) are written to
  * variants/ms (may be NULL), their count to *n_variants. */
 int crab_pair_plan_autotune(crab_ctx* ctx, crab_pair_plan* plan, int32_t* chosen, int32_t* variants, double* ms,

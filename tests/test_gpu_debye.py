@@ -310,7 +310,8 @@ ALL_VARIANTS = [8 * 16 + 2, 16 * 16 + 2, 32 * 16 + 2, 48 * 16 + 2, 64 * 16 + 2, 
                 64 * 16 + 4, 96 * 16 + 4, 64 * 16 + 10, 96 * 16 + 10, 128 * 16 + 9, 128 * 16 + 10, 128 * 16 + 13,
                 100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9, 168 * 16 + 9,
                 168 * 16 + 5, 150 * 16 + 5, 168 * 16 + 6, 150 * 16 + 6, 128 * 16 + 6, 126 * 16 + 7, 100 * 16 + 7,
-                84 * 16 + 3]
+                84 * 16 + 3, 126 * 16 + 14, 126 * 16 + 15, 100 * 16 + 14, 100 * 16 + 15,
+                84 * 16 + 12, 100 * 16 + 12]
 
 
 @pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "wide"])

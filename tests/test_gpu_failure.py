@@ -41,6 +41,24 @@ def test_pair_kernel_wait_runs_out_then_context_recovers(engine, fresh):
     assert np.array_equal(got, ref) or np.max(np.abs(got - ref) / ref) <= 1e-12
 
 
+@pytest.mark.parametrize("variant", [168 * 16 + 5, 126 * 16 + 13, 126 * 16 + 14, 126 * 16 + 15, 100 * 16 + 15,
+                                     84 * 16 + 12])
+def test_every_pair_kernel_family_wait_runs_out_then_recovers(engine, fresh, variant):
+    """The folded q-packed kernel, the three-CTA build and the set-up /
+    recurrence split: each gives up at its first wait, reports, and leaves the
+    context usable."""
+    s = synth.protein(307, 2500, 20.0)
+    ref = cs.debye_intensity(s, Q, engine=engine)
+    fresh.check(N.lib.crab_ctx_set_pair_variant(fresh.handle, variant))
+    fresh.set_wait_budget(0)
+    for _ in range(2):
+        with pytest.raises(Other, match="ETIMEOUT"):
+            cs.debye_intensity(s, Q, engine=fresh)
+    fresh.set_wait_budget(None)
+    got = cs.debye_intensity(s, Q, engine=fresh)
+    np.testing.assert_allclose(got, ref, rtol=2e-6)
+
+
 def test_solvent_basis_wait_runs_out_then_recovers(engine, fresh):
     s = synth.protein(302, 900, 15.0)
     p = cs.SolventParams(c1=1.02, c2=1.3, hydration_model=cs.HydrationModel.AdaptiveGrid)
