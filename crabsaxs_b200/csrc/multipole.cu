@@ -570,9 +570,10 @@ constexpr size_t tc_smem_bytes() {
 // P_{l-1}^m, P_l^m, cos m phi, sin m phi) carries from one 128-row lm tile
 // to the next.  A CTA owns a chunk of stages of one group and runs every lm
 // tile over it, tile-major; the walk state of its points waits in a device
-// array between tiles (40 bytes per point, L2-resident).  The values are the
-// ones k_mp_prep writes, bit for bit: the same f64 operations in the same
-// order, then the same rounding to the operand type.  k_mp_reduce maps rows
+// array between tiles (40 bytes per point, L2-resident).  In the TF32 modes the
+// values are the ones k_mp_prep writes, bit for bit: the same f64 operations
+// in the same order, then the same rounding to the operand type; the BF16
+// modes take each recurrence step as one fused multiply-add (fu_next_l).  k_mp_reduce maps rows
 // back to the l^2 + l + m order of the moments.
 //
 // Element types; both give 128-byte stage rows, so the swizzled layout, the
@@ -585,10 +586,11 @@ constexpr size_t tc_smem_bytes() {
 // already split and swizzled, one 8 KB block per (stage, term), and the
 // producer warp of a stage fetches its blocks with a 1D bulk copy.
 //
-// Roles: producer warps 0..P-1 (warp p takes the stages c = p mod P of
-// every tile into its own slot p, so a stage's walk state and a slot are
-// handled by one warp only), the MMA
-// issuer (warp P, lane 0) and 8 drain warps, which read each stage's FP32
+// Roles: producer warps 0..PW-1 (slot p takes the stages c = p mod P of
+// every tile; a TF32 slot has one producer warp, a BF16 slot two, warps p
+// and p + P, each walking half of the stage's points with one point per
+// lane, so a point's walk state is handled by one warp only), the MMA
+// issuer (warp PW, lane 0) and 8 drain warps, which read each stage's FP32
 // accumulator from TMEM into f64 registers (one stage per accumulator, as in
 // the staged kernel) and store the f64 tile of the chunk at the end of each
 // lm tile.  Every wait is bounded, and the role waits suspend the warp
@@ -596,21 +598,29 @@ constexpr size_t tc_smem_bytes() {
 // producers; a CTA that gives up drains its bulk copies and MMAs before it
 // frees TMEM and exits.
 constexpr int kFuDrainers = 256;
-template <int S>
+constexpr int kFuBatch = 4;  // recurrence steps a producer lane runs ahead of its row stores
+template <int E, int S>
 struct FuCfg {
-  static constexpr int P = S == 1 ? 6 : 4;  // producer warps, one slot each
+  // slots, and producer warps per slot: a BF16 stage (64 points) is walked by
+  // two warps, one point per lane each, so every scheduler runs two
+  // independent walks; a TF32 stage (32 points) by one
+  static constexpr int P = (E == 0 && S == 1) ? 6 : 4;
   static constexpr int Slots = P;
+  static constexpr int WPS = E == 1 ? 2 : 1;
+  static constexpr int PW = P * WPS;  // producer warps
   static constexpr int SlotBytes = S * (kTcABytes + kTcBBytes);
-  static constexpr int Threads = (P + 1) * 32 + kFuDrainers;
+  static constexpr int Threads = (PW + 1) * 32 + kFuDrainers;
   static constexpr int Bars = 3 * Slots + 2 * kTcAccs + 1;
   // slots, then per producer warp the normalisations of one tile's rows
   // (kGemmM doubles), the 1/k table (kMaxL + 2 doubles), the barriers
   static constexpr size_t NormOff = (size_t)Slots * SlotBytes;
-  static constexpr size_t InvOff = NormOff + (size_t)P * kGemmM * sizeof(double);
+  static constexpr size_t InvOff = NormOff + (size_t)PW * kGemmM * sizeof(double);
   static constexpr size_t BarOff = InvOff + (kMaxL + 2) * sizeof(double);
   static constexpr size_t Smem = 1024 + BarOff + sizeof(uint64_t) * Bars + 16;
 };
-static_assert(FuCfg<1>::Smem <= 232448 && FuCfg<2>::Smem <= 232448, "shared memory of the fused GEMM");
+static_assert(FuCfg<0, 1>::Smem <= 232448 && FuCfg<0, 2>::Smem <= 232448 && FuCfg<1, 1>::Smem <= 232448 &&
+                  FuCfg<1, 2>::Smem <= 232448,
+              "shared memory of the fused GEMM");
 
 template <int E>
 __host__ __device__ constexpr int fu_stage_points() { return E == 0 ? 32 : 64; }
@@ -651,9 +661,11 @@ __host__ __device__ __forceinline__ uint32_t fu_swz(int row, int k) {
 // the walk keeps P_m^m (pmm), P_{l-1}^m, P_l^m (prev, cur) and cos, sin (m phi);
 // the walk position (m, l, and whether the next row is the sin row of (l, m))
 // is the same for every point.  The f64 operations and their order are
-// k_mp_prep's, so the values are its values bit for bit.
+// k_mp_prep's (in the BF16 modes except the l step, fu_next_l), so the TF32
+// values are its values bit for bit.
 struct FuWalk {
   double pmm, prev, cur, cm, sm;
+  float cmf, smf;  // cos, sin (m phi) rounded to FP32 (the BF16 modes' rows)
 };
 // P_{m+1}^m = (x (2m+1)) P_m^m
 __device__ __forceinline__ void fu_first_l(int m, const double4& k4, FuWalk& w) {
@@ -662,11 +674,24 @@ __device__ __forceinline__ void fu_first_l(int m, const double4& k4, FuWalk& w) 
   w.cur = nxt;
 }
 // P_l^m = ((2l-1) x P_{l-1}^m - (l+m-1) P_{l-2}^m) / (l-m), with a = 2l-1,
-// b = l+m-1 and iv = 1/(l-m) given
+// b = l+m-1 and iv = 1/(l-m) given.  EXACT: k_mp_prep's operations in its
+// order (the TF32 modes, whose fused and staged curves are equal).  Otherwise
+// (the BF16 modes) the same recurrence as one fused multiply-add on the walk's
+// dependency chain, P_l = fma((a iv) x, P_{l-1}, -(b iv) P_{l-2}): the other
+// products do not wait on P_{l-1}, so a step costs one f64 latency instead of
+// three; its rounding differs from k_mp_prep's by about an ulp.
+template <bool EXACT = true>
 __device__ __forceinline__ void fu_next_l(double a, double b, double iv, const double4& k4, FuWalk& w) {
-  const double num = __dadd_rn(__dmul_rn(__dmul_rn(a, k4.x), w.cur), -__dmul_rn(b, w.prev));
-  w.prev = w.cur;
-  w.cur = __dmul_rn(num, iv);
+  if (EXACT) {
+    const double num = __dadd_rn(__dmul_rn(__dmul_rn(a, k4.x), w.cur), -__dmul_rn(b, w.prev));
+    w.prev = w.cur;
+    w.cur = __dmul_rn(num, iv);
+  } else {
+    const double ax = __dmul_rn(__dmul_rn(a, iv), k4.x), bp = __dmul_rn(__dmul_rn(b, iv), w.prev);
+    const double nxt = __fma_rn(ax, w.cur, -bp);
+    w.prev = w.cur;
+    w.cur = nxt;
+  }
 }
 // next m: P_m^m = P_{m-1}^{m-1} (-(2m-1) sin theta), (cos, sin)(m phi) rotated
 __device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
@@ -674,23 +699,30 @@ __device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
   const double next_cos = __dadd_rn(__dmul_rn(w.cm, k4.z), -__dmul_rn(w.sm, k4.w));
   w.sm = __dadd_rn(__dmul_rn(w.sm, k4.z), __dmul_rn(w.cm, k4.w));
   w.cm = next_cos;
+  w.cmf = (float)w.cm;
+  w.smf = (float)w.sm;
   w.cur = w.pmm;
   w.prev = 0.0;
 }
 
 // One row of the A tile: the S operand terms of this lane's PPT values at
-// row r of the slot (shared address sa_s).
+// row r of the slot, in columns col .. col + PPT - 1.
 // The slot (sa) and the tables the generator reads (srow, inv) are passed as
 // __restrict__ pointers: the compiler may then move the table loads of the
 // next rows above this row's stores, and the rows' dependency chains overlap.
 template <int E, int S, int PPT>
-__device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, int lane, const double (&v)[PPT]) {
-  const uint32_t off = fu_swz<E>(r, PPT * lane);
+__device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, int col, const double (&v)[PPT]) {
+  const uint32_t off = fu_swz<E>(r, col);
   if (E == 0) {
     const float f = (float)v[0];
     const float h = tf32_rna(f);
     *reinterpret_cast<float*>(sa + off) = h;
     if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - h);
+  } else if (PPT == 1) {
+    const float f = (float)v[0];
+    const uint16_t h = bf16_rn(f);
+    *reinterpret_cast<uint16_t*>(sa + off) = h;
+    if (S == 2) *reinterpret_cast<uint16_t*>(sa + kTcABytes + off) = bf16_rn(f - __uint_as_float((uint32_t)h << 16));
   } else {
     const float fa = (float)v[0], fb = (float)v[PPT - 1];
     const uint32_t h = bf16x2_rn(fa, fb);
@@ -701,26 +733,59 @@ __device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, i
 
 // The rows of (l, m): one row for m = 0 (norm P_l^0), else the cos and the
 // sin row (sqrt(2) norm P_l^m times cos / sin (m phi)); sn is the row's
-// normalisation.
+// normalisation and cur the points' P_l^m.
 template <int E, int S, int PPT>
-__device__ __forceinline__ void fu_emit_entry(unsigned char* __restrict__ sa, int r, int lane, int m, double sn,
-                                              const FuWalk (&w)[PPT]) {
+__device__ __forceinline__ void fu_emit_vals(unsigned char* __restrict__ sa, int r, int col, int m, double sn,
+                                             const double (&cur)[PPT], const FuWalk (&w)[PPT]) {
+  if (E == 1 && PPT == 1) {
+    // BF16, one point per lane: the entry's value rounded to FP32 once, the
+    // cos and sin rows as FP32 products, both rounded to BF16 (and their lo
+    // terms) by one packed conversion each (a few 1e-8 of relative rounding
+    // beyond the f64 products, far below the BF16 terms)
+    const float cf = (float)__dmul_rn(sn, cur[0]);
+    if (m == 0) {
+      const uint16_t h = bf16_rn(cf);
+      const uint32_t off = fu_swz<E>(r, col);
+      *reinterpret_cast<uint16_t*>(sa + off) = h;
+      if (S == 2) *reinterpret_cast<uint16_t*>(sa + kTcABytes + off) = bf16_rn(cf - __uint_as_float((uint32_t)h << 16));
+    } else {
+      const float c = cf * w[0].cmf, v = cf * w[0].smf;
+      const uint32_t h2 = bf16x2_rn(c, v);  // low half c, high half v
+      const uint32_t oc = fu_swz<E>(r, col), ov = fu_swz<E>(r + 1, col);
+      *reinterpret_cast<uint16_t*>(sa + oc) = (uint16_t)h2;
+      *reinterpret_cast<uint16_t*>(sa + ov) = (uint16_t)(h2 >> 16);
+      if (S == 2) {
+        const uint32_t l2 = bf16x2_rn(c - bf16_lo_f32(h2), v - bf16_hi_f32(h2));
+        *reinterpret_cast<uint16_t*>(sa + kTcABytes + oc) = (uint16_t)l2;
+        *reinterpret_cast<uint16_t*>(sa + kTcABytes + ov) = (uint16_t)(l2 >> 16);
+      }
+    }
+    return;
+  }
   double v[PPT];
   if (m == 0) {
 #pragma unroll
-    for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(sn, w[jj].cur);
-    fu_emit<E, S, PPT>(sa, r, lane, v);
+    for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(sn, cur[jj]);
+    fu_emit<E, S, PPT>(sa, r, col, v);
   } else {
     double c[PPT];
 #pragma unroll
     for (int jj = 0; jj < PPT; ++jj) {
-      const double vv = __dmul_rn(sn, w[jj].cur);
+      const double vv = __dmul_rn(sn, cur[jj]);
       c[jj] = __dmul_rn(vv, w[jj].cm);
       v[jj] = __dmul_rn(vv, w[jj].sm);
     }
-    fu_emit<E, S, PPT>(sa, r, lane, c);
-    fu_emit<E, S, PPT>(sa, r + 1, lane, v);
+    fu_emit<E, S, PPT>(sa, r, col, c);
+    fu_emit<E, S, PPT>(sa, r + 1, col, v);
   }
+}
+template <int E, int S, int PPT>
+__device__ __forceinline__ void fu_emit_entry(unsigned char* __restrict__ sa, int r, int col, int m, double sn,
+                                              const FuWalk (&w)[PPT]) {
+  double cur[PPT];
+#pragma unroll
+  for (int jj = 0; jj < PPT; ++jj) cur[jj] = w[jj].cur;
+  fu_emit_vals<E, S, PPT>(sa, r, col, m, sn, cur, w);
 }
 
 // The 128 rows of one lm tile for this lane's points, from the walk position
@@ -730,10 +795,16 @@ __device__ __forceinline__ void fu_emit_entry(unsigned char* __restrict__ sa, in
 // run = the l = m..L of one m); inside a run the steps are the same, so the
 // loop over them has no branches and consecutive rows overlap.
 template <int E, int S, int PPT>
-__device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int lane, int4 ts, int L,
+__device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int col, int4 ts, int L,
                                             const double4 (&k4)[PPT], FuWalk (&w)[PPT],
                                             const double* __restrict__ srow, const double* __restrict__ inv) {
   int m = ts.x, l = ts.y, half = ts.z, r = 0;
+  if (E == 1)
+#pragma unroll
+    for (int jj = 0; jj < PPT; ++jj) {
+      w[jj].cmf = (float)w[jj].cm;
+      w[jj].smf = (float)w[jj].sm;
+    }
   auto next_m = [&]() {
     ++m;
     if (m <= L) {
@@ -749,7 +820,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
 #pragma unroll
       for (int jj = 0; jj < PPT; ++jj) {
         if (l == m) fu_first_l(m, k4[jj], w[jj]);
-        else fu_next_l((double)(2 * l + 1), (double)(l + m), inv[l + 1 - m], k4[jj], w[jj]);
+        else fu_next_l<E == 0>((double)(2 * l + 1), (double)(l + m), inv[l + 1 - m], k4[jj], w[jj]);
       }
       ++l;
     }
@@ -757,15 +828,17 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
   while (r < kGemmM) {
     if (m > L) {  // padding rows past the last harmonic
       const double z[PPT] = {};
-      for (; r < kGemmM; ++r) fu_emit<E, S, PPT>(sa, r, lane, z);
+      for (; r < kGemmM; ++r) fu_emit<E, S, PPT>(sa, r, col, z);
       break;
     }
     const double sn = srow[r];
     if (half) {  // the sin row of (l, m) opens the tile
       double v[PPT];
 #pragma unroll
-      for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].sm);
-      fu_emit<E, S, PPT>(sa, r++, lane, v);
+      for (int jj = 0; jj < PPT; ++jj)
+        v[jj] = E == 1 ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].smf)  // as fu_emit_vals
+                       : __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].sm);
+      fu_emit<E, S, PPT>(sa, r++, col, v);
       half = 0;
       step_from();
       continue;
@@ -774,31 +847,56 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
     if (r + per > kGemmM) {  // one row left: the cos row of (l, m); its sin row opens the next tile
       double v[PPT];
 #pragma unroll
-      for (int jj = 0; jj < PPT; ++jj) v[jj] = __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].cm);
-      fu_emit<E, S, PPT>(sa, r++, lane, v);
+      for (int jj = 0; jj < PPT; ++jj)
+        v[jj] = E == 1 ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].cmf)
+                       : __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].cm);
+      fu_emit<E, S, PPT>(sa, r++, col, v);
       break;
     }
     const int n = min(L - l + 1, (kGemmM - r) / per);  // entries of this run in this tile (>= 1)
-    fu_emit_entry<E, S, PPT>(sa, r, lane, m, sn, w);
+    fu_emit_entry<E, S, PPT>(sa, r, col, m, sn, w);
     r += per;
     step_from();
     if (m > L || l == m) continue;  // the run ended with its first entry
     // entries 2..n: every one but a run-closing (L, m) steps with the same form
     const int rest = n - 1, steady = min(rest, L - l);
     double a = (double)(2 * l + 1), b = (double)(l + m);  // coefficients of the step from l to l+1
-#pragma unroll 4
-    for (int k = 0; k < steady; ++k) {
-      fu_emit_entry<E, S, PPT>(sa, r, lane, m, srow[r], w);
+    // in batches of kFuBatch entries: the batch's recurrence steps first (the
+    // one dependent chain; each entry's P_l^m is kept), then its entries' rows,
+    // which depend on nothing but those values, so a warp's in-order issue
+    // overlaps their latencies with one another and with the chain
+    int k = 0;
+    for (; k + kFuBatch <= steady; k += kFuBatch) {
+      double cv[kFuBatch][PPT];
+#pragma unroll
+      for (int u = 0; u < kFuBatch; ++u) {
+        const double iv = inv[l + 1 - m];
+#pragma unroll
+        for (int jj = 0; jj < PPT; ++jj) {
+          cv[u][jj] = w[jj].cur;
+          fu_next_l<E == 0>(a, b, iv, k4[jj], w[jj]);
+        }
+        a += 2.0;
+        b += 1.0;
+        ++l;
+      }
+#pragma unroll
+      for (int u = 0; u < kFuBatch; ++u) fu_emit_vals<E, S, PPT>(sa, r + u * per, col, m, srow[r + u * per], cv[u], w);
+      r += kFuBatch * per;
+    }
+#pragma unroll 1
+    for (; k < steady; ++k) {
+      fu_emit_entry<E, S, PPT>(sa, r, col, m, srow[r], w);
       r += per;
       const double iv = inv[l + 1 - m];
 #pragma unroll
-      for (int jj = 0; jj < PPT; ++jj) fu_next_l(a, b, iv, k4[jj], w[jj]);
+      for (int jj = 0; jj < PPT; ++jj) fu_next_l<E == 0>(a, b, iv, k4[jj], w[jj]);
       a += 2.0;
       b += 1.0;
       ++l;
     }
     if (rest > steady) {  // (L, m) closes the run inside this tile
-      fu_emit_entry<E, S, PPT>(sa, r, lane, m, srow[r], w);
+      fu_emit_entry<E, S, PPT>(sa, r, col, m, srow[r], w);
       r += per;
       next_m();
     }
@@ -885,13 +983,13 @@ __global__ void k_mp_prep_fused(const double* __restrict__ pts, const int32_t* _
 
 // Work item of the fused GEMM: (group, first stage, stage count, unused).
 template <int E, int S>
-__global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
+__global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
     k_mp_moments_fused(const double4* __restrict__ cst, const unsigned char* __restrict__ Bimg,
                        const int4* __restrict__ work, const int4* __restrict__ tstart, int n_lmt, int L,
                        const double* __restrict__ snorm_rows, const double* __restrict__ inv, FuState state,
                        double* __restrict__ part, int* __restrict__ status, int budget) {
-  using Cfg = FuCfg<S>;
-  constexpr int P = Cfg::P, Slots = Cfg::Slots, KS = fu_stage_points<E>();
+  using Cfg = FuCfg<E, S>;
+  constexpr int P = Cfg::P, Slots = Cfg::Slots, PW = Cfg::PW, WPS = Cfg::WPS, KS = fu_stage_points<E>();
   static_assert(Slots == P, "one slot per producer warp");
   extern __shared__ __align__(1024) unsigned char fu_smem[];
   if (budget < 0) budget = dev::kWaitBudget;  // the context's default
@@ -919,7 +1017,7 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
   }
   if (tid == 0) {
     for (int d = 0; d < Slots; ++d) {
-      dev::mbar_init(&full[d], 32);
+      dev::mbar_init(&full[d], 32 * WPS);
       dev::mbar_init(&bfull[d], 1);
       dev::mbar_init(&empty[d], 1);
     }
@@ -939,13 +1037,16 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
   bool ok = true;
   auto failed = [&]() { return *((volatile int*)&s_fail) != 0; };
 
-  if (warp < P) {
+  if (warp < PW) {
     // ---------------- producers
-    // this warp's stages: c = warp + k P of every tile, item j = t * n_mine + k,
-    // which is also the use index of its slot
-    constexpr int PPT = E == 0 ? 1 : 2;  // points per lane
-    const int n_mine = nc > warp ? (nc - warp + P - 1) / P : 0, total = n_mine * n_lmt;
-    unsigned char* sa = smem + (size_t)warp * Cfg::SlotBytes;
+    // slot d = warp mod P, half h of its stage's points; this warp's stages:
+    // c = d + k P of every tile, item j = t * n_mine + k, which is also the
+    // use index of its slot
+    constexpr int PPT = (E == 0 || WPS == 2) ? 1 : 2;  // points per lane
+    const int d = warp % P, h = warp / P;
+    const int col = WPS == 2 ? h * 32 + lane : PPT * lane;  // this lane's first point in the stage
+    const int n_mine = nc > d ? (nc - d + P - 1) / P : 0, total = n_mine * n_lmt;
+    unsigned char* sa = smem + (size_t)d * Cfg::SlotBytes;
     unsigned char* sb = sa + S * kTcABytes;
     double* srow = reinterpret_cast<double*>(smem + Cfg::NormOff) + (size_t)warp * kGemmM;
     double nrm[kGemmM / 32];  // this lane's share of the next tile's row normalisations
@@ -960,21 +1061,21 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
     if (total > 0)
 #pragma unroll
       for (int jj = 0; jj < PPT; ++jj) {
-        k4[jj] = cst[(int64_t)(wk.y + warp) * KS + PPT * lane + jj];
-        wv[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0};
+        k4[jj] = cst[(int64_t)(wk.y + d) * KS + col + jj];
+        wv[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0, 1.0f, 0.0f};
       }
     for (int j = 0; j < total; ++j) {
-      const int t = j / n_mine, c = warp + (j % n_mine) * P;
-      if (j > 0 && (failed() || !dev::mbar_wait(&empty[warp], (unsigned)((j - 1) & 1), budget))) {
+      const int t = j / n_mine, c = d + (j % n_mine) * P;
+      if (j > 0 && (failed() || !dev::mbar_wait(&empty[d], (unsigned)((j - 1) & 1), budget))) {
         ok = false;
         break;
       }
-      if (lane == 0) {
-        dev::mbar_expect_tx(&bfull[warp], S * kTcBBytes);
+      if (lane == 0 && h == 0) {
+        dev::mbar_expect_tx(&bfull[d], S * kTcBBytes);
 #pragma unroll
         for (int p = 0; p < S; ++p)
           dev::bulk_g2s(sb + p * kTcBBytes, Bimg + ((size_t)(wk.y + c) * S + p) * kTcBBytes, kTcBBytes,
-                        &bfull[warp]);
+                        &bfull[d]);
         issued = true;
         issued_ph = (unsigned)(j & 1);
       }
@@ -987,7 +1088,7 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
 #pragma unroll
           for (int i = 0; i < kGemmM / 32; ++i) nrm[i] = snorm_rows[(size_t)(t + 1) * kGemmM + lane + 32 * i];
       }
-      const int64_t p0 = (int64_t)(wk.y + c) * KS + PPT * lane;
+      const int64_t p0 = (int64_t)(wk.y + c) * KS + col;
       // prefetch the next item's constants and walk state (a stage of this
       // warp whose state was stored an item or more ago); with one stage per
       // tile the state simply stays in registers
@@ -995,21 +1096,21 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
       double4 k4n[PPT];
       FuWalk wn[PPT];
       if (has_next && !same) {
-        const int tn = (j + 1) / n_mine, cn = warp + ((j + 1) % n_mine) * P;
-        const int64_t pn = (int64_t)(wk.y + cn) * KS + PPT * lane;
+        const int tn = (j + 1) / n_mine, cn = d + ((j + 1) % n_mine) * P;
+        const int64_t pn = (int64_t)(wk.y + cn) * KS + col;
 #pragma unroll
         for (int jj = 0; jj < PPT; ++jj) {
           k4n[jj] = cst[pn + jj];
-          if (tn == 0) wn[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0};
+          if (tn == 0) wn[jj] = FuWalk{1.0, 0.0, 1.0, 1.0, 0.0, 1.0f, 0.0f};
           else fu_load(state, pn + jj, wn[jj]);
         }
       }
-      fu_generate<E, S, PPT>(sa, lane, tstart[t], L, k4, wv, srow, s_inv);
+      fu_generate<E, S, PPT>(sa, col, tstart[t], L, k4, wv, srow, s_inv);
       if (has_next && !same && t + 1 < n_lmt)
 #pragma unroll
         for (int jj = 0; jj < PPT; ++jj) fu_store(state, p0 + jj, wv[jj]);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&full[warp]);
+      mbar_arrive(&full[d]);
       if (has_next && !same)
 #pragma unroll
         for (int jj = 0; jj < PPT; ++jj) {
@@ -1018,8 +1119,8 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
         }
     }
     if (lane == 0 && issued && !ok)  // no bulk copy may land after the CTA exits
-      dev::mbar_wait(&bfull[warp], issued_ph, dev::kDrainBudget);
-  } else if (warp == P) {
+      dev::mbar_wait(&bfull[d], issued_ph, dev::kDrainBudget);
+  } else if (warp == PW) {
     // ---------------- MMA issuer
     if (lane == 0) {
       const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
@@ -1051,7 +1152,7 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
     }
   } else {
     // ---------------- drainers
-    const int quarter = warp & 3, hf = (warp - P - 1) >> 2;
+    const int quarter = warp & 3, hf = (warp - PW - 1) >> 2;
     double acc[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) acc[i] = 0.0;
@@ -1087,7 +1188,7 @@ __global__ void __launch_bounds__(FuCfg<S>::Threads, 1)
   __syncthreads();
   if (s_fail) {
     // bounded wait for every MMA this CTA issued before freeing TMEM
-    if (tid == P * 32) {
+    if (tid == PW * 32) {
       tc_commit(done);
       atomicExch(status, CRAB_ETIMEOUT);
     }
@@ -1564,8 +1665,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
     CRAB_CUDA_CHECK(cudaEventRecord(ev[1], s));                                                                    \
     if (!fwork.empty()) {                                                                                          \
       CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_fused<EE, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                           (int)FuCfg<SS>::Smem));                                                 \
-      k_mp_moments_fused<EE, SS><<<(unsigned)fwork.size(), FuCfg<SS>::Threads, FuCfg<SS>::Smem, s>>>(              \
+                                           (int)FuCfg<EE, SS>::Smem));                                             \
+      k_mp_moments_fused<EE, SS><<<(unsigned)fwork.size(), FuCfg<EE, SS>::Threads, FuCfg<EE, SS>::Smem, s>>>(      \
           d_cst, d_Bimg, d_fwork, d_tstart, n_lmt, L, d_snorm, d_inv, fst, d_part, d_status, ctx->wait_budget);   \
     }                                                                                                              \
   }
