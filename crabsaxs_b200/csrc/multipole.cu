@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "device_math.cuh"
@@ -609,7 +610,12 @@ struct FuCfg {
   static constexpr int WPS = E == 1 ? 2 : 1;
   static constexpr int PW = P * WPS;  // producer warps
   static constexpr int SlotBytes = S * (kTcABytes + kTcBBytes);
-  static constexpr int Threads = (PW + 1) * 32 + kFuDrainers;
+  // drain threads: 256 (two per lm row, 32 node columns each), or for BF16
+  // 128 (one per row, all 64 columns), which leaves the BF16 producers more
+  // registers; draining a 64-point stage takes a fraction of producing it
+  static constexpr int Drainers = E == 1 ? 128 : kFuDrainers;
+  static constexpr int DrainCols = 64 * 128 / Drainers;
+  static constexpr int Threads = (PW + 1) * 32 + Drainers;
   static constexpr int Bars = 3 * Slots + 2 * kTcAccs + 1;
   // slots, then per producer warp the normalisations of one tile's rows
   // (kGemmM doubles), the 1/k table (kMaxL + 2 doubles), the barriers
@@ -1023,7 +1029,7 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
     }
     for (int a = 0; a < kTcAccs; ++a) {
       dev::mbar_init(&accfull[a], 1);
-      dev::mbar_init(&accfree[a], kFuDrainers);
+      dev::mbar_init(&accfree[a], Cfg::Drainers);
     }
     dev::mbar_init(done, 1);
     dev::fence_mbar_init();
@@ -1153,9 +1159,14 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
   } else {
     // ---------------- drainers
     const int quarter = warp & 3, hf = (warp - PW - 1) >> 2;
-    double acc[32];
+    constexpr int DC = Cfg::DrainCols;  // this thread's lm row and DC of the 64 node columns
+    // the chunk's sum of its stages' FP32 accumulators: in f64 for TF32; in
+    // FP32 for BF16, round to nearest over the chunk's stages (a few 1e-7
+    // relative, far below the BF16 terms), which halves its registers
+    using Acc = typename std::conditional<E == 1, float, double>::type;
+    Acc acc[DC];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+    for (int i = 0; i < DC; ++i) acc[i] = Acc(0);
     for (int t = 0; t < n_lmt && ok; ++t)
       for (int c = 0; c < nc; ++c) {
         const int u = t * nc + c, a = u % kTcAccs;
@@ -1165,20 +1176,20 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-        for (int c16 = 0; c16 < 2; ++c16) {
+        for (int c16 = 0; c16 < DC / 16; ++c16) {
           float v[16];
-          tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + hf * 32 + c16 * 16), v);
+          tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + hf * DC + c16 * 16), v);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+          for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (Acc)v[i];
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(&accfree[a]);
         if (c == nc - 1) {
           double* tile = part + ((int64_t)blockIdx.x * n_lmt + t) * kTileElems + quarter * 32 + lane;
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            tile[(hf * 32 + i) * kGemmM] = acc[i];
-            acc[i] = 0.0;
+          for (int i = 0; i < DC; ++i) {
+            tile[(hf * DC + i) * kGemmM] = (double)acc[i];
+            acc[i] = Acc(0);
           }
         }
       }
