@@ -18,6 +18,7 @@
 //      reweight.rs:84-154 from a uniform prior.
 // Steps 1-4 are captured once in a CUDA graph and replayed.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -258,15 +259,9 @@ struct RwOpts {
   double scale_value, bg_value;
 };
 
-// reweight.rs:236-301 on the mixture.
-__device__ void rw_fit(const double* cv, const double* w, int K, int nq, const double* y, const double* sg,
-                       const RwOpts& o, double* mix, double* red, double* s_out, double* b_out, double* chi_out) {
-  for (int p = threadIdx.x; p < nq; p += blockDim.x) {
-    double m = 0.0;
-    for (int k = 0; k < K; ++k) m += cv[(size_t)k * nq + p] * w[k];
-    mix[p] = m;
-  }
-  __syncthreads();
+// reweight.rs:236-301 on the mixture mix[p] (scale, background, reduced χ²).
+__device__ void rw_solve(const double* mix, int nq, const double* y, const double* sg, const RwOpts& o, double* red,
+                         double* s_out, double* b_out, double* chi_out) {
   double sw = 0, sx = 0, sy = 0, sxx = 0, sxy = 0;
   for (int p = threadIdx.x; p < nq; p += blockDim.x) {
     const double ww = 1.0 / (sg[p] * sg[p]);
@@ -309,124 +304,227 @@ __device__ void rw_fit(const double* cv, const double* w, int K, int nq, const d
   *chi_out = chi / (double)max(nq - 1, 1);
 }
 
-__device__ double kl_div(const double* w, int K, double prior, double* red) {
-  double s = 0.0;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) s += w[k] * log(w[k] / prior);
-  return block_sum(s, red);
-}
+// ---- KL reweighting over a cluster of kRwCluster CTAs ----------------------
+// reweight.rs:84-154 on the best candidate's K curves.  CTA r of the cluster
+// keeps rows [r kr, (r+1) kr) of those curves (kr = ceil(K / kRwCluster)) in
+// its shared memory, with their weights, gradients and proposals; the
+// mixture and every sum or maximum over K are exchanged through distributed
+// shared memory: each CTA publishes its partial, one cluster barrier, and
+// every CTA adds the partials of all ranks in rank order, so every CTA holds
+// the same values and takes the same branches.  Exchange buffers alternate
+// between two halves, so the barrier of one exchange also releases the
+// buffer of the exchange before it.
+constexpr int kRwCluster = 8;
+namespace cg = cooperative_groups;
 
-__device__ void apply_floor_dev(double* w, int K, double floor, double* red) {
+struct RwCluster {
+  cg::cluster_group cl;
+  double* xs;  // [2] scalar partial
+  double* pm;  // [2][3 nq] array partials
+  double* red;
+  int nq, par;
+  __device__ double sum(double v) {
+    v = block_sum(v, red);
+    if (threadIdx.x == 0) xs[par] = v;
+    cl.sync();
+    double t = 0.0;
+    for (int r = 0; r < kRwCluster; ++r) t += *cl.map_shared_rank(&xs[par], r);
+    par ^= 1;
+    return t;
+  }
+  __device__ double max(double v) {
+    v = block_max(v, red);
+    if (threadIdx.x == 0) xs[par] = v;
+    cl.sync();
+    double t = -INFINITY;
+    for (int r = 0; r < kRwCluster; ++r) t = fmax(t, *cl.map_shared_rank(&xs[par], r));
+    par ^= 1;
+    return t;
+  }
+  // out[i] = sum over ranks of the published part[i], i < n (n <= 3 nq); part
+  // is written by this CTA into pm[par] by the caller's loop before the call
+  __device__ double* slot() { return pm + (size_t)par * 3 * nq; }
+  __device__ void sum_array(double* out, int n) {
+    __syncthreads();
+    cl.sync();
+    double* mine = slot();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double t = 0.0;
+      for (int r = 0; r < kRwCluster; ++r) t += cl.map_shared_rank(mine, r)[i];
+      out[i] = t;
+    }
+    par ^= 1;
+    __syncthreads();
+  }
+};
+
+// The mixture Σ_k w_k I_k(q) over the cluster's rows, then reweight.rs:236-301.
+__device__ void rw_fit_cl(RwCluster& X, const double* cvr, const double* w, int nk, int nq, const double* y,
+                          const double* sg, const RwOpts& o, double* mix, double* s_out, double* b_out,
+                          double* chi_out) {
+  double* part = X.slot();
+  for (int p = threadIdx.x; p < nq; p += blockDim.x) {
+    double m = 0.0;
+    for (int k = 0; k < nk; ++k) m += cvr[(size_t)k * nq + p] * w[k];
+    part[p] = m;
+  }
+  X.sum_array(mix, nq);
+  rw_solve(mix, nq, y, sg, o, X.red, s_out, b_out, chi_out);
+}
+__device__ double kl_div_cl(RwCluster& X, const double* w, int nk, double prior) {
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) s += w[k] * log(w[k] / prior);
+  return X.sum(s);
+}
+__device__ void apply_floor_cl(RwCluster& X, double* w, int nk, int K, double floor) {
   double sum = 0.0;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) sum += w[k];
-  sum = fmax(block_sum(sum, red), 1e-300);
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) sum += w[k];
+  sum = fmax(X.sum(sum), 1e-300);
   const double residual = 1.0 - floor * (double)K;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) w[k] = floor <= 0.0 ? w[k] / sum : floor + residual * w[k] / sum;
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) w[k] = floor <= 0.0 ? w[k] / sum : floor + residual * w[k] / sum;
   __syncthreads();
 }
 
-// One CTA: best candidate, ∂χ²/∂(c1, c2) there, then reweight.rs:84-154.
+// Shared memory of one cluster CTA for K curves of nq points: weights,
+// gradients and proposals of its rows, the mixture, the exchange buffers and,
+// when they fit, its rows of the curves.
+__host__ __device__ inline int rw_rows(int K) { return (K + kRwCluster - 1) / kRwCluster; }
+__host__ __device__ inline bool rw_rows_on_chip(int K, int nq) {
+  return (size_t)rw_rows(K) * (size_t)nq * sizeof(double) <= 128 * 1024;
+}
+__host__ __device__ inline size_t rw_smem(int K, int nq) {
+  const size_t kr = (size_t)rw_rows(K);
+  return (3 * kr + (size_t)nq + 6 * (size_t)nq + 2 + (rw_rows_on_chip(K, nq) ? kr * (size_t)nq : 0)) * sizeof(double);
+}
+
+// Best candidate, ∂χ²/∂(c1, c2) there, then reweight.rs:84-154.
 // out: [0] best candidate, [1] scale, [2] bg, [3] reduced chi2, [4] KL,
 // [5] iterations, [6] converged, [7] dchi/dc1, [8] dchi/dc2.
-__global__ void __launch_bounds__(kEW)
+__global__ void __cluster_dims__(kRwCluster, 1, 1) __launch_bounds__(kEW)
     k_ens_reweight(const double* __restrict__ curves, const double* __restrict__ fitc, int n_cand, int K, int nq,
                    const double* __restrict__ y, const double* __restrict__ sg, const double* __restrict__ weights,
                    const double* __restrict__ dcurves, RwOpts o, double* __restrict__ w_out,
                    double* __restrict__ out) {
   extern __shared__ double sm[];
-  double* w = sm;          // K
-  double* g = w + K;       // K
-  double* pr = g + K;      // K
-  double* mix = pr + K;    // nq
   __shared__ double red[32];
   __shared__ int best;
+  RwCluster X{cg::this_cluster(), nullptr, nullptr, red, nq, 0};
+  const int rank = (int)X.cl.block_rank();
+  const int kr = rw_rows(K), k0 = min(K, rank * kr), nk = min(K, k0 + kr) - k0;
+  double* w = sm;              // kr
+  double* g = w + kr;          // kr
+  double* pr = g + kr;         // kr
+  double* mix = pr + kr;       // nq
+  X.pm = mix + nq;             // 2 x 3 nq
+  X.xs = X.pm + 6 * (size_t)nq;  // 2
+  double* cvs = X.xs + 2;      // kr x nq, when the rows fit
   if (threadIdx.x == 0) {
     best = 0;
     for (int c = 1; c < n_cand; ++c)
       if (fitc[4 * c + 2] < fitc[4 * best + 2]) best = c;
   }
   __syncthreads();
-  const double* cv = curves + (size_t)best * K * nq;
+  const double* cvg = curves + ((size_t)best * K + k0) * nq;  // this CTA's rows
+  const double* cvr = cvg;
+  if (rw_rows_on_chip(K, nq)) {
+    for (size_t i = threadIdx.x; i < (size_t)nk * nq; i += blockDim.x) cvs[i] = cvg[i];
+    cvr = cvs;
+  }
+  __syncthreads();
   // ∂χ²/∂c1 and ∂χ²/∂c2 at the best candidate's weights, scale and background
   {
     const double s = fitc[4 * best], b = fitc[4 * best + 1];
-    const double* wb = weights + (size_t)best * K;
-    double g1 = 0.0, g2 = 0.0;
+    const double* wb = weights + (size_t)best * K + k0;
+    const double* d1c = dcurves + ((size_t)(2 * best) * K + k0) * nq;
+    const double* d2c = dcurves + ((size_t)(2 * best + 1) * K + k0) * nq;
+    double* part = X.slot();
     for (int p = threadIdx.x; p < nq; p += blockDim.x) {
       double m = 0.0, d1 = 0.0, d2 = 0.0;
-      for (int k = 0; k < K; ++k) {
-        m += cv[(size_t)k * nq + p] * wb[k];
-        d1 += dcurves[((size_t)(2 * best) * K + k) * nq + p] * wb[k];
-        d2 += dcurves[((size_t)(2 * best + 1) * K + k) * nq + p] * wb[k];
+      for (int k = 0; k < nk; ++k) {
+        m += cvr[(size_t)k * nq + p] * wb[k];
+        d1 += d1c[(size_t)k * nq + p] * wb[k];
+        d2 += d2c[(size_t)k * nq + p] * wb[k];
       }
-      const double wgt = 2.0 * (s * m + b - y[p]) / (sg[p] * sg[p]) / (double)max(nq - 1, 1) * s;
-      g1 += wgt * d1;
-      g2 += wgt * d2;
+      part[p] = m;
+      part[nq + p] = d1;
+      part[2 * nq + p] = d2;
+    }
+    // the sums land in this CTA's other exchange half: no peer reads it
+    // before the next array exchange, which comes after their last use here
+    double* sums = X.pm + (size_t)(X.par ^ 1) * 3 * nq;
+    X.sum_array(sums, 3 * nq);
+    double g1 = 0.0, g2 = 0.0;
+    for (int p = threadIdx.x; p < nq; p += blockDim.x) {
+      const double wgt = 2.0 * (s * sums[p] + b - y[p]) / (sg[p] * sg[p]) / (double)max(nq - 1, 1) * s;
+      g1 += wgt * sums[nq + p];
+      g2 += wgt * sums[2 * nq + p];
     }
     g1 = block_sum(g1, red);
     g2 = block_sum(g2, red);
-    if (threadIdx.x == 0) {
+    if (rank == 0 && threadIdx.x == 0) {
       out[7] = g1;
       out[8] = g2;
     }
+    __syncthreads();
   }
   const double prior = 1.0 / (double)K;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) w[k] = prior;
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) w[k] = prior;
   __syncthreads();
-  apply_floor_dev(w, K, o.floor, red);
+  apply_floor_cl(X, w, nk, K, o.floor);
   int iterations = 0, converged = 0;
   const double dof = (double)max(nq - 1, 1);
   double s, b, chi;
   for (int it = 0; it < o.max_iter; ++it) {
     iterations = it + 1;
-    rw_fit(cv, w, K, nq, y, sg, o, mix, red, &s, &b, &chi);
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    rw_fit_cl(X, cvr, w, nk, nq, y, sg, o, mix, &s, &b, &chi);
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
       double dg = 0.0;
       for (int p = 0; p < nq; ++p)
-        dg += 2.0 * ((s * mix[p] + b) - y[p]) * s * cv[(size_t)k * nq + p] / (sg[p] * sg[p]) / dof;
+        dg += 2.0 * ((s * mix[p] + b) - y[p]) * s * cvr[(size_t)k * nq + p] / (sg[p] * sg[p]) / dof;
       g[k] = dg + o.kl * (log(w[k] / prior) + 1.0);
     }
     __syncthreads();
     double gmax = 0.0;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) gmax = fmax(gmax, fabs(g[k]));
-    gmax = fmax(block_max(gmax, red), 1e-12);
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) gmax = fmax(gmax, fabs(g[k]));
+    gmax = fmax(X.max(gmax), 1e-12);
     double step = o.step / gmax;
-    const double objective = chi + o.kl * kl_div(w, K, prior, red);
+    const double objective = chi + o.kl * kl_div_cl(X, w, nk, prior);
     bool accepted = false;
     for (int h = 0; h < 14 && !accepted; ++h) {
       double mx = -INFINITY;
-      for (int k = threadIdx.x; k < K; k += blockDim.x) {
+      for (int k = threadIdx.x; k < nk; k += blockDim.x) {
         pr[k] = log(fmax(w[k], 1e-300)) - step * g[k];
         mx = fmax(mx, pr[k]);
       }
-      mx = block_max(mx, red);
-      for (int k = threadIdx.x; k < K; k += blockDim.x) pr[k] = exp(pr[k] - mx);
+      mx = X.max(mx);
+      for (int k = threadIdx.x; k < nk; k += blockDim.x) pr[k] = exp(pr[k] - mx);
       __syncthreads();
       double sum = 0.0;
-      for (int k = threadIdx.x; k < K; k += blockDim.x) sum += pr[k];
-      sum = fmax(block_sum(sum, red), 1e-300);
-      for (int k = threadIdx.x; k < K; k += blockDim.x) pr[k] /= sum;
+      for (int k = threadIdx.x; k < nk; k += blockDim.x) sum += pr[k];
+      sum = fmax(X.sum(sum), 1e-300);
+      for (int k = threadIdx.x; k < nk; k += blockDim.x) pr[k] /= sum;
       __syncthreads();
-      apply_floor_dev(pr, K, o.floor, red);
+      apply_floor_cl(X, pr, nk, K, o.floor);
       double s2, b2, chi2;
-      rw_fit(cv, pr, K, nq, y, sg, o, mix, red, &s2, &b2, &chi2);
-      if (chi2 + o.kl * kl_div(pr, K, prior, red) <= objective + 1e-12) accepted = true;
+      rw_fit_cl(X, cvr, pr, nk, nq, y, sg, o, mix, &s2, &b2, &chi2);
+      if (chi2 + o.kl * kl_div_cl(X, pr, nk, prior) <= objective + 1e-12) accepted = true;
       else step *= 0.5;
     }
     if (!accepted) break;
     double delta = 0.0;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) delta += fabs(pr[k] - w[k]);
-    delta = block_sum(delta, red);
-    for (int k = threadIdx.x; k < K; k += blockDim.x) w[k] = pr[k];
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) delta += fabs(pr[k] - w[k]);
+    delta = X.sum(delta);
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) w[k] = pr[k];
     __syncthreads();
     if (delta <= o.tol) {
       converged = 1;
       break;
     }
   }
-  rw_fit(cv, w, K, nq, y, sg, o, mix, red, &s, &b, &chi);
-  const double kl = kl_div(w, K, prior, red);
-  for (int k = threadIdx.x; k < K; k += blockDim.x) w_out[k] = w[k];
-  if (threadIdx.x == 0) {
+  rw_fit_cl(X, cvr, w, nk, nq, y, sg, o, mix, &s, &b, &chi);
+  const double kl = kl_div_cl(X, w, nk, prior);
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) w_out[k0 + k] = w[k];
+  if (rank == 0 && threadIdx.x == 0) {
     out[0] = best;
     out[1] = s;
     out[2] = b;
@@ -435,6 +533,7 @@ __global__ void __launch_bounds__(kEW)
     out[5] = iterations;
     out[6] = converged;
   }
+  X.cl.sync();  // no CTA leaves while a peer may still read its shared memory
 }
 
 // Derivative curves dI/dc1 and dI/dc2 of every conformer at every candidate:
@@ -646,7 +745,7 @@ static size_t weights_smem(int K, int64_t nq) {
 static void ensemble_fit_buffers(EnsemblePlan& E, const double* y, const double* sg) {
   crab_ctx* ctx = E.ctx;
   // shared-memory opt-in for the largest subset, done before any graph capture
-  const size_t shm = weights_smem(E.K, E.nq), shr = (size_t)(3 * E.K + E.nq) * sizeof(double);
+  const size_t shm = weights_smem(E.K, E.nq), shr = rw_smem(E.K, (int)E.nq);
   require(shm <= 200 * 1024 && shr <= 200 * 1024, "ensemble too large for the on-chip weight fit");
   CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_ens_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(shm, 48 * 1024)));
   CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_ens_reweight, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(shr, 48 * 1024)));
@@ -679,9 +778,9 @@ static void ensemble_launch_fit(EnsemblePlan& E, int Ksel, const EnsOpts& eo, co
                                                            E.d_damp, E.d_self, E.d_sumw, Ksel, E.d_curves,
                                                            E.d_dcurves);
     CRAB_CUDA_CHECK(cudaGetLastError());
-    const size_t shr = (size_t)(3 * Ksel + E.nq) * sizeof(double);
-    k_ens_reweight<<<1, kEW, shr, sm>>>(E.d_curves, E.d_fit, E.n_cand, Ksel, (int)E.nq, E.d_y, E.d_sg, E.d_weights,
-                                        E.d_dcurves, *ro, E.d_wkl, E.d_out);
+    const size_t shr = rw_smem(Ksel, (int)E.nq);
+    k_ens_reweight<<<kRwCluster, kEW, shr, sm>>>(E.d_curves, E.d_fit, E.n_cand, Ksel, (int)E.nq, E.d_y, E.d_sg,
+                                                 E.d_weights, E.d_dcurves, *ro, E.d_wkl, E.d_out);
     CRAB_CUDA_CHECK(cudaGetLastError());
     ctx->launches += 2;
   }
