@@ -574,8 +574,9 @@ constexpr size_t tc_smem_bytes() {
 // array between tiles (40 bytes per point, L2-resident).  In the TF32 modes the
 // values are the ones k_mp_prep writes, bit for bit: the same f64 operations
 // in the same order, then the same rounding to the operand type; the BF16
-// modes take each recurrence step as one fused multiply-add (fu_next_l).  k_mp_reduce maps rows
-// back to the l^2 + l + m order of the moments.
+// hi+lo mode takes each recurrence step as one fused multiply-add
+// (fu_next_l).  k_mp_reduce maps rows back to the l^2 + l + m order of the
+// moments.
 //
 // Element types; both give 128-byte stage rows, so the swizzled layout, the
 // descriptors and the four K steps of 32 bytes per stage are those of the
@@ -602,18 +603,19 @@ constexpr int kFuDrainers = 256;
 constexpr int kFuBatch = 4;  // recurrence steps a producer lane runs ahead of its row stores
 template <int E, int S>
 struct FuCfg {
-  // slots, and producer warps per slot: a BF16 stage (64 points) is walked by
-  // two warps, one point per lane each, so every scheduler runs two
-  // independent walks; a TF32 stage (32 points) by one
-  static constexpr int P = (E == 0 && S == 1) ? 6 : 4;
+  // slots, and producer warps per slot: a BF16 hi+lo stage (64 points, two
+  // terms) is walked by two warps, one point per lane each, so every
+  // scheduler runs two independent walks; a single-term stage by one warp
+  // (two points per lane for BF16), which is faster there
+  static constexpr int P = S == 1 ? 6 : 4;
   static constexpr int Slots = P;
-  static constexpr int WPS = E == 1 ? 2 : 1;
+  static constexpr int WPS = (E == 1 && S == 2) ? 2 : 1;
   static constexpr int PW = P * WPS;  // producer warps
   static constexpr int SlotBytes = S * (kTcABytes + kTcBBytes);
   // drain threads: 256 (two per lm row, 32 node columns each), or for BF16
-  // 128 (one per row, all 64 columns), which leaves the BF16 producers more
+  // hi+lo 128 (one per row, all 64 columns), which leaves its producers more
   // registers; draining a 64-point stage takes a fraction of producing it
-  static constexpr int Drainers = E == 1 ? 128 : kFuDrainers;
+  static constexpr int Drainers = WPS == 2 ? 128 : kFuDrainers;
   static constexpr int DrainCols = 64 * 128 / Drainers;
   static constexpr int Threads = (PW + 1) * 32 + Drainers;
   static constexpr int Bars = 3 * Slots + 2 * kTcAccs + 1;
@@ -667,7 +669,7 @@ __host__ __device__ __forceinline__ uint32_t fu_swz(int row, int k) {
 // the walk keeps P_m^m (pmm), P_{l-1}^m, P_l^m (prev, cur) and cos, sin (m phi);
 // the walk position (m, l, and whether the next row is the sin row of (l, m))
 // is the same for every point.  The f64 operations and their order are
-// k_mp_prep's (in the BF16 modes except the l step, fu_next_l), so the TF32
+// k_mp_prep's (in the BF16 hi+lo mode except the l step, fu_next_l), so the TF32
 // values are its values bit for bit.
 struct FuWalk {
   double pmm, prev, cur, cm, sm;
@@ -681,11 +683,14 @@ __device__ __forceinline__ void fu_first_l(int m, const double4& k4, FuWalk& w) 
 }
 // P_l^m = ((2l-1) x P_{l-1}^m - (l+m-1) P_{l-2}^m) / (l-m), with a = 2l-1,
 // b = l+m-1 and iv = 1/(l-m) given.  EXACT: k_mp_prep's operations in its
-// order (the TF32 modes, whose fused and staged curves are equal).  Otherwise
-// (the BF16 modes) the same recurrence as one fused multiply-add on the walk's
+// order (the TF32 modes, whose fused and staged curves are equal, and BF16).
+// Otherwise (BF16 hi+lo) the same recurrence as one fused multiply-add on the walk's
 // dependency chain, P_l = fma((a iv) x, P_{l-1}, -(b iv) P_{l-2}): the other
 // products do not wait on P_{l-1}, so a step costs one f64 latency instead of
-// three; its rounding differs from k_mp_prep's by about an ulp.
+// three; its rounding differs from k_mp_prep's by about an ulp.  The
+// generator takes the second form, the batches of fu_generate and the
+// single-rounding rows of fu_emit_vals in the BF16 hi+lo layout (one point
+// per lane), where they were measured faster, and the first elsewhere.
 template <bool EXACT = true>
 __device__ __forceinline__ void fu_next_l(double a, double b, double iv, const double4& k4, FuWalk& w) {
   if (EXACT) {
@@ -700,13 +705,16 @@ __device__ __forceinline__ void fu_next_l(double a, double b, double iv, const d
   }
 }
 // next m: P_m^m = P_{m-1}^{m-1} (-(2m-1) sin theta), (cos, sin)(m phi) rotated
+template <bool F32ROWS = false>
 __device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
   w.pmm = __dmul_rn(w.pmm, __dmul_rn(-(double)(2 * m - 1), k4.y));
   const double next_cos = __dadd_rn(__dmul_rn(w.cm, k4.z), -__dmul_rn(w.sm, k4.w));
   w.sm = __dadd_rn(__dmul_rn(w.sm, k4.z), __dmul_rn(w.cm, k4.w));
   w.cm = next_cos;
-  w.cmf = (float)w.cm;
-  w.smf = (float)w.sm;
+  if (F32ROWS) {
+    w.cmf = (float)w.cm;
+    w.smf = (float)w.sm;
+  }
   w.cur = w.pmm;
   w.prev = 0.0;
 }
@@ -805,7 +813,8 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
                                             const double4 (&k4)[PPT], FuWalk (&w)[PPT],
                                             const double* __restrict__ srow, const double* __restrict__ inv) {
   int m = ts.x, l = ts.y, half = ts.z, r = 0;
-  if (E == 1)
+  constexpr bool kHiLoRows = E == 1 && PPT == 1;  // the BF16 hi+lo layout's rows (fu_emit_vals)
+  if (kHiLoRows)
 #pragma unroll
     for (int jj = 0; jj < PPT; ++jj) {
       w[jj].cmf = (float)w[jj].cm;
@@ -815,7 +824,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
     ++m;
     if (m <= L) {
 #pragma unroll
-      for (int jj = 0; jj < PPT; ++jj) fu_next_m(m, k4[jj], w[jj]);
+      for (int jj = 0; jj < PPT; ++jj) fu_next_m<kHiLoRows>(m, k4[jj], w[jj]);
     }
     l = m;
   };
@@ -826,7 +835,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
 #pragma unroll
       for (int jj = 0; jj < PPT; ++jj) {
         if (l == m) fu_first_l(m, k4[jj], w[jj]);
-        else fu_next_l<E == 0>((double)(2 * l + 1), (double)(l + m), inv[l + 1 - m], k4[jj], w[jj]);
+        else fu_next_l<!(E == 1 && PPT == 1)>((double)(2 * l + 1), (double)(l + m), inv[l + 1 - m], k4[jj], w[jj]);
       }
       ++l;
     }
@@ -842,7 +851,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
       double v[PPT];
 #pragma unroll
       for (int jj = 0; jj < PPT; ++jj)
-        v[jj] = E == 1 ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].smf)  // as fu_emit_vals
+        v[jj] = kHiLoRows ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].smf)  // as fu_emit_vals
                        : __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].sm);
       fu_emit<E, S, PPT>(sa, r++, col, v);
       half = 0;
@@ -854,7 +863,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
       double v[PPT];
 #pragma unroll
       for (int jj = 0; jj < PPT; ++jj)
-        v[jj] = E == 1 ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].cmf)
+        v[jj] = kHiLoRows ? (double)((float)__dmul_rn(sn, w[jj].cur) * w[jj].cmf)
                        : __dmul_rn(__dmul_rn(sn, w[jj].cur), w[jj].cm);
       fu_emit<E, S, PPT>(sa, r++, col, v);
       break;
@@ -872,7 +881,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
     // which depend on nothing but those values, so a warp's in-order issue
     // overlaps their latencies with one another and with the chain
     int k = 0;
-    for (; k + kFuBatch <= steady; k += kFuBatch) {
+    for (; E == 1 && PPT == 1 && k + kFuBatch <= steady; k += kFuBatch) {  // the BF16 hi+lo layout
       double cv[kFuBatch][PPT];
 #pragma unroll
       for (int u = 0; u < kFuBatch; ++u) {
@@ -880,7 +889,7 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
 #pragma unroll
         for (int jj = 0; jj < PPT; ++jj) {
           cv[u][jj] = w[jj].cur;
-          fu_next_l<E == 0>(a, b, iv, k4[jj], w[jj]);
+          fu_next_l<!(E == 1 && PPT == 1)>(a, b, iv, k4[jj], w[jj]);
         }
         a += 2.0;
         b += 1.0;
@@ -890,13 +899,13 @@ __device__ __forceinline__ void fu_generate(unsigned char* __restrict__ sa, int 
       for (int u = 0; u < kFuBatch; ++u) fu_emit_vals<E, S, PPT>(sa, r + u * per, col, m, srow[r + u * per], cv[u], w);
       r += kFuBatch * per;
     }
-#pragma unroll 1
+#pragma unroll 4
     for (; k < steady; ++k) {
       fu_emit_entry<E, S, PPT>(sa, r, col, m, srow[r], w);
       r += per;
       const double iv = inv[l + 1 - m];
 #pragma unroll
-      for (int jj = 0; jj < PPT; ++jj) fu_next_l<E == 0>(a, b, iv, k4[jj], w[jj]);
+      for (int jj = 0; jj < PPT; ++jj) fu_next_l<!(E == 1 && PPT == 1)>(a, b, iv, k4[jj], w[jj]);
       a += 2.0;
       b += 1.0;
       ++l;
@@ -1160,10 +1169,10 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
     // ---------------- drainers
     const int quarter = warp & 3, hf = (warp - PW - 1) >> 2;
     constexpr int DC = Cfg::DrainCols;  // this thread's lm row and DC of the 64 node columns
-    // the chunk's sum of its stages' FP32 accumulators: in f64 for TF32; in
-    // FP32 for BF16, round to nearest over the chunk's stages (a few 1e-7
+    // the chunk's sum of its stages' FP32 accumulators: in f64, or for BF16
+    // hi+lo in FP32, round to nearest over the chunk's stages (a few 1e-7
     // relative, far below the BF16 terms), which halves its registers
-    using Acc = typename std::conditional<E == 1, float, double>::type;
+    using Acc = typename std::conditional<Cfg::WPS == 2, float, double>::type;
     Acc acc[DC];
 #pragma unroll
     for (int i = 0; i < DC; ++i) acc[i] = Acc(0);
