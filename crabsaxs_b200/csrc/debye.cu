@@ -1231,7 +1231,8 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
 // CTAs per SM at Q = 100, 126 and 128; one chain and two CTAs at Q = 150 and
 // 168, whose fewer seeds per pair outweigh the lower occupancy: 3 x 168 for
 // 500 q and 2 x 150 for 300 q are 1.3 % and 3 % faster than 4 x 126 and
-// 3 x 100; two chains below Q = 100).
+// 3 x 100; two chains below Q = 100), with the weight folded in where that
+// build exists.
 int2 default_variant(const std::vector<double>& q) {
   int bestQ = 64;
   long best_cost = -1;
@@ -1242,9 +1243,12 @@ int2 default_variant(const std::vector<double>& q) {
       bestQ = Qc;
     }
   }
-  if (bestQ == 128 || bestQ == 126 || bestQ == 100) return make_int2(bestQ, 1 + kPackedQ + kDenser);
+  // the folded builds (pair weight in the recurrence state), which the
+  // autotuner measured 0.5-1.3 % faster than the unfolded ones
+  if (bestQ == 126 || bestQ == 100) return make_int2(bestQ, kFolded1x3);
+  if (bestQ == 128) return make_int2(bestQ, 1 + kPackedQ + kDenser);
   // 75 or 84 packed accumulators: two CTAs per SM
-  if (bestQ == 150 || bestQ == 168) return make_int2(bestQ, 1 + kPackedQ);
+  if (bestQ == 150 || bestQ == 168) return make_int2(bestQ, kFolded1);
   const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
