@@ -1247,8 +1247,10 @@ int2 default_variant(const std::vector<double>& q) {
   // autotuner measured 0.5-1.3 % faster than the unfolded ones
   if (bestQ == 126 || bestQ == 100) return make_int2(bestQ, kFolded1x3);
   if (bestQ == 128) return make_int2(bestQ, 1 + kPackedQ + kDenser);
-  // 75 or 84 packed accumulators: two CTAs per SM
-  if (bestQ == 150 || bestQ == 168) return make_int2(bestQ, kFolded1);
+  // 75 or 84 packed accumulators: two CTAs per SM; at Q = 150 two chains per
+  // thread (1.4 % faster on the 300-q ensemble pass, 1.7 % at 500 q), at 168 one
+  if (bestQ == 150) return make_int2(bestQ, kFolded2);
+  if (bestQ == 168) return make_int2(bestQ, kFolded1);
   const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
