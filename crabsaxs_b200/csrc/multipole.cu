@@ -26,6 +26,9 @@
 //                    spherical.rs:95-133 in f64
 //   k_mp_gram        per q: A^c_lm for each requested amplitude combination c
 //                    and 4 pi sum_{l <= l_q, m} A^c A^d
+#include <cuda.h>  // CUtensorMap and the tensor-map encoder's types
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -260,49 +263,55 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 // ---- tensor-core moment GEMM (tcgen05, TF32 operands split into terms) ----
 //
 // The same product part[w] = YT-tile . WT-tile^T (128 lm rows x 64 nodes over
-// the item's points) on the 5th-generation tensor cores.  Each FP32 operand x
-// is split into TF32 terms (h = x rounded to TF32, m = x - h rounded to TF32):
-//   S = 1: h h'                  (TF32, relative error ~5e-4)
-//   S = 2: h h' + h m' + m h'    (relative error ~5e-7)
+// the item's points) on the 5th-generation tensor cores, with TF32 terms:
+//   S = 1: h h'                  h = x rounded to TF32 (relative error ~5e-4)
+//   S = 2: h h' + h m' + m h'    h = x truncated to TF32 (the tensor core
+//          reads a raw FP32 operand so), m = x - h rounded to TF32
+//          (relative error ~5e-7)
 // The S = 2 error is set by the tensor core's FP32 accumulation, which rounds
 // toward zero (about 2^-24 of the accumulator per MMA), so a TMEM accumulator
 // covers one 32-point stage only and is then drained into f64 registers.
 //
-// Warp-specialised pipeline (17 warps):
-//  * producers, warps 0-7: each thread copies its six 16-byte chunks of a
+// Warp-specialised pipeline (18 warps):
+//  * TMA, warp 9 lane 0: waits until term slot d is empty, then loads the
 //    stage's FP32 tiles (A: 128 rows x 32 points, B: 64 x 32; point-blocked,
-//    so each tile is contiguous) with cp.async into a private slot of a
-//    3-deep ring, reads them back, waits until term slot d is empty, stores
-//    the S TF32 terms in the K-major 128-byte-swizzled layout (row r at
-//    (r/8)*1024 + (r%8)*128, 16-byte chunk c at position c ^ (r%8)), fences
-//    the generic-proxy writes for the tensor core and arrives on full[d];
+//    so each tile is a 2D box of 128-byte rows) with two tensor copies into
+//    the slot's first-term areas, 128-byte swizzled by the copy itself (row r
+//    at (r/8)*1024 + (r%8)*128, 16-byte chunk c at position c ^ (r%8)), the
+//    K-major layout the MMA reads; the copies complete on tfull[d];
+//  * producers, warps 0-7: wait tfull[d]; each thread takes six 16-byte
+//    chunks of the tiles and, for S = 2, writes their m terms at the same
+//    offsets of the second-term areas (the h terms are the copied values),
+//    for S = 1 rounds the values in place; then fences the generic-proxy
+//    writes for the tensor core and arrives on full[d];
 //  * MMA issuer, warp 8 lane 0: waits full[d] and accfree[a], issues
 //    tcgen05.mma (M = 128, N = 64, K = 8, descriptor start +32 B per K step)
 //    into TMEM accumulator a and commits to empty[d] and accfull[a];
-//  * drainers, warps 9-16: wait accfull[a], read their lane quarter (warp % 4)
-//    and 32 of the 64 columns with tcgen05.ld, add them into f64 registers and
-//    arrive on accfree[a]; at the end they store the f64 tile.
-// Three term slots, four accumulators.  Every wait is bounded: a role whose
+//  * drainers, warps 10-17: wait accfull[a], read their lane quarter (warp %
+//    4) and 32 of the 64 columns with tcgen05.ld, add them into f64
+//    registers and arrive on accfree[a]; at the end they store the f64 tile.
+// Four term slots, four accumulators.  The copies read only this GPU's
+// memory and use no cluster multicast.  Every wait is bounded: a role whose
 // wait runs out stops, the others run out in turn, and the CTA flags
-// CRAB_ETIMEOUT, waits (bounded) for its own MMAs and frees its TMEM.
+// CRAB_ETIMEOUT, waits (bounded) for its own copies and MMAs and frees its
+// TMEM.
 constexpr int kTcK = 32;                    // points per stage
 constexpr int kTcProducers = 256;           // warps 0-7
 constexpr int kTcMmaWarp = 8;
-constexpr int kTcDrainers = 256;            // warps 9-16
-constexpr int kTcThreads = kTcProducers + 32 + kTcDrainers;
-constexpr int kTcSlots = 3;                 // term buffers
+constexpr int kTcTmaWarp = 9;
+constexpr int kTcDrainers = 256;            // warps 10-17
+constexpr int kTcThreads = kTcProducers + 64 + kTcDrainers;
+constexpr int kTcSlots = 4;                 // term buffers
 constexpr int kTcAccs = 4;                  // 64-column TMEM accumulators
 constexpr int kTcTmemCols = 256;
-constexpr int kTcRing = 3;                  // raw FP32 stages in flight per producer
-constexpr int kTcChunks = 6;                // 16-byte chunks per producer per stage (4 of A, 2 of B)
-constexpr int kTcAChunks = 4;
-static_assert(kTcAChunks * kTcProducers * 4 == kGemmM * kTcK, "A tile chunks");
-static_assert((kTcChunks - kTcAChunks) * kTcProducers * 4 == kMaxNodes * kTcK, "B tile chunks");
+constexpr int kTcAChunks = 4;               // 16-byte chunks per producer per stage: 4 of A, 2 of B
+constexpr int kTcChunks = 6;
+static_assert(kTcAChunks * kTcProducers * 16 == kGemmM * kTcK * 4, "A tile chunks");
+static_assert((kTcChunks - kTcAChunks) * kTcProducers * 16 == kMaxNodes * kTcK * 4, "B tile chunks");
 static_assert(kTcThreads % 32 == 0 && kTcProducers == 32 * kTcMmaWarp, "warp roles");
 constexpr int kTcABytes = kGemmM * kTcK * 4;     // 16 KB
 constexpr int kTcBBytes = kMaxNodes * kTcK * 4;  // 8 KB
-constexpr int kTcRingBytes = kTcRing * kTcProducers * kTcChunks * 16;  // 72 KB
-constexpr int kTcBars = 2 * kTcSlots + 2 * kTcAccs + 1;
+constexpr int kTcBars = 3 * kTcSlots + 2 * kTcAccs + 1;
 // TF32, FP32 accumulate, K-major A and B, N = 64 (bits 17-22, N>>3), M = 128 (bits 24-28, M>>4)
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -348,56 +357,51 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// x truncated to TF32 (the 13 low mantissa bits cleared), as the tensor core
+// reads a raw FP32 operand of kind::tf32.
+__device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+// 2D tensor copy of one box into shared memory, completing on an mbarrier
+// (no multicast: the box lies in this GPU's memory and lands in this CTA).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst), b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(d), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(b)
+      : "memory");
 }
 
-// Split 4 values into S TF32 terms and store each term's 16-byte chunk.
+// The producers' pass over one 16-byte chunk at byte offset off of a copied
+// tile (part_bytes: one term's tile size): S = 2 writes the m terms of the
+// four values into the second-term tile, S = 1 rounds them to TF32 in place.
 template <int S>
-__device__ __forceinline__ void tc_store_split(unsigned char* base, int part_bytes, int off, float4 v) {
-  const float x[4] = {v.x, v.y, v.z, v.w};
-  float t[2][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    t[0][i] = tf32_rna(x[i]);
-    if (S >= 2) t[1][i] = tf32_rna(x[i] - t[0][i]);
+__device__ __forceinline__ void tc_term_pass(unsigned char* __restrict__ base, int part_bytes, int off) {
+  const float4 x = *reinterpret_cast<const float4*>(base + off);
+  if (S == 2) {
+    *reinterpret_cast<float4*>(base + part_bytes + off) =
+        make_float4(tf32_rna(x.x - tf32_trunc(x.x)), tf32_rna(x.y - tf32_trunc(x.y)), tf32_rna(x.z - tf32_trunc(x.z)),
+                    tf32_rna(x.w - tf32_trunc(x.w)));
+  } else {
+    *reinterpret_cast<float4*>(base + off) = make_float4(tf32_rna(x.x), tf32_rna(x.y), tf32_rna(x.z), tf32_rna(x.w));
   }
-#pragma unroll
-  for (int p = 0; p < S; ++p)
-    *reinterpret_cast<float4*>(base + p * part_bytes + off) = make_float4(t[p][0], t[p][1], t[p][2], t[p][3]);
-}
-
-// Chunk c of producer thread t in a stage: A rows for c < kTcAChunks, B rows
-// after; 16-byte column c4 of the row.
-__device__ __forceinline__ void tc_chunk(int c, int t, int& row, int& c4) {
-  const int idx = (c < kTcAChunks ? c : c - kTcAChunks) * kTcProducers + t;
-  row = idx >> 3;
-  c4 = idx & 7;
 }
 
 template <int S>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_mp_moments_tc(const float* __restrict__ YT, const float* __restrict__ WT, int64_t n_pad, int lm_pad,
+    k_mp_moments_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int lm_pad,
                     const MpWork* __restrict__ work, double* __restrict__ part, int* __restrict__ status,
                     int budget) {
   static_assert(S == 1 || S == 2, "one or two TF32 terms");
   if (budget < 0) budget = dev::kSpinBudget;  // the context's default
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   constexpr int slot_bytes = S * (kTcABytes + kTcBBytes);  // S A terms, then S B terms
-  // 1024-byte alignment as an offset into the shared array, so that pointers
-  // derived from it keep the shared state space (shared loads and stores,
-  // not generic ones)
+  // 1024-byte alignment (the 128-byte swizzle's period) as an offset into the
+  // shared array, so that pointers derived from it keep the shared state space
   unsigned char* smem = tc_smem + ((1024u - ((uint32_t)__cvta_generic_to_shared(tc_smem) & 1023u)) & 1023u);
-  unsigned char* ring = smem + kTcSlots * slot_bytes + kTcBBytes;  // after a B-sized gap
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + kTcRingBytes);
-  uint64_t* full = bars;                      // [kTcSlots], one arrival per producer
-  uint64_t* empty = bars + kTcSlots;          // [kTcSlots], MMA commit
-  uint64_t* accfull = bars + 2 * kTcSlots;    // [kTcAccs], MMA commit
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcSlots * slot_bytes);
+  uint64_t* tfull = bars;                     // [kTcSlots], the copies' bytes
+  uint64_t* full = bars + kTcSlots;           // [kTcSlots], one arrival per producer
+  uint64_t* empty = bars + 2 * kTcSlots;      // [kTcSlots], MMA commit
+  uint64_t* accfull = bars + 3 * kTcSlots;    // [kTcAccs], MMA commit
   uint64_t* accfree = accfull + kTcAccs;      // [kTcAccs], one arrival per drainer
   uint64_t* done = accfree + kTcAccs;         // error path: all MMAs complete
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kTcBars);
@@ -412,6 +416,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   if (tid == 0) {
     for (int d = 0; d < kTcSlots; ++d) {
+      dev::mbar_init(&tfull[d], 1);
       dev::mbar_init(&full[d], kTcProducers);
       dev::mbar_init(&empty[d], 1);
     }
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const int nk = (int)((wk.k1 - wk.k0) / kTcK);
-  const int64_t kb0 = wk.k0 >> 5;  // first 32-point block of the item
+  const int kb0 = (int)(wk.k0 >> 5);  // first 32-point block of the item
   bool ok = true;
   // set when a role gave up; the others stop at their next wait
   auto failed = [&]() { return *((volatile int*)&s_fail) != 0; };
@@ -436,47 +441,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp < kTcMmaWarp) {
     // ---------------- producers
     const int t = tid;
-    const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
-    auto issue = [&](int s) {
-      if (s < nk) {
-        const uint32_t slot = ring_base + (uint32_t)(((s % kTcRing) * kTcProducers + t) * kTcChunks * 16);
-        const float* a_blk = YT + ((kb0 + s) * lm_pad + wk.lm0) * 32;
-        const float* b_blk = WT + (kb0 + s) * kMaxNodes * 32;
-#pragma unroll
-        for (int c = 0; c < kTcChunks; ++c) {
-          int row, c4;
-          tc_chunk(c, t, row, c4);
-          cp_async16(slot + c * 16, (c < kTcAChunks ? a_blk : b_blk) + row * 32 + c4 * 4);
-        }
-      }
-      cp_async_commit();  // one group per stage, empty past the end
-    };
-#pragma unroll
-    for (int s = 0; s < kTcRing; ++s) issue(s);
     for (int s = 0; s < nk; ++s) {
       const int d = s % kTcSlots;
-      cp_async_wait<kTcRing - 1>();  // this thread's chunks of stage s have landed
-      const float4* mine = reinterpret_cast<const float4*>(ring + ((s % kTcRing) * kTcProducers + t) * kTcChunks * 16);
-      if (s >= kTcSlots && (failed() || !dev::mbar_spin(&empty[d], (unsigned)((s / kTcSlots - 1) & 1), budget))) {
+      if (failed() || !dev::mbar_spin(&tfull[d], (unsigned)((s / kTcSlots) & 1), budget)) {
         ok = false;
         break;
       }
       unsigned char* sa = smem + d * slot_bytes;
       unsigned char* sb = sa + S * kTcABytes;
 #pragma unroll
-      for (int c = 0; c < kTcChunks; ++c) {
-        int row, c4;
-        tc_chunk(c, t, row, c4);
-        const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c4 ^ (row & 7)) << 4);
-        const float4 raw = mine[c];
-        if (c < kTcAChunks) tc_store_split<S>(sa, kTcABytes, off, raw);
-        else tc_store_split<S>(sb, kTcBBytes, off, raw);
-      }
-      issue(s + kTcRing);  // the ring slot just read is refilled kTcRing stages ahead
+      for (int c = 0; c < kTcAChunks; ++c) tc_term_pass<S>(sa, kTcABytes, (c * kTcProducers + t) * 16);
+#pragma unroll
+      for (int c = 0; c < kTcChunks - kTcAChunks; ++c) tc_term_pass<S>(sb, kTcBBytes, (c * kTcProducers + t) * 16);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full[d]);
     }
-    cp_async_wait<0>();  // no copy may land after the CTA exits
+  } else if (warp == kTcTmaWarp) {
+    // ---------------- tensor copies
+    if (lane == 0) {
+      int issued = 0;
+      for (int s = 0; s < nk; ++s) {
+        const int d = s % kTcSlots;
+        if (s >= kTcSlots &&
+            (failed() || !dev::mbar_spin(&empty[d], (unsigned)((s / kTcSlots - 1) & 1), budget))) {
+          ok = false;
+          break;
+        }
+        unsigned char* sa = smem + d * slot_bytes;
+        dev::mbar_expect_tx(&tfull[d], kTcABytes + kTcBBytes);
+        tma_load_2d(sa, &tmA, 0, (kb0 + s) * lm_pad + wk.lm0, &tfull[d]);
+        tma_load_2d(sa + S * kTcABytes, &tmB, 0, (kb0 + s) * kMaxNodes, &tfull[d]);
+        issued = s + 1;
+      }
+      // no copy may land after the CTA exits: when any role gave up, wait
+      // (bounded) for the last copy issued into each slot
+      if (!ok || failed())
+        for (int s = issued - 1; s >= 0 && s >= issued - kTcSlots; --s)
+          dev::mbar_spin(&tfull[s % kTcSlots], (unsigned)((s / kTcSlots) & 1), dev::kDrainBudget);
+    }
   } else if (warp == kTcMmaWarp) {
     // ---------------- MMA issuer
     if (lane == 0) {
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   } else {
     // ---------------- drainers
-    const int quarter = warp & 3, half = (warp - kTcMmaWarp - 1) >> 2;
+    const int quarter = warp & 3, half = (warp - kTcTmaWarp - 1) >> 2;
     double acc[32];  // this thread's lm row and 32 of the 64 node columns
 #pragma unroll
     for (int i = 0; i < 32; ++i) acc[i] = 0.0;
@@ -548,12 +550,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
 }
 
-// Dynamic shared memory of one CTA (one CTA per SM: the 256 TMEM columns
-// always fit and tcgen05.alloc never waits).
 template <int S>
 constexpr size_t tc_smem_bytes() {
-  return 1024 /* alignment slack */ + kTcSlots * (size_t)S * (kTcABytes + kTcBBytes) + kTcBBytes /* gap */ +
-         kTcRingBytes + sizeof(uint64_t) * kTcBars + 16;
+  return 1024 /* alignment slack */ + kTcSlots * (size_t)S * (kTcABytes + kTcBBytes) + sizeof(uint64_t) * kTcBars + 16;
+}
+
+// Tensor map of a point-blocked FP32 operand viewed as rows of 32 floats
+// (128 bytes): rows x 32, copied in boxes of box_rows x 32 with the 128-byte
+// swizzle of the tensor-core tiles.  The encoder comes from the driver
+// through the runtime's entry-point query, so the library links no libcuda.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+CUtensorMap tf32_tile_map(const void* base, uint64_t rows, uint32_t box_rows) {
+  static EncodeTiledFn encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    CRAB_CUDA_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    require(q == cudaDriverEntryPointSuccess && fn, "the driver has no cuTensorMapEncodeTiled");
+    return reinterpret_cast<EncodeTiledFn>(fn);
+  }();
+  require(((uintptr_t)base & 15u) == 0, "tensor-map base must be 16-byte aligned");
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {32, rows};
+  const cuuint64_t strides[1] = {32 * sizeof(float)};
+  const cuuint32_t box[2] = {32, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(CRAB_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return map;
 }
 
 // ---- fused moment GEMM: Y_lm generated by the producer warps ----
@@ -727,11 +754,10 @@ __device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
 template <int E, int S, int PPT>
 __device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, int col, const double (&v)[PPT]) {
   const uint32_t off = fu_swz<E>(r, col);
-  if (E == 0) {
+  if (E == 0) {  // the terms of k_mp_moments_tc: raw h with S = 2 (read truncated), rounded h with S = 1
     const float f = (float)v[0];
-    const float h = tf32_rna(f);
-    *reinterpret_cast<float*>(sa + off) = h;
-    if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - h);
+    *reinterpret_cast<float*>(sa + off) = S == 2 ? f : tf32_rna(f);
+    if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - tf32_trunc(f));
   } else if (PPT == 1) {
     const float f = (float)v[0];
     const uint16_t h = bf16_rn(f);
@@ -984,10 +1010,9 @@ __global__ void k_mp_prep_fused(const double* __restrict__ pts, const int32_t* _
     }
     const float f = (float)v;
     const uint32_t off = fu_swz<E>(b, k);
-    if (E == 0) {
-      const float h = tf32_rna(f);
-      *reinterpret_cast<float*>(blk + off) = h;
-      if (S == 2) *reinterpret_cast<float*>(blk + kTcBBytes + off) = tf32_rna(f - h);
+    if (E == 0) {  // the terms of k_mp_moments_tc
+      *reinterpret_cast<float*>(blk + off) = S == 2 ? f : tf32_rna(f);
+      if (S == 2) *reinterpret_cast<float*>(blk + kTcBBytes + off) = tf32_rna(f - tf32_trunc(f));
     } else {
       const uint16_t h = bf16_rn(f);
       *reinterpret_cast<uint16_t*>(blk + off) = h;
@@ -1712,12 +1737,14 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
       k_mp_moments<float><<<(unsigned)work.size(), 256, 0, s>>>((const float*)d_YT, (const float*)d_WT, n_pad,
                                                                  lm_pad, d_work, d_part);
     } else {
+      const CUtensorMap tmA = tf32_tile_map(d_YT, (uint64_t)(n_pad / kTcK) * (uint64_t)lm_pad, kGemmM);
+      const CUtensorMap tmB = tf32_tile_map(d_WT, (uint64_t)(n_pad / kTcK) * kMaxNodes, kMaxNodes);
 #define CRAB_TC(SS)                                                                                               \
   if (tc_terms == SS) {                                                                                           \
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_mp_moments_tc<SS>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                          (int)tc_smem_bytes<SS>()));                                              \
     k_mp_moments_tc<SS><<<(unsigned)work.size(), kTcThreads, tc_smem_bytes<SS>(), s>>>(                           \
-        (const float*)d_YT, (const float*)d_WT, n_pad, lm_pad, d_work, d_part, d_status, ctx->wait_budget);          \
+        tmA, tmB, lm_pad, d_work, d_part, d_status, ctx->wait_budget);                                              \
   }
       CRAB_TC(1)
       CRAB_TC(2)
