@@ -263,11 +263,10 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 // ---- tensor-core moment GEMM (tcgen05, TF32 operands split into terms) ----
 //
 // The same product part[w] = YT-tile . WT-tile^T (128 lm rows x 64 nodes over
-// the item's points) on the 5th-generation tensor cores, with TF32 terms:
-//   S = 1: h h'                  h = x rounded to TF32 (relative error ~5e-4)
-//   S = 2: h h' + h m' + m h'    h = x truncated to TF32 (the tensor core
-//          reads a raw FP32 operand so), m = x - h rounded to TF32
-//          (relative error ~5e-7)
+// the item's points) on the 5th-generation tensor cores, with TF32 terms
+// (h = x rounded to TF32, m = x - h rounded to TF32):
+//   S = 1: h h'                  (relative error ~5e-4)
+//   S = 2: h h' + h m' + m h'    (relative error ~5e-7)
 // The S = 2 error is set by the tensor core's FP32 accumulation, which rounds
 // toward zero (about 2^-24 of the accumulator per MMA), so a TMEM accumulator
 // covers one 32-point stage only and is then drained into f64 registers.
@@ -280,10 +279,10 @@ __global__ void __launch_bounds__(256) k_mp_moments(const E* __restrict__ YT, co
 //    at (r/8)*1024 + (r%8)*128, 16-byte chunk c at position c ^ (r%8)), the
 //    K-major layout the MMA reads; the copies complete on tfull[d];
 //  * producers, warps 0-7: wait tfull[d]; each thread takes six 16-byte
-//    chunks of the tiles and, for S = 2, writes their m terms at the same
-//    offsets of the second-term areas (the h terms are the copied values),
-//    for S = 1 rounds the values in place; then fences the generic-proxy
-//    writes for the tensor core and arrives on full[d];
+//    chunks of the tiles, rounds them to TF32 in place (h) and, for S = 2,
+//    writes their m terms at the same offsets of the second-term areas; then
+//    fences the generic-proxy writes for the tensor core and arrives on
+//    full[d];
 //  * MMA issuer, warp 8 lane 0: waits full[d] and accfree[a], issues
 //    tcgen05.mma (M = 128, N = 64, K = 8, descriptor start +32 B per K step)
 //    into TMEM accumulator a and commits to empty[d] and accfull[a];
@@ -357,9 +356,6 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-// x truncated to TF32 (the 13 low mantissa bits cleared), as the tensor core
-// reads a raw FP32 operand of kind::tf32.
-__device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 // 2D tensor copy of one box into shared memory, completing on an mbarrier
 // (no multicast: the box lies in this GPU's memory and lands in this CTA).
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
@@ -371,18 +367,19 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // The producers' pass over one 16-byte chunk at byte offset off of a copied
-// tile (part_bytes: one term's tile size): S = 2 writes the m terms of the
-// four values into the second-term tile, S = 1 rounds them to TF32 in place.
+// tile (part_bytes: one term's tile size): the four values rounded to TF32 in
+// place (h), and for S = 2 their m terms into the second-term tile.  A
+// truncated h (the copied values as the tensor core reads them) would save
+// the in-place store but bias the dropped m m' product by about 2^-22 of the
+// product, since m then has the sign of x.
 template <int S>
 __device__ __forceinline__ void tc_term_pass(unsigned char* __restrict__ base, int part_bytes, int off) {
   const float4 x = *reinterpret_cast<const float4*>(base + off);
-  if (S == 2) {
+  const float4 h = make_float4(tf32_rna(x.x), tf32_rna(x.y), tf32_rna(x.z), tf32_rna(x.w));
+  *reinterpret_cast<float4*>(base + off) = h;
+  if (S == 2)
     *reinterpret_cast<float4*>(base + part_bytes + off) =
-        make_float4(tf32_rna(x.x - tf32_trunc(x.x)), tf32_rna(x.y - tf32_trunc(x.y)), tf32_rna(x.z - tf32_trunc(x.z)),
-                    tf32_rna(x.w - tf32_trunc(x.w)));
-  } else {
-    *reinterpret_cast<float4*>(base + off) = make_float4(tf32_rna(x.x), tf32_rna(x.y), tf32_rna(x.z), tf32_rna(x.w));
-  }
+        make_float4(tf32_rna(x.x - h.x), tf32_rna(x.y - h.y), tf32_rna(x.z - h.z), tf32_rna(x.w - h.w));
 }
 
 template <int S>
@@ -754,10 +751,11 @@ __device__ __forceinline__ void fu_next_m(int m, const double4& k4, FuWalk& w) {
 template <int E, int S, int PPT>
 __device__ __forceinline__ void fu_emit(unsigned char* __restrict__ sa, int r, int col, const double (&v)[PPT]) {
   const uint32_t off = fu_swz<E>(r, col);
-  if (E == 0) {  // the terms of k_mp_moments_tc: raw h with S = 2 (read truncated), rounded h with S = 1
+  if (E == 0) {  // the terms of k_mp_moments_tc
     const float f = (float)v[0];
-    *reinterpret_cast<float*>(sa + off) = S == 2 ? f : tf32_rna(f);
-    if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - tf32_trunc(f));
+    const float h = tf32_rna(f);
+    *reinterpret_cast<float*>(sa + off) = h;
+    if (S == 2) *reinterpret_cast<float*>(sa + kTcABytes + off) = tf32_rna(f - h);
   } else if (PPT == 1) {
     const float f = (float)v[0];
     const uint16_t h = bf16_rn(f);
@@ -1011,8 +1009,9 @@ __global__ void k_mp_prep_fused(const double* __restrict__ pts, const int32_t* _
     const float f = (float)v;
     const uint32_t off = fu_swz<E>(b, k);
     if (E == 0) {  // the terms of k_mp_moments_tc
-      *reinterpret_cast<float*>(blk + off) = S == 2 ? f : tf32_rna(f);
-      if (S == 2) *reinterpret_cast<float*>(blk + kTcBBytes + off) = tf32_rna(f - tf32_trunc(f));
+      const float h = tf32_rna(f);
+      *reinterpret_cast<float*>(blk + off) = h;
+      if (S == 2) *reinterpret_cast<float*>(blk + kTcBBytes + off) = tf32_rna(f - h);
     } else {
       const uint16_t h = bf16_rn(f);
       *reinterpret_cast<uint16_t*>(blk + off) = h;
