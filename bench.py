@@ -649,11 +649,11 @@ def run_ours(args, rank, world, local):
     import crabsaxs_b200 as cs
     from crabsaxs_b200 import _native as N
 
-    dist = Dist(world, "nccl")
-    if world > 1:
+    if world > 1:  # this rank's GPU first, so the NCCL group binds to it
         import torch
 
         torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
     eng = cs.Engine(local)
     lib = N.lib
     peak = C.c_double()
