@@ -138,10 +138,23 @@ static bool excluded_zero(const AtomClass& c, bool implicit) {
 }
 
 TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites) {
+  TypedAtoms t;
+  type_atoms_into(st, implicit, need, sites, t);
+  return t;
+}
+
+TypedAtoms& typed_scratch(crab_ctx* ctx) {
+  if (!ctx->typed_scratch) ctx->typed_scratch = std::make_shared<TypedAtoms>();
+  return *ctx->typed_scratch;
+}
+
+void type_atoms_into(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites,
+                     TypedAtoms& t) {
   // Classes are (element 0..14, united-atom group -1..13), numbered in
   // (element, group) order; a direct 15 x 15 table replaces a map lookup per
   // atom.  Pass 1 finds the classes present and the kept count; pass 2 fills.
-  TypedAtoms t;
+  t.cls.clear();
+  t.T = 0;
   constexpr int kE = CRAB_EL_OTHER + 1, kG = 15;
   bool drop[kE][kG];
   for (int e = 0; e < kE; ++e)
@@ -195,7 +208,6 @@ TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const 
     t.src[k] = -1;
   }
   t.T = (int)t.cls.size();
-  return t;
 }
 
 void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const crab_solvent* solvent, bool implicit,
@@ -257,11 +269,12 @@ void debye_basis(crab_ctx* ctx, const crab_struct* st, const double* q, int64_t 
     TraceScope tg("hydration_sites");
     g = hydration_sites(ctx, st, s);
   }
-  TypedAtoms t;
+  TypedAtoms& t = typed_scratch(ctx);
   std::vector<double> V, E, H;
   {
     TraceScope tt("type_atoms+tables");
-    t = type_atoms(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &g.sites : nullptr);
+    type_atoms_into(st, implicit, grid ? TermSet::SolventGrid : TermSet::SolventAnalytic, grid ? &g.sites : nullptr,
+                    t);
     amplitude_tables(t, q, nq, &s, implicit, g.voxel_volume, V, E, H);
   }
   Partials P = partials_for(ctx, t, q, nq, fp64, grid ? &g : nullptr, shard, n_shards);

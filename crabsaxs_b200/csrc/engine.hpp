@@ -81,6 +81,7 @@ struct HostBuf {
 
 namespace crab {
 struct GridMemo;
+struct TypedAtoms;
 }
 
 struct crab_ctx {
@@ -121,6 +122,13 @@ struct crab_ctx {
   // Site list of the last hydration-grid size query (sites == NULL), kept
   // for the fill call that follows it with the same structure and options.
   std::shared_ptr<crab::GridMemo> grid_memo;
+  // Host scratch of the one-structure calls, kept across calls so that their
+  // multi-megabyte arrays are not mapped and faulted in afresh each time
+  // (calls on a context are serialised): the typed atoms of the Debye and
+  // multipole paths and the multipole's per-point radius, segment and group.
+  std::shared_ptr<crab::TypedAtoms> typed_scratch;
+  std::vector<double> mp_r;
+  std::vector<int32_t> mp_seg_of, mp_group_of;
   uint64_t grid_builds = 0;  // hydration-grid builds on this context (each reuses the "grid." device slots)
 
   void* dev(const std::string& name, size_t bytes);

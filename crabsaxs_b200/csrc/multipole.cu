@@ -1533,7 +1533,8 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   // atoms of this rank's moments (all of them unless sharded)
   const int64_t own0 = n * in.shard / in.n_shards, own1 = n * (in.shard + 1) / in.n_shards;
   // geometry relative to the structure centroid (spherical.rs:165-199)
-  std::vector<double> r(n);
+  std::vector<double>& r = ctx->mp_r;  // the context's scratch: no fresh pages per call
+  r.resize((size_t)n);
   double R = 0.0, qmax = 0.0;
   for (int64_t i = 0; i < n; ++i) {
     const double dx = t.xyz[3 * i] - in.centre[0], dy = t.xyz[3 * i + 1] - in.centre[1],
@@ -1546,7 +1547,10 @@ void multipole_run(crab_ctx* ctx, const MpInput& in, const double* q, int64_t nq
   const RadialBasis B = radial_basis(R, qmax);
   const int S = B.S, nb = B.nb, G = T * S;
   // group = type * S + segment; points sorted by group, padded per group
-  std::vector<int32_t> seg_of(n), group_of(n);
+  std::vector<int32_t>& seg_of = ctx->mp_seg_of;  // written for the owned points before any read
+  std::vector<int32_t>& group_of = ctx->mp_group_of;
+  seg_of.resize((size_t)n);
+  group_of.resize((size_t)n);
   std::vector<int64_t> count(G, 0);
   for (int64_t i = own0; i < own1; ++i) {
     seg_of[i] = std::min(S - 1, (int)(r[i] / R * S));
@@ -1919,12 +1923,12 @@ void multipole_intensity_impl(crab_ctx* ctx, const crab_struct* st, const double
     return;
   }
   TraceScope trace("multipole_intensity");
-  TypedAtoms t;
+  TypedAtoms& t = typed_scratch(ctx);
   MpInput in;
   std::vector<double> V, E, H;
   {
     TraceScope tt("mp_type_atoms+tables");
-    t = type_atoms(st, implicit, TermSet::Vacuum, nullptr);
+    type_atoms_into(st, implicit, TermSet::Vacuum, nullptr, t);
     in.t = &t;
     double rmax;
     centre_and_rmax(st, in.centre, &rmax);

@@ -27,6 +27,11 @@ struct TypedAtoms {
   int T = 0;
 };
 TypedAtoms type_atoms(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites);
+// The same into t, reusing its arrays' capacity.
+void type_atoms_into(const crab_struct* st, bool implicit, TermSet need, const std::vector<double>* sites,
+                     TypedAtoms& t);
+// The context's reusable TypedAtoms (one per context; one user per call).
+TypedAtoms& typed_scratch(crab_ctx* ctx);
 
 // Per-type Debye amplitude tables [T][nq] (no occupancy).  solvent == NULL
 // means vacuum form factors only.
