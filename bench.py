@@ -58,7 +58,8 @@ FLUSH_BYTES = 256 << 20
 def _variant_name(v: int) -> str:
     """Autotuner variant code Q*16 + jb; jb >= 8 is the q-packed kernel with (jb-8) % 4 chains,
     jb >= 12 its build for three CTAs per SM; jb 5, 6, 7, 3 the q-packed kernel with the weight
-    folded into the recurrence (1 chain / 2 CTAs, 2 / 2, 1 / 3, 1 / 4); jb 14, 15 the folded
+    folded into the recurrence (1 chain / 2 CTAs, 2 / 2, 1 / 3, 1 / 4); jb 11 the folded kernel with
+    two chains per pair (q points 4n, 4n+1 and 4n+2, 4n+3); jb 14, 15 the folded
     recurrence with the set-up in its own warpgroup (1 or 2 chains per recurrence thread), jb 12
     the same with one recurrence warpgroup per q block, three blocks per work item."""
     q, jb = int(v) // 16, int(v) % 16
@@ -66,6 +67,8 @@ def _variant_name(v: int) -> str:
         return f"Q{q}xJ{jb - 13}-split"
     if jb == 12:
         return f"Q{q}x3blocks-split"
+    if jb == 11:
+        return f"Q{q}xJ1pq-fold-2chain-2cta"
     folded = {5: (1, 2), 6: (2, 2), 7: (1, 3), 3: (1, 4)}
     if jb in folded:
         chains, ctas = folded[jb]

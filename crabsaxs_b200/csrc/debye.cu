@@ -51,6 +51,11 @@ constexpr int kDenser = 4;
 // q-packed with the weight folded into the recurrence state (pair_setup_pq_folded):
 // one chain at two CTAs per SM, two chains at two, one chain at three, one at four
 constexpr int kFolded1 = 5, kFolded2 = 6, kFolded1x3 = 7, kFolded1x4 = 3;
+// folded, two packed chains per pair (q points 4n, 4n+1 and 4n+2, 4n+3),
+// two CTAs per SM; plans whose half step angle Δr/2 exceeds kMax2cHalfAngle
+// run the one-chain build kFolded1 of the same length instead
+constexpr int kFolded2c = 11;
+constexpr double kMax2cHalfAngle = 0.2;
 // set-up and recurrences in separate warpgroups (k_pair_split), one or two
 // chains per recurrence thread
 constexpr int kSplit1 = 14, kSplit2 = 15;
@@ -180,6 +185,62 @@ __device__ __forceinline__ void pair_setup_pq_folded(const float4& ai, const flo
   pair_setup_pq(ai, aj, wj, qp, wide, u2, nl2, s2, d2);
   asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(s2) : "l"(u2));
   asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(d2) : "l"(u2));
+}
+
+// Two packed chains per pair, each stepping 4Δ: chain X holds the q points
+// (4n, 4n+1) of the block and chain Y (4n+2, 4n+3), so a thread has two
+// independent recurrences in flight with the registers of one.  With
+// φ = q0 r, g = Δr, s1, c1 = sin, cos g (as in pair_seed_pq) and
+// s2 = sin 2g = 2 s1 c1, c2 = cos 2g = 1 - 2 s1²:
+//   s = sin φ, sin(φ+g), sin(φ+2g), sin(φ+3g) by angle addition,
+//   d = s - sin(· - 4g) = 2 s2 cos(· - 2g), i.e. 2 s2 times
+//       cos(φ-2g), cos(φ-g), cos φ, cos(φ+g),
+//   λ' = 4 sin²(2g).
+// The host runs this build only while g = Δr <= 0.4 (half step angle at most
+// kMax2cHalfAngle), so the chains' step angle 4g stays at most 1.6 rad, where
+// the difference form of the recurrence loses nothing (cos 2g > 0.69); s1, c1
+// come from their Taylor series, to g^7 and g^6 while g <= 0.25 (wide == 0,
+// truncation below 4e-10), else to g^9 and g^8 (below 3e-11).
+__device__ __forceinline__ void pair_setup_pq2c_folded(const float4& ai, const float4& aj, float wj, const float4& qp,
+                                                       int wide, unsigned long long& nl2, unsigned long long& sx,
+                                                       unsigned long long& dx, unsigned long long& sy,
+                                                       unsigned long long& dy) {
+  float r, u;
+  pair_geom(ai, aj, wj, r, u);
+  const float phi = fmaf(qp.x, r, qp.y * r);
+  const float g = 2.0f * fmaf(qp.z, r, qp.w * r);  // Δr
+  float S, C;
+  sincos_seed(phi, &S, &C);
+  const float g2 = g * g;
+  float ps, pc;
+  if (wide) {  // g <= 0.4: two more terms
+    ps = fmaf(g2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+    ps = fmaf(g2, ps, 1.0f / 120.0f);
+    pc = fmaf(g2, 1.0f / 40320.0f, -1.0f / 720.0f);
+    pc = fmaf(g2, pc, 1.0f / 24.0f);
+  } else {
+    ps = fmaf(g2, -1.0f / 5040.0f, 1.0f / 120.0f);
+    pc = fmaf(g2, -1.0f / 720.0f, 1.0f / 24.0f);
+  }
+  ps = fmaf(g2, ps, -1.0f / 6.0f);
+  const float s1 = fmaf(g * g2, ps, g);
+  pc = fmaf(g2, pc, -0.5f);
+  const float c1 = fmaf(g2, pc, 1.0f);
+  const float s2 = 2.0f * s1 * c1, c2 = fmaf(-2.0f * s1, s1, 1.0f);
+  const float sp1 = fmaf(S, c1, C * s1);   // sin(φ+g)
+  const float cp1 = fmaf(C, c1, -S * s1);  // cos(φ+g)
+  const float cm1 = fmaf(C, c1, S * s1);   // cos(φ-g)
+  const float t = 2.0f * s2;
+  const unsigned long long u2 = pack2(u, u);
+  nl2 = pack2(-t * t, -t * t);
+  sx = pack2(S, sp1);
+  sy = pack2(fmaf(S, c2, C * s2), fmaf(sp1, c2, cp1 * s2));
+  dx = pack2(t * fmaf(C, c2, S * s2), t * cm1);
+  dy = pack2(t * C, t * cp1);
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(sx) : "l"(u2));
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(dx) : "l"(u2));
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(sy) : "l"(u2));
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(dy) : "l"(u2));
 }
 
 // Work item: (i tile, first j tile, end j tile, q block); items are taken
@@ -336,13 +397,14 @@ __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2],
   __syncthreads();
 }
 
-template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)), bool FOLD = false>
+template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)), bool FOLD = false, int CH = 1>
 __global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                    int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
                    int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
                    const int64_t* __restrict__ work_out, int budget) {
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
+  static_assert(CH == 1 || (CH == 2 && JB == 1 && FOLD && Q % 4 == 0), "two chains per pair: folded, one pair");
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
@@ -410,6 +472,24 @@ __global__ void __launch_bounds__(kThreads, OCC)
         break;
       }
       const bool diag = (jt == it);
+      if constexpr (CH == 2) {
+#pragma unroll 1
+        for (int j = 0; j < kTile; ++j) {
+          const float4 aj = sj[buf][j];
+          const float wj = (diag && j <= tid) ? 0.0f : aj.w;
+          unsigned long long nl2, sx, dx, sy, dy;
+          pair_setup_pq2c_folded(ai, aj, wj, qp, wide >= 1, nl2, sx, dx, sy, dy);
+#pragma unroll
+          for (int n = 0; n < Q / 4; ++n) {
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc2[2 * n]) : "l"(sx));
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc2[2 * n + 1]) : "l"(sy));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(dx) : "l"(nl2), "l"(sx));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(dy) : "l"(nl2), "l"(sy));
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(sx) : "l"(dx));
+            asm("add.rn.f32x2 %0, %0, %1;" : "+l"(sy) : "l"(dy));
+          }
+        }
+      } else
 #pragma unroll 1
       for (int j = 0; j < kTile; j += JB) {
         unsigned long long u2[JB], nl2[JB], s2[JB], d2[JB];
@@ -978,15 +1058,15 @@ void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const i
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
-template <int Q, int JB, int OCC, bool FOLD = false>
+template <int Q, int JB, int OCC, bool FOLD = false, int CH = 1>
 void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                     int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
                     int* status, int* next_work, const int64_t* work_out, int budget) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC, FOLD>, kThreads, 0));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC, FOLD, CH>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
-  k_pair_fp32_pq<Q, JB, OCC, FOLD><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
+  k_pair_fp32_pq<Q, JB, OCC, FOLD, CH><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
                                                         status, next_work, work_out, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
@@ -1232,7 +1312,7 @@ void make_work_segments(const PairPlan& P, int n_qblocks, int run, std::vector<i
 // 168, whose fewer seeds per pair outweigh the lower occupancy: 3 x 168 for
 // 500 q and 2 x 150 for 300 q are 1.3 % and 3 % faster than 4 x 126 and
 // 3 x 100; two chains below Q = 100), with the weight folded in where that
-// build exists.
+// build exists, and two chains per pair at 168.
 int2 default_variant(const std::vector<double>& q) {
   int bestQ = 64;
   long best_cost = -1;
@@ -1249,8 +1329,9 @@ int2 default_variant(const std::vector<double>& q) {
   if (bestQ == 128) return make_int2(bestQ, 1 + kPackedQ + kDenser);
   // 75 or 84 packed accumulators: two CTAs per SM; at Q = 150 two chains per
   // thread (1.4 % faster on the 300-q ensemble pass, 1.7 % at 500 q), at 168 one
+  // 168: two chains per pair (4.8 % faster than one at 500 q)
   if (bestQ == 150) return make_int2(bestQ, kFolded2);
-  if (bestQ == 168) return make_int2(bestQ, kFolded1);
+  if (bestQ == 168) return make_int2(bestQ, kFolded2c);
   const bool packed = bestQ == 64 || bestQ == 96;
   return make_int2(bestQ, packed ? 2 + kPackedQ : 2);
 }
@@ -1279,6 +1360,7 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   // whose step is 2h (1); otherwise both use short polynomials (0)
   const double hmax = max_half * (P.L.extent + 1.0);
   P.wide = hmax > 0.8 ? 2 : (hmax > 0.125 ? 1 : 0);
+  P.hmax = hmax;
   // work items name a q block, or for k_pair_split3 a group of kS3Blocks
   const int item_blocks = jb == kSplit3 ? (P.n_qblocks + kS3Blocks - 1) / kS3Blocks : P.n_qblocks;
   std::vector<int4> work;
@@ -1452,6 +1534,22 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
     CRAB_LAUNCH_PQF(100, 1, 3, kFolded1x3)
     CRAB_LAUNCH_PQF(84, 1, 4, kFolded1x4)
 #undef CRAB_LAUNCH_PQF
+    // two chains per pair; a plan with a larger step angle runs the one-chain
+    // build of the same length
+#define CRAB_LAUNCH_PQ2C(QQ)                                                                                    \
+  if (P.Q == QQ && P.jb == kFolded2c) {                                                                          \
+    if (P.hmax > kMax2cHalfAngle)                                                                                \
+      launch_fp32_pq<QQ, 1, 2, true>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,    \
+                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,      \
+                                     ctx->wait_budget);                                                           \
+    else                                                                                                         \
+      launch_fp32_pq<QQ, 1, 2, true, 2>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work,          \
+                                        P.d_qpar, P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next,       \
+                                        P.d_work_out, ctx->wait_budget);                                          \
+    launched = true;                                                                                             \
+  }
+    CRAB_LAUNCH_PQ2C(168)
+#undef CRAB_LAUNCH_PQ2C
 #define CRAB_LAUNCH_SPLIT(QQ, JJ, CODE)                                                                          \
   if (P.Q == QQ && P.jb == CODE) {                                                                               \
     launch_split<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
@@ -1613,7 +1711,7 @@ static const int kLaunchable[][2] = {{8, 2},   {16, 2}, {32, 2}, {48, 2}, {64, 2
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
                                      {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
                                      {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
-                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4},
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}, {168, kFolded2c},
                                      {126, kSplit1}, {126, kSplit2}, {100, kSplit1}, {100, kSplit2},
                                      {84, kSplit3}, {100, kSplit3}};
 
@@ -1641,7 +1739,7 @@ int pair_plan_autotune(crab_ctx* ctx, PairPlan& P, int* variants, double* ms_out
                                      {128, 1 + kPackedQ + kDenser}, {100, 1 + kPackedQ + kDenser},
                                      {126, 1 + kPackedQ + kDenser}, {150, 1 + kPackedQ}, {168, 1 + kPackedQ},
                                      {168, kFolded1}, {150, kFolded1}, {168, kFolded2}, {150, kFolded2},
-                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4},
+                                     {128, kFolded2}, {126, kFolded1x3}, {100, kFolded1x3}, {84, kFolded1x4}, {168, kFolded2c},
                                      {126, kSplit1}, {126, kSplit2}, {100, kSplit1}, {100, kSplit2},
                                      {84, kSplit3}, {100, kSplit3}};
   int bestQ = P.Q, bestJ = P.jb, n = 0;

@@ -233,6 +233,7 @@ struct PairPlan {
   int64_t nq = 0;
   std::vector<double> q;
   int n_pairs = 0, Q = 0, jb = 2, n_qblocks = 0, n_work = 0, wide = 0;
+  double hmax = 0.0;  // largest half step angle Δr/2 of the plan's q blocks (rad)
   std::vector<void*> owned;
   std::vector<void*> qcfg;  // q-block and work-list buffers (rebuilt when Q changes)
   bool pooled = false;      // buffers from the context pool (a plan that lives inside one call)

@@ -248,7 +248,10 @@ int crab_pair_plan_run(crab_ctx* ctx, crab_pair_plan* plan, int32_t repeats, int
  * registers hold two consecutive q points, with (JB-8) % 4 independent chains,
  * built for three CTAs per SM when JB >= 12; JB = 5, 6, 7, 3: the q-packed
  * kernel with the pair weight folded into the recurrence state, with 1, 2,
- * 1, 1 chains at 2, 2, 3, 4 CTAs per SM; JB = 14, 15: the folded recurrence
+ * 1, 1 chains at 2, 2, 3, 4 CTAs per SM; JB = 11: the folded kernel with two
+ * chains per pair (q points 4n, 4n+1 and 4n+2, 4n+3, each stepping 4 q
+ * steps), two CTAs per SM, run as JB = 5 on plans whose step angle exceeds
+ * 0.25 rad; JB = 14, 15: the folded recurrence
  * with the per-pair set-up in a warpgroup of its own that feeds two
  * recurrence warpgroups through shared memory, 1 or 2 chains per thread, one
  * CTA per SM; JB = 12: the same split with one recurrence warpgroup for each

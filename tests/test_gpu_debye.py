@@ -305,16 +305,17 @@ def test_lattice_plan_matches_fp64_20k(engine):
 
 
 # Every kernel variant the plan can dispatch (Q*16 + jb; jb >= 8: q-packed, jb >= 12: 3 CTAs/SM;
-# jb 5, 6, 7, 3: q-packed with the weight folded into the recurrence, 1 or 2 chains, 2 to 4 CTAs/SM).
+# jb 5, 6, 7, 3: q-packed with the weight folded into the recurrence, 1 or 2 chains, 2 to 4 CTAs/SM;
+# jb 11: folded with two chains per pair, q points 4n, 4n+1 and 4n+2, 4n+3, the one-chain build on wide plans).
 ALL_VARIANTS = [8 * 16 + 2, 16 * 16 + 2, 32 * 16 + 2, 48 * 16 + 2, 64 * 16 + 2, 96 * 16 + 2, 128 * 16 + 2,
                 64 * 16 + 4, 96 * 16 + 4, 64 * 16 + 10, 96 * 16 + 10, 128 * 16 + 9, 128 * 16 + 10, 128 * 16 + 13,
                 100 * 16 + 13, 126 * 16 + 13, 150 * 16 + 9, 168 * 16 + 9,
                 168 * 16 + 5, 150 * 16 + 5, 168 * 16 + 6, 150 * 16 + 6, 128 * 16 + 6, 126 * 16 + 7, 100 * 16 + 7,
                 84 * 16 + 3, 126 * 16 + 14, 126 * 16 + 15, 100 * 16 + 14, 100 * 16 + 15,
-                84 * 16 + 12, 100 * 16 + 12]
+                84 * 16 + 12, 100 * 16 + 12, 168 * 16 + 11]
 
 
-@pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "wide"])
+@pytest.mark.parametrize("qkind", ["uniform", "nonuniform", "coarse", "wide"])
 def test_every_kernel_variant_matches_fp64(engine, qkind):
     import ctypes as C
 
@@ -327,6 +328,8 @@ def test_every_kernel_variant_matches_fp64(engine, qkind):
         q = np.linspace(0.001, 0.5, 333)
     elif qkind == "nonuniform":
         q = np.concatenate([np.linspace(0.0, 0.1, 57), np.linspace(0.102, 0.6, 141), [0.65, 0.7, 0.8]])
+    elif qkind == "coarse":  # half step angle about 0.19 rad over the 63 Å extent: near the largest
+        q = np.linspace(0.01, 1.202, 201)  # that the two-chain build takes (its chains step 1.5 rad)
     else:  # steps of about 0.05 Å⁻¹ over a 70 Å extent: the seed path for the step angle
         q = np.linspace(0.01, 3.0, 61)
     q = np.ascontiguousarray(q)

@@ -41,7 +41,7 @@ def test_pair_kernel_wait_runs_out_then_context_recovers(engine, fresh):
     assert np.array_equal(got, ref) or np.max(np.abs(got - ref) / ref) <= 1e-12
 
 
-@pytest.mark.parametrize("variant", [168 * 16 + 5, 126 * 16 + 13, 126 * 16 + 14, 126 * 16 + 15, 100 * 16 + 15,
+@pytest.mark.parametrize("variant", [168 * 16 + 5, 168 * 16 + 11, 126 * 16 + 13, 126 * 16 + 14, 126 * 16 + 15, 100 * 16 + 15,
                                      84 * 16 + 12])
 def test_every_pair_kernel_family_wait_runs_out_then_recovers(engine, fresh, variant):
     """The folded q-packed kernel, the three-CTA build and the set-up /
