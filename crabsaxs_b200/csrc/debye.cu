@@ -209,8 +209,11 @@ __device__ __forceinline__ void pair_setup_pq2c_folded(const float4& ai, const f
   pair_geom(ai, aj, wj, r, u);
   const float phi = fmaf(qp.x, r, qp.y * r);
   const float g = 2.0f * fmaf(qp.z, r, qp.w * r);  // Δr
-  float S, C;
-  sincos_seed(phi, &S, &C);
+  float S0, C0;
+  sincos_seed(phi, &S0, &C0);
+  // every seed and difference below is linear in (sin φ, cos φ): scaling
+  // these two by u folds the weight into the whole state
+  const float S = u * S0, C = u * C0;
   const float g2 = g * g;
   float ps, pc;
   if (wide) {  // g <= 0.4: two more terms
@@ -231,16 +234,12 @@ __device__ __forceinline__ void pair_setup_pq2c_folded(const float4& ai, const f
   const float cp1 = fmaf(C, c1, -S * s1);  // cos(φ+g)
   const float cm1 = fmaf(C, c1, S * s1);   // cos(φ-g)
   const float t = 2.0f * s2;
-  const unsigned long long u2 = pack2(u, u);
-  nl2 = pack2(-t * t, -t * t);
+  const float nl = -t * t;
+  nl2 = pack2(nl, nl);
   sx = pack2(S, sp1);
   sy = pack2(fmaf(S, c2, C * s2), fmaf(sp1, c2, cp1 * s2));
   dx = pack2(t * fmaf(C, c2, S * s2), t * cm1);
   dy = pack2(t * C, t * cp1);
-  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(sx) : "l"(u2));
-  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(dx) : "l"(u2));
-  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(sy) : "l"(u2));
-  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(dy) : "l"(u2));
 }
 
 // Work item: (i tile, first j tile, end j tile, q block); items are taken

@@ -71,8 +71,13 @@ __device__ __forceinline__ void sincos_small(float h, float* sh, float* ch) {
 // into C1 + C2 + C3 (C1 and C2 carry 12 significant bits, so k·C1 and k·C2
 // are exact for k < 4096), then Taylor polynomials on |y| <= π/4 (truncation
 // below 2e-9) and quadrant selection.  Used for the per-pair seed sin(q0 r).
+// k = nearest integer to x·2/π comes from adding 1.5·2^23 in the same fused
+// multiply-add (the sum's unit is 1, so its low bits are k's quadrant), which
+// keeps the conversions off the pipe the recurrence does not use.
 __device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
-  const float k = rintf(x * 0x1.45f306p-1f);  // x·2/π
+  const float kMagic = 12582912.0f;  // 1.5·2^23
+  const float tk = fmaf(x, 0x1.45f306p-1f, kMagic);  // kMagic + x·2/π, rounded to an integer
+  const float k = tk - kMagic;
   float y = fmaf(-k, 0x1.92p+0f, x);
   y = fmaf(-k, 0x1.fb4p-12f, y);
   y = fmaf(-k, 0x1.4442d2p-24f, y);
@@ -86,7 +91,7 @@ __device__ __forceinline__ void sincos_seed(float x, float* s, float* c) {
   pc = fmaf(y2, pc, 1.0f / 24.0f);
   pc = fmaf(y2, pc, -0.5f);
   const float cy = fmaf(y2, pc, 1.0f);
-  const int qd = __float2int_rn(k) & 3;
+  const int qd = __float_as_int(tk) & 3;
   const float ss = (qd & 1) ? cy : sy;
   const float cc = (qd & 1) ? sy : cy;
   *s = (qd & 2) ? -ss : ss;
