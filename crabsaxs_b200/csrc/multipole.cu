@@ -313,6 +313,14 @@ constexpr int kTcBBytes = kMaxNodes * kTcK * 4;  // 8 KB
 constexpr int kTcBars = 3 * kTcSlots + 2 * kTcAccs + 1;
 // TF32, FP32 accumulate, K-major A and B, N = 64 (bits 17-22, N>>3), M = 128 (bits 24-28, M>>4)
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// the same with N = 128: the hi and lo B terms of a slot as one operand (rows 0-63 and 64-127)
+constexpr uint32_t kTcIdescN128 = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+// TMEM columns of the staged kernel: S = 2 keeps 128 columns per accumulator
+// (hi*hi' in the first 64, the hi*lo' + lo*hi' corrections in the next 64)
+template <int S>
+__host__ __device__ constexpr int tc_tmem_cols() {
+  return S == 2 ? 512 : 256;
+}
 
 __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
@@ -329,11 +337,12 @@ __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
 __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
-__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                       uint32_t idesc = kTcIdesc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -355,6 +364,15 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 // 2D tensor copy of one box into shared memory, completing on an mbarrier
 // (no multicast: the box lies in this GPU's memory and lands in this CTA).
@@ -407,7 +425,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const MpWork wk = work[blockIdx.x];
   if (warp == 0) {
     const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTcTmemCols)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                 "r"(tc_tmem_cols<S>())
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -480,8 +499,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // ---------------- MMA issuer
     if (lane == 0) {
       const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem);
-      constexpr int np = S == 1 ? 1 : 3;  // (A term, B term): hh', hm', mh'
-      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+      constexpr int acc_stride = S == 2 ? 128 : 64;
       for (int s = 0; s < nk; ++s) {
         const int d = s % kTcSlots, a = s % kTcAccs;
         if (failed() || !dev::mbar_spin(&full[d], (unsigned)((s / kTcSlots) & 1), budget) ||
@@ -491,13 +509,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a0 = smem_base + d * slot_bytes, b0 = a0 + S * kTcABytes;
-        const uint32_t acc_cols = tmem + (uint32_t)(a * 64);
+        const uint32_t acc_cols = tmem + (uint32_t)(a * acc_stride);
 #pragma unroll
-        for (int kk = 0; kk < kTcK / 8; ++kk)
-#pragma unroll
-          for (int p = 0; p < np; ++p)
-            tc_mma(acc_cols, tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32),
-                   tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32), (kk || p) ? 1u : 0u);
+        for (int kk = 0; kk < kTcK / 8; ++kk) {
+          if (S == 1) {
+            tc_mma(acc_cols, tc_smem_desc(a0 + kk * 32), tc_smem_desc(b0 + kk * 32), kk ? 1u : 0u);
+          } else {
+            // A_hi against [B_hi; B_lo] (N = 128): hh' in columns 0-63, hm' in 64-127;
+            // then A_lo against B_hi adds mh' to the corrections
+            tc_mma(acc_cols, tc_smem_desc(a0 + kk * 32), tc_smem_desc(b0 + kk * 32), kk ? 1u : 0u, kTcIdescN128);
+            tc_mma(acc_cols + 64u, tc_smem_desc(a0 + kTcABytes + kk * 32), tc_smem_desc(b0 + kk * 32), 1u);
+          }
+        }
         tc_commit(&empty[d]);
         tc_commit(&accfull[a]);
       }
@@ -515,12 +538,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      constexpr int acc_stride = S == 2 ? 128 : 64;
+      const uint32_t row = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * acc_stride + half * 32);
+      if (S == 1) {
 #pragma unroll
-      for (int c16 = 0; c16 < 2; ++c16) {
-        float v[16];
-        tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + half * 32 + c16 * 16), v);
+        for (int c16 = 0; c16 < 2; ++c16) {
+          float v[16];
+          tc_ld16(row + (uint32_t)(c16 * 16), v);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+          for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (double)v[i];
+        }
+      } else {
+        // hh' plus the corrections, 8 columns at a time (the f64 sums hold 64 registers)
+#pragma unroll
+        for (int c8 = 0; c8 < 4; ++c8) {
+          float v[8], w[8];
+          tc_ld8(row + (uint32_t)(c8 * 8), v);
+          tc_ld8(row + (uint32_t)(64 + c8 * 8), w);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) acc[c8 * 8 + i] += (double)(v[i] + w[i]);
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&accfree[a]);
@@ -544,7 +581,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc_tmem_cols<S>())
+                 : "memory");
 }
 
 template <int S>
@@ -1030,6 +1068,8 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
   using Cfg = FuCfg<E, S>;
   constexpr int P = Cfg::P, Slots = Cfg::Slots, PW = Cfg::PW, WPS = Cfg::WPS, KS = fu_stage_points<E>();
   static_assert(Slots == P, "one slot per producer warp");
+  // TF32 hi+lo: the B terms as one N = 128 operand, 128 TMEM columns per accumulator
+  constexpr bool kMergeB = E == 0 && S == 2;
   extern __shared__ __align__(1024) unsigned char fu_smem[];
   if (budget < 0) budget = dev::kWaitBudget;  // the context's default
   // 1024-byte alignment as an offset into the shared array (pointers derived
@@ -1050,7 +1090,8 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
   const int nc = wk.z, n_units = n_lmt * nc;
   if (warp == 0) {
     const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTcTmemCols)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                 "r"(tc_tmem_cols<(E == 0 ? S : 1)>())
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -1175,16 +1216,25 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a0 = smem_base + (uint32_t)d * Cfg::SlotBytes, b0 = a0 + S * kTcABytes;
-        const uint32_t acc_cols = tmem + (uint32_t)(a * 64);
+        const uint32_t acc_cols = tmem + (uint32_t)(a * (kMergeB ? 128 : 64));
+        if (kMergeB) {
+          // as k_mp_moments_tc<2>: A_hi against [B_hi; B_lo] (N = 128), then A_lo against B_hi
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-          for (int p = 0; p < np; ++p) {
-            const uint64_t da = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32);
-            const uint64_t db = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32);
-            if (E == 0) tc_mma(acc_cols, da, db, (kk || p) ? 1u : 0u);
-            else tc_mma_bf16(acc_cols, da, db, (kk || p) ? 1u : 0u);
+          for (int kk = 0; kk < 4; ++kk) {
+            tc_mma(acc_cols, tc_smem_desc(a0 + kk * 32), tc_smem_desc(b0 + kk * 32), kk ? 1u : 0u, kTcIdescN128);
+            tc_mma(acc_cols + 64u, tc_smem_desc(a0 + kTcABytes + kk * 32), tc_smem_desc(b0 + kk * 32), 1u);
           }
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int p = 0; p < np; ++p) {
+              const uint64_t da = tc_smem_desc(a0 + pa[p] * kTcABytes + kk * 32);
+              const uint64_t db = tc_smem_desc(b0 + pb[p] * kTcBBytes + kk * 32);
+              if (E == 0) tc_mma(acc_cols, da, db, (kk || p) ? 1u : 0u);
+              else tc_mma_bf16(acc_cols, da, db, (kk || p) ? 1u : 0u);
+            }
+        }
         tc_commit(&empty[d]);
         tc_commit(&accfull[a]);
       }
@@ -1208,12 +1258,24 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (kMergeB) {
+          const uint32_t row = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 128 + hf * DC);
 #pragma unroll
-        for (int c16 = 0; c16 < DC / 16; ++c16) {
-          float v[16];
-          tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + hf * DC + c16 * 16), v);
+          for (int c8 = 0; c8 < DC / 8; ++c8) {
+            float v[8], w[8];
+            tc_ld8(row + (uint32_t)(c8 * 8), v);
+            tc_ld8(row + (uint32_t)(64 + c8 * 8), w);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (Acc)v[i];
+            for (int i = 0; i < 8; ++i) acc[c8 * 8 + i] += (Acc)(v[i] + w[i]);
+          }
+        } else {
+#pragma unroll
+          for (int c16 = 0; c16 < DC / 16; ++c16) {
+            float v[16];
+            tc_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 64 + hf * DC + c16 * 16), v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[c16 * 16 + i] += (Acc)v[i];
+          }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(&accfree[a]);
@@ -1240,7 +1302,9 @@ __global__ void __launch_bounds__(FuCfg<E, S>::Threads, 1)
   }
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(tc_tmem_cols<(E == 0 ? S : 1)>())
+                 : "memory");
 }
 
 // M[g][b][perm(t*128 + r)] = sum over the point splits of group g of the
