@@ -1026,7 +1026,8 @@ uint32_t morton10(uint32_t v) {
 // items keep the q block fastest so concurrently running CTAs add into
 // different q ranges.
 std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_from) {
-  std::vector<std::pair<int, int4>> items;
+  static thread_local std::vector<std::pair<int, int4>> items;  // keeps its capacity (and pages) across calls
+  items.clear();
   for (int it = 0; it < L.n_tiles; ++it) {
     if (it >= skip_from) break;
     for (int j0 = it; j0 < L.n_tiles; j0 += run) {
@@ -1153,7 +1154,12 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
   for (int64_t i = 0; i < n; ++i) count[type[i]]++;
   std::vector<int64_t> tstart(T + 1, 0);
   for (int t = 0; t < T; ++t) tstart[t + 1] = tstart[t] + count[t];
-  std::vector<uint64_t> word(n), tmp(n);
+  // sort scratch kept per host thread with its capacity, so repeated calls
+  // reuse its pages instead of faulting in fresh ones
+  static thread_local std::vector<uint64_t> word, tmp;
+  static thread_local std::vector<int64_t> order;
+  word.resize((size_t)n);
+  tmp.resize((size_t)n);
   {
     std::vector<int64_t> pos(tstart.begin(), tstart.end() - 1);
     for (int64_t i = 0; i < n; ++i) {
@@ -1177,7 +1183,7 @@ Layout build_layout(const double* xyz, const double* w, const int32_t* type, int
       std::copy(tmp.begin() + a, tmp.begin() + b, word.begin() + a);
     }
   }
-  std::vector<int64_t> order(n);
+  order.resize((size_t)n);
   for (int64_t k = 0; k < n; ++k) order[k] = (int64_t)(word[k] & 0xffffffffu);
   int64_t n_pad = 0;
   for (int t = 0; t < T; ++t) n_pad += (count[t] + kTile - 1) / kTile * kTile;
