@@ -64,9 +64,16 @@ constexpr int kSplit1 = 14, kSplit2 = 15;
 constexpr int kSplit3 = 12;
 static_assert(kThreads == kTile, "tile size and CTA size must match");
 
+// v on the plan's fixed-point grid of step 1/sc (sc a power of two chosen on
+// the host so that every partial sum stays below 2^52 steps): f64 sums of such
+// values are exact, so the order in which the atomic adds land does not change
+// the partials (bit-reproducible results), and the step, about 2^-52 of a
+// bound on the sums, lies far below the FP32 terms' own rounding
+__device__ __forceinline__ double on_grid(double v, double sc) { return rint(v * sc) / sc; }
+
 template <int Q>
 __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int ab, int qstart, int qcount, int nq,
-                                           double* __restrict__ partials) {
+                                           double* __restrict__ partials, double sc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < Q; ++k) {
@@ -84,7 +91,7 @@ __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; ++w) s += (double)red[w][k];
-    atomicAdd(&partials[(size_t)ab * nq + qstart + k], s);
+    atomicAdd(&partials[(size_t)ab * nq + qstart + k], on_grid(s, sc));
   }
   __syncthreads();
 }
@@ -250,7 +257,8 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     k_pair_fp32(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                 int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T, int wide,
                 double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
-                const int64_t* __restrict__ work_out, int budget) {
+                const int64_t* __restrict__ work_out,
+                const double* __restrict__ item_scale, int budget) {
   __shared__ __align__(16) float4 sj[2][kTile];
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
@@ -275,6 +283,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
     double* __restrict__ out = partials + (work_out ? work_out[w] : 0);  // per-structure output in a batch
+    const double sc = item_scale[w];
     const float4 ai = atoms[(size_t)it * kTile + tid];
     const float4 qp = qpar[qb];
     const int2 qr = qrange[qb];
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
         cur = tj;
       }
       // issue the next tile into the other buffer (its previous readers
@@ -358,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
     }
   }
 }
@@ -369,7 +378,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
 // pair·q, as the j-packed form, but with JB chains in flight per warp).
 template <int Q>
 __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2], float (*red)[Q], int ab, int qstart,
-                                              int qcount, int nq, double* __restrict__ partials) {
+                                              int qcount, int nq, double* __restrict__ partials, double sc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int m = 0; m < Q / 2; ++m) {
@@ -391,7 +400,7 @@ __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2],
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; ++w) s += (double)red[w][k];
-    atomicAdd(&partials[(size_t)ab * nq + qstart + k], s);
+    atomicAdd(&partials[(size_t)ab * nq + qstart + k], on_grid(s, sc));
   }
   __syncthreads();
 }
@@ -401,7 +410,8 @@ __global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                    int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
                    int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
-                   const int64_t* __restrict__ work_out, int budget) {
+                   const int64_t* __restrict__ work_out,
+                const double* __restrict__ item_scale, int budget) {
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
   static_assert(CH == 1 || (CH == 2 && JB == 1 && FOLD && Q % 4 == 0), "two chains per pair: folded, one pair");
   __shared__ __align__(16) float4 sj[2][kTile];
@@ -428,6 +438,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
     double* __restrict__ out = partials + (work_out ? work_out[w] : 0);
+    const double sc = item_scale[w];
     const float4 ai = atoms[(size_t)it * kTile + tid];
     const float4 qp = qpar[qb];
     const int2 qr = qrange[qb];
@@ -445,7 +456,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
         cur = tj;
       }
       if (tid == 0 && jt + 1 < jt1) {
@@ -515,7 +526,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
     }
   }
 }
@@ -575,7 +586,7 @@ __device__ __forceinline__ void sp_wait(uint64_t* bar, unsigned parity, int budg
 // own q points into the f64 partials.  Resets the accumulators.
 template <int Q>
 __device__ __forceinline__ void flush_split(unsigned long long (&acc2)[Q / 2], int ab, int qstart, int qcount,
-                                            int nq, double* __restrict__ partials) {
+                                            int nq, double* __restrict__ partials, double sc) {
   constexpr int N = Q / 2;
   constexpr int P = (N + 31) / 32 * 32;
   const int lane = threadIdx.x & 31;
@@ -609,8 +620,8 @@ __device__ __forceinline__ void flush_split(unsigned long long (&acc2)[Q / 2], i
     const int k = 2 * (lane * per + m);
     float a, b;
     unpack2(v[m], a, b);
-    if (k < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k], (double)a);
-    if (k + 1 < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k + 1], (double)b);
+    if (k < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k], on_grid((double)a, sc));
+    if (k + 1 < qcount) atomicAdd(&partials[(size_t)ab * nq + qstart + k + 1], on_grid((double)b, sc));
   }
 }
 
@@ -619,7 +630,8 @@ __global__ void __launch_bounds__(kSpThreads, 1)
     k_pair_split(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                  int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int nq, int T,
                  int wide, double* __restrict__ partials, int* __restrict__ status, int* __restrict__ next_work,
-                 const int64_t* __restrict__ work_out, int budget) {
+                 const int64_t* __restrict__ work_out,
+                const double* __restrict__ item_scale, int budget) {
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
   static_assert(kSpJ % (2 * JB) == 0, "each warpgroup takes JB of its j atoms per step");
   extern __shared__ __align__(16) unsigned char sp_smem[];
@@ -699,6 +711,7 @@ __global__ void __launch_bounds__(kSpThreads, 1)
   int cur_w = -1, ti = 0, cur = 0, jlo = 0, jhi = 0;
   int2 qr = make_int2(0, 0);
   double* __restrict__ out = partials;
+  double sc = 1.0;
   for (int n = 0;; ++n) {
     const int stage = n % kSpStages;
     sp_wait(&full[stage], (n / kSpStages) & 1, budget, ok, status);
@@ -711,7 +724,7 @@ __global__ void __launch_bounds__(kSpThreads, 1)
     if (h.x != cur_w) {
       if (cur_w >= 0) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
       }
       const int4 wk = work[h.x];
       cur_w = h.x;
@@ -721,13 +734,14 @@ __global__ void __launch_bounds__(kSpThreads, 1)
       jhi = wk.z;
       qr = qrange[wk.w];
       out = partials + (work_out ? work_out[h.x] : 0);
+      sc = item_scale[h.x];
     }
     if (h.y < jlo || h.y >= jhi) break;
     if (h.z == 0) {
       const int tj = tile_type[h.y];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
         cur = tj;
       }
     }
@@ -757,7 +771,7 @@ __global__ void __launch_bounds__(kSpThreads, 1)
   }
   if (cur_w >= 0) {
     const int a = min(ti, cur), b = max(ti, cur);
-    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
   }
 }
 
@@ -790,7 +804,8 @@ __global__ void __launch_bounds__(kS3Threads, 1)
     k_pair_split3(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
                   int n_work, const float4* __restrict__ qpar, const int2* __restrict__ qrange, int n_qblocks,
                   int nq, int T, int wide, double* __restrict__ partials, int* __restrict__ status,
-                  int* __restrict__ next_work, const int64_t* __restrict__ work_out, int budget) {
+                  int* __restrict__ next_work, const int64_t* __restrict__ work_out,
+                const double* __restrict__ item_scale, int budget) {
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
   extern __shared__ __align__(16) unsigned char s3_smem[];
   ulonglong2* sd = (ulonglong2*)(s3_smem + S3Smem::kSd);
@@ -884,6 +899,7 @@ __global__ void __launch_bounds__(kS3Threads, 1)
   bool live = false;  // this warpgroup's block of the current item exists
   int2 qr = make_int2(0, 0);
   double* __restrict__ out = partials;
+  double sc = 1.0;
   for (int n = 0;; ++n) {
     const int stage = n % kS3Stages;
     sp_wait(&full[stage], (n / kS3Stages) & 1, budget, ok, status);
@@ -896,7 +912,7 @@ __global__ void __launch_bounds__(kS3Threads, 1)
     if (h.x != cur_w) {
       if (live) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
       }
       const int4 wk = work[h.x];
       cur_w = h.x;
@@ -908,6 +924,7 @@ __global__ void __launch_bounds__(kS3Threads, 1)
       jhi = wk.z;
       qr = live ? qrange[qb] : make_int2(0, 0);
       out = partials + (work_out ? work_out[h.x] : 0);
+      sc = item_scale[h.x];
     }
     if (h.y < jlo || h.y >= jhi) break;
     if (h.z == 0) {
@@ -915,7 +932,7 @@ __global__ void __launch_bounds__(kS3Threads, 1)
       if (tj != cur) {
         if (live) {
           const int a = min(ti, cur), b = max(ti, cur);
-          flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+          flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
         }
         cur = tj;
       }
@@ -941,7 +958,7 @@ __global__ void __launch_bounds__(kS3Threads, 1)
   }
   if (live) {
     const int a = min(ti, cur), b = max(ti, cur);
-    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out);
+    flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
   }
 }
 
@@ -1049,32 +1066,35 @@ std::vector<int4> make_work(const Layout& L, int n_qblocks, int run, int skip_fr
 template <int Q, int JB>
 void launch_fp32(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
                  const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
-                 int* next_work, const int64_t* work_out, int budget) {
+                 int* next_work, const int64_t* work_out, const double* item_scale,
+                    int budget) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32<Q, JB>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32<Q, JB><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
-                                                     status, next_work, work_out, budget);
+                                                     status, next_work, work_out, item_scale, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
 template <int Q, int JB, int OCC, bool FOLD = false, int CH = 1>
 void launch_fp32_pq(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                     int n_work, const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials,
-                    int* status, int* next_work, const int64_t* work_out, int budget) {
+                    int* status, int* next_work, const int64_t* work_out, const double* item_scale,
+                    int budget) {
   int per_sm = 0;
   CRAB_CUDA_CHECK(
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_fp32_pq<Q, JB, OCC, FOLD, CH>, kThreads, 0));
   int grid = std::max(1, std::min(n_work, sm_count * std::max(per_sm, 1)));
   k_pair_fp32_pq<Q, JB, OCC, FOLD, CH><<<grid, kThreads, 0, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T, wide, partials,
-                                                        status, next_work, work_out, budget);
+                                                        status, next_work, work_out, item_scale, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
 template <int Q, int JB>
 void launch_split(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work, int n_work,
                   const float4* qpar, const int2* qrange, int nq, int T, int wide, double* partials, int* status,
-                  int* next_work, const int64_t* work_out, int budget) {
+                  int* next_work, const int64_t* work_out, const double* item_scale,
+                    int budget) {
   static bool attr = false;  // one CTA per SM: the ring takes most of the shared memory
   if (!attr) {
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pair_split<Q, JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1084,14 +1104,15 @@ void launch_split(cudaStream_t stream, int sm_count, const float4* atoms, const 
   const int grid = std::max(1, std::min(n_work, sm_count));
   k_pair_split<Q, JB><<<grid, kSpThreads, SpSmem::kBytes, stream>>>(atoms, tt, work, n_work, qpar, qrange, nq, T,
                                                                     wide, partials, status, next_work, work_out,
-                                                                    budget);
+                                                                    item_scale, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
 template <int Q>
 void launch_split3(cudaStream_t stream, int sm_count, const float4* atoms, const int* tt, const int4* work,
                    int n_work, const float4* qpar, const int2* qrange, int n_qblocks, int nq, int T, int wide,
-                   double* partials, int* status, int* next_work, const int64_t* work_out, int budget) {
+                   double* partials, int* status, int* next_work, const int64_t* work_out, const double* item_scale,
+                    int budget) {
   static bool attr = false;
   if (!attr) {
     CRAB_CUDA_CHECK(cudaFuncSetAttribute(k_pair_split3<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1101,7 +1122,7 @@ void launch_split3(cudaStream_t stream, int sm_count, const float4* atoms, const
   const int grid = std::max(1, std::min(n_work, sm_count));
   k_pair_split3<Q><<<grid, kS3Threads, S3Smem::kBytes, stream>>>(atoms, tt, work, n_work, qpar, qrange, n_qblocks,
                                                                  nq, T, wide, partials, status, next_work, work_out,
-                                                                 budget);
+                                                                 item_scale, budget);
   CRAB_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1368,18 +1389,43 @@ void configure_fp32(crab_ctx* ctx, PairPlan& P, int Q, int jb) {
   P.hmax = hmax;
   // work items name a q block, or for k_pair_split3 a group of kS3Blocks
   const int item_blocks = jb == kSplit3 ? (P.n_qblocks + kS3Blocks - 1) / kS3Blocks : P.n_qblocks;
+  // Fixed-point grid of each structure's partials: the largest power of two
+  // 2^e with q_max (Σ|w|)² 2^e < 2^52.  Every pair term w_i w_j sin(q r)/r
+  // is at most |w_i w_j| q in magnitude, so every sum of the structure's
+  // terms stays below 2^52 steps of 2^-e, and f64 sums of values on that grid
+  // are exact in any order.
+  double qmax = 0.0;
+  for (double v : P.q) qmax = std::max(qmax, std::fabs(v));
+  auto scale_of = [&](int t0, int t1) {
+    double s1 = 0.0;
+    for (int64_t k = (int64_t)t0 * kTile; k < (int64_t)t1 * kTile; ++k) s1 += std::fabs((double)P.L.atoms[4 * k + 3]);
+    const double bound = qmax * s1 * s1;
+    if (!(bound > 0.0) || !std::isfinite(bound)) return 1.0;
+    int ex = 0;
+    std::frexp(bound, &ex);  // bound < 2^ex
+    return std::ldexp(1.0, std::max(-1000, std::min(1000, 52 - ex)));
+  };
   std::vector<int4> work;
+  std::vector<double> scale;
   if (P.segments.empty()) {
     // runs of up to 8 j tiles per item, shorter when that leaves fewer items
     // than about four per resident CTA (small structures)
     const int64_t tile_pairs = (int64_t)P.L.n_tiles * (P.L.n_tiles + 1) / 2 * item_blocks;
     const int run = (int)std::max<int64_t>(1, std::min<int64_t>(8, tile_pairs / (4 * 3 * (int64_t)ctx->sm_count)));
     work = shard_work(make_work(P.L, item_blocks, run, P.lattice_first_tile), P.shard, P.n_shards);
+    scale.assign(work.size(), scale_of(0, P.L.n_tiles));
   } else {
     std::vector<int64_t> out;
     make_work_segments(P, item_blocks, 8, work, out);
     P.d_work_out = upload(ctx, P, P.qcfg, "work_out", out.data(), out.size(), ctx->stream);
+    const int K = (int)P.segments.size() - 1;
+    std::vector<double> seg_scale(K);
+    for (int c = 0; c < K; ++c) seg_scale[c] = scale_of(P.segments[c], P.segments[c + 1]);
+    const int64_t per = (int64_t)P.n_pairs * P.nq;
+    scale.resize(work.size());
+    for (size_t k = 0; k < work.size(); ++k) scale[k] = seg_scale[(size_t)(out[k] / per)];
   }
+  P.d_scale = upload(ctx, P, P.qcfg, "scale", scale.data(), scale.size(), ctx->stream);
   P.n_work = (int)work.size();
   P.d_work = upload(ctx, P, P.qcfg, "work", work.data(), work.size(), ctx->stream);
   P.d_qpar = upload(ctx, P, P.qcfg, "qpar", qpar.data(), qpar.size(), ctx->stream);
@@ -1492,7 +1538,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH(QQ, JJ)                                                                                    \
   if (P.Q == QQ && P.jb == JJ) {                                                                                 \
     launch_fp32<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
-                        T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget);               \
+                        T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale, ctx->wait_budget);               \
     launched = true;                                                                                             \
   }
     bool launched = false;
@@ -1509,7 +1555,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH_PQ(QQ, JJ, OO, CODE)                                                                        \
   if (P.Q == QQ && P.jb == CODE) {                                                                               \
     launch_fp32_pq<QQ, JJ, OO>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,          \
-                               P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,            \
+                               P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale,            \
                                ctx->wait_budget);                                                                 \
     launched = true;                                                                                             \
   }
@@ -1526,7 +1572,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH_PQF(QQ, JJ, OO, CODE)                                                                       \
   if (P.Q == QQ && P.jb == CODE) {                                                                               \
     launch_fp32_pq<QQ, JJ, OO, true>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,    \
-                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,      \
+                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale,      \
                                      ctx->wait_budget);                                                           \
     launched = true;                                                                                             \
   }
@@ -1545,12 +1591,12 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
   if (P.Q == QQ && P.jb == kFolded2c) {                                                                          \
     if (P.hmax > kMax2cHalfAngle)                                                                                \
       launch_fp32_pq<QQ, 1, 2, true>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar,    \
-                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out,      \
+                                     P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale,      \
                                      ctx->wait_budget);                                                           \
     else                                                                                                         \
       launch_fp32_pq<QQ, 1, 2, true, 2>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work,          \
                                         P.d_qpar, P.d_qrange, nq, T, P.wide, P.d_out, P.d_status, P.d_next,       \
-                                        P.d_work_out, ctx->wait_budget);                                          \
+                                        P.d_work_out, P.d_scale, ctx->wait_budget);                                          \
     launched = true;                                                                                             \
   }
     CRAB_LAUNCH_PQ2C(168)
@@ -1558,7 +1604,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH_SPLIT(QQ, JJ, CODE)                                                                          \
   if (P.Q == QQ && P.jb == CODE) {                                                                               \
     launch_split<QQ, JJ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange, nq, \
-                         T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget);              \
+                         T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale, ctx->wait_budget);              \
     launched = true;                                                                                             \
   }
     CRAB_LAUNCH_SPLIT(126, 1, kSplit1)
@@ -1569,7 +1615,7 @@ void pair_plan_launch(crab_ctx* ctx, PairPlan& P, cudaStream_t s, bool timed) {
 #define CRAB_LAUNCH_SPLIT3(QQ)                                                                                    \
   if (P.Q == QQ && P.jb == kSplit3) {                                                                            \
     launch_split3<QQ>(s, ctx->sm_count, P.d_atoms, P.d_tile_type, P.d_work, P.n_work, P.d_qpar, P.d_qrange,       \
-                      P.n_qblocks, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, ctx->wait_budget); \
+                      P.n_qblocks, nq, T, P.wide, P.d_out, P.d_status, P.d_next, P.d_work_out, P.d_scale, ctx->wait_budget); \
     launched = true;                                                                                             \
   }
     CRAB_LAUNCH_SPLIT3(84)

@@ -248,6 +248,7 @@ struct PairPlan {
   int* d_status = nullptr;
   int* d_next = nullptr;  // work-queue counter (the int after d_status)
   int64_t* d_work_out = nullptr;  // per work item output offset (batches of structures), or null
+  double* d_scale = nullptr;      // per work item fixed-point scale of its structure's partials (a power of two)
   int lattice_first_tile = 0;
   // multi-GPU: this plan sums only the work items of shard `shard` of
   // `n_shards` (shard_owners); shard 0 alone adds the exact q = 0 sums and

@@ -259,6 +259,30 @@ def test_empty_structure_gives_zero_curve(engine):
     assert np.all(out == 0.0)
 
 
+def test_partials_are_bit_reproducible(engine):
+    """Each flushed FP32 sum is rounded onto a power-of-two fixed-point grid
+    sized by a bound on the structure's sums, so the f64 atomic adds are exact
+    in whatever order they land: repeated calls return identical bits, for one
+    structure and for a batch of structures (the ensemble's segmented plan)."""
+    from crabsaxs_b200 import synth
+
+    xyz, w, t = _random_typed(6000, 3, 29, radius=30.0)
+    t = t.astype(np.int32)
+    q = np.linspace(0.001, 0.5, 500)
+    first, _ = cs.debye_partials(xyz, w, t, 3, q, engine=engine)
+    for _ in range(3):
+        again, _ = cs.debye_partials(xyz, w, t, 3, q, engine=engine)
+        assert np.array_equal(again, first)
+    P64, _ = cs.debye_partials(xyz, w, t, 3, q, fp64=True, engine=engine)
+    assert np.max(np.abs(first - P64) / _partials_scale(w, t, 3)[:, None]) <= PARTIAL_ATOL
+    confs = [synth.protein(900 + i, n, 12.0 + 0.004 * n) for i, n in enumerate([700, 2500, 1200, 4000])]
+    qe = np.linspace(0.005, 0.45, 300)
+    cand = cs.solvent_candidates(cs.FitOptions())[[0, 12]]
+    c0 = cs.ensemble_curves(confs, qe, cs.SolventParams(), cand, engine=engine)
+    for _ in range(2):
+        assert np.array_equal(cs.ensemble_curves(confs, qe, cs.SolventParams(), cand, engine=engine), c0)
+
+
 def test_pair_kernel_launches_are_counted(engine):
     engine.reset_stats()
     xyz, w, t = _random_typed(300, 2, 1)
