@@ -69,7 +69,12 @@ static_assert(kThreads == kTile, "tile size and CTA size must match");
 // values are exact, so the order in which the atomic adds land does not change
 // the partials (bit-reproducible results), and the step, about 2^-52 of a
 // bound on the sums, lies far below the FP32 terms' own rounding
-__device__ __forceinline__ double on_grid(double v, double sc) { return rint(v * sc) / sc; }
+__device__ __forceinline__ double on_grid(double v, double sc) {
+  // 1/sc exactly: sc = 2^e (|e| <= 1000), whose reciprocal's exponent field is
+  // 2046 minus sc's
+  const double inv = __longlong_as_double(0x7FE0000000000000ll - __double_as_longlong(sc));
+  return rint(v * sc) * inv;
+}
 
 template <int Q>
 __device__ __forceinline__ void flush_fp32(float (&acc)[Q], float (*red)[Q], int ab, int qstart, int qcount, int nq,
@@ -263,6 +268,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_item;
+  __shared__ double s_scale;  // the item's fixed-point scale, read at its flushes
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -275,7 +281,11 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
   if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(next_work, 1);
+    if (tid == 0) {
+      const int wi = atomicAdd(next_work, 1);
+      s_item = wi;
+      if (wi < n_work) s_scale = item_scale[wi];
+    }
     __syncthreads();
     const int w = s_item;
     __syncthreads();
@@ -283,7 +293,6 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
     double* __restrict__ out = partials + (work_out ? work_out[w] : 0);  // per-structure output in a batch
-    const double sc = item_scale[w];
     const float4 ai = atoms[(size_t)it * kTile + tid];
     const float4 qp = qpar[qb];
     const int2 qr = qrange[qb];
@@ -303,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
+        flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
         cur = tj;
       }
       // issue the next tile into the other buffer (its previous readers
@@ -367,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
+      flush_fp32<Q>(acc, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
     }
   }
 }
@@ -418,6 +427,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
   __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_item;
+  __shared__ double s_scale;  // the item's fixed-point scale, read at its flushes
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -430,7 +440,11 @@ __global__ void __launch_bounds__(kThreads, OCC)
   if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(next_work, 1);
+    if (tid == 0) {
+      const int wi = atomicAdd(next_work, 1);
+      s_item = wi;
+      if (wi < n_work) s_scale = item_scale[wi];
+    }
     __syncthreads();
     const int w = s_item;
     __syncthreads();
@@ -438,7 +452,6 @@ __global__ void __launch_bounds__(kThreads, OCC)
     const int4 wk = work[w];
     const int it = wk.x, jt0 = wk.y, jt1 = wk.z, qb = wk.w;
     double* __restrict__ out = partials + (work_out ? work_out[w] : 0);
-    const double sc = item_scale[w];
     const float4 ai = atoms[(size_t)it * kTile + tid];
     const float4 qp = qpar[qb];
     const int2 qr = qrange[qb];
@@ -456,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
+        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
         cur = tj;
       }
       if (tid == 0 && jt + 1 < jt1) {
@@ -526,7 +539,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, sc);
+      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
     }
   }
 }
