@@ -281,13 +281,12 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
   if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
-    if (tid == 0) {
-      const int wi = atomicAdd(next_work, 1);
-      s_item = wi;
-      if (wi < n_work) s_scale = item_scale[wi];
-    }
+    if (tid == 0) s_item = atomicAdd(next_work, 1);
     __syncthreads();
     const int w = s_item;
+    // written between the two barriers: every thread has finished the last
+    // item's flushes (which read it) before the first one
+    if (tid == 0 && w < n_work) s_scale = item_scale[w];
     __syncthreads();
     if (w >= n_work || !ok) break;
     const int4 wk = work[w];
@@ -414,6 +413,10 @@ __device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2],
   __syncthreads();
 }
 
+template <int Q>
+__device__ __forceinline__ void flush_split(unsigned long long (&acc2)[Q / 2], int ab, int qstart, int qcount,
+                                            int nq, double* __restrict__ partials, double sc);
+
 template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)), bool FOLD = false, int CH = 1>
 __global__ void __launch_bounds__(kThreads, OCC)
     k_pair_fp32_pq(const float4* __restrict__ atoms, const int* __restrict__ tile_type, const int4* __restrict__ work,
@@ -440,13 +443,12 @@ __global__ void __launch_bounds__(kThreads, OCC)
   if (budget < 0) budget = kWaitBudget;  // the context's default
 
   for (;;) {
-    if (tid == 0) {
-      const int wi = atomicAdd(next_work, 1);
-      s_item = wi;
-      if (wi < n_work) s_scale = item_scale[wi];
-    }
+    if (tid == 0) s_item = atomicAdd(next_work, 1);
     __syncthreads();
     const int w = s_item;
+    // written between the two barriers: every thread has finished the last
+    // item's flushes (which read it) before the first one
+    if (tid == 0 && w < n_work) s_scale = item_scale[w];
     __syncthreads();
     if (w >= n_work || !ok) break;
     const int4 wk = work[w];
@@ -469,7 +471,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
       const int tj = tile_type[jt];
       if (tj != cur) {
         const int a = min(ti, cur), b = max(ti, cur);
-        flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
+        flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
         cur = tj;
       }
       if (tid == 0 && jt + 1 < jt1) {
@@ -539,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, OCC)
     }
     if (ok) {
       const int a = min(ti, cur), b = max(ti, cur);
-      flush_fp32_pq<Q>(acc2, red, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
+      flush_split<Q>(acc2, a * T - a * (a - 1) / 2 + (b - a), qr.x, qr.y, nq, out, s_scale);
     }
   }
 }
