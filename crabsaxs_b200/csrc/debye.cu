@@ -380,42 +380,17 @@ __global__ void __launch_bounds__(kThreads, JB == 2 ? (Q <= 64 ? 4 : (Q <= 96 ? 
   }
 }
 
-// The same work items with the q-packed recurrence: accumulators are f32x2
-// pairs (q points 2m, 2m+1), and JB j atoms run JB independent packed chains,
-// 3 packed instructions per chain and step (6 FP32 lane operations for 2
-// pair·q, as the j-packed form, but with JB chains in flight per warp).
-template <int Q>
-__device__ __forceinline__ void flush_fp32_pq(unsigned long long (&acc2)[Q / 2], float (*red)[Q], int ab, int qstart,
-                                              int qcount, int nq, double* __restrict__ partials, double sc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int m = 0; m < Q / 2; ++m) {
-    float a, b;
-    unpack2(acc2[m], a, b);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-    }
-    if (lane == 0) {
-      red[warp][2 * m] = a;
-      red[warp][2 * m + 1] = b;
-    }
-    acc2[m] = 0ull;
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < qcount; k += kThreads) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) s += (double)red[w][k];
-    atomicAdd(&partials[(size_t)ab * nq + qstart + k], on_grid(s, sc));
-  }
-  __syncthreads();
-}
-
+// Per-warp flush of packed accumulators (defined with the split kernels below).
 template <int Q>
 __device__ __forceinline__ void flush_split(unsigned long long (&acc2)[Q / 2], int ab, int qstart, int qcount,
                                             int nq, double* __restrict__ partials, double sc);
+
+// The same work items with the q-packed recurrence: accumulators are f32x2
+// pairs (q points 2m, 2m+1), and JB j atoms run JB independent packed chains,
+// 3 packed instructions per chain and step (6 FP32 lane operations for 2
+// pair·q, as the j-packed form, but with JB chains in flight per warp).  Each
+// warp flushes its own sums (flush_split): on the fixed-point grid the order
+// of the adds does not matter.
 
 template <int Q, int JB, int OCC = (Q <= 64 ? 4 : (Q <= 96 ? 3 : 2)), bool FOLD = false, int CH = 1>
 __global__ void __launch_bounds__(kThreads, OCC)
@@ -427,7 +402,6 @@ __global__ void __launch_bounds__(kThreads, OCC)
   static_assert(Q % 2 == 0, "q-packed blocks hold an even number of q points");
   static_assert(CH == 1 || (CH == 2 && JB == 1 && FOLD && Q % 4 == 0), "two chains per pair: folded, one pair");
   __shared__ __align__(16) float4 sj[2][kTile];
-  __shared__ float red[kThreads / 32][Q];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int s_item;
   __shared__ double s_scale;  // the item's fixed-point scale, read at its flushes
