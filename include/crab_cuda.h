@@ -201,7 +201,10 @@ int crab_combine_solvent_basis(const double* q, int64_t nq, const double* basis6
  *   out[ab*nq+k] = Σ_{i<j,{t_i,t_j}={a,b}} w_i w_j sinc(q_k r_ij), a<=b,
  *   ab = a*T - a*(a-1)/2 + (b-a);  self_out[a] = Σ_{t_i=a} w_i².
  * xyz n*3 f64, w n f64, type n in [0,T). The pair sum runs in FP32 on the
- * device with FP64 cross-block reduction. */
+ * device with FP64 cross-block reduction; the f64 sums are exact on a
+ * power-of-two fixed-point grid (step about 2^-52 of q_max (Σ|w|)²), so the
+ * result is bit-identical from call to call on the same inputs and kernel
+ * variant. */
 int crab_debye_partials(crab_ctx* ctx, const double* xyz, const double* w, const int32_t* type, int64_t n,
                         int32_t n_types, const double* q, int64_t nq, double* out, double* self_out);
 /* Same partials computed in FP64 on the device with direct sin (no
