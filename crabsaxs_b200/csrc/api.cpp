@@ -217,23 +217,18 @@ void amplitude_tables(const TypedAtoms& t, const double* q, int64_t nq, const cr
   E.assign((size_t)T * nq, 0.0);
   H.assign((size_t)T * nq, 0.0);
   const bool grid = solvent && solvent->hydration_model != CRAB_HYD_ANALYTIC;
-  for (int a = 0; a < T; ++a)
-    for (int64_t k = 0; k < nq; ++k) {
-      const size_t o = (size_t)a * nq + k;
-      if (t.cls[a].element < 0) {
-        H[o] = solvent->bulk_density / 10.0 * site_volume * water_form_factor(q[k]);
-        continue;
-      }
-      if (!solvent) {
-        V[o] = form_factor(t.cls[a].element, t.cls[a].group, 1.0, implicit, q[k]);
-        continue;
-      }
-      double v, e, h;
-      debye_class_amplitudes(t.cls[a], implicit, q[k], solvent->bulk_density, solvent->shell_thickness, &v, &e, &h);
-      V[o] = v;
-      E[o] = e;
-      H[o] = grid ? 0.0 : h;
+  for (int a = 0; a < T; ++a) {
+    const size_t o = (size_t)a * nq;
+    if (t.cls[a].element < 0) {
+      for (int64_t k = 0; k < nq; ++k)
+        H[o + k] = solvent->bulk_density / 10.0 * site_volume * water_form_factor(q[k]);
+    } else if (!solvent) {
+      for (int64_t k = 0; k < nq; ++k) V[o + k] = form_factor(t.cls[a].element, t.cls[a].group, 1.0, implicit, q[k]);
+    } else {
+      debye_class_amplitude_rows(t.cls[a], implicit, q, nq, solvent->bulk_density, solvent->shell_thickness,
+                                 V.data() + o, E.data() + o, grid ? nullptr : H.data() + o);
     }
+  }
 }
 
 Partials partials_for(crab_ctx* ctx, const TypedAtoms& t, const double* q, int64_t nq, bool fp64,

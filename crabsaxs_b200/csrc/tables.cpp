@@ -152,6 +152,24 @@ void debye_class_amplitudes(const AtomClass& c, bool implicit_h, double q, doubl
   *h = density * 0.1 * fraser_gaussian(q, shell_volume);
 }
 
+void debye_class_amplitude_rows(const AtomClass& c, bool implicit_h, const double* q, int64_t nq, double density,
+                                double thickness, double* v, double* e, double* h) {
+  // debye_class_amplitudes at every q, with the class's volumes and their
+  // 2/3 powers formed once: the same operations in the same order per q
+  // (h may be null: the shell term is not needed with a hydration grid)
+  const double volume = excluded_volume_for_atom(c.element, c.group, implicit_h);
+  const double radius = std::cbrt(3.0 * volume / (4.0 * kPi));
+  const double rs = radius + thickness / 2.0;
+  const double shell_volume = 4.0 * kPi * (rs * rs) * thickness;
+  const double pv = std::pow(volume, 2.0 / 3.0), ps = std::pow(shell_volume, 2.0 / 3.0);
+  for (int64_t k = 0; k < nq; ++k) {
+    const double qk = q[k];
+    v[k] = form_factor(c.element, c.group, 1.0, implicit_h, qk);
+    e[k] = density * (volume * std::exp(-pv * qk * qk / (4.0 * kPi)));
+    if (h) h[k] = density * 0.1 * (shell_volume * std::exp(-ps * qk * qk / (4.0 * kPi)));
+  }
+}
+
 void multipole_class_amplitudes(const AtomClass& c, bool implicit_h, double q, double density, double thickness,
                                 double* v, double* e, double* h) {
   const double volume = excluded_volume_for_atom(c.element, c.group, implicit_h);
