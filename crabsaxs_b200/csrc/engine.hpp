@@ -181,6 +181,9 @@ void debye_class_amplitude_rows(const AtomClass& c, bool implicit_h, const doubl
 // Same for the multipole solvent model (spherical.rs:205-231).
 void multipole_class_amplitudes(const AtomClass& c, bool implicit_h, double q, double density, double thickness,
                                 double* v, double* e, double* h);
+// The same at nq values of q into rows v, e, h (bit-identical per q; h may be null).
+void multipole_class_amplitude_rows(const AtomClass& c, bool implicit_h, const double* q, int64_t nq, double density,
+                                    double thickness, double* v, double* e, double* h);
 
 // ---------------------------------------------------------------- layout
 // Atoms of one pair-sum problem, grouped by type, spatially ordered inside

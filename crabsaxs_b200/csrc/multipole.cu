@@ -1923,23 +1923,17 @@ void multipole_tables(const TypedAtoms& t, const double* q, int64_t nq, const cr
   E.assign((size_t)T * nq, 0.0);
   H.assign((size_t)T * nq, 0.0);
   const bool grid = s && s->hydration_model != CRAB_HYD_ANALYTIC;
-  for (int a = 0; a < T; ++a)
-    for (int64_t k = 0; k < nq; ++k) {
-      const size_t o = (size_t)a * nq + k;
-      if (t.cls[a].element < 0) {
-        H[o] = s->bulk_density / 10.0 * site_volume * water_form_factor(q[k]);
-        continue;
-      }
-      if (!s) {
-        V[o] = form_factor(t.cls[a].element, t.cls[a].group, 1.0, implicit, q[k]);
-        continue;
-      }
-      double v, e, h;
-      multipole_class_amplitudes(t.cls[a], implicit, q[k], s->bulk_density, s->shell_thickness, &v, &e, &h);
-      V[o] = v;
-      E[o] = e;
-      H[o] = grid ? 0.0 : h;
+  for (int a = 0; a < T; ++a) {
+    const size_t o = (size_t)a * nq;
+    if (t.cls[a].element < 0) {
+      for (int64_t k = 0; k < nq; ++k) H[o + k] = s->bulk_density / 10.0 * site_volume * water_form_factor(q[k]);
+    } else if (!s) {
+      for (int64_t k = 0; k < nq; ++k) V[o + k] = form_factor(t.cls[a].element, t.cls[a].group, 1.0, implicit, q[k]);
+    } else {
+      multipole_class_amplitude_rows(t.cls[a], implicit, q, nq, s->bulk_density, s->shell_thickness, V.data() + o,
+                                     E.data() + o, grid ? nullptr : H.data() + o);
     }
+  }
 }
 
 // Atoms (and grid sites) with their amplitude tables, the centroid and the

@@ -181,6 +181,23 @@ void multipole_class_amplitudes(const AtomClass& c, bool implicit_h, double q, d
   *v = form_factor(c.element, c.group, 1.0, implicit_h, q);
 }
 
+void multipole_class_amplitude_rows(const AtomClass& c, bool implicit_h, const double* q, int64_t nq, double density,
+                                    double thickness, double* v, double* e, double* h) {
+  // multipole_class_amplitudes at every q, with the class's constants formed
+  // once: the same operations in the same order per q (h may be null)
+  const double volume = excluded_volume_for_atom(c.element, c.group, implicit_h);
+  const double radius = std::cbrt(3.0 * volume / (4.0 * kPi));
+  const double pv = std::pow(volume, 2.0 / 3.0);
+  const double sr = radius + thickness / 2.0;
+  const double shell_volume = 4.0 * kPi * (sr * sr) * thickness;
+  for (int64_t k = 0; k < nq; ++k) {
+    const double qk = q[k];
+    e[k] = density * volume * std::exp(-pv * qk * qk / (4.0 * kPi));
+    if (h) h[k] = density * 0.1 * shell_volume * std::exp(-qk * qk * sr * sr / 4.0);
+    v[k] = form_factor(c.element, c.group, 1.0, implicit_h, qk);
+  }
+}
+
 // Residue/atom-name typing of formfactor.rs:280-417.
 int united_atom_group(const char* residue_in, const char* name_in) {
   const std::string res = upper_trim(residue_in);
